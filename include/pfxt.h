@@ -1,0 +1,275 @@
+/*
+ * pfxt.h - C ABI of the B200 path tracer (libpfxtrace.so).
+ *
+ * It stands in for the trace crate of pfx (crates/trace): a scene, a camera and
+ * a sample budget go in, RGBA32F films come out.  Each entry point below names
+ * the reference interface it replaces (file:line inside the pfx repository).
+ *
+ * Conventions (crates/trace/src/gpu.rs:269-307 TraceError, docs/trace.md:121):
+ *   - every call returns an int status, PFXT_OK (0) or a PFXT_ERR_* code; the
+ *     message of the last failure on the calling thread is pfxt_last_error();
+ *   - the library owns all device memory; host arrays passed in are copied;
+ *   - a pfxt_trace handle is used by one thread at a time (the Rust Trace takes
+ *     &mut self); calls block until the GPU work they start has finished, as
+ *     Trace::sample does (docs/trace.md:466), except the *_device entry points,
+ *     which enqueue on the caller's stream and return.
+ */
+#ifndef PFXT_H
+#define PFXT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PFXT_ABI_VERSION 1
+
+#define PFXT_OK 0
+#define PFXT_ERR_INVALID 1 /* invalid scene, settings or arguments (TraceError::Setup) */
+#define PFXT_ERR_REFUSED 2 /* the device refused: no CUDA device, out of memory (TraceError::Refused) */
+#define PFXT_ERR_CUDA 3    /* a CUDA call failed */
+#define PFXT_ERR_DEVICE 4  /* a kernel set its error word (a bounded loop ran out) */
+
+/* ------------------------------------------------------------ scene input */
+
+/* TriangleDetail without the second uv set (crates/trace/src/detail.rs:7-13). */
+typedef struct pfxt_triangle {
+  float v[3][3];
+  float n[3][3];
+  float uv[3][2];
+  uint32_t material;
+} pfxt_triangle;
+
+typedef struct pfxt_mesh {
+  const pfxt_triangle* triangles;
+  uint32_t count;
+} pfxt_mesh;
+
+/* Instance (detail.rs:53-60); meshes shared by several instances become one
+ * bottom-level BVH, as Arc-shared triangle lists do in levels.rs:252-350. */
+typedef struct pfxt_instance {
+  uint32_t mesh;
+  uint32_t shadow_only;  /* Instance::shadow_only -> SHADOW_ONLY */
+  uint32_t two_sided;    /* Instance::two_sided; 0 sets ONE_SIDED */
+  uint32_t casts_shadow; /* InstanceSurface::casts_shadow; 0 sets CASTS_NO_SHADOW */
+  float transform[16];   /* column-major affine 4x4 (detail.rs Transform) */
+} pfxt_instance;
+
+/* The hot material record fields (materials/src/material.rs:827-843). */
+typedef struct pfxt_material {
+  float base[3];
+  float roughness;
+  float metalness, specular, clearcoat, clearcoat_roughness;
+  float sheen, transmission, ior, dispersion;
+  float thickness, subsurface, thin_film, thin_film_ior;
+  float subsurface_tint[3];
+  float absorption;
+  float emission[3];
+  float thin_film_amount;
+  float fresnel_power;
+  float pad[3];
+} pfxt_material;
+
+#define PFXT_LIGHT_POINT 0u
+#define PFXT_LIGHT_SPOT 1u
+#define PFXT_LIGHT_RECT 2u
+#define PFXT_LIGHT_DISC 3u
+
+/* LocalLight (crates/trace/src/lights.rs:11-39). */
+typedef struct pfxt_light {
+  uint32_t shape;     /* PFXT_LIGHT_* */
+  uint32_t shadow;    /* casts shadows */
+  uint32_t two_sided; /* rect and disc */
+  uint32_t pad;
+  float position[3];
+  float colour[3];
+  float intensity;
+  float radius; /* point/spot source radius */
+  float range;  /* point/spot range; rect and disc are unlimited */
+  float direction[3]; /* spot axis, or disc normal */
+  float inner_deg, outer_deg;  /* spot cone */
+  float half_u[3], half_v[3];  /* rect half extents */
+  float disc_radius;
+} pfxt_light;
+
+/* Camera (gpu.rs:173-179). */
+typedef struct pfxt_camera {
+  float origin[3];
+  float forward[3];
+  float right[3];
+  float up[3];
+} pfxt_camera;
+
+/* Sun (gpu.rs:231-236) plus Detail::sun_radius_deg. */
+typedef struct pfxt_sun {
+  float direction[3];
+  float color[3];
+  float intensity;
+  float radius_deg;
+} pfxt_sun;
+
+typedef struct pfxt_scene {
+  const pfxt_triangle* triangles; /* world triangles (not instanced) */
+  uint32_t triangle_count;
+  const pfxt_mesh* meshes;
+  uint32_t mesh_count;
+  const pfxt_instance* instances;
+  uint32_t instance_count;
+  const pfxt_material* materials;
+  uint32_t material_count;
+  const pfxt_light* lights;
+  uint32_t light_count;
+  float sky[3];        /* uniform environment radiance; 0 = black sky */
+  uint32_t sky_width;  /* sky CDF columns (the reference uses 256) */
+  uint32_t sky_height; /* sky CDF rows (the reference uses 128) */
+  uint32_t pad;
+  pfxt_camera camera;
+  pfxt_sun sun;
+} pfxt_scene;
+
+#define PFXT_SAMPLER_PCG 0u
+#define PFXT_SAMPLER_SOBOL 1u
+#define PFXT_PROJECTION_PERSPECTIVE 0u
+#define PFXT_PROJECTION_ORTHOGRAPHIC 1u
+#define PFXT_PROJECTION_EQUIRECT 2u
+
+/* Detail settings that specialise the tracer (detail.rs:374-455, gpu.rs:1140-1196). */
+typedef struct pfxt_settings {
+  uint32_t bounces[4];     /* total, diffuse, glossy, transmission (Bounces) */
+  uint32_t sampler;        /* PFXT_SAMPLER_* */
+  uint32_t sobol_samples;  /* Sampler::Sobol { samples } */
+  float clamp_indirect;    /* CLAMP_INDIRECT, 0 = off */
+  float filter_glossy;     /* FILTER_GLOSSY, 0 = off */
+  uint32_t projection;     /* PFXT_PROJECTION_* */
+  float ortho[2];          /* orthographic width, height */
+  float lens[4];           /* shift x, shift y, aperture, focus distance (Lens) */
+  uint32_t pad;
+} pfxt_settings;
+
+/* ------------------------------------------------- packed scene buffers
+ * The byte layouts of SceneBuffers (gpu.rs:412-436): the seam at which a host
+ * that packs its own buffers hands them over. */
+typedef struct pfxt_buffers {
+  const void* triangles; size_t triangles_bytes;     /* GpuTriangle, 96 B each, BVH slot order */
+  const void* nodes; size_t nodes_bytes;             /* Node, 48 B each */
+  const void* materials; size_t materials_bytes;     /* Hot records, 128 B each, row 0 = effects */
+  const void* uv; size_t uv_bytes;                   /* [v0 v1 v2 0] per triangle */
+  const void* surfaces; size_t surfaces_bytes;       /* GpuSurface, 176 B each, record 0 = world */
+  const void* emitters; size_t emitters_bytes;       /* GpuEmitter, 64 B, entry 0 = header */
+  const void* emitter_cdf; size_t emitter_cdf_bytes; /* f32 per emitter */
+  const void* lights; size_t lights_bytes;           /* GpuLight, 64 B, tree rows after the lights */
+  uint32_t triangle_count, shape_count, emitter_count, light_count;
+  const float* sky_rows;    /* sky_height floats */
+  const float* sky_columns; /* sky_width * sky_height floats */
+  uint32_t sky_width, sky_height;
+  float sky_radiance[3];
+  float sky_sun_probability;
+  const float* sobol; /* RGBA32F table, 256 patterns x sobol_length, or NULL for PCG */
+  uint32_t sobol_length;
+  uint32_t max_depth; /* deepest traversal stack the node array can need */
+} pfxt_buffers;
+
+typedef struct pfxt_scene_blobs pfxt_scene_blobs;
+typedef struct pfxt_trace pfxt_trace;
+
+/* ------------------------------------------------------------ ray batches */
+typedef struct pfxt_ray {
+  float origin[3];
+  float tmax;     /* limit: 1e20 for camera rays in scene(), the shadow limit for occluded() */
+  float direction[3];
+  uint32_t pad;
+} pfxt_ray; /* 32 bytes */
+
+typedef struct pfxt_hit {
+  float t;        /* hit distance; tmax when nothing was hit */
+  uint32_t slot;  /* triangle slot (Hit.surface) */
+  uint32_t record;/* instance record (Hit.record), 0 = world */
+  uint32_t hit;   /* 1 when a triangle was hit */
+} pfxt_hit; /* 16 bytes */
+
+/* Rounds (adaptive.rs:73-77). */
+typedef struct pfxt_round {
+  uint32_t samples;
+  uint32_t pad;
+  uint64_t active;
+} pfxt_round;
+
+/* Adaptive (adaptive.rs:10-15). */
+typedef struct pfxt_adaptive {
+  float threshold;
+  uint32_t min_samples;
+  uint32_t max_samples;
+  float growth;
+} pfxt_adaptive;
+
+/* ---------------------------------------------------------------- library */
+int pfxt_abi_version(void);
+/* Message of the last failed call on this thread; "" when none. */
+const char* pfxt_last_error(void);
+/* Number of CUDA devices, or a negative value when the runtime has none. */
+int pfxt_device_count(void);
+
+/* SceneBuffers::build (crates/trace/src/gpu.rs:566-1061): BVH layout
+ * (bvh.rs:95-266, levels.rs:225-470), light tree (tree.rs:220-395), light rows
+ * and emitter CDF (lights.rs:182-243, 391-440), material records
+ * (record.rs:57-180), sky CDF (sky.rs:212-275) and the Sobol table
+ * (sobol.rs:109-153).  Host only; no device is needed. */
+int pfxt_scene_build(const pfxt_scene* scene, const pfxt_settings* settings,
+                     pfxt_scene_blobs** out);
+void pfxt_scene_free(pfxt_scene_blobs* blobs);
+/* The packed buffers of a built scene (pointers stay valid until pfxt_scene_free). */
+int pfxt_scene_buffers(const pfxt_scene_blobs* blobs, pfxt_buffers* out);
+/* Triangle slot order of the world triangles (Bvh::order, bvh.rs:38). */
+int pfxt_scene_order(const pfxt_scene_blobs* blobs, const uint32_t** order, uint32_t* count);
+
+/* Trace::new_detailed (crates/trace/src/gpu.rs:1926-2360): uploads the scene
+ * and allocates the 48 B/pixel accumulation and the three films. */
+int pfxt_create(const pfxt_buffers* buffers, const pfxt_scene* view, const pfxt_settings* settings,
+                uint32_t width, uint32_t height, pfxt_trace** out);
+void pfxt_destroy(pfxt_trace* trace);
+
+/* Trace::set_camera / set_lens / set_projection (gpu.rs:2817-2890); they
+ * restart the accumulation. */
+int pfxt_set_camera(pfxt_trace* trace, const pfxt_camera* camera);
+int pfxt_set_lens(pfxt_trace* trace, const float lens[4]);
+/* Trace::set_window (gpu.rs:2834): full frame size and this tile's origin. */
+int pfxt_set_window(pfxt_trace* trace, const uint32_t full[2], const uint32_t origin[2]);
+
+/* Trace::sample (gpu.rs:2942): `count` more samples per pixel with `seed`. */
+int pfxt_sample(pfxt_trace* trace, uint32_t count, uint32_t seed);
+/* Trace::samples (gpu.rs:3233). */
+uint32_t pfxt_samples(const pfxt_trace* trace);
+/* Trace::sample_adaptive (adaptive.rs:112-325): rounds of samples with the
+ * per-pixel convergence test between them; writes up to `cap` rounds. */
+int pfxt_sample_adaptive(pfxt_trace* trace, const pfxt_adaptive* adaptive, uint32_t seed,
+                         pfxt_round* rounds, uint32_t cap, uint32_t* written);
+/* Adaptive::rounds (adaptive.rs:46-63). */
+int pfxt_adaptive_rounds(const pfxt_adaptive* adaptive, uint32_t* rounds, uint32_t cap,
+                         uint32_t* written);
+/* Trace::readback (gpu.rs:3240): RGBA32F colour, albedo and normal films,
+ * width*height*4 floats each; any pointer may be NULL. */
+int pfxt_readback(pfxt_trace* trace, float* color, float* albedo, float* normal);
+/* Trace::sample_counts (adaptive.rs:328): |accum.color.w| per pixel. */
+int pfxt_sample_counts(pfxt_trace* trace, uint32_t* counts);
+/* The raw 48 B/pixel accumulation (Accum, trace.wgsl:84). */
+int pfxt_read_accum(pfxt_trace* trace, float* accum);
+
+/* scene() closest hit (crates/trace/src/trace.wgsl:999-1075) over a batch of
+ * rays in host memory; the parity entry for identical ray batches. */
+int pfxt_trace_rays(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count, pfxt_hit* hits);
+/* occluded() any hit (trace.wgsl:1096-1168); blocked[i] = 1 when ray i is
+ * blocked before its tmax. */
+int pfxt_occluded(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count, uint8_t* blocked);
+/* The same two queries on device memory, enqueued on `stream` (a
+ * cudaStream_t, NULL = the legacy default stream); no host synchronisation. */
+int pfxt_trace_rays_device(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count,
+                           pfxt_hit* hits, void* stream);
+int pfxt_occluded_device(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count,
+                         uint32_t* blocked, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFXT_H */

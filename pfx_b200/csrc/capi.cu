@@ -1,0 +1,336 @@
+// The C ABI of libpfxtrace (include/pfxt.h): handle management, uploads and
+// the blocking host-memory entry points.  Kernels live in the other .cu files.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "pfxt.h"
+#include "pfxt_internal.h"
+#include "tracer.h"
+
+using namespace pfxt;
+
+namespace pfxt {
+static thread_local std::string g_error;
+void set_error(const std::string& message) { g_error = message; }
+}  // namespace pfxt
+
+struct pfxt_scene_blobs {
+  std::unique_ptr<SceneBlobs> blobs;
+};
+
+namespace {
+
+struct CudaFailure : std::runtime_error {
+  explicit CudaFailure(const std::string& m) : std::runtime_error(m) {}
+};
+
+void check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    throw Refused(std::string(what) + ": out of device memory");
+  }
+  throw CudaFailure(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    set_error("");
+    return PFXT_OK;
+  } catch (const Invalid& e) {
+    set_error(e.what());
+    return PFXT_ERR_INVALID;
+  } catch (const Refused& e) {
+    set_error(e.what());
+    return PFXT_ERR_REFUSED;
+  } catch (const CudaFailure& e) {
+    set_error(e.what());
+    return PFXT_ERR_CUDA;
+  } catch (const DeviceError& e) {
+    set_error(e.what());
+    return PFXT_ERR_DEVICE;
+  } catch (const std::bad_alloc&) {
+    set_error("out of host memory");
+    return PFXT_ERR_REFUSED;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return PFXT_ERR_INVALID;
+  }
+}
+
+template <typename T>
+T* upload(const void* host, size_t bytes, const char* what) {
+  if (bytes == 0) bytes = 16;
+  void* d = nullptr;
+  check(cudaMalloc(&d, bytes), what);
+  if (host) {
+    cudaError_t e = cudaMemcpy(d, host, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cudaFree(d);
+      check(e, what);
+    }
+  } else {
+    cudaMemset(d, 0, bytes);
+  }
+  return static_cast<T*>(d);
+}
+
+// Device staging for the host-memory ray entry points: grown on demand and
+// kept by the handle, so repeated calls do not allocate.
+char* staging(pfxt_trace& t, size_t bytes) {
+  if (bytes > t.stage_bytes) {
+    if (t.d_stage) cudaFree(t.d_stage);
+    t.d_stage = nullptr;
+    t.stage_bytes = 0;
+    check(cudaMalloc(&t.d_stage, bytes), "ray staging");
+    t.stage_bytes = bytes;
+  }
+  return static_cast<char*>(t.d_stage);
+}
+
+void ensure_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    throw Refused("no CUDA device is available");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int pfxt_abi_version(void) { return PFXT_ABI_VERSION; }
+
+const char* pfxt_last_error(void) { return g_error.c_str(); }
+
+int pfxt_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return n;
+}
+
+int pfxt_scene_build(const pfxt_scene* scene, const pfxt_settings* settings, pfxt_scene_blobs** out) {
+  return guarded([&]() {
+    if (!scene || !settings || !out) throw Invalid("null argument");
+    *out = nullptr;
+    auto holder = std::make_unique<pfxt_scene_blobs>();
+    holder->blobs.reset(build_scene(*scene, *settings));
+    *out = holder.release();
+  });
+}
+
+void pfxt_scene_free(pfxt_scene_blobs* blobs) { delete blobs; }
+
+int pfxt_scene_buffers(const pfxt_scene_blobs* h, pfxt_buffers* out) {
+  return guarded([&]() {
+    if (!h || !out) throw Invalid("null argument");
+    const SceneBlobs& b = *h->blobs;
+    memset(out, 0, sizeof(*out));
+    out->triangles = b.triangles.data();
+    out->triangles_bytes = b.triangles.size() * sizeof(GpuTriangle);
+    out->nodes = b.nodes.data();
+    out->nodes_bytes = b.nodes.size() * sizeof(GpuNode);
+    out->materials = b.materials.data();
+    out->materials_bytes = b.materials.size() * sizeof(GpuHot);
+    out->uv = b.uv.data();
+    out->uv_bytes = b.uv.size() * 16;
+    out->surfaces = b.surfaces.data();
+    out->surfaces_bytes = b.surfaces.size() * sizeof(GpuSurface);
+    out->emitters = b.emitters.data();
+    out->emitters_bytes = b.emitters.size() * sizeof(GpuEmitter);
+    out->emitter_cdf = b.emitter_cdf.data();
+    out->emitter_cdf_bytes = b.emitter_cdf.size() * 4;
+    out->lights = b.lights.data();
+    out->lights_bytes = b.lights.size() * sizeof(GpuLight);
+    out->triangle_count = b.triangle_count;
+    out->shape_count = 0;
+    out->emitter_count = b.emitter_count;
+    out->light_count = b.light_count;
+    out->sky_rows = b.sky_rows.data();
+    out->sky_columns = b.sky_columns.data();
+    out->sky_width = b.sky_width;
+    out->sky_height = b.sky_height;
+    memcpy(out->sky_radiance, b.sky_radiance, sizeof(out->sky_radiance));
+    out->sky_sun_probability = 0.0f;
+    out->sobol = b.sobol.empty() ? nullptr : b.sobol.data();
+    out->sobol_length = b.sobol_length;
+    out->max_depth = b.max_depth;
+  });
+}
+
+int pfxt_scene_order(const pfxt_scene_blobs* h, const uint32_t** order, uint32_t* count) {
+  return guarded([&]() {
+    if (!h || !order || !count) throw Invalid("null argument");
+    *order = h->blobs->order.data();
+    *count = (uint32_t)h->blobs->order.size();
+  });
+}
+
+int pfxt_create(const pfxt_buffers* b, const pfxt_scene* view, const pfxt_settings* settings, uint32_t width,
+                uint32_t height, pfxt_trace** out) {
+  return guarded([&]() {
+    if (!b || !view || !settings || !out) throw Invalid("null argument");
+    *out = nullptr;
+    if (width == 0 || height == 0) throw Invalid("the film needs a width and a height");
+    if ((uint64_t)width * height > (1ull << 31)) throw Invalid("the film is too large");
+    if (b->shape_count != 0) throw Invalid("analytic shapes are not supported by this tracer");
+    if (b->max_depth > REF_STACK) throw Invalid("the BVH needs more than the 64-entry traversal stack");
+    if (b->triangles_bytes % sizeof(GpuTriangle) || b->nodes_bytes % sizeof(GpuNode) ||
+        b->materials_bytes % sizeof(GpuHot) || b->surfaces_bytes < sizeof(GpuSurface) ||
+        b->lights_bytes % sizeof(GpuLight) || b->emitters_bytes < sizeof(GpuEmitter))
+      throw Invalid("scene buffers have invalid sizes");
+    ensure_device();
+    auto t = std::make_unique<pfxt_trace>();
+    trace_init(*t, *b, *view, *settings, width, height);
+    *out = t.release();
+  });
+}
+
+void pfxt_destroy(pfxt_trace* t) {
+  if (!t) return;
+  trace_release(*t);
+  delete t;
+}
+
+int pfxt_trace_rays(pfxt_trace* t, const pfxt_ray* rays, uint32_t count, pfxt_hit* hits) {
+  return guarded([&]() {
+    if (!t || (count && (!rays || !hits))) throw Invalid("null argument");
+    if (count == 0) return;
+    char* stage = staging(*t, (size_t)count * (sizeof(pfxt_ray) + sizeof(pfxt_hit)));
+    pfxt_ray* d_rays = reinterpret_cast<pfxt_ray*>(stage);
+    pfxt_hit* d_hits = reinterpret_cast<pfxt_hit*>(stage + (size_t)count * sizeof(pfxt_ray));
+    check(cudaMemcpyAsync(d_rays, rays, (size_t)count * sizeof(pfxt_ray), cudaMemcpyHostToDevice, t->stream),
+          "ray upload");
+    check(launch_closest(t->view, d_rays, count, d_hits, t->stream), "closest-hit kernel");
+    check(cudaMemcpyAsync(hits, d_hits, (size_t)count * sizeof(pfxt_hit), cudaMemcpyDeviceToHost, t->stream),
+          "hit readback");
+    check(cudaStreamSynchronize(t->stream), "closest-hit kernel");
+  });
+}
+
+int pfxt_occluded(pfxt_trace* t, const pfxt_ray* rays, uint32_t count, uint8_t* blocked) {
+  return guarded([&]() {
+    if (!t || (count && (!rays || !blocked))) throw Invalid("null argument");
+    if (count == 0) return;
+    char* stage = staging(*t, (size_t)count * (sizeof(pfxt_ray) + 4 + 1));
+    pfxt_ray* d_rays = reinterpret_cast<pfxt_ray*>(stage);
+    uint32_t* d_blocked = reinterpret_cast<uint32_t*>(stage + (size_t)count * sizeof(pfxt_ray));
+    uint8_t* d_bytes = reinterpret_cast<uint8_t*>(stage + (size_t)count * (sizeof(pfxt_ray) + 4));
+    check(cudaMemcpyAsync(d_rays, rays, (size_t)count * sizeof(pfxt_ray), cudaMemcpyHostToDevice, t->stream),
+          "ray upload");
+    check(launch_any(t->view, d_rays, count, d_blocked, t->stream), "any-hit kernel");
+    check(launch_pack_flags(d_blocked, d_bytes, count, t->stream), "flag packing");
+    check(cudaMemcpyAsync(blocked, d_bytes, count, cudaMemcpyDeviceToHost, t->stream), "flag readback");
+    check(cudaStreamSynchronize(t->stream), "any-hit kernel");
+  });
+}
+
+int pfxt_trace_rays_device(pfxt_trace* t, const pfxt_ray* rays, uint32_t count, pfxt_hit* hits, void* stream) {
+  return guarded([&]() {
+    if (!t || (count && (!rays || !hits))) throw Invalid("null argument");
+    check(launch_closest(t->view, rays, count, hits, (cudaStream_t)stream), "closest-hit kernel");
+  });
+}
+
+int pfxt_occluded_device(pfxt_trace* t, const pfxt_ray* rays, uint32_t count, uint32_t* blocked, void* stream) {
+  return guarded([&]() {
+    if (!t || (count && (!rays || !blocked))) throw Invalid("null argument");
+    check(launch_any(t->view, rays, count, blocked, (cudaStream_t)stream), "any-hit kernel");
+  });
+}
+
+/* Work counters per ray (box tests, triangle tests); not part of the public
+ * header, used by the measurement harness. */
+int pfxt_trace_counts_device(pfxt_trace* t, const pfxt_ray* rays, uint32_t count, uint32_t any, uint32_t* counts,
+                             void* stream) {
+  return guarded([&]() {
+    if (!t || (count && (!rays || !counts))) throw Invalid("null argument");
+    check(launch_counts(t->view, rays, count, any != 0, reinterpret_cast<uint2*>(counts), (cudaStream_t)stream),
+          "counting kernel");
+  });
+}
+
+int pfxt_set_camera(pfxt_trace* t, const pfxt_camera* camera) {
+  return guarded([&]() {
+    if (!t || !camera) throw Invalid("null argument");
+    trace_set_camera(*t, *camera);
+  });
+}
+
+int pfxt_set_lens(pfxt_trace* t, const float lens[4]) {
+  return guarded([&]() {
+    if (!t || !lens) throw Invalid("null argument");
+    trace_set_lens(*t, lens);
+  });
+}
+
+int pfxt_set_window(pfxt_trace* t, const uint32_t full[2], const uint32_t origin[2]) {
+  return guarded([&]() {
+    if (!t || !full || !origin) throw Invalid("null argument");
+    trace_set_window(*t, full, origin);
+  });
+}
+
+int pfxt_sample(pfxt_trace* t, uint32_t count, uint32_t seed) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    trace_sample(*t, count, seed);
+  });
+}
+
+uint32_t pfxt_samples(const pfxt_trace* t) { return t ? t->samples : 0u; }
+
+int pfxt_adaptive_rounds(const pfxt_adaptive* a, uint32_t* rounds, uint32_t cap, uint32_t* written) {
+  return guarded([&]() {
+    if (!a || !written) throw Invalid("null argument");
+    std::vector<uint32_t> r = adaptive_rounds(*a);
+    *written = (uint32_t)std::min<size_t>(r.size(), cap);
+    if (rounds)
+      for (uint32_t i = 0; i < *written; ++i) rounds[i] = r[i];
+    if (r.size() > cap && rounds) throw Invalid("the rounds array is too short");
+  });
+}
+
+int pfxt_sample_adaptive(pfxt_trace* t, const pfxt_adaptive* a, uint32_t seed, pfxt_round* rounds, uint32_t cap,
+                         uint32_t* written) {
+  return guarded([&]() {
+    if (!t || !a || !written) throw Invalid("null argument");
+    trace_sample_adaptive(*t, *a, seed, rounds, cap, written);
+  });
+}
+
+int pfxt_readback(pfxt_trace* t, float* color, float* albedo, float* normal) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    trace_readback(*t, color, albedo, normal);
+  });
+}
+
+int pfxt_sample_counts(pfxt_trace* t, uint32_t* counts) {
+  return guarded([&]() {
+    if (!t || !counts) throw Invalid("null argument");
+    trace_sample_counts(*t, counts);
+  });
+}
+
+int pfxt_read_accum(pfxt_trace* t, float* accum) {
+  return guarded([&]() {
+    if (!t || !accum) throw Invalid("null argument");
+    trace_read_accum(*t, accum);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,58 @@
+// Internal declarations shared by the host builder and the CUDA side of
+// libpfxtrace.  Not part of the C ABI.
+#pragma once
+#include <array>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "pfxt.h"
+#include "pfxt_math.h"
+#include "pfxt_types.h"
+
+#define PFXT_PI_F 3.14159265358979323846f
+
+namespace pfxt {
+
+struct Invalid : std::runtime_error {
+  explicit Invalid(const std::string& m) : std::runtime_error(m) {}
+};
+struct Refused : std::runtime_error {
+  explicit Refused(const std::string& m) : std::runtime_error(m) {}
+};
+
+// The packed buffers of one scene (SceneBuffers, gpu.rs:412-436).
+struct SceneBlobs {
+  std::vector<GpuTriangle> triangles;
+  std::vector<GpuNode> nodes;
+  std::vector<GpuHot> materials;
+  std::vector<std::array<float, 4>> uv;
+  std::vector<GpuSurface> surfaces;
+  std::vector<GpuEmitter> emitters;
+  std::vector<float> emitter_cdf;
+  std::vector<GpuLight> lights;
+  std::vector<uint32_t> order;
+  std::vector<float> sky_rows, sky_columns;
+  uint32_t sky_width = 1, sky_height = 1;
+  float sky_radiance[3] = {0, 0, 0};
+  std::vector<float> sobol;
+  uint32_t sobol_length = 0;
+  uint32_t triangle_count = 0, light_count = 0, emitter_count = 0;
+  uint32_t max_depth = 0;
+};
+
+SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings);
+
+// Thread-local last error of the C ABI.
+void set_error(const std::string& message);
+
+// Convert reference nodes into the B200 traversal layout (layout.cpp).
+struct TraversalLayout {
+  std::vector<WideNode> wide;
+  std::vector<TravTri> tris;
+  std::vector<InstRec> insts;
+  uint32_t root = REF_NONE;  // wide node whose child 0 is the scene root
+};
+TraversalLayout make_layout(const pfxt_buffers& buffers);
+
+}  // namespace pfxt

@@ -1,0 +1,131 @@
+// Tracer state behind a pfxt_trace handle and the host functions that drive
+// the path-tracing kernels (tracer.cu, converge.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "pfxt.h"
+#include "pfxt_internal.h"
+#include "traverse.cuh"
+
+namespace pfxt {
+
+struct DeviceError : std::runtime_error {
+  explicit DeviceError(const std::string& m) : std::runtime_error(m) {}
+};
+
+// The per-pass uniform of the reference (Frame, gpu.rs:157-171) for the
+// fields this tracer reads.
+struct FrameParams {
+  uint32_t size[4];    // width, height, accumulated samples, samples this pass
+  uint32_t counts[4];  // triangles, shapes, seed, unused
+  float origin[4];     // camera origin, w = projection kind
+  float forward[4];
+  float right[4];      // w = orthographic half width
+  float up[4];         // w = orthographic half height
+  float sun_dir[4];    // w = cos(sun radius)
+  float sun_color[4];  // w = intensity
+  float lens[4];       // shift x, shift y, aperture radius, focus distance
+  uint32_t window[4];  // full width, full height, tile origin x, y
+};
+
+// Pipeline-constant specialisation (gpu.rs:1140-1196).
+struct Specialise {
+  uint32_t total_bounces, diffuse_bounces, glossy_bounces, transmission_bounces;
+  uint32_t sobol;         // SOBOL
+  uint32_t sobol_length;  // SOBOL_LENGTH
+  float clamp_indirect;   // CLAMP_INDIRECT
+  float filter_glossy;    // FILTER_GLOSSY
+};
+
+// Everything the shading kernels read, as device pointers.
+struct ShadeView {
+  const GpuTriangle* __restrict__ triangles;
+  const float4* __restrict__ uv;
+  const float4* __restrict__ materials;  // rows of 16 B; record m at (m+1)*8
+  const GpuSurface* __restrict__ surfaces;
+  const GpuEmitter* __restrict__ emitters;
+  const float* __restrict__ emitter_cdf;
+  const GpuLight* __restrict__ lights;
+  const float* __restrict__ sky_rows;
+  const float* __restrict__ sky_columns;
+  const float4* __restrict__ sobol;
+  uint32_t sky_width, sky_height;
+  float sky_radiance[3];
+  float sky_sun_probability;
+  uint32_t material_count;
+  uint32_t emitter_count;   // emitters[0].a.x
+  uint32_t looped;          // emitters[0].a.y
+  uint32_t tree;            // emitters[0].a.w
+};
+
+struct Accum {
+  float4 color, albedo, normal;
+};
+
+}  // namespace pfxt
+
+// The handle behind the C ABI.
+struct pfxt_trace {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t width = 0, height = 0;
+  uint32_t samples = 0;
+  pfxt::FrameParams base{};
+  pfxt::Specialise spec{};
+  uint32_t projection = 0;
+  // traversal layout
+  pfxt::WideNode* d_wide = nullptr;
+  pfxt::TravTri* d_tris = nullptr;
+  pfxt::InstRec* d_insts = nullptr;
+  pfxt::SceneView view{};
+  // shading buffers
+  void* d_triangles = nullptr;
+  void* d_uv = nullptr;
+  void* d_materials = nullptr;
+  void* d_surfaces = nullptr;
+  void* d_emitters = nullptr;
+  void* d_emitter_cdf = nullptr;
+  void* d_lights = nullptr;
+  void* d_sky_rows = nullptr;
+  void* d_sky_columns = nullptr;
+  void* d_sobol = nullptr;
+  pfxt::ShadeView shade{};
+  // films
+  pfxt::Accum* d_accum = nullptr;
+  float4* d_color = nullptr;
+  float4* d_albedo = nullptr;
+  float4* d_normal = nullptr;
+  // adaptive sampling
+  float4* d_snaps = nullptr;  // 32 B per pixel: mean, info
+  uint32_t* d_running = nullptr;
+  // wavefront scratch (allocated on first use)
+  void* d_wave = nullptr;
+  size_t wave_bytes = 0;
+  uint32_t wave_capacity = 0;
+  uint32_t* d_error = nullptr;  // device error word
+  void* d_stage = nullptr;      // staging of the host-memory ray entry points
+  size_t stage_bytes = 0;
+  std::vector<void*> owned;
+};
+
+namespace pfxt {
+
+void trace_init(pfxt_trace& t, const pfxt_buffers& b, const pfxt_scene& view, const pfxt_settings& s, uint32_t width,
+                uint32_t height);
+void trace_release(pfxt_trace& t);
+void trace_set_camera(pfxt_trace& t, const pfxt_camera& c);
+void trace_set_lens(pfxt_trace& t, const float lens[4]);
+void trace_set_window(pfxt_trace& t, const uint32_t full[2], const uint32_t origin[2]);
+void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed);
+void trace_sample_adaptive(pfxt_trace& t, const pfxt_adaptive& a, uint32_t seed, pfxt_round* rounds, uint32_t cap,
+                           uint32_t* written);
+std::vector<uint32_t> adaptive_rounds(const pfxt_adaptive& a);
+void trace_readback(pfxt_trace& t, float* color, float* albedo, float* normal);
+void trace_sample_counts(pfxt_trace& t, uint32_t* counts);
+void trace_read_accum(pfxt_trace& t, float* accum);
+
+}  // namespace pfxt

@@ -1,0 +1,251 @@
+// Host side of the tracer handle: uploads (Trace::new_detailed, gpu.rs:1926),
+// camera/lens/window updates (gpu.rs:2817-2890), readback (gpu.rs:3240) and
+// sample counts (adaptive.rs:328).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "tracer.h"
+
+namespace pfxt {
+
+namespace {
+
+void check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  cudaGetLastError();
+  if (e == cudaErrorMemoryAllocation) throw Refused(std::string(what) + ": out of device memory");
+  throw DeviceError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void* dev_copy(pfxt_trace& t, const void* host, size_t bytes, const char* what) {
+  size_t n = bytes ? bytes : 16;
+  void* d = nullptr;
+  check(cudaMalloc(&d, n), what);
+  t.owned.push_back(d);
+  if (host && bytes)
+    check(cudaMemcpy(d, host, bytes, cudaMemcpyHostToDevice), what);
+  else
+    check(cudaMemset(d, 0, n), what);
+  return d;
+}
+
+template <typename T>
+T* dev_alloc(pfxt_trace& t, size_t count, const char* what) {
+  return static_cast<T*>(dev_copy(t, nullptr, count * sizeof(T), what));
+}
+
+bool finite3(const float* p) { return std::isfinite(p[0]) && std::isfinite(p[1]) && std::isfinite(p[2]); }
+
+}  // namespace
+
+void trace_init(pfxt_trace& t, const pfxt_buffers& b, const pfxt_scene& view, const pfxt_settings& s, uint32_t width,
+                uint32_t height) {
+  check(cudaGetDevice(&t.device), "cudaGetDevice");
+  check(cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking), "stream");
+  t.width = width;
+  t.height = height;
+  t.samples = 0;
+  if (s.sampler == PFXT_SAMPLER_SOBOL && (!b.sobol || b.sobol_length < 256 || b.sobol_length > 8192 ||
+                                          (b.sobol_length & (b.sobol_length - 1)) != 0))
+    throw Invalid("the Sobol sampler needs its table (256 patterns x a power-of-two length in [256, 8192])");
+  for (int i = 0; i < 4; ++i)
+    if (s.bounces[i] > 64) throw Invalid("bounces above 64");
+  if (!finite3(view.camera.origin) || !finite3(view.camera.forward) || !finite3(view.camera.right) ||
+      !finite3(view.camera.up))
+    throw Invalid("camera contains invalid parameters");
+  if (b.sky_width == 0 || b.sky_height == 0 || !b.sky_rows || !b.sky_columns) throw Invalid("invalid sky");
+
+  // ---- traversal layout
+  TraversalLayout layout = make_layout(b);
+  t.d_wide = static_cast<WideNode*>(dev_copy(t, layout.wide.data(), layout.wide.size() * sizeof(WideNode), "nodes"));
+  t.d_tris = static_cast<TravTri*>(dev_copy(t, layout.tris.data(), layout.tris.size() * sizeof(TravTri), "triangles"));
+  t.d_insts =
+      static_cast<InstRec*>(dev_copy(t, layout.insts.data(), layout.insts.size() * sizeof(InstRec), "instances"));
+  t.view.wide = t.d_wide;
+  t.view.tris = t.d_tris;
+  t.view.insts = t.d_insts;
+  t.view.root = layout.root;
+
+  // ---- shading buffers (reference layouts)
+  t.d_triangles = dev_copy(t, b.triangles, b.triangles_bytes, "triangle records");
+  t.d_uv = dev_copy(t, b.uv, b.uv_bytes, "uv");
+  t.d_materials = dev_copy(t, b.materials, b.materials_bytes, "materials");
+  t.d_surfaces = dev_copy(t, b.surfaces, b.surfaces_bytes, "surfaces");
+  t.d_emitters = dev_copy(t, b.emitters, b.emitters_bytes, "emitters");
+  t.d_emitter_cdf = dev_copy(t, b.emitter_cdf, b.emitter_cdf_bytes, "emitter cdf");
+  t.d_lights = dev_copy(t, b.lights, b.lights_bytes, "lights");
+  t.d_sky_rows = dev_copy(t, b.sky_rows, (size_t)b.sky_height * 4, "sky rows");
+  t.d_sky_columns = dev_copy(t, b.sky_columns, (size_t)b.sky_width * b.sky_height * 4, "sky columns");
+  if (s.sampler == PFXT_SAMPLER_SOBOL)
+    t.d_sobol = dev_copy(t, b.sobol, (size_t)b.sobol_length * 256 * 16, "sobol table");
+  const GpuEmitter* head = static_cast<const GpuEmitter*>(b.emitters);
+  ShadeView& v = t.shade;
+  v.triangles = static_cast<const GpuTriangle*>(t.d_triangles);
+  v.uv = static_cast<const float4*>(t.d_uv);
+  v.materials = static_cast<const float4*>(t.d_materials);
+  v.surfaces = static_cast<const GpuSurface*>(t.d_surfaces);
+  v.emitters = static_cast<const GpuEmitter*>(t.d_emitters);
+  v.emitter_cdf = static_cast<const float*>(t.d_emitter_cdf);
+  v.lights = static_cast<const GpuLight*>(t.d_lights);
+  v.sky_rows = static_cast<const float*>(t.d_sky_rows);
+  v.sky_columns = static_cast<const float*>(t.d_sky_columns);
+  v.sobol = static_cast<const float4*>(t.d_sobol);
+  v.sky_width = b.sky_width;
+  v.sky_height = b.sky_height;
+  memcpy(v.sky_radiance, b.sky_radiance, sizeof(v.sky_radiance));
+  v.sky_sun_probability = b.sky_sun_probability;
+  v.material_count = (uint32_t)(b.materials_bytes / sizeof(GpuHot)) - 1u;
+  v.emitter_count = f2u(head->a[0]);
+  v.looped = f2u(head->a[1]);
+  v.tree = f2u(head->a[3]);
+
+  // ---- films: 48 B accumulation + three RGBA32F films per pixel
+  size_t pixels = (size_t)width * height;
+  t.d_accum = dev_alloc<Accum>(t, pixels, "accumulation");
+  t.d_color = dev_alloc<float4>(t, pixels, "colour film");
+  t.d_albedo = dev_alloc<float4>(t, pixels, "albedo film");
+  t.d_normal = dev_alloc<float4>(t, pixels, "normal film");
+  t.d_snaps = dev_alloc<float4>(t, pixels * 2, "adaptive snapshots");
+  t.d_running = dev_alloc<uint32_t>(t, 4, "adaptive count");
+  t.d_error = dev_alloc<uint32_t>(t, 4, "error word");
+
+  // ---- base frame (gpu.rs:2295-2316)
+  FrameParams& f = t.base;
+  memset(&f, 0, sizeof(f));
+  f.size[0] = width;
+  f.size[1] = height;
+  f.counts[0] = b.triangle_count;
+  f.counts[1] = 0;
+  for (int k = 0; k < 3; ++k) {
+    f.origin[k] = view.camera.origin[k];
+    f.forward[k] = view.camera.forward[k];
+    f.right[k] = view.camera.right[k];
+    f.up[k] = view.camera.up[k];
+    f.sun_dir[k] = view.sun.direction[k];
+    f.sun_color[k] = view.sun.color[k];
+  }
+  f.sun_color[3] = view.sun.intensity;
+  for (int k = 0; k < 4; ++k) f.lens[k] = s.lens[k];
+  f.lens[2] = s.lens[2] * 0.5f;  // aperture * 0.5
+  f.window[0] = width;
+  f.window[1] = height;
+  // Projection::place (gpu.rs:206-216)
+  t.projection = s.projection;
+  if (s.projection == PFXT_PROJECTION_ORTHOGRAPHIC) {
+    if (!(s.ortho[0] > 0.0f) || !(s.ortho[1] > 0.0f)) throw Invalid("invalid projection");
+    f.origin[3] = 1.0f;
+    f.right[3] = s.ortho[0] * 0.5f;
+    f.up[3] = s.ortho[1] * 0.5f;
+  } else if (s.projection == PFXT_PROJECTION_EQUIRECT) {
+    f.origin[3] = 2.0f;
+  }
+  // base.sun_dir[3] = sun_radius_deg.to_radians().cos()
+  f.sun_dir[3] = std::cos(view.sun.radius_deg * (PFXT_PI_F / 180.0f));
+
+  Specialise& sp = t.spec;
+  sp.total_bounces = s.bounces[0];
+  sp.diffuse_bounces = s.bounces[1];
+  sp.glossy_bounces = s.bounces[2];
+  sp.transmission_bounces = s.bounces[3];
+  sp.sobol = s.sampler == PFXT_SAMPLER_SOBOL ? 1u : 0u;
+  sp.sobol_length = sp.sobol ? b.sobol_length : 256u;
+  sp.clamp_indirect = s.clamp_indirect;
+  sp.filter_glossy = s.filter_glossy;
+}
+
+void trace_release(pfxt_trace& t) {
+  if (t.device >= 0) cudaSetDevice(t.device);
+  if (t.stream) cudaStreamSynchronize(t.stream);
+  for (void* p : t.owned) cudaFree(p);
+  t.owned.clear();
+  if (t.d_wave) cudaFree(t.d_wave);
+  t.d_wave = nullptr;
+  if (t.d_stage) cudaFree(t.d_stage);
+  t.d_stage = nullptr;
+  if (t.stream) cudaStreamDestroy(t.stream);
+  t.stream = nullptr;
+}
+
+void trace_set_camera(pfxt_trace& t, const pfxt_camera& c) {
+  if (!finite3(c.origin) || !finite3(c.forward) || !finite3(c.right) || !finite3(c.up))
+    throw Invalid("camera contains invalid parameters");
+  if (t.projection != PFXT_PROJECTION_PERSPECTIVE) {
+    const float* axes[] = {c.forward, c.right, c.up};
+    for (auto a : axes)
+      if (!(a[0] * a[0] + a[1] * a[1] + a[2] * a[2] > 1e-12f))
+        throw Invalid("an orthographic or equirect camera needs forward, right and up");
+  }
+  for (int k = 0; k < 3; ++k) {
+    t.base.origin[k] = c.origin[k];
+    t.base.forward[k] = c.forward[k];
+    t.base.right[k] = c.right[k];
+    t.base.up[k] = c.up[k];
+  }
+  t.samples = 0;
+}
+
+void trace_set_lens(pfxt_trace& t, const float lens[4]) {
+  for (int k = 0; k < 4; ++k)
+    if (!std::isfinite(lens[k])) throw Invalid("invalid lens");
+  if (lens[2] < 0.0f || lens[3] <= 0.0f) throw Invalid("invalid lens");
+  t.base.lens[0] = lens[0];
+  t.base.lens[1] = lens[1];
+  t.base.lens[2] = lens[2] * 0.5f;
+  t.base.lens[3] = lens[3];
+  t.samples = 0;
+}
+
+void trace_set_window(pfxt_trace& t, const uint32_t full[2], const uint32_t origin[2]) {
+  auto fits = [&](int k, uint32_t side) {
+    uint64_t end = (uint64_t)origin[k] + side;
+    return end <= full[k];
+  };
+  if (!fits(0, t.width) || !fits(1, t.height)) throw Invalid("the window must lie inside the full frame");
+  if ((uint64_t)full[0] * full[1] > 0xffffffffull) throw Invalid("the full frame is too large");
+  t.base.window[0] = full[0];
+  t.base.window[1] = full[1];
+  t.base.window[2] = origin[0];
+  t.base.window[3] = origin[1];
+  t.samples = 0;
+}
+
+void trace_readback(pfxt_trace& t, float* color, float* albedo, float* normal) {
+  size_t bytes = (size_t)t.width * t.height * 16;
+  check(cudaStreamSynchronize(t.stream), "readback");
+  if (color) check(cudaMemcpy(color, t.d_color, bytes, cudaMemcpyDeviceToHost), "colour readback");
+  if (albedo) check(cudaMemcpy(albedo, t.d_albedo, bytes, cudaMemcpyDeviceToHost), "albedo readback");
+  if (normal) check(cudaMemcpy(normal, t.d_normal, bytes, cudaMemcpyDeviceToHost), "normal readback");
+}
+
+void trace_read_accum(pfxt_trace& t, float* accum) {
+  check(cudaStreamSynchronize(t.stream), "readback");
+  check(cudaMemcpy(accum, t.d_accum, (size_t)t.width * t.height * sizeof(Accum), cudaMemcpyDeviceToHost),
+        "accumulation readback");
+}
+
+void trace_sample_counts(pfxt_trace& t, uint32_t* counts) {
+  size_t pixels = (size_t)t.width * t.height;
+  std::vector<float> accum(pixels * 12);
+  trace_read_accum(t, accum.data());
+  for (size_t i = 0; i < pixels; ++i) counts[i] = (uint32_t)std::fabs(accum[i * 12 + 3]);
+}
+
+// Adaptive::rounds (adaptive.rs:46-63).
+std::vector<uint32_t> adaptive_rounds(const pfxt_adaptive& a) {
+  std::vector<uint32_t> rounds{std::max(a.min_samples / 2u, 1u)};
+  for (;;) {
+    uint32_t last = rounds.back();
+    if (last >= a.max_samples) return rounds;
+    float grown = std::ceil((float)last * a.growth);
+    uint32_t next = f2u(grown);
+    next = std::max(next, last + 1u);
+    next = std::max(next, rounds.size() == 1 ? a.min_samples : 0u);
+    next = std::min(next, a.max_samples);
+    rounds.push_back(next);
+  }
+}
+
+}  // namespace pfxt

@@ -1,0 +1,336 @@
+"""Host-side mirror of the reference's `Trace` (crates/trace/src/gpu.rs and
+adaptive.rs) over the C ABI of libpfxtrace.
+
+    scene = SceneDesc(...)                       # Scene + Detail
+    trace = Trace(scene, Settings(...), w, h)    # Trace::new_detailed
+    trace.sample(16, seed=0)                     # Trace::sample
+    conv = trace.sample_adaptive(Adaptive(...), seed=0)
+    out = trace.readback()                       # Output{color, albedo, normal}
+
+Errors surface as `TraceError` (refusals and setup errors of the reference).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+from .abi import TraceError, check
+
+TRIANGLE = np.dtype(abi.Triangle)
+INSTANCE = np.dtype(abi.Instance)
+MATERIAL = np.dtype(abi.Material)
+LIGHT = np.dtype(abi.Light)
+RAY = np.dtype(abi.Ray)
+HIT = np.dtype(abi.Hit)
+assert TRIANGLE.itemsize == 100 and RAY.itemsize == 32 and HIT.itemsize == 16
+
+
+@dataclass
+class Camera:
+    origin: tuple
+    forward: tuple
+    right: tuple
+    up: tuple
+
+    def c(self) -> abi.Camera:
+        return abi.Camera(abi.f3(*self.origin), abi.f3(*self.forward), abi.f3(*self.right), abi.f3(*self.up))
+
+
+@dataclass
+class Sun:
+    direction: tuple = (0.0, 1.0, 0.0)
+    color: tuple = (1.0, 1.0, 1.0)
+    intensity: float = 0.0
+    radius_deg: float = 0.0
+
+
+@dataclass
+class SceneDesc:
+    """Scene (gpu.rs:242-249) plus the Detail fields this tracer covers."""
+    triangles: np.ndarray                      # TRIANGLE records, world space
+    materials: np.ndarray                      # MATERIAL records
+    camera: Camera
+    lights: np.ndarray = field(default_factory=lambda: np.zeros(0, LIGHT))
+    meshes: list = field(default_factory=list)  # list of TRIANGLE arrays
+    instances: np.ndarray = field(default_factory=lambda: np.zeros(0, INSTANCE))
+    sky: tuple = (0.0, 0.0, 0.0)
+    sun: Sun = field(default_factory=Sun)
+    sky_width: int = 256
+    sky_height: int = 128
+
+    def c(self):
+        """ctypes Scene; the returned keep-alive list must outlive the call."""
+        keep = []
+        tri = np.ascontiguousarray(self.triangles, TRIANGLE)
+        mats = np.ascontiguousarray(self.materials, MATERIAL)
+        lights = np.ascontiguousarray(self.lights, LIGHT)
+        inst = np.ascontiguousarray(self.instances, INSTANCE)
+        keep += [tri, mats, lights, inst]
+        mesh_arr = (abi.Mesh * max(1, len(self.meshes)))()
+        for i, m in enumerate(self.meshes):
+            m = np.ascontiguousarray(m, TRIANGLE)
+            keep.append(m)
+            mesh_arr[i].triangles = m.ctypes.data
+            mesh_arr[i].count = len(m)
+        keep.append(mesh_arr)
+        s = abi.Scene()
+        s.triangles, s.triangle_count = tri.ctypes.data, len(tri)
+        s.meshes, s.mesh_count = C.cast(mesh_arr, C.c_void_p), len(self.meshes)
+        s.instances, s.instance_count = inst.ctypes.data, len(inst)
+        s.materials, s.material_count = mats.ctypes.data, len(mats)
+        s.lights, s.light_count = lights.ctypes.data, len(lights)
+        s.sky = abi.f3(*self.sky)
+        s.sky_width, s.sky_height = self.sky_width, self.sky_height
+        s.camera = self.camera.c()
+        s.sun = abi.Sun(abi.f3(*self.sun.direction), abi.f3(*self.sun.color), self.sun.intensity,
+                        self.sun.radius_deg)
+        return s, keep
+
+    @property
+    def world_triangle_count(self) -> int:
+        return len(self.triangles) + sum(len(self.meshes[int(i["mesh"])]) for i in self.instances)
+
+
+@dataclass
+class Settings:
+    """Detail fields that specialise the tracer (detail.rs, gpu.rs:1140-1196)."""
+    bounces: tuple = (16, 4, 8, 12)   # Bounces::REFERENCE
+    sampler: str = "sobol"            # "sobol" | "pcg"
+    sobol_samples: int = 256
+    clamp_indirect: float = 0.0
+    filter_glossy: float = 0.0
+    projection: int = abi.PROJECTION_PERSPECTIVE
+    ortho: tuple = (0.0, 0.0)
+    lens: tuple = (0.0, 0.0, 0.0, 1.0)
+
+    @staticmethod
+    def deep(n: int, **kw) -> "Settings":
+        """Bounces::deep(n) (detail.rs:435)."""
+        return Settings(bounces=(n, n, n, n), **kw)
+
+    def c(self) -> abi.Settings:
+        s = abi.Settings()
+        s.bounces = abi.u4(*self.bounces)
+        s.sampler = abi.SAMPLER_SOBOL if self.sampler == "sobol" else abi.SAMPLER_PCG
+        s.sobol_samples = self.sobol_samples
+        s.clamp_indirect = self.clamp_indirect
+        s.filter_glossy = self.filter_glossy
+        s.projection = self.projection
+        s.ortho = (C.c_float * 2)(*self.ortho)
+        s.lens = abi.f4(*self.lens)
+        return s
+
+
+@dataclass
+class Adaptive:
+    """Adaptive (adaptive.rs:10-26)."""
+    threshold: float = 0.005
+    min_samples: int = 32
+    max_samples: int = 1024
+    growth: float = 1.5
+
+    def c(self) -> abi.Adaptive:
+        return abi.Adaptive(self.threshold, self.min_samples, self.max_samples, self.growth)
+
+    def valid(self) -> bool:
+        return (np.isfinite(self.threshold) and self.threshold > 0 and self.min_samples >= 2
+                and self.max_samples >= self.min_samples and np.isfinite(self.growth) and self.growth > 1.0)
+
+    def rounds(self) -> list:
+        lib = abi.load()
+        buf = (C.c_uint32 * 4096)()
+        n = C.c_uint32()
+        check(lib.pfxt_adaptive_rounds(C.byref(self.c()), buf, 4096, C.byref(n)))
+        return list(buf[: n.value])
+
+
+@dataclass
+class Round:
+    samples: int
+    active: int
+
+
+@dataclass
+class Converged:
+    """Converged (adaptive.rs:66-102)."""
+    rounds: list
+    pixels: int
+
+    def mean_samples(self) -> float:
+        if self.pixels == 0:
+            return 0.0
+        total, before, running = 0.0, 0, self.pixels
+        for r in self.rounds:
+            total += (r.samples - before) * running
+            before, running = r.samples, r.active
+        return total / self.pixels
+
+    def converged(self) -> bool:
+        return bool(self.rounds) and self.rounds[-1].active == 0
+
+
+@dataclass
+class Output:
+    color: np.ndarray
+    albedo: np.ndarray
+    normal: np.ndarray
+
+
+class SceneBuffers:
+    """SceneBuffers::build (gpu.rs:566) on the host, through the C ABI."""
+
+    def __init__(self, scene: SceneDesc, settings: Settings):
+        self._lib = abi.load()
+        s, keep = scene.c()
+        st = settings.c()
+        h = C.c_void_p()
+        check(self._lib.pfxt_scene_build(C.byref(s), C.byref(st), C.byref(h)))
+        self._h = h
+        self.buffers = abi.Buffers()
+        check(self._lib.pfxt_scene_buffers(self._h, C.byref(self.buffers)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.pfxt_scene_free(h)
+            self._h = None
+
+    def _bytes(self, ptr, n) -> np.ndarray:
+        if not n:
+            return np.zeros(0, np.uint8)
+        return np.ctypeslib.as_array((C.c_uint8 * n).from_address(ptr)).copy()
+
+    def array(self, name: str) -> np.ndarray:
+        b = self.buffers
+        return self._bytes(getattr(b, name), getattr(b, name + "_bytes"))
+
+    def order(self) -> np.ndarray:
+        p = C.POINTER(C.c_uint32)()
+        n = C.c_uint32()
+        check(self._lib.pfxt_scene_order(self._h, C.byref(p), C.byref(n)))
+        return np.ctypeslib.as_array(p, (n.value,)).copy() if n.value else np.zeros(0, np.uint32)
+
+    def sky(self):
+        b = self.buffers
+        rows = np.ctypeslib.as_array((C.c_float * b.sky_height).from_address(b.sky_rows)).copy()
+        cols = np.ctypeslib.as_array((C.c_float * (b.sky_width * b.sky_height)).from_address(b.sky_columns)).copy()
+        return rows, cols
+
+    def sobol(self) -> np.ndarray:
+        b = self.buffers
+        if not b.sobol:
+            return np.zeros((0, 4), np.float32)
+        n = b.sobol_length * 256 * 4
+        return np.ctypeslib.as_array((C.c_float * n).from_address(b.sobol)).copy().reshape(-1, 4)
+
+
+class Trace:
+    """The tracer handle (Trace, gpu.rs:309-342)."""
+
+    def __init__(self, scene: SceneDesc, settings: Settings, width: int, height: int,
+                 buffers: SceneBuffers | None = None):
+        self._lib = abi.load()
+        self.width, self.height = int(width), int(height)
+        self.settings = settings
+        self.scene_buffers = buffers if buffers is not None else SceneBuffers(scene, settings)
+        s, keep = scene.c()
+        st = settings.c()
+        h = C.c_void_p()
+        check(self._lib.pfxt_create(C.byref(self.scene_buffers.buffers), C.byref(s), C.byref(st),
+                                    self.width, self.height, C.byref(h)))
+        self._h = h
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.pfxt_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---------------------------------------------------------- sampling
+    def sample(self, count: int, seed: int) -> None:
+        check(self._lib.pfxt_sample(self._h, count, seed))
+
+    def samples(self) -> int:
+        return int(self._lib.pfxt_samples(self._h))
+
+    def sample_adaptive(self, adaptive: Adaptive, seed: int) -> Converged:
+        cap = 4096
+        rounds = (abi.Round * cap)()
+        n = C.c_uint32()
+        check(self._lib.pfxt_sample_adaptive(self._h, C.byref(adaptive.c()), seed, rounds, cap, C.byref(n)))
+        return Converged([Round(int(rounds[i].samples), int(rounds[i].active)) for i in range(n.value)],
+                         self.width * self.height)
+
+    # ---------------------------------------------------------- readback
+    def readback(self) -> Output:
+        shape = (self.height, self.width, 4)
+        c, a, n = (np.empty(shape, np.float32) for _ in range(3))
+        check(self._lib.pfxt_readback(self._h, c.ctypes.data, a.ctypes.data, n.ctypes.data))
+        return Output(c, a, n)
+
+    def sample_counts(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.uint32)
+        check(self._lib.pfxt_sample_counts(self._h, out.ctypes.data))
+        return out
+
+    def read_accum(self) -> np.ndarray:
+        out = np.empty((self.height, self.width, 12), np.float32)
+        check(self._lib.pfxt_read_accum(self._h, out.ctypes.data))
+        return out
+
+    # ---------------------------------------------------------- view
+    def set_camera(self, camera: Camera) -> None:
+        check(self._lib.pfxt_set_camera(self._h, C.byref(camera.c())))
+
+    def set_lens(self, shift=(0.0, 0.0), aperture=0.0, focus_distance=1.0) -> None:
+        lens = abi.f4(shift[0], shift[1], aperture, focus_distance)
+        check(self._lib.pfxt_set_lens(self._h, lens))
+
+    def set_window(self, full, origin) -> None:
+        f = (C.c_uint32 * 2)(*full)
+        o = (C.c_uint32 * 2)(*origin)
+        check(self._lib.pfxt_set_window(self._h, f, o))
+
+    # ---------------------------------------------------------- ray batches
+    def trace_rays(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, RAY)
+        hits = np.zeros(len(rays), HIT)
+        check(self._lib.pfxt_trace_rays(self._h, rays.ctypes.data, len(rays), hits.ctypes.data))
+        return hits
+
+    def occluded(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, RAY)
+        out = np.zeros(len(rays), np.uint8)
+        check(self._lib.pfxt_occluded(self._h, rays.ctypes.data, len(rays), out.ctypes.data))
+        return out.astype(bool)
+
+    def trace_rays_device(self, rays_ptr: int, count: int, hits_ptr: int, stream: int = 0) -> None:
+        check(self._lib.pfxt_trace_rays_device(self._h, rays_ptr, count, hits_ptr, stream))
+
+    def occluded_device(self, rays_ptr: int, count: int, blocked_ptr: int, stream: int = 0) -> None:
+        check(self._lib.pfxt_occluded_device(self._h, rays_ptr, count, blocked_ptr, stream))
+
+    def counts_device(self, rays_ptr: int, count: int, any_hit: bool, counts_ptr: int, stream: int = 0) -> None:
+        check(self._lib.pfxt_trace_counts_device(self._h, rays_ptr, count, 1 if any_hit else 0, counts_ptr, stream))
+
+
+def make_rays(origins: np.ndarray, directions: np.ndarray, tmax) -> np.ndarray:
+    rays = np.zeros(len(origins), RAY)
+    rays["origin"] = origins
+    rays["direction"] = directions
+    rays["tmax"] = tmax
+    return rays
+
+
+__all__ = ["SceneDesc", "Settings", "Camera", "Sun", "Adaptive", "Converged", "Round", "Output", "Trace",
+           "SceneBuffers", "TraceError", "make_rays", "TRIANGLE", "INSTANCE", "MATERIAL", "LIGHT", "RAY", "HIT"]
