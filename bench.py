@@ -299,7 +299,7 @@ def main():
         peak, peak_kind = peaks()
         closest_s = statistics.mean(closest_ms) / 1e3
         achieved = bytes_closest / closest_s / 1e9
-        traffic = ncu_traffic("k_closest")
+        traffic = ncu_traffic("k_trace<0>")
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -308,7 +308,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": int((nc + ns) * 32),
                     "d2h_bytes_per_step": int(nc * 16 + ns)},
             "gpu_launches": 2 * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "k_closest (closest-hit traversal)", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "k_trace<0> (closest-hit traversal)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": traffic,
                          "algorithmic_bytes_per_launch": bytes_closest,

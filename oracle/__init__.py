@@ -44,6 +44,7 @@ def lib() -> C.CDLL:
             "orc_automatic_min_samples": (u32, [f32]),
             "orc_adaptive_error": (f32, [vp, f32, vp, f32]),
             "orc_falloff": (f32, [f32, f32, f32, f32]),
+            "orc_check_div": (C.c_uint64, [C.c_uint64, C.c_uint64]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -127,3 +128,8 @@ def adaptive_error(prior, prior_count, now, count) -> float:
 
 def falloff(intensity, radius, range_, distance) -> float:
     return float(lib().orc_falloff(intensity, radius, range_, distance))
+
+
+def check_div(per_family: int, seed: int = 1) -> int:
+    """Mismatches between the kernels' correctly-rounded division (div_rn) and IEEE division."""
+    return int(lib().orc_check_div(per_family, seed))

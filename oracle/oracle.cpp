@@ -657,3 +657,48 @@ float orc_falloff(float intensity, float radius, float range, float distance) {
 }
 
 }  // extern "C"
+
+// ======================================================= division identity
+namespace {
+uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9e3779b97f4a7c15ull);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+}  // namespace
+
+extern "C" {
+// Number of (x, d) pairs, over four input families, where the shared
+// div_rn (pfxt_math.h) differs from IEEE division.  The kernels compute every
+// slab quotient with div_rn; the oracle divides.
+uint64_t orc_check_div(uint64_t per_family, uint64_t seed) {
+  uint64_t bad = 0;
+  for (int fam = 0; fam < 4; ++fam) {
+    uint64_t s = seed * 4 + fam;
+    for (uint64_t i = 0; i < per_family; ++i) {
+      uint64_t r = splitmix(s);
+      float x, d;
+      if (fam == 0) {
+        x = bits2f((uint32_t)r);
+        d = bits2f((uint32_t)(r >> 32));
+        if (!isfinite(x) || !isfinite(d) || fabsf(d) < 1e-12f) continue;
+      } else if (fam == 1) {
+        x = ((float)(uint32_t)r * 0x1p-32f - 0.5f) * 2000.0f - ((float)(uint32_t)(r >> 32) * 0x1p-32f) * 1000.0f;
+        d = (float)(uint32_t)(r >> 16) * 0x1p-32f * 2.0f - 1.0f;
+        if (fabsf(d) < 1e-12f) continue;
+      } else if (fam == 2) {
+        x = bits2f(0x3f800000u | ((uint32_t)r & 0x7fffffu));
+        d = bits2f(0x3f800000u | ((uint32_t)(r >> 32) & 0x7fffffu));
+      } else {
+        x = ((float)(uint32_t)r * 0x1p-32f - 0.5f) * 100.0f;
+        d = bits2f(0x2b8cbcccu + (uint32_t)((r >> 32) % 0x14000000u));
+        if (r & 1) d = -d;
+      }
+      float a = x / d, b = div_rn(x, d, 1.0f / d);
+      if (f2bits(a) != f2bits(b) && !(a == 0.0f && b == 0.0f)) ++bad;
+    }
+  }
+  return bad;
+}
+}  // extern "C"

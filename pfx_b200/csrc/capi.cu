@@ -214,7 +214,7 @@ int pfxt_trace_rays(pfxt_trace* t, const pfxt_ray* rays, uint32_t count, pfxt_hi
     pfxt_hit* d_hits = reinterpret_cast<pfxt_hit*>(stage + (size_t)count * sizeof(pfxt_ray));
     check(cudaMemcpyAsync(d_rays, rays, (size_t)count * sizeof(pfxt_ray), cudaMemcpyHostToDevice, t->stream),
           "ray upload");
-    check(launch_closest(t->view, d_rays, count, d_hits, t->stream), "closest-hit kernel");
+    check(launch_closest(t->view, d_rays, count, d_hits, next_counter(*t), t->stream), "closest-hit kernel");
     check(cudaMemcpyAsync(hits, d_hits, (size_t)count * sizeof(pfxt_hit), cudaMemcpyDeviceToHost, t->stream),
           "hit readback");
     check(cudaStreamSynchronize(t->stream), "closest-hit kernel");
@@ -231,7 +231,7 @@ int pfxt_occluded(pfxt_trace* t, const pfxt_ray* rays, uint32_t count, uint8_t* 
     uint8_t* d_bytes = reinterpret_cast<uint8_t*>(stage + (size_t)count * (sizeof(pfxt_ray) + 4));
     check(cudaMemcpyAsync(d_rays, rays, (size_t)count * sizeof(pfxt_ray), cudaMemcpyHostToDevice, t->stream),
           "ray upload");
-    check(launch_any(t->view, d_rays, count, d_blocked, t->stream), "any-hit kernel");
+    check(launch_any(t->view, d_rays, count, d_blocked, next_counter(*t), t->stream), "any-hit kernel");
     check(launch_pack_flags(d_blocked, d_bytes, count, t->stream), "flag packing");
     check(cudaMemcpyAsync(blocked, d_bytes, count, cudaMemcpyDeviceToHost, t->stream), "flag readback");
     check(cudaStreamSynchronize(t->stream), "any-hit kernel");
@@ -241,14 +241,14 @@ int pfxt_occluded(pfxt_trace* t, const pfxt_ray* rays, uint32_t count, uint8_t* 
 int pfxt_trace_rays_device(pfxt_trace* t, const pfxt_ray* rays, uint32_t count, pfxt_hit* hits, void* stream) {
   return guarded([&]() {
     if (!t || (count && (!rays || !hits))) throw Invalid("null argument");
-    check(launch_closest(t->view, rays, count, hits, (cudaStream_t)stream), "closest-hit kernel");
+    check(launch_closest(t->view, rays, count, hits, next_counter(*t), (cudaStream_t)stream), "closest-hit kernel");
   });
 }
 
 int pfxt_occluded_device(pfxt_trace* t, const pfxt_ray* rays, uint32_t count, uint32_t* blocked, void* stream) {
   return guarded([&]() {
     if (!t || (count && (!rays || !blocked))) throw Invalid("null argument");
-    check(launch_any(t->view, rays, count, blocked, (cudaStream_t)stream), "any-hit kernel");
+    check(launch_any(t->view, rays, count, blocked, next_counter(*t), (cudaStream_t)stream), "any-hit kernel");
   });
 }
 
@@ -258,7 +258,8 @@ int pfxt_trace_counts_device(pfxt_trace* t, const pfxt_ray* rays, uint32_t count
                              void* stream) {
   return guarded([&]() {
     if (!t || (count && (!rays || !counts))) throw Invalid("null argument");
-    check(launch_counts(t->view, rays, count, any != 0, reinterpret_cast<uint2*>(counts), (cudaStream_t)stream),
+    check(launch_counts(t->view, rays, count, any != 0, reinterpret_cast<uint2*>(counts), next_counter(*t),
+                        (cudaStream_t)stream),
           "counting kernel");
   });
 }

@@ -7,10 +7,14 @@
 
 namespace pfxt {
 
-cudaError_t launch_closest(const SceneView& s, const pfxt_ray* rays, uint32_t n, pfxt_hit* hits, cudaStream_t stream);
-cudaError_t launch_any(const SceneView& s, const pfxt_ray* rays, uint32_t n, uint32_t* blocked, cudaStream_t stream);
+// `counter` is one u32 of device scratch (the work-sharing counter), reset by
+// the launcher on `stream` before the kernel starts.
+cudaError_t launch_closest(const SceneView& s, const pfxt_ray* rays, uint32_t n, pfxt_hit* hits, uint32_t* counter,
+                           cudaStream_t stream);
+cudaError_t launch_any(const SceneView& s, const pfxt_ray* rays, uint32_t n, uint32_t* blocked, uint32_t* counter,
+                       cudaStream_t stream);
 cudaError_t launch_pack_flags(const uint32_t* flags, uint8_t* bytes, uint32_t n, cudaStream_t stream);
 cudaError_t launch_counts(const SceneView& s, const pfxt_ray* rays, uint32_t n, bool any, uint2* counts,
-                          cudaStream_t stream);
+                          uint32_t* counter, cudaStream_t stream);
 
 }  // namespace pfxt

@@ -83,6 +83,21 @@ PFXT_HD float fract_(float x) { return x - floorf(x); }
 PFXT_HD float mix_(float a, float b, float t) { return a * (1.0f - t) + b * t; }
 PFXT_HD float select_(float f, float t, bool c) { return c ? t : f; }
 PFXT_HD float fmod_wgsl(float x, float y) { return x - y * truncf(x / y); }
+
+// x / d, correctly rounded, given r = x-independent RN(1/d): one product and
+// one fused correction (P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990: with r
+// the correctly rounded reciprocal and q within an ulp of x/d, the fused
+// residual x - q*d is exact and q + residual*r rounds to RN(x/d)).  The
+// theorem assumes no underflow or overflow, so tiny numerators or quotients
+// and huge quotients take the plain division.  fmaf is exact on both sides.
+PFXT_HD float div_rn(float x, float d, float r) {
+  float q = x * r;
+  float e = fmaf(-q, d, x);
+  float q2 = fmaf(e, r, q);
+  if (!(abs_(x) >= 0x1p-96f) || !(abs_(q2) >= 0x1p-100f) || !(abs_(q2) <= 0x1p+120f)) return x / d;
+  return q2;
+}
 PFXT_HD float smoothstep_(float e0, float e1, float x) {
   float t = clamp_((x - e0) / (e1 - e0), 0.0f, 1.0f);
   return t * t * (3.0f - 2.0f * t);

@@ -107,6 +107,8 @@ struct pfxt_trace {
   size_t wave_bytes = 0;
   uint32_t wave_capacity = 0;
   uint32_t* d_error = nullptr;  // device error word
+  uint32_t* d_counters = nullptr;  // ring of work-sharing counters (device scratch)
+  uint32_t counter_slot = 0;
   void* d_stage = nullptr;      // staging of the host-memory ray entry points
   size_t stage_bytes = 0;
   std::vector<void*> owned;
@@ -127,5 +129,12 @@ std::vector<uint32_t> adaptive_rounds(const pfxt_adaptive& a);
 void trace_readback(pfxt_trace& t, float* color, float* albedo, float* normal);
 void trace_sample_counts(pfxt_trace& t, uint32_t* counts);
 void trace_read_accum(pfxt_trace& t, float* accum);
+// Next counter of the ring: consecutive launches (possibly on different
+// streams) never share a counter.
+inline uint32_t* next_counter(pfxt_trace& t) {
+  uint32_t* c = t.d_counters + (t.counter_slot % 64u);
+  t.counter_slot += 1u;
+  return c;
+}
 
 }  // namespace pfxt

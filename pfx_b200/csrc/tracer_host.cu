@@ -111,6 +111,7 @@ void trace_init(pfxt_trace& t, const pfxt_buffers& b, const pfxt_scene& view, co
   t.d_snaps = dev_alloc<float4>(t, pixels * 2, "adaptive snapshots");
   t.d_running = dev_alloc<uint32_t>(t, 4, "adaptive count");
   t.d_error = dev_alloc<uint32_t>(t, 4, "error word");
+  t.d_counters = dev_alloc<uint32_t>(t, 64, "work counters");
 
   // ---- base frame (gpu.rs:2295-2316)
   FrameParams& f = t.base;

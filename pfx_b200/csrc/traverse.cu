@@ -1,6 +1,15 @@
 // Ray-batch kernels: closest hit and any hit over caller-supplied rays.  These
 // back pfxt_trace_rays / pfxt_occluded (the parity entry on identical ray
 // batches) and the traversal benchmark.
+//
+// Persistent warps with per-lane refill: the grid fills the GPU once (SM count
+// x resident blocks), and whenever lanes of a warp finish their query they
+// take the next ray indices from one atomic counter (one atomic per warp per
+// refill).  A warp therefore keeps its lanes busy instead of idling behind its
+// slowest ray, which is what limits a one-ray-per-thread launch on incoherent
+// batches.  Inside a lane the walk alternates an inner-node phase and a leaf
+// phase (the "while-while" loop), so lanes of a warp tend to run the same
+// phase together.
 #include <cuda_runtime.h>
 
 #include "kernels.h"
@@ -10,6 +19,8 @@ namespace pfxt {
 
 namespace {
 
+constexpr int kThreads = 128;
+
 __device__ __forceinline__ void load_ray(const pfxt_ray* __restrict__ rays, uint32_t i, v3& o, v3& d, float& tmax) {
   const float4* p = reinterpret_cast<const float4*>(rays + i);
   float4 a = __ldg(p), b = __ldg(p + 1);
@@ -18,41 +29,58 @@ __device__ __forceinline__ void load_ray(const pfxt_ray* __restrict__ rays, uint
   d = mk3(b.x, b.y, b.z);
 }
 
-__global__ void __launch_bounds__(128) k_closest(SceneView s, const pfxt_ray* __restrict__ rays, uint32_t n,
-                                                 pfxt_hit* __restrict__ hits) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  v3 o, d;
-  float tmax;
-  load_ray(rays, i, o, d, tmax);
-  TraceHit h = traverse<false, false>(s, o, d, tmax, nullptr);
-  reinterpret_cast<uint4*>(hits)[i] = make_uint4(__float_as_uint(h.t), h.slot, h.record, h.hit);
-}
-
-__global__ void __launch_bounds__(128) k_any(SceneView s, const pfxt_ray* __restrict__ rays, uint32_t n,
-                                             uint32_t* __restrict__ blocked) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  v3 o, d;
-  float tmax;
-  load_ray(rays, i, o, d, tmax);
-  TraceHit h = traverse<true, false>(s, o, d, tmax, nullptr);
-  blocked[i] = h.hit;
-}
-
-__global__ void __launch_bounds__(128) k_counts(SceneView s, const pfxt_ray* __restrict__ rays, uint32_t n,
-                                                uint32_t any, uint2* __restrict__ counts) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  v3 o, d;
-  float tmax;
-  load_ray(rays, i, o, d, tmax);
-  TraceCounts c{0u, 0u};
-  if (any)
-    traverse<true, true>(s, o, d, tmax, &c);
-  else
-    traverse<false, true>(s, o, d, tmax, &c);
-  counts[i] = make_uint2(c.boxes, c.tris);
+// MODE 0: closest hit -> pfxt_hit; MODE 1: any hit -> u32 flag;
+// MODE 2/3: work counters of closest / any hit -> uint2.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) k_trace(SceneView s, const pfxt_ray* __restrict__ rays, uint32_t n,
+                                                    void* __restrict__ out, uint32_t* __restrict__ counter) {
+  constexpr bool ANY = (MODE == 1 || MODE == 3);
+  constexpr bool COUNT = (MODE >= 2);
+  constexpr unsigned FULL = 0xffffffffu;
+  uint32_t sref[REF_STACK];
+  float snear[REF_STACK];
+  Walker<ANY, COUNT> w;
+  const int lane = threadIdx.x & 31;
+  uint32_t idx = 0;
+  bool have = false, retired = false;
+  for (;;) {
+    bool need = !have && !retired;
+    unsigned m = __ballot_sync(FULL, need);
+    if (m) {
+      int leader = __ffs(m) - 1;
+      uint32_t first = 0;
+      if (lane == leader) first = atomicAdd(counter, (uint32_t)__popc(m));
+      first = __shfl_sync(FULL, first, leader);
+      if (need) {
+        idx = first + (uint32_t)__popc(m & ((1u << lane) - 1u));
+        if (idx < n) {
+          v3 o, d;
+          float tmax;
+          load_ray(rays, idx, o, d, tmax);
+          w.start(s, o, d, tmax);
+          have = true;
+        } else {
+          retired = true;
+        }
+      }
+    }
+    if (__all_sync(FULL, retired)) break;
+    if (have) {
+      w.inner_phase(s, sref, snear);
+      if (!w.done) w.leaf_phase(s, sref, snear);
+      if (w.done) {
+        if (MODE == 0) {
+          reinterpret_cast<uint4*>(out)[idx] =
+              make_uint4(__float_as_uint(w.hit.t), w.hit.slot, w.hit.record, w.hit.hit);
+        } else if (MODE == 1) {
+          reinterpret_cast<uint32_t*>(out)[idx] = w.hit.hit;
+        } else {
+          reinterpret_cast<uint2*>(out)[idx] = make_uint2(w.counts.boxes, w.counts.tris);
+        }
+        have = false;
+      }
+    }
+  }
 }
 
 // Narrow 32-bit flags to bytes (separate input and output regions).
@@ -61,33 +89,52 @@ __global__ void k_pack(const uint32_t* __restrict__ in, uint8_t* __restrict__ ou
   if (i < n) out[i] = in[i] ? 1 : 0;
 }
 
-}  // namespace
+template <int MODE>
+int persistent_blocks() {
+  static int blocks = 0;
+  if (blocks == 0) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<MODE>, kThreads, 0);
+    blocks = sms * (per > 0 ? per : 1);
+  }
+  return blocks;
+}
 
-cudaError_t launch_closest(const SceneView& s, const pfxt_ray* rays, uint32_t n, pfxt_hit* hits, cudaStream_t stream) {
+template <int MODE>
+cudaError_t launch(const SceneView& s, const pfxt_ray* rays, uint32_t n, void* out, uint32_t* counter,
+                   cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  uint32_t blocks = (n + 127u) / 128u;
-  k_closest<<<blocks, 128, 0, stream>>>(s, rays, n, hits);
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  uint32_t need = (n + kThreads - 1) / kThreads;
+  uint32_t blocks = (uint32_t)persistent_blocks<MODE>();
+  if (need < blocks) blocks = need;
+  k_trace<MODE><<<blocks, kThreads, 0, stream>>>(s, rays, n, out, counter);
   return cudaGetLastError();
 }
 
-cudaError_t launch_any(const SceneView& s, const pfxt_ray* rays, uint32_t n, uint32_t* blocked, cudaStream_t stream) {
-  if (n == 0) return cudaSuccess;
-  uint32_t blocks = (n + 127u) / 128u;
-  k_any<<<blocks, 128, 0, stream>>>(s, rays, n, blocked);
-  return cudaGetLastError();
+}  // namespace
+
+cudaError_t launch_closest(const SceneView& s, const pfxt_ray* rays, uint32_t n, pfxt_hit* hits, uint32_t* counter,
+                           cudaStream_t stream) {
+  return launch<0>(s, rays, n, hits, counter, stream);
+}
+
+cudaError_t launch_any(const SceneView& s, const pfxt_ray* rays, uint32_t n, uint32_t* blocked, uint32_t* counter,
+                       cudaStream_t stream) {
+  return launch<1>(s, rays, n, blocked, counter, stream);
+}
+
+cudaError_t launch_counts(const SceneView& s, const pfxt_ray* rays, uint32_t n, bool any, uint2* counts,
+                          uint32_t* counter, cudaStream_t stream) {
+  return any ? launch<3>(s, rays, n, counts, counter, stream) : launch<2>(s, rays, n, counts, counter, stream);
 }
 
 cudaError_t launch_pack_flags(const uint32_t* flags, uint8_t* bytes, uint32_t n, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   k_pack<<<(n + 255u) / 256u, 256, 0, stream>>>(flags, bytes, n);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_counts(const SceneView& s, const pfxt_ray* rays, uint32_t n, bool any, uint2* counts,
-                          cudaStream_t stream) {
-  if (n == 0) return cudaSuccess;
-  uint32_t blocks = (n + 127u) / 128u;
-  k_counts<<<blocks, 128, 0, stream>>>(s, rays, n, any ? 1u : 0u, counts);
   return cudaGetLastError();
 }
 

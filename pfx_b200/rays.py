@@ -26,13 +26,29 @@ def geometric_normals(buffers, slots: np.ndarray, records: np.ndarray, instances
     return n.astype(F32)
 
 
+def pixel_rays(cam, width: int, height: int, n: int, rng, tmax: float = 1e20) -> np.ndarray:
+    """Camera rays for n consecutive pixels in scanline order (wrapping), one
+    jittered sample each, as one pass of the tracer generates them."""
+    start = int(rng.integers(0, width * height))
+    pix = (start + np.arange(n)) % (width * height)
+    px = (pix % width).astype(F32) + rng.uniform(0, 1, n).astype(F32)
+    py = (pix // width).astype(F32) + rng.uniform(0, 1, n).astype(F32)
+    ndc_x = px / F32(width) * F32(2) - F32(1)
+    ndc_y = py / F32(height) * F32(2) - F32(1)
+    f, r, u = (np.asarray(x, F32) for x in (cam.forward, cam.right, cam.up))
+    d = f[None] + r[None] * ndc_x[:, None] + u[None] * (-ndc_y)[:, None]
+    d = d / np.sqrt((d * d).sum(-1))[:, None]
+    o = np.broadcast_to(np.asarray(cam.origin, F32), d.shape)
+    return make_rays(o, d.astype(F32), tmax)
+
+
 def pass_mix(trace, scene, width, height, n: int, seed: int = 0):
     """(closest-hit rays, any-hit rays): n/2 camera + bounce rays traced for the
     closest hit, and up to n/2 shadow rays; uses the tracer itself to find the
     camera rays' hit points."""
     rng = np.random.default_rng(seed)
     half = n // 2
-    cam = camera_rays(scene.camera, width, height, half, rng)
+    cam = pixel_rays(scene.camera, width, height, half, rng)
     hits = trace.trace_rays(cam)
     ok = hits["hit"] == 1
     p = cam["origin"] + cam["direction"] * hits["t"][:, None]

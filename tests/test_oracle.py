@@ -75,3 +75,9 @@ def test_falloff_known_answer():
     want = 4.0 * (1.0 - 0.2 ** 4) ** 2 / 4.0
     assert abs(got - want) < 1e-6
     assert oracle.falloff(4.0, 0.0, 10.0, 10.0) == 0.0
+
+
+def test_kernel_division_is_ieee_division():
+    # the slab quotients of the kernels use div_rn (Markstein's correction);
+    # it must round exactly like the reference's division
+    assert oracle.check_div(1_500_000, seed=7) == 0
