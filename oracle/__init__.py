@@ -27,7 +27,7 @@ def lib() -> C.CDLL:
     global _lib
     if _lib is None:
         if not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime
-                                   for p in [HERE / "oracle.cpp", HERE.parent / "pfx_b200/csrc/pfxt_math.h"]
+                                   for p in [HERE / "oracle.cpp", HERE / "render.cpp", HERE.parent / "pfx_b200/csrc/pfxt_math.h"]
                                    if p.exists()):
             build()
         L = C.CDLL(str(LIB))
@@ -133,3 +133,97 @@ def falloff(intensity, radius, range_, distance) -> float:
 def check_div(per_family: int, seed: int = 1) -> int:
     """Mismatches between the kernels' correctly-rounded division (div_rn) and IEEE division."""
     return int(lib().orc_check_div(per_family, seed))
+
+
+class _OrcScene(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("node_count", C.c_uint32), ("tris", C.c_void_p), ("tri_count", C.c_uint32),
+                ("surfaces", C.c_void_p), ("materials", C.c_void_p), ("material_rows", C.c_uint32),
+                ("emitters", C.c_void_p), ("emitter_cdf", C.c_void_p), ("lights", C.c_void_p),
+                ("sky_rows", C.c_void_p), ("sky_columns", C.c_void_p), ("sky_width", C.c_uint32),
+                ("sky_height", C.c_uint32), ("sky_radiance", C.c_float * 3), ("sky_sun_probability", C.c_float),
+                ("sobol", C.c_void_p), ("sobol_length", C.c_uint32), ("sobol_on", C.c_uint32),
+                ("bounces", C.c_uint32 * 4), ("clamp_indirect", C.c_float), ("filter_glossy", C.c_float)]
+
+
+class Renderer:
+    """main()/radiance() of the reference restated on the CPU over one scene's
+    packed buffers (a pfx_b200 SceneBuffers) and settings."""
+
+    def __init__(self, buffers, settings):
+        L = lib()
+        L.orc_render.restype = C.c_int
+        L.orc_render.argtypes = [C.c_void_p] * 6
+        L.orc_converge.restype = C.c_uint32
+        L.orc_converge.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_int]
+        L.orc_tree_pick.restype = None
+        L.orc_tree_pick.argtypes = [C.c_void_p] * 4 + [C.c_uint32] + [C.c_void_p] * 3
+        self.keep = {k: buffers.array(k) for k in ("nodes", "triangles", "surfaces", "materials", "emitters",
+                                                   "emitter_cdf", "lights")}
+        rows, cols = buffers.sky()
+        self.keep["sky_rows"], self.keep["sky_cols"] = rows, cols
+        self.keep["sobol"] = np.ascontiguousarray(buffers.sobol(), np.float32)
+        b = buffers.buffers
+        s = _OrcScene()
+        s.nodes, s.node_count = _p(self.keep["nodes"]), len(self.keep["nodes"]) // 48
+        s.tris, s.tri_count = _p(self.keep["triangles"]), len(self.keep["triangles"]) // 96
+        s.surfaces = _p(self.keep["surfaces"])
+        s.materials, s.material_rows = _p(self.keep["materials"]), len(self.keep["materials"]) // 16
+        s.emitters = _p(self.keep["emitters"])
+        s.emitter_cdf = _p(self.keep["emitter_cdf"]) if len(self.keep["emitter_cdf"]) else None
+        s.lights = _p(self.keep["lights"]) if len(self.keep["lights"]) else None
+        s.sky_rows, s.sky_columns = _p(rows), _p(cols)
+        s.sky_width, s.sky_height = b.sky_width, b.sky_height
+        s.sky_radiance = (C.c_float * 3)(*b.sky_radiance)
+        s.sky_sun_probability = b.sky_sun_probability
+        sob = self.keep["sobol"]
+        s.sobol = _p(sob) if len(sob) else None
+        s.sobol_length = b.sobol_length
+        s.sobol_on = 1 if settings.sampler == "sobol" else 0
+        s.bounces = (C.c_uint32 * 4)(*settings.bounces)
+        s.clamp_indirect, s.filter_glossy = settings.clamp_indirect, settings.filter_glossy
+        self.scene = s
+
+    def render(self, frame: np.ndarray, accum: np.ndarray, accumulated: int, count: int, seed: int):
+        """One Trace::sample(count, seed) pass on `accum` (H, W, 12 floats,
+        updated in place); returns (color, albedo, normal) films."""
+        f = np.array(frame, np.uint32).copy()
+        f[2], f[3], f[6] = accumulated, count, seed
+        h, w = accum.shape[:2]
+        color = np.zeros((h, w, 4), np.float32)
+        albedo = np.zeros_like(color)
+        normal = np.zeros_like(color)
+        lib().orc_render(C.byref(self.scene), _p(f), _p(accum), _p(color), _p(albedo), _p(normal))
+        return color, albedo, normal
+
+    def converge(self, accum: np.ndarray, snaps: np.ndarray, min_samples: int, threshold: float, mark: bool) -> int:
+        h, w = accum.shape[:2]
+        return int(lib().orc_converge(_p(accum), _p(snaps), w, h, min_samples, threshold, 1 if mark else 0))
+
+    def tree_pick(self, points: np.ndarray, normals: np.ndarray, rands: np.ndarray):
+        n = len(points)
+        pts = np.ascontiguousarray(points, np.float32)
+        nrm = np.ascontiguousarray(normals, np.float32)
+        r = np.ascontiguousarray(rands, np.float32)
+        light = np.zeros(n, np.int32)
+        pmf = np.zeros(n, np.float32)
+        leaf = np.zeros(n, np.uint32)
+        lib().orc_tree_pick(C.byref(self.scene), _p(pts), _p(nrm), _p(r), n, _p(light), _p(pmf), _p(leaf))
+        return light, pmf, leaf
+
+    def sample_adaptive(self, frame, width, height, adaptive, seed):
+        """Trace::sample_adaptive (adaptive.rs:136-325) on the CPU: returns
+        (rounds [(samples, active)], accum, films)."""
+        accum = np.zeros((height, width, 12), np.float32)
+        snaps = np.zeros((height, width, 8), np.float32)
+        samples, rounds, films = 0, [], None
+        for step, target in enumerate(adaptive.rounds()):
+            count = max(target - samples, 0)
+            if count:
+                films = self.render(frame, accum, samples, count, seed)
+            samples += count
+            running = self.converge(accum, snaps, adaptive.min_samples, adaptive.threshold, step > 0)
+            active = running if step > 0 else width * height
+            rounds.append((target, active))
+            if active == 0:
+                break
+        return rounds, accum, films

@@ -167,6 +167,7 @@ struct Walk {
   float t;
   uint32_t surface, record;
   bool hit;
+  float u, v;
 };
 
 // tri_hit (trace.wgsl:780-804); cut_out is false for the scenes in scope
@@ -198,6 +199,8 @@ void tri_hit(const Scene& s, uint32_t i, uint32_t record, uint32_t word, float i
     hit->surface = i;
     hit->record = record;
     hit->hit = true;
+    hit->u = u;
+    hit->v = v;
   }
 }
 
@@ -229,7 +232,7 @@ bool tri_blocks(const Scene& s, uint32_t i, uint32_t record, uint32_t word, floa
 // `any` selects occluded().  Counts: one box test per popped node, one
 // triangle test per leaf slot visited.
 Walk walk(const Scene& s, v3 o, v3 d, float limit, bool any, uint32_t* boxes, uint32_t* tris, uint32_t* overflow) {
-  Walk hit{limit, 0u, 0u, false};
+  Walk hit{limit, 0u, 0u, false, 0.0f, 0.0f};
   if (s.tri_count == 0 || s.node_count == 0) return hit;
   uint32_t stack[64];
   uint32_t top = 1u;
@@ -300,6 +303,9 @@ Walk walk(const Scene& s, v3 o, v3 d, float limit, bool any, uint32_t* boxes, ui
 }
 
 }  // namespace
+
+// Shared with render.cpp (the path integrator restatement).
+Walk orc_walk(const Scene& s, v3 o, v3 d, float limit, bool any) { return walk(s, o, d, limit, any, nullptr, nullptr, nullptr); }
 
 extern "C" {
 
@@ -702,3 +708,6 @@ uint64_t orc_check_div(uint64_t per_family, uint64_t seed) {
   return bad;
 }
 }  // extern "C"
+
+// The path integrator restatement shares this translation unit.
+#include "render.cpp"

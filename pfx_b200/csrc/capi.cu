@@ -335,3 +335,16 @@ int pfxt_read_accum(pfxt_trace* t, float* accum) {
 }
 
 }  // extern "C"
+
+extern "C" {
+/* The base per-pass uniform of a handle (FrameParams: size, counts, camera,
+ * sun, lens, window; 160 bytes).  Not part of the public header; the
+ * measurement and parity harness reads it to drive the oracle with the same
+ * frame. */
+int pfxt_debug_frame(const pfxt_trace* t, void* out) {
+  return guarded([&]() {
+    if (!t || !out) throw Invalid("null argument");
+    memcpy(out, &t->base, sizeof(t->base));
+  });
+}
+}  // extern "C"

@@ -1,24 +1,777 @@
-// Path-tracing passes (placeholder until the wavefront tracer lands).
+// The wavefront path tracer: Trace::sample (crates/trace/src/gpu.rs:2942) as a
+// sequence of kernels over path queues instead of the reference's megakernel
+// main() (trace.wgsl:2503-2579).
+//
+// One wave traces one sample for every active pixel.  Per bounce:
+//   extend   closest hit of every queued path (persistent traversal kernel)
+//   shade    the body of radiance()'s bounce loop (trace.wgsl:2169-2500):
+//            emission, light selection and BSDF sampling; writes up to `cap`
+//            shadow-ray slots per path, appends occlusion queries to the shadow
+//            queue and surviving paths to the next ray queue (warp-aggregated
+//            atomics, so both queues stay compact)
+//   connect  any hit of every queued shadow ray (persistent traversal kernel)
+// The light-loop contributions of a bounce are added to the path's result at
+// the start of the path's next shade (or in finish), in light-slot order, so
+// the result is summed in exactly the reference's order; with the draws of
+// the reference's random sequence kept in order, a pixel's value equals the
+// reference's bit for bit.  Waves run in sample order, so the accumulation of
+// samples into the 48 B/pixel Accum also keeps the reference's order.
+//
+// Zero-valued light-slot contributions (a black sky, a light behind the
+// surface) add nothing and trace no shadow ray; their random draws are still
+// taken.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "shade.cuh"
 #include "tracer.h"
+#include "traverse.cuh"
 
 namespace pfxt {
 
-void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
-  (void)t;
-  (void)count;
-  (void)seed;
-  throw Invalid("sampling is not built yet");
+namespace {
+
+constexpr int kThreads = 128;
+constexpr uint32_t CAP_MAX = 8u;
+
+// Path flag word (ray_d.w bits).
+constexpr uint32_t F_CARRIED = 0x3u;  // bits 0-1
+constexpr int F_LOBE0 = 2, F_LOBE1 = 9, F_LOBE2 = 16;  // 7 bits each
+constexpr uint32_t F_LAST = 1u << 23, F_THROUGH = 1u << 24, F_LIT = 1u << 25, F_DIFFUSED = 1u << 26;
+constexpr int F_PEND = 27;  // 4 bits: pending light-slot contributions
+
+struct Wave {
+  float4* ray_o;   // o.xyz, previous pdf
+  float4* ray_d;   // d.xyz, flag word
+  float4* thr;     // throughput.xyz, pcg state
+  float4* res;     // result.xyz, pixel index
+  float4* alb;     // first albedo
+  float4* nrm;     // first normal
+  float4* hit;     // t, slot, record, u
+  float* hit_v;    // v
+  float4* sh_o;    // per slot: origin.xyz, limit
+  float4* sh_d;    // per slot: direction.xyz, visible flag
+  float4* sh_c;    // per slot: contribution.xyz
+  uint32_t* queue[2];
+  uint32_t* squeue;
+  uint32_t* active;
+  uint32_t* counters;  // 0,1: ray queues, 2: shadow queue, 3: active paths, 4: work counter
+};
+
+struct Pass {
+  FrameParams f;
+  Specialise sp;
+  ShadeView v;
+  SceneView s;
+  Wave w;
+  uint32_t sample;     // sample index inside the pass
+  uint32_t bounce;
+  uint32_t cap;        // shadow slots per path
+  uint32_t deferred;   // 1: light-slot shadow rays go through the shadow queue
+  uint32_t light_rows;
+  uint32_t slots;      // 2 + light_slots()
+  uint32_t width, height;
+};
+
+__device__ __forceinline__ uint32_t lobe_count(uint32_t f, int shift) { return (f >> shift) & 127u; }
+
+__device__ __forceinline__ v3 capped(const Pass& P, v3 value, bool deep) {
+  float cap = P.sp.clamp_indirect;
+  if (!(cap > 0.0f) || !deep) return value;
+  float luma = dot3(value, mk3(0.2126f, 0.7152f, 0.0722f));
+  if (!(luma > cap)) return value;
+  return scl3(value, cap / luma);
 }
 
+// Warp-aggregated append to a queue.
+__device__ __forceinline__ void append(uint32_t* queue, uint32_t* count, uint32_t value, bool want) {
+  unsigned m = __ballot_sync(__activemask(), want);
+  if (!want) return;
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+  base = __shfl_sync(m, base, leader);
+  queue[base + (uint32_t)__popc(m & ((1u << lane) - 1u))] = value;
+}
+
+// ------------------------------------------------------------------ active
+// Pixels that still sample: the reference returns early when accum.color.w
+// is negative (trace.wgsl:2517), the mark of a converged pixel.
+__global__ void k_collect(Pass P, const Accum* __restrict__ accum) {
+  uint32_t n = P.width * P.height;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    bool live = P.f.size[2] == 0u || !(accum[i].color.w < 0.0f);
+    append(P.w.active, P.w.counters + 3, i, live);
+  }
+}
+
+// ------------------------------------------------------------------ generate
+// main() up to the call of radiance(): seeding, pixel filter, camera ray.
+__global__ void k_gen(Pass P) {
+  const uint32_t n = P.w.counters[3];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t pixel = P.w.active[i];
+    uint32_t gx = pixel % P.width, gy = pixel / P.width;
+    uint32_t px = gx + P.f.window[2], py = gy + P.f.window[3];
+    uint32_t stream = py * P.f.window[0] + px;
+    uint32_t absolute = P.f.size[2] + P.sample;
+    uint32_t state = pcg(stream * 1973u + pcg(P.f.counts[2] * 9277u + absolute * 7919u + 26699u));
+    Rng r{hash_iqnt2d(px, py) ^ P.f.counts[2], absolute, 0u};
+    float4 pf = sobol4(P.v, P.sp, r, 0u);
+    float jx = rnd(P.sp, state, pf.x);
+    float jy = rnd(P.sp, state, pf.y);
+    float ndc_x = ((float)px + jx) / (float)P.f.window[0] * 2.0f - 1.0f;
+    float ndc_y = ((float)py + jy) / (float)P.f.window[1] * 2.0f - 1.0f;
+    uint32_t kind = f2u(rint_(P.f.origin[3]));
+    v3 cam_o = mk3(P.f.origin[0], P.f.origin[1], P.f.origin[2]);
+    v3 cam_f = mk3(P.f.forward[0], P.f.forward[1], P.f.forward[2]);
+    v3 cam_r = mk3(P.f.right[0], P.f.right[1], P.f.right[2]);
+    v3 cam_u = mk3(P.f.up[0], P.f.up[1], P.f.up[2]);
+    v3 direction = normalize3(add3(add3(cam_f, scl3(cam_r, ndc_x + P.f.lens[0])), scl3(cam_u, -ndc_y + P.f.lens[1])));
+    v3 origin = cam_o;
+    if (kind == 1u) {
+      direction = normalize3(cam_f);
+      origin = add3(origin, add3(scl3(normalize3(cam_r), (ndc_x + P.f.lens[0]) * P.f.right[3]),
+                                 scl3(normalize3(cam_u), (-ndc_y + P.f.lens[1]) * P.f.up[3])));
+    } else if (kind == 2u) {
+      float phi = (ndc_x * 0.5f) * 2.0f * SH_PI;
+      float theta = (ndc_y * 0.5f + 0.5f) * SH_PI;
+      v3 local = mk3(sin_(theta) * sin_(phi), cos_(theta), -sin_(theta) * cos_(phi));
+      direction = normalize3(sub3(add3(scl3(normalize3(cam_r), local.x), scl3(normalize3(cam_u), local.y)),
+                                  scl3(normalize3(cam_f), local.z)));
+    } else if (P.f.lens[2] > 0.0f) {
+      v3 focus = add3(origin, scl3(direction, P.f.lens[3] / dot3(direction, normalize3(cam_f))));
+      float4 ap = sobol4(P.v, P.sp, r, 1u);
+      float radius = sqrtf(rnd(P.sp, state, ap.x)) * P.f.lens[2];
+      float phi = 2.0f * SH_PI * rnd(P.sp, state, ap.y);
+      origin = add3(origin, add3(scl3(normalize3(cam_r), radius * cos_(phi)), scl3(normalize3(cam_u), radius * sin_(phi))));
+      direction = normalize3(sub3(focus, origin));
+    }
+    P.w.ray_o[i] = make_float4(origin.x, origin.y, origin.z, 0.0f);
+    P.w.ray_d[i] = make_float4(direction.x, direction.y, direction.z, __uint_as_float(3u));  // carried = 3
+    P.w.thr[i] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(state));
+    P.w.res[i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(pixel));
+    P.w.alb[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    P.w.nrm[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    P.w.queue[0][i] = i;
+  }
+}
+
+__global__ void k_seed_counts(Pass P) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    P.w.counters[0] = P.w.counters[3];
+    P.w.counters[1] = 0u;
+    P.w.counters[2] = 0u;
+  }
+}
+
+// Before a bounce: empty the next ray queue and the shadow queue, rewind the
+// work counter of the extend kernel.
+__global__ void k_reset(Pass P, uint32_t cur) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    P.w.counters[cur ^ 1u] = 0u;
+    P.w.counters[2] = 0u;
+    P.w.counters[4] = 0u;
+  }
+}
+__global__ void k_rewind(Pass P) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) P.w.counters[4] = 0u;
+}
+
+// ------------------------------------------------------------------ extend
+template <bool ANY>
+__global__ void __launch_bounds__(kThreads) k_trace_queue(Pass P, uint32_t which) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const uint32_t* queue = ANY ? P.w.squeue : P.w.queue[which];
+  const uint32_t n = ANY ? P.w.counters[2] : P.w.counters[which];
+  uint32_t* counter = P.w.counters + 4;
+  uint32_t sref[REF_STACK];
+  float snear[REF_STACK];
+  Walker<ANY, false> w;
+  const int lane = threadIdx.x & 31;
+  uint32_t idx = 0, item = 0;
+  bool have = false, retired = false;
+  for (;;) {
+    bool need = !have && !retired;
+    unsigned m = __ballot_sync(FULL, need);
+    if (m) {
+      int leader = __ffs(m) - 1;
+      uint32_t first = 0;
+      if (lane == leader) first = atomicAdd(counter, (uint32_t)__popc(m));
+      first = __shfl_sync(FULL, first, leader);
+      if (need) {
+        idx = first + (uint32_t)__popc(m & ((1u << lane) - 1u));
+        if (idx < n) {
+          item = queue[idx];
+          float4 a = ANY ? P.w.sh_o[item] : P.w.ray_o[item];
+          float4 b = ANY ? P.w.sh_d[item] : P.w.ray_d[item];
+          w.start(P.s, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), ANY ? a.w : 1e20f);
+          have = true;
+        } else {
+          retired = true;
+        }
+      }
+    }
+    if (__all_sync(FULL, retired)) break;
+    if (have) {
+      w.inner_phase(P.s, sref, snear);
+      if (!w.done) w.leaf_phase(P.s, sref, snear);
+      if (w.done) {
+        if (ANY) {
+          reinterpret_cast<float*>(P.w.sh_d + item)[3] = __uint_as_float(w.hit.hit ? 0u : 1u);
+        } else {
+          P.w.hit[item] = make_float4(w.hit.t, __uint_as_float(w.hit.slot), __uint_as_float(w.hit.record), w.hit.u);
+          P.w.hit_v[item] = w.hit.v;
+        }
+        have = false;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ shade
+struct HitInfo {
+  float t;
+  v3 n, geometric;
+  uint32_t material, surface, record;
+};
+
+// tri_fill (trace.wgsl:754-779) + world_hit (:682-694) from the stored hit.
+__device__ __forceinline__ HitInfo fill_hit(const Pass& P, float4 h, float hv) {
+  HitInfo out;
+  out.t = h.x;
+  out.surface = __float_as_uint(h.y);
+  out.record = __float_as_uint(h.z);
+  float u = h.w, v = hv;
+  const float4* tp = reinterpret_cast<const float4*>(P.v.triangles + out.surface);
+  float4 ta = __ldg(tp), tb = __ldg(tp + 1), tc = __ldg(tp + 2), na = __ldg(tp + 3), nb = __ldg(tp + 4),
+         nc = __ldg(tp + 5);
+  v3 a = f3of(ta);
+  v3 e1 = sub3(f3of(tb), a);
+  v3 e2 = sub3(f3of(tc), a);
+  v3 geometric = normalize3(cross3(e1, e2));
+  v3 shaded = add3(add3(scl3(f3of(na), 1.0f - u - v), scl3(f3of(nb), u)), scl3(f3of(nc), v));
+  v3 fallback = out.record > 0u ? splat3(0.0f) : geometric;
+  v3 n = dot3(shaded, shaded) > 1e-12f ? normalize3(shaded) : fallback;
+  const float4* sp = reinterpret_cast<const float4*>(P.v.surfaces + out.record);
+  uint4 info = __ldg(reinterpret_cast<const uint4*>(sp + 4));
+  out.material = info.y == NO_MATERIAL ? f2u(ta.w) : info.y;
+  if (out.record == 0u) {
+    out.n = n;
+    out.geometric = geometric;
+    return out;
+  }
+  float mirror = __uint_as_float(info.w) < 0.0f ? -1.0f : 1.0f;
+  v3 i0 = f3of(__ldg(sp + 8)), i1 = f3of(__ldg(sp + 9)), i2 = f3of(__ldg(sp + 10));
+  v3 wg = scl3(normalize3(add3(add3(scl3(i0, geometric.x), scl3(i1, geometric.y)), scl3(i2, geometric.z))), mirror);
+  v3 sh = add3(add3(scl3(i0, n.x), scl3(i1, n.y)), scl3(i2, n.z));
+  bool zero = n.x == 0.0f && n.y == 0.0f && n.z == 0.0f;
+  out.n = zero ? wg : normalize3(sh);
+  out.geometric = wg;
+  return out;
+}
+
+__device__ __forceinline__ float emitter_weight(const Pass& P, const HitInfo& hit, v3 p, v3 previous_point,
+                                                float previous_pdf) {
+  float4 em = __ldg(P.v.materials + (size_t)(hit.material + 1u) * 8u + 5u);
+  if (previous_pdf <= 0.0f || (em.x <= 0.0f && em.y <= 0.0f && em.z <= 0.0f)) return 1.0f;
+  uint32_t index = f2u(__ldg(reinterpret_cast<const float*>(P.v.triangles + hit.surface) + 11));
+  if (index == 0u) return 1.0f;
+  return mis_power(previous_pdf, emitter_pdf(load_emitter(P.v, index), p, previous_point, hit.geometric));
+}
+
+// Adds the pending light-slot contributions of path i (previous bounce) in
+// slot order.
+__device__ __forceinline__ v3 flush_pending(const Pass& P, uint32_t i, uint32_t flags, v3 result) {
+  uint32_t pending = (flags >> F_PEND) & 15u;
+  for (uint32_t j = 0; j < pending; ++j) {
+    uint32_t slot = i * P.cap + j;
+    float vis = reinterpret_cast<const float*>(P.w.sh_d + slot)[3];
+    if (__float_as_uint(vis) != 0u) result = add3(result, f3of(P.w.sh_c[slot]));
+  }
+  return result;
+}
+
+__global__ void __launch_bounds__(kThreads) k_shade(Pass P, uint32_t which) {
+  const uint32_t n = P.w.counters[which];
+  const uint32_t* queue = P.w.queue[which];
+  uint32_t* next_queue = P.w.queue[which ^ 1u];
+  uint32_t* next_count = P.w.counters + (which ^ 1u);
+  const uint32_t bounce = P.bounce;
+  const Specialise& sp = P.sp;
+  const ShadeView& V = P.v;
+  const uint32_t TOTAL = sp.total_bounces;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    uint32_t qi = base + threadIdx.x;
+    bool active = qi < n;
+    bool cont = false;
+    uint32_t i = active ? queue[qi] : 0u;
+    if (active) {
+      float4 ro = P.w.ray_o[i], rd = P.w.ray_d[i], th = P.w.thr[i], rs = P.w.res[i];
+      v3 o = mk3(ro.x, ro.y, ro.z), d = mk3(rd.x, rd.y, rd.z);
+      float previous_pdf = ro.w;
+      uint32_t flags = __float_as_uint(rd.w);
+      v3 throughput = mk3(th.x, th.y, th.z);
+      uint32_t state = __float_as_uint(th.w);
+      v3 result = flush_pending(P, i, flags, mk3(rs.x, rs.y, rs.z));
+      flags &= ~(15u << F_PEND);
+      uint32_t pixel = __float_as_uint(rs.w);
+      uint32_t px = pixel % P.width + P.f.window[2], py = pixel / P.width + P.f.window[3];
+      Rng r{hash_iqnt2d(px, py) ^ P.f.counts[2], P.f.size[2] + P.sample, 16u * (bounce + 1u)};
+      float4 h = P.w.hit[i];
+      float reach = h.x;
+      v3 origin_point = spawn_point(o, neg3(d), o, 0.0f);
+      result = add3(result, capped(P, mul3(throughput, light_hits(V, o, d, reach, origin_point, previous_pdf)),
+                                   bounce > 1u));
+      uint32_t pending = 0u;
+      if (h.x >= 1e19f) {
+        if (!(bounce == 0u && P.f.forward[3] > 0.0f)) {
+          float pdf = sky_pdf(V, d);
+          float weight = (bounce > 0u && previous_pdf > 0.0f) ? previous_pdf / (previous_pdf + pdf) : 1.0f;
+          result = add3(result, capped(P, scl3(mul3(throughput, sky_radiance(V)), weight), bounce > 1u));
+        }
+      } else {
+        HitInfo hit = fill_hit(P, h, P.w.hit_v[i]);
+        v3 p = add3(o, scl3(d, hit.t));
+        v3 nn = dot3(hit.n, d) > 0.0f ? neg3(hit.n) : hit.n;
+        Shaded s = load_surface(V, hit.material);
+        v3 geometric = dot3(hit.geometric, d) > 0.0f ? neg3(hit.geometric) : hit.geometric;
+        if (dot3(nn, geometric) < 0.05f) nn = normalize3(add3(nn, scl3(geometric, 0.1f)));
+        s.roughness = fmax_(s.roughness, 0.05f);
+        s.clearcoat_roughness = fmax_(s.clearcoat_roughness, 0.05f);
+        if (sp.filter_glossy > 0.0f && (flags & F_DIFFUSED)) {
+          s.roughness = fmax_(s.roughness, sp.filter_glossy);
+          s.clearcoat_roughness = fmax_(s.clearcoat_roughness, sp.filter_glossy);
+        }
+        if (bounce == 0u) {
+          P.w.alb[i] = make_float4(s.base.x, s.base.y, s.base.z, 1.0f);
+          P.w.nrm[i] = make_float4(nn.x, nn.y, nn.z, 1.0f);
+        }
+        s.emission = scl3(s.emission, emitter_weight(P, hit, p, origin_point, previous_pdf));
+        result = add3(result, capped(P, mul3(throughput, s.emission), bounce > 1u));
+        if (!(flags & F_LAST)) {
+          m3 transform = basis(nn);
+          v3 wo = mulmtv(transform, neg3(d));
+          v3 origin = spawn_point(p, nn, o, hit.t);
+          bool entering = dot3(hit.n, d) < 0.0f;
+          for (uint32_t k = 0u; k < P.slots; ++k) {
+            float4 u = sobol4(V, sp, r, light_dim(k));
+            v3 local = mk3(0.0f, 0.0f, 1.0f), direction = mk3(0.0f, 0.0f, 1.0f), strength = splat3(0.0f);
+            float limit = 1e19f, pdf = 0.0f;
+            float lit_roughness = s.roughness;
+            if (k == 0u) {
+              if (P.f.sun_color[3] <= 0.0f) continue;
+              direction = normalize3(mk3(P.f.sun_dir[0], P.f.sun_dir[1], P.f.sun_dir[2]));
+              if (P.f.sun_dir[3] < 1.0f) {
+                float height = 1.0f - rnd(sp, state, u.x) * (1.0f - P.f.sun_dir[3]);
+                float radius = sqrtf(fmax_(0.0f, 1.0f - height * height));
+                float phi = 2.0f * SH_PI * rnd(sp, state, u.y);
+                m3 orient = basis(direction);
+                direction = normalize3(mulmv(orient, mk3(radius * cos_(phi), radius * sin_(phi), height)));
+              }
+              local = mulmtv(transform, direction);
+              if (local.z <= 0.0f) continue;
+              strength = scl3(mk3(P.f.sun_color[0], P.f.sun_color[1], P.f.sun_color[2]), P.f.sun_color[3] * 1.0f);
+            } else if (k == 1u) {
+              if (V.sky_width == 0u) continue;
+              float ux = rnd(sp, state, u.x);
+              float uy = rnd(sp, state, u.y);
+              SkySample light = sky_sample(V, ux, uy);
+              direction = light.direction;
+              local = mulmtv(transform, direction);
+              if (local.z <= 0.0f) continue;
+              strength = scl3(sky_radiance(V), 1.0f);
+              pdf = light.pdf;
+              if (!(pdf > 0.0f)) continue;
+            } else {
+              uint32_t slot = k - 2u;
+              Candidate picked;
+              if (slot > V.looped) {
+                float2 pk = tree_pick(V, P.light_rows, p, transform.c2, rnd(sp, state, u.z), nullptr);
+                if (!(pk.y > 0.0f)) {
+                  picked = candidate_none();
+                } else {
+                  picked = light_candidate(sp, load_light(V, f2u(pk.x)), transform, p, origin, geometric, state, u);
+                  picked.scale = divs3(picked.scale, pk.y);
+                }
+              } else if (slot > 0u) {
+                picked = light_candidate(sp, load_light(V, slot - 1u), transform, p, origin, geometric, state, u);
+              } else if (V.emitter_count == 0u) {
+                picked = candidate_none();
+              } else {
+                picked = emitter_candidate(V, sp, transform, p, origin, state, u);
+              }
+              if (picked.limit < 0.0f) continue;
+              local = picked.wi;
+              direction = picked.direction;
+              strength = picked.scale;
+              pdf = picked.pdf;
+              limit = picked.limit;
+              lit_roughness = fmax_(s.roughness, picked.roughness);
+            }
+            if (pdf > 0.0f) {
+              float bsdf = bsdf_pdf(s, wo, local);
+              if (k == 1u) {
+                strength = divs3(strength, pdf + bsdf);
+              } else {
+                float ratio = bsdf / pdf;
+                strength = divs3(strength, pdf * (1.0f + ratio * ratio));
+              }
+            }
+            Shaded lit = s;
+            lit.roughness = lit_roughness;
+            v3 term = mul3(scl3(scl3(mul3(throughput, bsdf_eval(lit, wo, local)), pdf > 0.0f ? glossy_share(s) : 1.0f),
+                                local.z),
+                           strength);
+            term = capped(P, term, bounce > 0u);
+            if (term.x == 0.0f && term.y == 0.0f && term.z == 0.0f) continue;  // adds nothing, traces nothing
+            if (!P.deferred) {
+              if (limit > 0.0f && traverse<true>(P.s, origin, direction, limit).hit) continue;
+              result = add3(result, term);
+              continue;
+            }
+            uint32_t slot_index = i * P.cap + pending;
+            P.w.sh_c[slot_index] = make_float4(term.x, term.y, term.z, 0.0f);
+            P.w.sh_o[slot_index] = make_float4(origin.x, origin.y, origin.z, limit);
+            P.w.sh_d[slot_index] = make_float4(direction.x, direction.y, direction.z, __uint_as_float(limit > 0.0f ? 0u : 1u));
+            if (limit > 0.0f) {
+              uint32_t at = atomicAdd(P.w.counters + 2, 1u);
+              P.w.squeue[at] = slot_index;
+            }
+            pending += 1u;
+          }
+          // BSDF sampling and the next ray (trace.wgsl:2472-2500)
+          uint32_t carried = flags & F_CARRIED;
+          BsdfSample sample = sample_bsdf(sp, s, wo, entering, carried, state, sobol4(V, sp, r, 3u));
+          v3 wi = sample.dir;
+          uint32_t l0 = lobe_count(flags, F_LOBE0) + (sample.lobe == 0u ? 1u : 0u);
+          uint32_t l1 = lobe_count(flags, F_LOBE1) + (sample.lobe == 1u ? 1u : 0u);
+          uint32_t l2 = lobe_count(flags, F_LOBE2) + (sample.lobe == 2u ? 1u : 0u);
+          bool diffused = (flags & F_DIFFUSED) || sample.lobe == 0u;
+          bool last = bounce >= TOTAL || l0 > sp.diffuse_bounces || l1 > sp.glossy_bounces || l2 > sp.transmission_bounces;
+          bool lit_vertex = (flags & F_LIT) != 0u;
+          bool through = sample.pdf < -1.5f && lit_vertex;
+          lit_vertex = sample.pdf > 0.0f || through;
+          bool go = true;
+          if (sample.pdf < 0.0f) {
+            throughput = mul3(throughput, sample.weight);
+            carried = sample.channel;
+            if (sample.pdf < -1.5f)
+              throughput = mul3(throughput, mul3(mk3(sqrtf(clamp_(s.base.x, 0.0f, 1.0f)), sqrtf(clamp_(s.base.y, 0.0f, 1.0f)),
+                                                     sqrtf(clamp_(s.base.z, 0.0f, 1.0f))),
+                                                 beer(s.thickness, s.subsurface_tint, s.absorption)));
+            d = normalize3(mulmv(transform, wi));
+            previous_pdf = 0.0f;
+          } else if (wi.z <= 0.0f || sample.pdf <= 0.0f) {
+            go = false;
+          } else {
+            throughput = mul3(throughput, scl3(divs3(scl3(scl3(bsdf_eval(s, wo, wi), glossy_share(s)), wi.z), sample.pdf), 1.0f));
+            d = normalize3(mulmv(transform, wi));
+            previous_pdf = sample.pdf;
+          }
+          if (go) {
+            o = spawn_point(p, d, o, hit.t);
+            if (bounce >= 3u) {
+              float keep = clamp_(fmax_(throughput.x, fmax_(throughput.y, throughput.z)), 0.05f, 0.95f);
+              Rng r0 = r;
+              if (rnd(sp, state, sobol4(V, sp, r0, 0u).x) > keep)
+                go = false;
+              else
+                throughput = divs3(throughput, keep);
+            }
+          }
+          flags = (carried & F_CARRIED) | (l0 << F_LOBE0) | (l1 << F_LOBE1) | (l2 << F_LOBE2) | (last ? F_LAST : 0u) |
+                  (through ? F_THROUGH : 0u) | (lit_vertex ? F_LIT : 0u) | (diffused ? F_DIFFUSED : 0u);
+          cont = go;
+        }
+      }
+      flags |= pending << F_PEND;
+      P.w.ray_o[i] = make_float4(o.x, o.y, o.z, previous_pdf);
+      P.w.ray_d[i] = make_float4(d.x, d.y, d.z, __uint_as_float(flags));
+      P.w.thr[i] = make_float4(throughput.x, throughput.y, throughput.z, __uint_as_float(state));
+      P.w.res[i] = make_float4(result.x, result.y, result.z, __uint_as_float(pixel));
+    }
+    append(next_queue, next_count, i, active && cont);
+  }
+}
+
+// ------------------------------------------------------------------ finish
+// Pending contributions of the last bounce, then Accum += (result, first
+// albedo, first normal) in sample order (trace.wgsl:2564-2567).
+__global__ void k_finish(Pass P, Accum* __restrict__ accum) {
+  const uint32_t n = P.w.counters[3];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 rs = P.w.res[i];
+    uint32_t flags = __float_as_uint(P.w.ray_d[i].w);
+    v3 result = flush_pending(P, i, flags, mk3(rs.x, rs.y, rs.z));
+    uint32_t pixel = __float_as_uint(rs.w);
+    Accum a = accum[pixel];
+    float4 al = P.w.alb[i], nr = P.w.nrm[i];
+    a.color.x = a.color.x + result.x;
+    a.color.y = a.color.y + result.y;
+    a.color.z = a.color.z + result.z;
+    a.albedo = make_float4(a.albedo.x + al.x, a.albedo.y + al.y, a.albedo.z + al.z, a.albedo.w + al.w);
+    a.normal = make_float4(a.normal.x + nr.x, a.normal.y + nr.y, a.normal.z + nr.z, a.normal.w + nr.w);
+    accum[pixel] = a;
+  }
+}
+
+// Films (trace.wgsl:2568-2578) for the pixels of this pass.
+__global__ void k_films(Pass P, Accum* __restrict__ accum, float4* color, float4* albedo, float4* normal) {
+  const uint32_t n = P.w.counters[3];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t pixel = P.w.active[i];
+    Accum a = accum[pixel];
+    a.color.w = (float)(P.f.size[2] + P.f.size[3]);
+    accum[pixel] = a;
+    float count = fmax_(a.color.w, 1.0f);
+    v3 nn = divs3(mk3(a.normal.x, a.normal.y, a.normal.z), count);
+    color[pixel] = make_float4(a.color.x / count, a.color.y / count, a.color.z / count,
+                               P.f.forward[3] > 0.0f ? a.albedo.w / count : 1.0f);
+    albedo[pixel] = make_float4(a.albedo.x / count, a.albedo.y / count, a.albedo.z / count, a.albedo.w / count);
+    v3 nv = length3(nn) > 1e-6f ? normalize3(nn) : splat3(0.0f);
+    normal[pixel] = make_float4(nv.x, nv.y, nv.z, a.normal.w / count);
+  }
+}
+
+// ------------------------------------------------------------------ host
+void check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  cudaGetLastError();
+  if (e == cudaErrorMemoryAllocation) throw Refused(std::string(what) + ": out of device memory");
+  throw DeviceError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int grid_for(const void* kernel, int threads) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
+  return sms * (per > 0 ? per : 1);
+}
+
+struct Grids {
+  int trace_closest = 0, trace_any = 0, shade = 0, flat = 0;
+};
+Grids& grids() {
+  static Grids g;
+  if (g.shade == 0) {
+    g.trace_closest = grid_for((const void*)k_trace_queue<false>, kThreads);
+    g.trace_any = grid_for((const void*)k_trace_queue<true>, kThreads);
+    g.shade = grid_for((const void*)k_shade, kThreads);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    g.flat = sms * 8;
+  }
+  return g;
+}
+
+// Path-state buffers for `capacity` paths and `cap` slots per path.
+void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
+  size_t need = 0;
+  auto add = [&](size_t bytes) {
+    size_t at = (need + 255) & ~size_t(255);
+    need = at + bytes;
+    return at;
+  };
+  size_t o_ray_o = add(16ull * capacity), o_ray_d = add(16ull * capacity), o_thr = add(16ull * capacity),
+         o_res = add(16ull * capacity), o_alb = add(16ull * capacity), o_nrm = add(16ull * capacity),
+         o_hit = add(16ull * capacity), o_hitv = add(4ull * capacity), o_sho = add(16ull * capacity * cap),
+         o_shd = add(16ull * capacity * cap), o_shc = add(16ull * capacity * cap), o_q0 = add(4ull * capacity),
+         o_q1 = add(4ull * capacity), o_sq = add(4ull * capacity * cap), o_act = add(4ull * capacity),
+         o_cnt = add(64);
+  if (need > t.wave_bytes) {
+    if (t.d_wave) cudaFree(t.d_wave);
+    t.d_wave = nullptr;
+    t.wave_bytes = 0;
+    check(cudaMalloc(&t.d_wave, need), "wavefront path state");
+    t.wave_bytes = need;
+  }
+  t.wave_capacity = capacity;
+  char* b = static_cast<char*>(t.d_wave);
+  Wave& w = *reinterpret_cast<Wave*>(&t.wave_layout);
+  w.ray_o = reinterpret_cast<float4*>(b + o_ray_o);
+  w.ray_d = reinterpret_cast<float4*>(b + o_ray_d);
+  w.thr = reinterpret_cast<float4*>(b + o_thr);
+  w.res = reinterpret_cast<float4*>(b + o_res);
+  w.alb = reinterpret_cast<float4*>(b + o_alb);
+  w.nrm = reinterpret_cast<float4*>(b + o_nrm);
+  w.hit = reinterpret_cast<float4*>(b + o_hit);
+  w.hit_v = reinterpret_cast<float*>(b + o_hitv);
+  w.sh_o = reinterpret_cast<float4*>(b + o_sho);
+  w.sh_d = reinterpret_cast<float4*>(b + o_shd);
+  w.sh_c = reinterpret_cast<float4*>(b + o_shc);
+  w.queue[0] = reinterpret_cast<uint32_t*>(b + o_q0);
+  w.queue[1] = reinterpret_cast<uint32_t*>(b + o_q1);
+  w.squeue = reinterpret_cast<uint32_t*>(b + o_sq);
+  w.active = reinterpret_cast<uint32_t*>(b + o_act);
+  w.counters = reinterpret_cast<uint32_t*>(b + o_cnt);
+}
+
+}  // namespace
+
+static_assert(sizeof(Wave) <= sizeof(((pfxt_trace*)nullptr)->wave_layout), "wave layout storage");
+
+void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
+  if (count == 0) return;
+  uint32_t pixels = t.width * t.height;
+  uint32_t light_slots = 1u + t.shade.looped + (t.shade.tree > 0u ? 1u : 0u);
+  uint32_t slots = 2u + light_slots;
+  uint32_t cap = std::min(slots, CAP_MAX);
+  bool deferred = slots <= CAP_MAX;
+  ensure_wave(t, pixels, cap);
+  Pass P;
+  memset(&P, 0, sizeof(P));
+  P.f = t.base;
+  P.f.size[2] = t.samples;
+  P.f.size[3] = count;
+  P.f.counts[2] = seed;
+  P.sp = t.spec;
+  P.v = t.shade;
+  P.s = t.view;
+  P.w = *reinterpret_cast<Wave*>(&t.wave_layout);
+  P.cap = cap;
+  P.deferred = deferred ? 1u : 0u;
+  P.light_rows = t.light_rows;
+  P.slots = slots;
+  P.width = t.width;
+  P.height = t.height;
+  Grids& g = grids();
+  cudaStream_t st = t.stream;
+  if (t.samples == 0) check(cudaMemsetAsync(t.d_accum, 0, (size_t)pixels * sizeof(Accum), st), "accumulation reset");
+  check(cudaMemsetAsync(P.w.counters, 0, 64, st), "counters");
+  k_collect<<<g.flat, 256, 0, st>>>(P, t.d_accum);
+  for (uint32_t sample = 0; sample < count; ++sample) {
+    P.sample = sample;
+    k_gen<<<g.flat, 256, 0, st>>>(P);
+    k_seed_counts<<<1, 32, 0, st>>>(P);
+    for (uint32_t bounce = 0; bounce <= t.spec.total_bounces + 1u; ++bounce) {
+      uint32_t cur = bounce & 1u;
+      P.bounce = bounce;
+      k_reset<<<1, 32, 0, st>>>(P, cur);
+      k_trace_queue<false><<<g.trace_closest, kThreads, 0, st>>>(P, cur);
+      k_shade<<<g.shade, kThreads, 0, st>>>(P, cur);
+      if (deferred) {
+        k_rewind<<<1, 32, 0, st>>>(P);
+        k_trace_queue<true><<<g.trace_any, kThreads, 0, st>>>(P, 0u);
+      }
+    }
+    k_finish<<<g.flat, 256, 0, st>>>(P, t.d_accum);
+  }
+  k_films<<<g.flat, 256, 0, st>>>(P, t.d_accum, t.d_color, t.d_albedo, t.d_normal);
+  check(cudaGetLastError(), "tracer launch");
+  check(cudaStreamSynchronize(st), "tracer pass");
+  t.samples += count;
+}
+
+namespace {
+
+// measure (converge.wgsl:9-30): the half-buffer error of every pixel against
+// its snapshot of the previous round.  snaps: 2 float4 per pixel (mean, info).
+__global__ void k_measure(const Accum* __restrict__ accum, float4* __restrict__ snaps, uint32_t W, uint32_t H) {
+  uint32_t n = W * H;
+  for (uint32_t index = blockIdx.x * blockDim.x + threadIdx.x; index < n; index += gridDim.x * blockDim.x) {
+    Accum sum = accum[index];
+    float count = sum.color.w;
+    if (count <= 0.0f) {
+      snaps[2 * index + 1].y = 0.0f;
+      continue;
+    }
+    float now[4] = {sum.color.x / count, sum.color.y / count, sum.color.z / count, sum.albedo.w / count};
+    float4 mean = snaps[2 * index];
+    float prior = snaps[2 * index + 1].x;
+    float m[4] = {mean.x, mean.y, mean.z, mean.w};
+    float error = 1e9f;
+    if (prior > 0.0f && count > prior) {
+      float scale = sqrtf(1.0f / count) / sqrtf(1.0f / prior + 1.0f / (count - prior));
+      float gap[4];
+      for (int k = 0; k < 4; ++k) {
+        float rest = (now[k] * count - m[k] * prior) / (count - prior);
+        gap[k] = abs_(m[k] - rest) * scale;
+      }
+      error = (gap[0] + gap[1] + gap[2]) / (1e-4f + sqrtf(fmax_(now[0] + now[1] + now[2], 0.0f))) + gap[3];
+    }
+    snaps[2 * index] = make_float4(now[0], now[1], now[2], now[3]);
+    snaps[2 * index + 1] = make_float4(count, error, 0.0f, 0.0f);
+  }
+}
+
+// mark (converge.wgsl:32-51): stop a pixel whose 3x3 neighbourhood error is
+// under the threshold once it has min_samples; count the pixels still running
+// (warp-aggregated into one atomic per warp).
+__global__ void k_mark(Accum* __restrict__ accum, const float4* __restrict__ snaps, uint32_t W, uint32_t H,
+                       uint32_t min_samples, float threshold, uint32_t* running) {
+  uint32_t n = W * H;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    uint32_t index = base + threadIdx.x;
+    bool run = false;
+    if (index < n) {
+      float count = accum[index].color.w;
+      if (count > 0.0f) {
+        int gx = (int)(index % W), gy = (int)(index / W);
+        float worst = 0.0f;
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            int x = min(max(gx + dx, 0), (int)W - 1);
+            int y = min(max(gy + dy, 0), (int)H - 1);
+            worst = fmax_(worst, __ldg(&snaps[2 * ((uint32_t)y * W + (uint32_t)x) + 1].y));
+          }
+        if (count >= (float)min_samples && worst < threshold)
+          accum[index].color.w = -count;
+        else
+          run = true;
+      }
+    }
+    unsigned m = __ballot_sync(0xffffffffu, run);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(running, (uint32_t)__popc(m));
+  }
+}
+
+}  // namespace
+
+// Trace::sample_adaptive_kept without a keeper (adaptive.rs:136-325).
 void trace_sample_adaptive(pfxt_trace& t, const pfxt_adaptive& a, uint32_t seed, pfxt_round* rounds, uint32_t cap,
                            uint32_t* written) {
-  (void)t;
-  (void)a;
-  (void)seed;
-  (void)rounds;
-  (void)cap;
-  (void)written;
-  throw Invalid("sampling is not built yet");
+  bool valid = std::isfinite(a.threshold) && a.threshold > 0.0f && a.min_samples >= 2u &&
+               a.max_samples >= a.min_samples && std::isfinite(a.growth) && a.growth > 1.0f;
+  if (!valid)
+    throw Invalid("adaptive sampling needs a positive threshold, a growth over 1 and at least 2 samples");
+  t.samples = 0;
+  uint32_t pixels = t.width * t.height;
+  cudaStream_t st = t.stream;
+  check(cudaMemsetAsync(t.d_snaps, 0, (size_t)pixels * 32, st), "snapshots");
+  std::vector<uint32_t> targets = adaptive_rounds(a);
+  Grids& g = grids();
+  uint32_t n = 0;
+  for (size_t step = 0; step < targets.size(); ++step) {
+    uint32_t target = targets[step];
+    uint32_t count = target > t.samples ? target - t.samples : 0u;
+    trace_sample(t, count, seed);
+    check(cudaMemsetAsync(t.d_running, 0, 4, st), "running count");
+    k_measure<<<g.flat, 256, 0, st>>>(t.d_accum, t.d_snaps, t.width, t.height);
+    if (step > 0) k_mark<<<g.flat, 256, 0, st>>>(t.d_accum, t.d_snaps, t.width, t.height, a.min_samples, a.threshold,
+                                                  t.d_running);
+    uint32_t running = 0;
+    check(cudaMemcpyAsync(&running, t.d_running, 4, cudaMemcpyDeviceToHost, st), "running count");
+    check(cudaStreamSynchronize(st), "convergence");
+    uint64_t active = step > 0 ? (uint64_t)running : (uint64_t)pixels;
+    if (rounds && n < cap) {
+      rounds[n].samples = target;
+      rounds[n].pad = 0;
+      rounds[n].active = active;
+    }
+    ++n;
+    if (active == 0) break;
+  }
+  *written = std::min(n, cap);
 }
 
 }  // namespace pfxt

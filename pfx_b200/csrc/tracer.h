@@ -106,6 +106,8 @@ struct pfxt_trace {
   void* d_wave = nullptr;
   size_t wave_bytes = 0;
   uint32_t wave_capacity = 0;
+  alignas(16) unsigned char wave_layout[256];  // pointers into d_wave (tracer.cu)
+  uint32_t light_rows = 0;                     // rows of the light buffer (lights + tree)
   uint32_t* d_error = nullptr;  // device error word
   uint32_t* d_counters = nullptr;  // ring of work-sharing counters (device scratch)
   uint32_t counter_slot = 0;

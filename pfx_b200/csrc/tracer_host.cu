@@ -101,6 +101,54 @@ void trace_init(pfxt_trace& t, const pfxt_buffers& b, const pfxt_scene& view, co
   v.emitter_count = f2u(head->a[0]);
   v.looped = f2u(head->a[1]);
   v.tree = f2u(head->a[3]);
+  t.light_rows = (uint32_t)(b.lights_bytes / sizeof(GpuLight));
+  if (v.looped > t.light_rows || (v.tree > 0u && v.looped + v.tree >= t.light_rows))
+    throw Invalid("the emitter header does not match the light rows");
+  // Every index a shading kernel reads must stay inside its buffer.
+  {
+    uint32_t emitter_rows = (uint32_t)(b.emitters_bytes / sizeof(GpuEmitter));
+    if (v.emitter_count + 1u > emitter_rows || b.emitter_cdf_bytes / 4 < v.emitter_count)
+      throw Invalid("the emitter list is shorter than its header");
+    uint32_t surfaces = (uint32_t)(b.surfaces_bytes / sizeof(GpuSurface));
+    const GpuSurface* sf = static_cast<const GpuSurface*>(b.surfaces);
+    for (uint32_t r = 0; r < surfaces; ++r)
+      if (sf[r].info[1] != NO_MATERIAL && sf[r].info[1] >= v.material_count)
+        throw Invalid("an instance record names a missing material");
+    const GpuTriangle* tr = static_cast<const GpuTriangle*>(b.triangles);
+    size_t tris = b.triangles_bytes / sizeof(GpuTriangle);
+    for (size_t i = 0; i < tris; ++i) {
+      if (!(tr[i].a[3] >= 0.0f) || f2u(tr[i].a[3]) >= v.material_count)
+        throw Invalid("a triangle names a missing material");
+      if (!(tr[i].c[3] >= 0.0f) || f2u(tr[i].c[3]) > v.emitter_count)
+        throw Invalid("a triangle names a missing emitter");
+    }
+    const GpuEmitter* em = static_cast<const GpuEmitter*>(b.emitters);
+    for (uint32_t e = 1; e <= v.emitter_count; ++e)
+      if (f2u(em[e].b[3]) >= surfaces) throw Invalid("an emitter names a missing instance record");
+    const GpuLight* lr = static_cast<const GpuLight*>(b.lights);
+    uint32_t lights_end = v.looped + v.tree;
+    if (v.tree > 0u) {
+      for (uint32_t r = lights_end; r < t.light_rows; ++r) {
+        uint32_t count = f2u(lr[r].d[1]), link = f2u(lr[r].d[2]);
+        if (count > 0u) {
+          if (count > 32u || link < v.looped || link + count > lights_end) throw Invalid("a light-tree leaf is malformed");
+        } else if (link >= t.light_rows || r + 1u >= t.light_rows) {
+          throw Invalid("a light-tree link is out of range");
+        } else {
+          // a child row with count 1 names its light directly (child_importance)
+          const uint32_t kids[2] = {r + 1u, link};
+          for (uint32_t k : kids)
+            if (f2u(lr[k].d[1]) == 1u && f2u(lr[k].d[2]) >= lights_end) throw Invalid("a light-tree leaf is malformed");
+        }
+      }
+    }
+  }
+  for (uint32_t m = 0; m < v.material_count; ++m) {
+    const GpuHot& h = static_cast<const GpuHot*>(b.materials)[m + 1];
+    if (h.thick_sub_film[2] > 0.0f && h.emission_film[3] > 0.0f)
+      throw Invalid("thin-film materials are outside this tracer's scope");
+    if (f2bits(h.extension[1]) != 0u) throw Invalid("material extension rows are outside this tracer's scope");
+  }
 
   // ---- films: 48 B accumulation + three RGBA32F films per pixel
   size_t pixels = (size_t)width * height;

@@ -45,6 +45,7 @@ struct TraceHit {
   uint32_t slot;
   uint32_t record;
   uint32_t hit;
+  float u, v;  // barycentrics of the closest hit (tri_fill's u, v)
 };
 
 // Box and triangle tests one query did, counted as the reference counts them.
@@ -134,6 +135,7 @@ struct Walker {
     done = (s.root == REF_NONE);
     hit.t = lim;
     hit.slot = hit.record = hit.hit = 0u;
+    hit.u = hit.v = 0.0f;
     counts.boxes = counts.tris = 0u;
   }
 
@@ -218,10 +220,11 @@ struct Walker {
   __device__ __forceinline__ void leaf_phase(const SceneView& s, uint32_t* sref, float* snear) {
     uint32_t first = ref & LEAF_FIRST_MASK;
     uint32_t n = ((ref >> LEAF_FIRST_BITS) & 15u) + 1u;
-    if (COUNT) counts.tris += n;
     bool skip = ANY ? ((word & CASTS_NO_SHADOW) != 0u) : ((word & SHADOW_ONLY) != 0u);
+    if (COUNT && skip) counts.tris += n;
     if (!skip) {
       for (uint32_t j = 0; j < n; ++j) {
+        if (COUNT) counts.tris += 1u;  // the reference stops counting at an any-hit blocker
         uint32_t i = base + first + j;
         const float4* tp = reinterpret_cast<const float4*>(s.tris + i);
         float4 ta = __ldg(tp + 0), te1 = __ldg(tp + 1), te2 = __ldg(tp + 2);
@@ -252,6 +255,8 @@ struct Walker {
           hit.slot = i;
           hit.record = record;
           hit.hit = 1u;
+          hit.u = u;
+          hit.v = v;
         }
       }
     }

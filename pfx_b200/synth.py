@@ -414,3 +414,30 @@ def random_rays(lo, hi, n: int, rng, tmax: float = 1e20) -> np.ndarray:
 
 
 WORKLOADS = {"plain_512": plain_512, "instanced_1080": instanced_1080, "room_4k": room_4k}
+
+
+def furnace() -> SceneDesc:
+    """The reference's furnace scene (crates/trace/src/gpu.rs:3787-3830): a white
+    diffuse unit sphere three units in front of the camera under a uniform white
+    sky; an icosphere stands in for the analytic ellipsoid."""
+    ico = icosphere(4, 0)
+    ico["v"] = ico["v"] + np.array([0.0, 0.0, -3.0], F32)
+    cam = Camera((0.0, 0.0, 0.0), (0.0, 0.0, -1.0), (1.0, 0.0, 0.0), (0.0, 1.0, 0.0))
+    return SceneDesc(ico, material((1.0, 1.0, 1.0), 1.0, specular=0.0), cam, sky=(1.0, 1.0, 1.0))
+
+
+def small(name: str, size=(64, 48), sampler: str = "pcg") -> Workload:
+    """A reduced-resolution copy of a workload for parity tests (same scene
+    generator, smaller film, fewer triangles where the generator allows)."""
+    if name == "plain_512":
+        w = plain_512(sampler=sampler)
+    elif name == "instanced_1080":
+        w = instanced_1080(target=20_000, sampler=sampler)
+    else:
+        w = room_4k(target=60_000, meshes_n=30, sampler=sampler)
+    w.width, w.height = size
+    cam = w.scene.camera
+    aspect = size[0] / size[1]
+    scale = aspect / (np.linalg.norm(cam.right) / np.linalg.norm(cam.up))
+    w.scene.camera = Camera(cam.origin, cam.forward, tuple(np.asarray(cam.right) * scale), cam.up)
+    return w

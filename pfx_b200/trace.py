@@ -320,6 +320,13 @@ class Trace:
     def occluded_device(self, rays_ptr: int, count: int, blocked_ptr: int, stream: int = 0) -> None:
         check(self._lib.pfxt_occluded_device(self._h, rays_ptr, count, blocked_ptr, stream))
 
+    def frame(self) -> np.ndarray:
+        """The base per-pass uniform (10 x 16 bytes: size, counts, origin, forward,
+        right, up, sun_dir, sun_color, lens, window)."""
+        out = np.zeros(40, np.uint32)
+        check(self._lib.pfxt_debug_frame(self._h, out.ctypes.data))
+        return out
+
     def counts_device(self, rays_ptr: int, count: int, any_hit: bool, counts_ptr: int, stream: int = 0) -> None:
         check(self._lib.pfxt_trace_counts_device(self._h, rays_ptr, count, 1 if any_hit else 0, counts_ptr, stream))
 

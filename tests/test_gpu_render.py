@@ -1,0 +1,100 @@
+"""The wavefront tracer against the oracle's restatement of main()/radiance():
+with the reference's random sequence reproduced (PCG and Sobol), every pixel of
+the accumulation and of the films must match within 1e-4 relative in FP32 (the
+tolerance of the parity contract); in practice the images are bit-identical.
+Also the reference's furnace and determinism pins, and adaptive sampling
+rounds against the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from pfx_b200 import synth
+from pfx_b200.trace import Adaptive, Settings, Trace
+
+pytestmark = pytest.mark.gpu
+
+RTOL, ATOL = 1e-4, 1e-6
+
+
+def assert_close(got, want, what):
+    bad = ~np.isclose(got, want, rtol=RTOL, atol=ATOL)
+    assert not bad.any(), f"{what}: {bad.sum()} of {bad.size} values differ, e.g. {got[bad][:4]} vs {want[bad][:4]}"
+    return float(np.mean(got.view(np.uint32) == want.view(np.uint32)))
+
+
+def render_both(w, spp, seeds):
+    trace = Trace(w.scene, w.settings, w.width, w.height)
+    r = oracle.Renderer(trace.scene_buffers, w.settings)
+    frame = trace.frame()
+    accum = np.zeros((w.height, w.width, 12), np.float32)
+    samples = 0
+    films = None
+    for seed in seeds:
+        trace.sample(spp, seed)
+        films = r.render(frame, accum, samples, spp, seed)
+        samples += spp
+    got = trace.read_accum()
+    out = trace.readback()
+    exact = assert_close(got, accum, "accumulation")
+    assert_close(out.color, films[0], "colour film")
+    assert_close(out.albedo, films[1], "albedo film")
+    assert_close(out.normal, films[2], "normal film")
+    assert np.isfinite(got).all()
+    assert trace.samples() == samples
+    return got, exact
+
+
+@pytest.mark.parametrize("sampler", ["pcg", "sobol"])
+def test_sphere_cloud_with_rect_lights(gpu, sampler):
+    w = synth.small("plain_512", (48, 40), sampler=sampler)
+    w.settings = Settings.deep(4, sampler=sampler, sobol_samples=16)
+    got, exact = render_both(w, 4, [0, 1])
+    assert got[..., :3].mean() > 0.0
+    assert exact > 0.99
+
+
+@pytest.mark.parametrize("sampler", ["pcg", "sobol"])
+def test_instances_and_light_tree(gpu, sampler):
+    w = synth.small("instanced_1080", (48, 32), sampler=sampler)
+    w.settings = Settings.deep(8, sampler=sampler, sobol_samples=64)
+    got, exact = render_both(w, 4, [3])
+    assert got[..., :3].mean() > 0.0
+    assert exact > 0.99
+
+
+def test_room_with_glass_and_metals(gpu):
+    w = synth.small("room_4k", (48, 32), sampler="sobol")
+    w.settings = Settings.deep(8, sampler="sobol", sobol_samples=64)
+    got, exact = render_both(w, 4, [9])
+    assert exact > 0.99
+
+
+def test_furnace_and_determinism(gpu):
+    # gpu.rs:3787-3830
+    scene = synth.furnace()
+    settings = Settings(sampler="pcg")
+    a = Trace(scene, settings, 16, 16)
+    b = Trace(scene, settings, 16, 16)
+    for p in range(32):
+        a.sample(4, 73 + p)
+        b.sample(4, 73 + p)
+    ca, cb = a.readback(), b.readback()
+    assert np.array_equal(ca.color, cb.color) and np.array_equal(ca.normal, cb.normal)
+    mid = ca.color[8, 8, :3]
+    assert np.all(np.abs(mid - 1.0) < 0.12), mid
+
+
+def test_adaptive_rounds_match_the_oracle(gpu):
+    w = synth.small("instanced_1080", (40, 30), sampler="sobol")
+    w.settings = Settings.deep(8, sampler="sobol", sobol_samples=64)
+    adaptive = Adaptive(threshold=0.05, min_samples=8, max_samples=32, growth=1.5)
+    trace = Trace(w.scene, w.settings, w.width, w.height)
+    conv = trace.sample_adaptive(adaptive, 11)
+    r = oracle.Renderer(trace.scene_buffers, w.settings)
+    rounds, accum, _ = r.sample_adaptive(trace.frame(), w.width, w.height, adaptive, 11)
+    assert [(x.samples, x.active) for x in conv.rounds] == rounds
+    got = trace.read_accum()
+    assert_close(got, accum, "adaptive accumulation")
+    counts = trace.sample_counts()
+    assert counts.max() <= adaptive.max_samples and counts.min() >= 1
+    assert 0 < conv.mean_samples() <= adaptive.max_samples
