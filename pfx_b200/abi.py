@@ -149,6 +149,8 @@ PROTOTYPES = [
 # Exported beside the header for the measurement harness.
 EXTRA = [
     ("pfxt_debug_frame", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pfxt_debug_rays", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pfxt_debug_stream", C.c_void_p, [C.c_void_p]),
     ("pfxt_trace_counts_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                            C.c_void_p]),
 ]

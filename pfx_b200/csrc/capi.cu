@@ -347,4 +347,20 @@ int pfxt_debug_frame(const pfxt_trace* t, void* out) {
     memcpy(out, &t->base, sizeof(t->base));
   });
 }
+
+/* Closest-hit and any-hit queries traced by the sampling passes of a handle
+ * so far (two u64), for the measurement harness. */
+int pfxt_debug_rays(pfxt_trace* t, uint64_t* out) {
+  return guarded([&]() {
+    if (!t || !out) throw Invalid("null argument");
+    out[0] = out[1] = 0;
+    if (!t->wave_counters) return;
+    cudaStreamSynchronize(t->stream);
+    check(cudaMemcpy(out, t->wave_counters + 8, 16, cudaMemcpyDeviceToHost), "ray counters");
+  });
+}
+
+/* The handle's CUDA stream (cudaStream_t), so a harness can record events on
+ * the stream the passes run on. */
+void* pfxt_debug_stream(pfxt_trace* t) { return t ? (void*)t->stream : nullptr; }
 }  // extern "C"

@@ -173,16 +173,21 @@ __global__ void k_seed_counts(Pass P) {
 }
 
 // Before a bounce: empty the next ray queue and the shadow queue, rewind the
-// work counter of the extend kernel.
+// work counter of the extend kernel, and count the closest-hit queries of the
+// bounce (64-bit totals at counters[8..9] closest, [10..11] any hit).
 __global__ void k_reset(Pass P, uint32_t cur) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     P.w.counters[cur ^ 1u] = 0u;
     P.w.counters[2] = 0u;
     P.w.counters[4] = 0u;
+    reinterpret_cast<unsigned long long*>(P.w.counters + 8)[0] += P.w.counters[cur];
   }
 }
 __global__ void k_rewind(Pass P) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) P.w.counters[4] = 0u;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    P.w.counters[4] = 0u;
+    reinterpret_cast<unsigned long long*>(P.w.counters + 8)[1] += P.w.counters[2];
+  }
 }
 
 // ------------------------------------------------------------------ extend
@@ -593,8 +598,10 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
     t.d_wave = nullptr;
     t.wave_bytes = 0;
     check(cudaMalloc(&t.d_wave, need), "wavefront path state");
+    check(cudaMemset(static_cast<char*>(t.d_wave) + o_cnt, 0, 64), "counters");
     t.wave_bytes = need;
   }
+  t.wave_counters = reinterpret_cast<uint32_t*>(static_cast<char*>(t.d_wave) + o_cnt);
   t.wave_capacity = capacity;
   char* b = static_cast<char*>(t.d_wave);
   Wave& w = *reinterpret_cast<Wave*>(&t.wave_layout);
@@ -647,7 +654,7 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   Grids& g = grids();
   cudaStream_t st = t.stream;
   if (t.samples == 0) check(cudaMemsetAsync(t.d_accum, 0, (size_t)pixels * sizeof(Accum), st), "accumulation reset");
-  check(cudaMemsetAsync(P.w.counters, 0, 64, st), "counters");
+  check(cudaMemsetAsync(P.w.counters, 0, 32, st), "counters");  // queues; the ray totals at [8..11] persist
   k_collect<<<g.flat, 256, 0, st>>>(P, t.d_accum);
   for (uint32_t sample = 0; sample < count; ++sample) {
     P.sample = sample;
