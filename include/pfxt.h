@@ -269,6 +269,21 @@ int pfxt_trace_rays_device(pfxt_trace* trace, const pfxt_ray* rays, uint32_t cou
 int pfxt_occluded_device(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count,
                          uint32_t* blocked, void* stream);
 
+/* Any-hit queries that allocate nothing, for callers that cannot call
+ * cudaMalloc (a host whose own allocator owns the device heap, or code that must
+ * not allocate while GPU work is in flight).  No counterpart in the reference.
+ * `rays` and `blocked` (one byte per ray, 1 = blocked) are device memory; the
+ * call enqueues on `stream` and returns.  Its scratch (the traversal work
+ * counter and the 32-bit flag words) lives in fixed device arrays sized for
+ * PFXT_NOALLOC_MAX_RAYS rays, which every GPU that loads the library holds until
+ * exit; larger batches are refused with PFXT_ERR_INVALID.  All calls share the
+ * arrays: calls whose GPU work overlaps race.  The first call on a device
+ * resolves the arrays' addresses (the handle's device must be current) and
+ * should come before any stream capture. */
+#define PFXT_NOALLOC_MAX_RAYS (1u << 20)
+int pfxt_occluded_noalloc(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count, uint8_t* blocked,
+                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif

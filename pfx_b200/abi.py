@@ -144,7 +144,9 @@ PROTOTYPES = [
     ("pfxt_occluded", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("pfxt_trace_rays_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pfxt_occluded_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("pfxt_occluded_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
 ]
+NOALLOC_MAX_RAYS = 1 << 20
 
 # Exported beside the header for the measurement harness.
 EXTRA = [

@@ -35,6 +35,7 @@ SOURCES = [
     ("tracer_host.cu", EXACT),
     ("traverse.cu", EXACT),
     ("tracer.cu", EXACT),
+    ("noalloc.cu", EXACT),
 ]
 
 HEADERS = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [REPO / "include" / "pfxt.h"]
