@@ -33,8 +33,13 @@
 
 #if defined(__CUDACC__)
 #define PFXT_HD __host__ __device__ __forceinline__
+// Out-of-line on the device: the transcendentals are called from many sites of
+// the shading kernel, and one shared copy keeps its code in the instruction
+// cache.
+#define PFXT_HDN static __host__ __device__ __noinline__
 #else
 #define PFXT_HD static inline
+#define PFXT_HDN static inline
 #endif
 
 namespace pfxt {
@@ -190,7 +195,7 @@ PFXT_HD void reduce_pio2(float x, float* r, int* q) {
   int ki = (int)k;
   *q = ki & 3;
 }
-PFXT_HD float sin_(float x) {
+PFXT_HDN float sin_(float x) {
   if (isnan_(x) || abs_(x) == INFINITY) return NAN;
   float r;
   int q;
@@ -198,7 +203,7 @@ PFXT_HD float sin_(float x) {
   float v = (q & 1) ? cos_kernel(r) : sin_kernel(r);
   return (q & 2) ? -v : v;
 }
-PFXT_HD float cos_(float x) {
+PFXT_HDN float cos_(float x) {
   if (isnan_(x) || abs_(x) == INFINITY) return NAN;
   float r;
   int q;
@@ -224,7 +229,7 @@ PFXT_HD float asin_series(float z) {
   p = p * z2 + 0x1.555556p-3f;
   return z + (z * z2) * p;
 }
-PFXT_HD float asin_(float x) {
+PFXT_HDN float asin_(float x) {
   if (isnan_(x) || x > 1.0f || x < -1.0f) return NAN;
   float ax = abs_(x);
   float a;
@@ -236,7 +241,7 @@ PFXT_HD float asin_(float x) {
   }
   return x < 0.0f ? -a : a;
 }
-PFXT_HD float acos_(float x) {
+PFXT_HDN float acos_(float x) {
   if (isnan_(x) || x > 1.0f || x < -1.0f) return NAN;
   float ax = abs_(x);
   if (ax <= 0.5f) return PFXT_HALF_PI - asin_series(x);
@@ -259,7 +264,7 @@ PFXT_HD float atan_unit(float t) {  // t in [0, 1]
   p = p * s + -0x1.555556p-2f;
   return 4.0f * (t2 + (t2 * s) * p);
 }
-PFXT_HD float atan2_(float y, float x) {
+PFXT_HDN float atan2_(float y, float x) {
   if (isnan_(x) || isnan_(y)) return NAN;
   float ax = abs_(x), ay = abs_(y);
   if (ax == 0.0f && ay == 0.0f) return 0.0f;
@@ -285,7 +290,7 @@ PFXT_HD float ldexp_(float x, int k) {  // x * 2^k, k in [-252, 254]
   }
   return x * bits2f((uint32_t)(k + 127) << 23);
 }
-PFXT_HD float exp_(float x) {
+PFXT_HDN float exp_(float x) {
   if (isnan_(x)) return NAN;
   if (x > 88.7228f) return INFINITY;
   if (x < -103.973f) return 0.0f;
@@ -303,7 +308,7 @@ PFXT_HD float exp_(float x) {
   float e = 1.0f + (r + (r * r) * p);
   return ldexp_(e, (int)k);
 }
-PFXT_HD float log_(float x) {
+PFXT_HDN float log_(float x) {
   if (isnan_(x) || x < 0.0f) return NAN;
   if (x == 0.0f) return -INFINITY;
   if (x == INFINITY) return INFINITY;

@@ -19,7 +19,10 @@
 
 namespace pfxt {
 
-constexpr float SH_PI = 0x1.921fb6p+1f;  // brdf.wgsl:1 `const PI: f32 = 3.141592653589793`
+constexpr float SH_PI = 0x1.921fb6p+1f;
+
+// Heavy helpers are kept out of line (one copy each in the shading kernel).
+#define SH_CALL static __device__ __noinline__  // brdf.wgsl:1 `const PI: f32 = 3.141592653589793`
 
 // ------------------------------------------------------------------ random
 __device__ __forceinline__ uint32_t pcg(uint32_t v) {
@@ -89,7 +92,7 @@ __device__ __forceinline__ uint32_t hash_shuffle_256(uint32_t i0, uint32_t seed)
   }
   return i;
 }
-__device__ __forceinline__ float4 sobol4(const ShadeView& v, const Specialise& sp, const Rng& r, uint32_t dimension) {
+SH_CALL float4 sobol4(const ShadeView& v, const Specialise& sp, const Rng& r, uint32_t dimension) {
   if (!sp.sobol) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   uint32_t L = sp.sobol_length;
   uint32_t seed = r.x;
@@ -189,7 +192,7 @@ __device__ __forceinline__ v3 beer(float distance, v3 tint, float absorption) {
 __device__ __forceinline__ float fresnel_exponent(const Shaded& s) {
   return s.fresnel_power <= 0.0f ? 5.0f : s.fresnel_power;
 }
-__device__ __forceinline__ v3 reflection(const Shaded& s, float ndh_cos) {
+SH_CALL v3 reflection(const Shaded& s, float ndh_cos) {
   float power = fresnel_exponent(s);
   v3 f0 = mix3(splat3(s.specular), s.base, clamp_(s.metalness, 0.0f, 1.0f));
   if (s.transmission > 0.0f || s.dispersion != 0.0f) {
@@ -206,7 +209,7 @@ __device__ __forceinline__ v3 ggx_spec(float ndv, float ndl, float ndh, float a2
   float g = smith_g1(ndv, a2) * smith_g1(ndl, a2);
   return divs3(scl3(scl3(fresnel, ggx_d(ndh, a2)), g), 4.0f * ndv * ndl);
 }
-__device__ __forceinline__ v3 bsdf_eval(const Shaded& s, v3 wo, v3 wi) {
+SH_CALL v3 bsdf_eval(const Shaded& s, v3 wo, v3 wi) {
   float ndv = wo.z;
   if (ndv <= 1e-5f) return splat3(0.0f);
   float ndl = wi.z;
@@ -251,7 +254,7 @@ __device__ __forceinline__ float glossy_share(const Shaded& s) {
 __device__ __forceinline__ float coat_weight_of(const Shaded& s, v3 wo) {
   return clamp_(s.clearcoat * (0.12f + 0.88f * (0.04f + 0.96f * pow_(1.0f - fmax_(wo.z, 0.0f), 5.0f))), 0.0f, 0.9f);
 }
-__device__ __forceinline__ float bsdf_pdf(const Shaded& s, v3 wo, v3 wi) {
+SH_CALL float bsdf_pdf(const Shaded& s, v3 wo, v3 wi) {
   if (wi.z <= 0.0f) return 0.0f;
   float trans = clamp_(s.transmission, 0.0f, 1.0f) * (1.0f - clamp_(s.metalness, 0.0f, 1.0f));
   float coat = coat_weight_of(s, wo);
@@ -277,7 +280,7 @@ struct BsdfSample {
   uint32_t lobe;
 };
 
-__device__ __forceinline__ BsdfSample sample_bsdf(const Specialise& sp, const Shaded& s, v3 wo, bool entering,
+SH_CALL BsdfSample sample_bsdf(const Specialise& sp, const Shaded& s, v3 wo, bool entering,
                                                   uint32_t carried, uint32_t& state, float4 u) {
   BsdfSample out;
   float transmission = clamp_(s.transmission, 0.0f, 1.0f) * (1.0f - clamp_(s.metalness, 0.0f, 1.0f));
@@ -365,7 +368,7 @@ __device__ __forceinline__ uint32_t cdf_find(const float* __restrict__ cdf, uint
 __device__ __forceinline__ v3 sky_radiance(const ShadeView& v) {
   return mk3(v.sky_radiance[0], v.sky_radiance[1], v.sky_radiance[2]);
 }
-__device__ __forceinline__ float sky_pdf(const ShadeView& v, v3 direction) {
+SH_CALL float sky_pdf(const ShadeView& v, v3 direction) {
   v3 d = normalize3(direction);
   float theta = acos_(clamp_(d.y, -1.0f, 1.0f));
   float phi = fmod_wgsl(atan2_(d.z, d.x) + 6.28318531f, 6.28318531f);
@@ -384,7 +387,7 @@ struct SkySample {
   v3 direction;
   float pdf;
 };
-__device__ __forceinline__ SkySample sky_sample(const ShadeView& v, float rx, float ry) {
+SH_CALL SkySample sky_sample(const ShadeView& v, float rx, float ry) {
   float u = clamp_(rx, 0.0f, 0.99999994f);
   float w = clamp_(ry, 0.0f, 0.99999994f);
   uint32_t row = cdf_find(v.sky_rows, v.sky_height, w);
@@ -449,7 +452,7 @@ __device__ __forceinline__ Plane area_frame(const LightRow& l) {
 }
 
 // light_hits (lights.wgsl:64-91)
-__device__ __forceinline__ v3 light_hits(const ShadeView& v, v3 o, v3 d, float limit, v3 previous_point,
+SH_CALL v3 light_hits(const ShadeView& v, v3 o, v3 d, float limit, v3 previous_point,
                                          float previous_pdf) {
   v3 total = splat3(0.0f);
   for (uint32_t i = 0u; i < v.looped; ++i) {
@@ -510,7 +513,7 @@ __device__ __forceinline__ void shadow_ray(v3 origin, v3 aim, bool shadow, v3& d
 }
 
 // light_candidate (lights.wgsl:145-200)
-__device__ __forceinline__ Candidate light_candidate(const Specialise& sp, const LightRow& light, const m3& transform,
+SH_CALL Candidate light_candidate(const Specialise& sp, const LightRow& light, const m3& transform,
                                                      v3 p, v3 origin, v3 geometric, uint32_t& state, float4 u) {
   Candidate out = candidate_none();
   bool shadow = light.d.w > 0.5f;
@@ -590,7 +593,7 @@ __device__ __forceinline__ Candidate light_candidate(const Specialise& sp, const
 __device__ __forceinline__ float sin_from_cos(float c) { return sqrtf(fmax_(1.0f - c * c, 0.0f)); }
 
 // tree_importance (lights.wgsl:204-237) -> (max, min)
-__device__ __forceinline__ float2 tree_importance(v3 n, v3 to, float cos_u, v3 axis, float theta_o, float theta_e,
+SH_CALL float2 tree_importance(v3 n, v3 to, float cos_u, v3 axis, float theta_o, float theta_e,
                                                   float far, float near, float energy) {
   float sin_u = sin_from_cos(cos_u);
   float cos_i = dot3(to, n);
@@ -622,7 +625,7 @@ __device__ __forceinline__ float2 tree_importance(v3 n, v3 to, float cos_u, v3 a
   float cos_max_out = cos_t_plus_u * cos_o - sin_from_cos(cos_t_plus_u) * sin_o;
   return make_float2(most, abs_(cos_max_i * energy * cos_max_out / (far * far)));
 }
-__device__ __forceinline__ float2 node_importance(const LightRow& node, v3 p, v3 n) {
+SH_CALL float2 node_importance(const LightRow& node, v3 p, v3 n) {
   v3 lo = f3of(node.a), hi = f3of(node.b);
   v3 centroid = scl3(add3(lo, hi), 0.5f);
   v3 extent = sub3(hi, centroid);
@@ -637,7 +640,7 @@ __device__ __forceinline__ float2 node_importance(const LightRow& node, v3 p, v3
   return tree_importance(n, divs3(to, fmax_(reach, 1e-30f)), cos_u, f3of(node.c), node.c.w, node.d.x, distance,
                          distance, node.a.w);
 }
-__device__ __forceinline__ float2 emitter_importance(const LightRow& light, v3 p, v3 n) {
+SH_CALL float2 emitter_importance(const LightRow& light, v3 p, v3 n) {
   v3 to = sub3(f3of(light.a), p);
   float near = length3(to);
   if (near >= light.b.w || near <= 1e-6f) return make_float2(0.0f, 0.0f);
@@ -661,7 +664,7 @@ __device__ __forceinline__ float2 child_importance(const ShadeView& v, const Lig
 }
 
 // tree_leaf (lights.wgsl:276-349): (selected row, pmf)
-__device__ __forceinline__ float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n,
+SH_CALL float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n,
                                             float start) {
   float rand = start;
   bool sample_max = rand > 0.5f;
@@ -736,7 +739,7 @@ __device__ __forceinline__ float2 tree_leaf(const ShadeView& v, uint32_t first, 
 
 // tree_pick (lights.wgsl:350-386): (light row, pmf).  The descent is bounded
 // by the number of tree rows; a malformed tree ends the descent with pmf 0.
-__device__ __forceinline__ float2 tree_pick(const ShadeView& v, uint32_t rows, v3 p, v3 n, float start,
+SH_CALL float2 tree_pick(const ShadeView& v, uint32_t rows, v3 p, v3 n, float start,
                                             uint32_t* leaf_row) {
   uint32_t at = f2u((float)v.looped + (float)v.tree);
   float rand = start;
@@ -827,7 +830,7 @@ __device__ __forceinline__ bool clipped_at(const GpuSurface* __restrict__ surfac
   return a || b;
 }
 // emitter_candidate (lights.wgsl:103-144) for triangle emitters
-__device__ __forceinline__ Candidate emitter_candidate(const ShadeView& v, const Specialise& sp, const m3& transform,
+SH_CALL Candidate emitter_candidate(const ShadeView& v, const Specialise& sp, const m3& transform,
                                                        v3 p, v3 origin, uint32_t& state, float4 u) {
   EmitterRow e = load_emitter(v, find_emitter(v, v.emitter_count, rnd(sp, state, u.z)) + 1u);
   Candidate out = candidate_none();

@@ -304,7 +304,10 @@ __device__ __forceinline__ v3 flush_pending(const Pass& P, uint32_t i, uint32_t 
   return result;
 }
 
-__global__ void __launch_bounds__(kThreads) k_shade(Pass P, uint32_t which) {
+// DEFERRED: light-slot shadow rays go through the shadow queue (the usual
+// case); otherwise (more than CAP_MAX light slots) they are traced inline.
+template <bool DEFERRED>
+__global__ void __launch_bounds__(kThreads, 4) k_shade(Pass P, uint32_t which) {
   const uint32_t n = P.w.counters[which];
   const uint32_t* queue = P.w.queue[which];
   uint32_t* next_queue = P.w.queue[which ^ 1u];
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(kThreads) k_shade(Pass P, uint32_t which) {
                            strength);
             term = capped(P, term, bounce > 0u);
             if (term.x == 0.0f && term.y == 0.0f && term.z == 0.0f) continue;  // adds nothing, traces nothing
-            if (!P.deferred) {
+            if (!DEFERRED) {
               if (limit > 0.0f && traverse<true>(P.s, origin, direction, limit).hit) continue;
               result = add3(result, term);
               continue;
@@ -563,14 +566,15 @@ int grid_for(const void* kernel, int threads) {
 }
 
 struct Grids {
-  int trace_closest = 0, trace_any = 0, shade = 0, flat = 0;
+  int trace_closest = 0, trace_any = 0, shade = 0, shade_inline = 0, flat = 0;
 };
 Grids& grids() {
   static Grids g;
   if (g.shade == 0) {
     g.trace_closest = grid_for((const void*)k_trace_queue<false>, kThreads);
     g.trace_any = grid_for((const void*)k_trace_queue<true>, kThreads);
-    g.shade = grid_for((const void*)k_shade, kThreads);
+    g.shade = grid_for((const void*)k_shade<true>, kThreads);
+    g.shade_inline = grid_for((const void*)k_shade<false>, kThreads);
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -665,7 +669,10 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
       P.bounce = bounce;
       k_reset<<<1, 32, 0, st>>>(P, cur);
       k_trace_queue<false><<<g.trace_closest, kThreads, 0, st>>>(P, cur);
-      k_shade<<<g.shade, kThreads, 0, st>>>(P, cur);
+      if (deferred)
+        k_shade<true><<<g.shade, kThreads, 0, st>>>(P, cur);
+      else
+        k_shade<false><<<g.shade_inline, kThreads, 0, st>>>(P, cur);
       if (deferred) {
         k_rewind<<<1, 32, 0, st>>>(P);
         k_trace_queue<true><<<g.trace_any, kThreads, 0, st>>>(P, 0u);
