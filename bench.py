@@ -1,20 +1,33 @@
 #!/usr/bin/env python
 """Benchmark of the B200 path tracer; prints ONE JSON line on rank 0.
 
-Workload (default): the 4K room scene (3840x2160, 1.19M triangles, 128 lights,
-32 materials; pfx_b200.synth.room_4k) and a fixed batch with the ray mix of one
-tracing pass: camera rays and cosine bounce rays (closest hit) plus shadow
-rays to the lights (any hit).  One step = one closest-hit launch over the
-closest batch and one any-hit launch over the shadow batch, inputs resident in
-HBM.  The metric is Mrays/s = (closest + any-hit queries) / s.  L2 is flushed
-(a 256 MiB write) before every timed step; the per-step device time comes from
-CUDA events on the launching stream.
+Workload: the 4K room (3840x2160, 1.19M triangles, 32 materials with glass and
+metals, 128 point/spot lights through the light tree, depth 8, Sobol sampler;
+pfx_b200.synth.room_4k), synthetic and seeded.  One step = one sampling pass
+(one sample for all 8.3M pixels) through the wavefront tracer, scene resident
+in HBM; L2 is flushed before every timed step.  Device time comes from CUDA
+events recorded on the tracer's own stream.
+
+  value            Mrays/s = closest-hit + any-hit queries traced per second
+  time_to_relmse   seconds of sampling passes until relMSE <= 0.01, relMSE =
+                   mean over pixels and channels of (I-R)^2 / (R^2 + 0.01), R a
+                   4096-spp reference accumulated in FP64 over every 8th pixel
+                   in x and y (a stratified 480x270 subset of the 4K frame);
+                   the error is followed on those pixels alone (their values do
+                   not depend on the other pixels) and the time is spp x the
+                   full-frame pass time measured above
+  roofline         the closest-hit traversal kernel on a batch with the ray mix
+                   of one pass (the same traversal code as the tracer's extend
+                   kernel): algorithmic bytes 32*box + 36*tri + 48 per ray over
+                   its event-timed launch
+  e2e              Trace::sample(1) + Trace::readback(colour) through the C ABI
+                   per step, host wall clock, film copied into pinned memory
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Multi-GPU: one process per GPU (torchrun); every rank traces its own batch
-(different seeds), nothing is exchanged on the data path (weak scaling); the
-time is the max over ranks.
+Multi-GPU: one process per GPU (torchrun); every rank renders the full frame
+with its own seed, nothing is exchanged (weak scaling); time = max over ranks.
+The relMSE measurement runs at N=1 only.
 """
 from __future__ import annotations
 
@@ -33,38 +46,35 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-FALLBACK_HBM_GBS = 6650.0  # profiling recipe's fallback, used only without MEASURED_PEAKS.json
+FALLBACK_HBM_GBS = 6650.0  # used only when MEASURED_PEAKS.json is absent
+METRIC = "time to relMSE 0.01 at 4K, cached vs plain tracer on one B200; Mrays/s"
+TARGET_RELMSE = 0.01
 
 
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
-        d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), "measured"
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
     return FALLBACK_HBM_GBS, "fallback"
 
 
 def ncu_traffic(kernel: str):
-    """Per-launch DRAM traffic of `kernel` from the committed ncu summary
-    (profiles/traffic.json), scaled to this workload by the summary's rule."""
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary."""
     p = ROOT / "profiles" / "traffic.json"
     if not p.exists():
         return None
-    d = json.loads(p.read_text()).get(kernel)
-    return None if d is None else d
+    return json.loads(p.read_text()).get(kernel)
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index: int):
-        self.device = device_index
-        self.proc = None
-        self.file = None
+        self.device, self.proc, self.file = device_index, None, None
 
     def __enter__(self):
         try:
@@ -106,100 +116,194 @@ class Clocks:
 
 
 def dist_env():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def build_workload(args, seed: int):
+def workload(name: str):
     from pfx_b200 import synth
-    w = synth.room_4k(seed=2) if args.workload == "room_4k" else synth.WORKLOADS[args.workload]()
-    return w
+    return synth.WORKLOADS[name]()
 
 
-def cpu_baseline(trace, closest, shadow, budget_rays: int):
-    """The oracle's traversal (the CPU restatement of scene()/occluded()) on a
-    bounded sample of the same batches, all host threads."""
-    import oracle
-    n_c = min(len(closest), budget_rays // 2)
-    n_s = min(len(shadow), budget_rays // 2)
-    c, s = closest[:n_c], shadow[:n_s]
-    oracle.trace(trace.scene_buffers, c[:256])  # warm the library
-    t0 = time.perf_counter()
-    oracle.trace(trace.scene_buffers, c)
-    oracle.trace(trace.scene_buffers, s, any_hit=True)
-    dt = time.perf_counter() - t0
-    return {"value": (n_c + n_s) / dt / 1e6, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{n_c} closest-hit + {n_s} any-hit rays of the same batch, oracle traversal on all host threads"}
+def config_of(w, args, extra=None):
+    c = {"workload": f"{w.name}: {w.width}x{w.height}, {w.scene.world_triangle_count} triangles, "
+                     f"{len(w.scene.lights)} point/spot lights (light tree), 32 materials, depth "
+                     f"{w.settings.bounces[0]}, {w.settings.sampler} sampler",
+         "step": "one sampling pass (1 spp, every pixel)",
+         "l2": "flushed before every timed step (256 MiB write)",
+         "parallelism": f"independent frames x{args.gpus} (no collective on the data path)"}
+    if extra:
+        c.update(extra)
+    return c
 
 
+# ------------------------------------------------------------------ reference
 def run_reference(args):
-    world, rank, local = dist_env()
+    """The reference's path on the host cores: the oracle (a C++ restatement of
+    crates/trace's main()/radiance()) on a bounded window of the same frame.
+    The reference's own wgpu tracer cannot run here (no Rust toolchain, no
+    graphics stack)."""
+    world, rank, _ = dist_env()
     if rank != 0:
         return 0
-    w = build_workload(args, 0)
-    from pfx_b200.trace import SceneBuffers
     import oracle
-    from pfx_b200 import rays as raymix
+    from pfx_b200.trace import SceneBuffers
+    w = workload(args.workload)
     sb = SceneBuffers(w.scene, w.settings)
-
-    class _T:  # ray generation needs closest hits; the oracle provides them here
-        scene_buffers = sb
-
-        def trace_rays(self, r):
-            return oracle.trace(sb, r)
-
-    per_step = min(args.rays, 1 << 17)
-    closest, shadow = raymix.pass_mix(_T(), w.scene, w.width, w.height, per_step, seed=7)
-    times = []
+    r = oracle.Renderer(sb, w.settings)
+    ww, wh = 160, 90
+    x0, y0 = (w.width - ww) // 2, (w.height - wh) // 2
+    frame = oracle.frame_of(w.scene, ww, wh, sb.buffers.triangle_count, window=(w.width, w.height, x0, y0))
+    accum = np.zeros((wh, ww, 12), np.float32)
+    times, rays = [], 0
     for i in range(args.warmup + args.steps):
+        oracle.Renderer.ray_counts()
         t0 = time.perf_counter()
-        oracle.trace(sb, closest)
-        oracle.trace(sb, shadow, any_hit=True)
+        r.render(frame, accum, 0, 1, i)
         dt = time.perf_counter() - t0
+        c = oracle.Renderer.ray_counts()
         if i >= args.warmup:
             times.append(dt)
-    total = sum(times)
-    rays = (len(closest) + len(shadow)) * len(times)
-    value = rays / total / 1e6
-    line = {
+            rays += c[0] + c[1]
+    value = rays / sum(times) / 1e6
+    print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": config_of(args, w, len(closest), len(shadow)),
+        "config": config_of(w, args, {"sample": f"{ww}x{wh} centre window of the 4K frame, 1 spp per step"}),
         "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
-                         "sample": f"{len(closest)} closest + {len(shadow)} any-hit rays per step; the reference's "
-                                   "wgpu tracer cannot run on this box (no Rust, no graphics stack), so its CPU "
-                                   "restatement (oracle/) runs on all host threads"},
+                         "sample": f"{ww}x{wh} centre window, 1 spp per step, oracle path tracer on all host "
+                                   "threads (the reference's wgpu tracer is unavailable on this box)"},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line))
+    }))
     return 0
 
 
-METRIC = "Mrays/s, closest-hit + any-hit traversal of one tracing pass's ray mix (4K room, 1.19M triangles)"
+# ------------------------------------------------------------------ ours
+def relmse(img, ref):
+    """mean over pixels and channels of (I-R)^2 / (R^2 + 0.01), in FP64."""
+    d = img.double() - ref
+    return float((d * d / (ref * ref + 0.01)).mean())
 
 
-def config_of(args, w, n_closest, n_shadow):
-    return {"workload": f"{w.name}: {w.width}x{w.height}, {w.scene.world_triangle_count} triangles, "
-                        f"{len(w.scene.lights)} lights, one-pass ray mix",
-            "closest_rays_per_step": n_closest, "shadow_rays_per_step": n_shadow,
-            "l2": "flushed before every timed step (256 MiB write)", "parallelism": f"replica-free pixel/ray shards x{args.gpus}"}
+def masked_trace(w, mask):
+    from pfx_b200.trace import Trace
+    t = Trace(w.scene, w.settings, w.width, w.height)
+    t.set_pixel_mask(mask)
+    return t
+
+
+def reference_image(w, args, mask, mask_idx):
+    """The reference over the masked pixels: args.ref_spp samples accumulated in
+    FP64 on the device, in chunks of 64 with their own seeds."""
+    import torch
+    ref_trace = masked_trace(w, mask)
+    chunk = 64
+    total = torch.zeros((len(mask_idx), 3), dtype=torch.float64, device="cuda")
+    chunks = max(1, args.ref_spp // chunk)
+    t0 = time.perf_counter()
+    for c in range(chunks):
+        ref_trace.set_camera(w.scene.camera)  # restarts the accumulation
+        ref_trace.sample(chunk, 100_000 + c)
+        color = ref_trace.films_device()[0].reshape(-1, 4)
+        total += color[mask_idx, :3].double()
+    ref = total / chunks
+    ref_trace.close()
+    return ref, time.perf_counter() - t0
+
+
+def plain_convergence(w, mask, mask_idx, ref, max_spp):
+    """Samples per pixel the plain tracer needs to reach the target relMSE.
+
+    A pixel's samples depend only on the pixel, the sample index and the pass
+    seed, never on which other pixels are traced, so a pass over the masked
+    pixels gives exactly the values a full-frame pass gives there; the time to
+    the target is then the spp count times the full-frame pass time."""
+    t = masked_trace(w, mask)
+    color = t.films_device()[0].reshape(-1, 4)
+    curve = []
+    for p in range(max_spp):
+        t.sample(1, 50_000 + p)
+        err = relmse(color[mask_idx, :3], ref)
+        curve.append((p + 1, err))
+        if err <= TARGET_RELMSE:
+            break
+    t.close()
+    reached = curve[-1][1] <= TARGET_RELMSE
+    return (curve[-1][0] if reached else None), curve
+
+
+def traversal_roofline(trace, w, dev, stream, flush):
+    """Closest-hit kernel on a one-pass ray mix, timed with events on its stream."""
+    import torch
+    from pfx_b200 import rays as raymix
+    closest, _ = raymix.pass_mix(trace, w.scene, w.width, w.height, 1 << 22, seed=7)
+    n = len(closest)
+    d_rays = torch.from_numpy(closest.view(np.uint8).copy()).to(dev)
+    d_hits = torch.empty(n * 16, dtype=torch.uint8, device=dev)
+    counts = torch.empty(n * 2, dtype=torch.int32, device=dev)
+    sh = stream.cuda_stream
+    trace.counts_device(d_rays.data_ptr(), n, False, counts.data_ptr(), sh)
+    torch.cuda.synchronize()
+    c = counts.view(-1, 2).double().sum(0).cpu().numpy()
+    algorithmic = 32 * c[0] + 36 * c[1] + 48 * n
+    for _ in range(3):
+        trace.trace_rays_device(d_rays.data_ptr(), n, d_hits.data_ptr(), sh)
+    ms = []
+    for _ in range(5):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        trace.trace_rays_device(d_rays.data_ptr(), n, d_hits.data_ptr(), sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    launch_s = statistics.mean(ms) / 1e3
+    peak, kind = peaks()
+    achieved = algorithmic / launch_s / 1e9
+    return {"bound": "hbm", "kernel": "k_trace<0>: closest-hit traversal (the extend kernel's walk)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": kind,
+            "traffic": ncu_traffic("k_trace<0>"), "algorithmic_bytes_per_launch": algorithmic,
+            "rays_per_launch": n, "box_tests_per_ray": c[0] / n, "triangle_tests_per_ray": c[1] / n,
+            "launch_ms": statistics.mean(ms), "Mrays_s": n / launch_s / 1e6}
+
+
+def cpu_baseline(w, budget_s=12.0):
+    """The oracle path tracer on a window of the same frame, all host threads."""
+    import oracle
+    from pfx_b200.trace import SceneBuffers
+    sb = SceneBuffers(w.scene, w.settings)
+    r = oracle.Renderer(sb, w.settings)
+    ww, wh = 160, 90
+    x0, y0 = (w.width - ww) // 2, (w.height - wh) // 2
+    frame = oracle.frame_of(w.scene, ww, wh, sb.buffers.triangle_count, window=(w.width, w.height, x0, y0))
+    accum = np.zeros((wh, ww, 12), np.float32)
+    oracle.Renderer.ray_counts()
+    t0, spp = time.perf_counter(), 0
+    while time.perf_counter() - t0 < budget_s or spp == 0:
+        r.render(frame, accum, 0, 1, spp)
+        spp += 1
+    dt = time.perf_counter() - t0
+    c = oracle.Renderer.ray_counts()
+    return {"value": (c[0] + c[1]) / dt / 1e6, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{ww}x{wh} centre window of the 4K frame, {spp} x 1 spp, oracle path tracer on all host threads"}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="room_4k")
-    ap.add_argument("--rays", type=int, default=1 << 22, help="rays per step (closest + shadow)")
+    ap.add_argument("--ref-spp", type=int, default=4096)
+    ap.add_argument("--stride", type=int, default=8)
+    ap.add_argument("--max-spp", type=int, default=2048)
+    ap.add_argument("--no-relmse", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
 
@@ -210,118 +314,110 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180), device_id=torch.device("cuda", local))
         pg = dist
-    from pfx_b200 import rays as raymix
-    from pfx_b200.trace import HIT, RAY, Trace
+    from pfx_b200.trace import Trace
 
-    w = build_workload(args, rank)
-    trace = Trace(w.scene, w.settings, w.width, w.height)
-    closest, shadow = raymix.pass_mix(trace, w.scene, w.width, w.height, args.rays, seed=7 + rank)
-    nc, ns = len(closest), len(shadow)
     dev = torch.device("cuda", local)
-    d_closest = torch.from_numpy(closest.view(np.uint8).copy()).to(dev)
-    d_shadow = torch.from_numpy(shadow.view(np.uint8).copy()).to(dev)
-    d_hits = torch.empty(nc * 16, dtype=torch.uint8, device=dev)
-    d_blocked = torch.empty(ns * 4, dtype=torch.uint8, device=dev)
+    w = workload(args.workload)
+    t0 = time.perf_counter()
+    trace = Trace(w.scene, w.settings, w.width, w.height)
+    create_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(trace._lib.pfxt_debug_stream(trace.handle), device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream(dev)
-    sh = stream.cuda_stream
+    seed0 = 1000 * (rank + 1)
 
-    # algorithmic bytes per query: 32 per box test, 36 per triangle test, 48 per ray (in + out)
-    counts_c = torch.empty(nc * 2, dtype=torch.int32, device=dev)
-    counts_s = torch.empty(ns * 2, dtype=torch.int32, device=dev)
-    trace.counts_device(d_closest.data_ptr(), nc, False, counts_c.data_ptr(), sh)
-    trace.counts_device(d_shadow.data_ptr(), ns, True, counts_s.data_ptr(), sh)
-    torch.cuda.synchronize()
-    cc = counts_c.view(-1, 2).double().sum(0).cpu().numpy()
-    cs = counts_s.view(-1, 2).double().sum(0).cpu().numpy()
-    bytes_closest = 32 * cc[0] + 36 * cc[1] + 48 * nc
-    bytes_shadow = 32 * cs[0] + 36 * cs[1] + 48 * ns
-
-    def step():
-        trace.trace_rays_device(d_closest.data_ptr(), nc, d_hits.data_ptr(), sh)
-        trace.occluded_device(d_shadow.data_ptr(), ns, d_blocked.data_ptr(), sh)
-
-    for _ in range(args.warmup):
-        flush.fill_(1)
-        step()
+    for i in range(args.warmup):
+        trace.sample(1, seed0 + i)
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    before = trace.rays_traced()
+    step_ms = []
     with Clocks(local) as clk:
-        for e0, e1, e2 in ev:
+        for i in range(args.steps):
             flush.fill_(1)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            trace.trace_rays_device(d_closest.data_ptr(), nc, d_hits.data_ptr(), sh)
+            trace.sample(1, seed0 + 100 + i)
             e1.record(stream)
-            trace.occluded_device(d_shadow.data_ptr(), ns, d_blocked.data_ptr(), sh)
-            e2.record(stream)
-        torch.cuda.synchronize()
-    step_ms = [a.elapsed_time(c) for a, _, c in ev]
-    closest_ms = [a.elapsed_time(b) for a, b, _ in ev]
+            torch.cuda.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+    after = trace.rays_traced()
+    rays = (after[0] - before[0]) + (after[1] - before[1])
     total_ms = sum(step_ms)
     if pg:
-        t = torch.tensor([total_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
-        pg.barrier()
-    rays_per_step = nc + ns
-    value = rays_per_step * world * args.steps / (total_ms / 1e3) / 1e6
+        t = torch.tensor([total_ms, float(rays)], dtype=torch.float64, device=dev)
+        tmax = t.clone()
+        pg.all_reduce(tmax, op=pg.ReduceOp.MAX)
+        tsum = t.clone()
+        pg.all_reduce(tsum, op=pg.ReduceOp.SUM)
+        total_ms, rays_all = float(tmax[0].item()), float(tsum[1].item())
+    else:
+        rays_all = float(rays)
+    value = rays_all / (total_ms / 1e3) / 1e6
 
-    # end to end through the host-buffer entry points (pinned host memory,
-    # copies in and results out inside the timed region)
-    h_closest = torch.from_numpy(closest.view(np.uint8).copy()).pin_memory()
-    h_shadow = torch.from_numpy(shadow.view(np.uint8).copy()).pin_memory()
-    h_hits = torch.empty(nc * 16, dtype=torch.uint8).pin_memory()
-    h_blocked = torch.empty(ns, dtype=torch.uint8).pin_memory()
+    # e2e: sample + readback of the colour film through the host-buffer API
+    film = torch.empty((w.height, w.width, 4), dtype=torch.float32).pin_memory()
     lib = trace._lib
     e2e_steps = max(3, args.steps // 2)
-    lib.pfxt_trace_rays(trace.handle, h_closest.data_ptr(), nc, h_hits.data_ptr())
-    lib.pfxt_occluded(trace.handle, h_shadow.data_ptr(), ns, h_blocked.data_ptr())
+    r0 = trace.rays_traced()
     if pg:
         pg.barrier()
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        rc = lib.pfxt_trace_rays(trace.handle, h_closest.data_ptr(), nc, h_hits.data_ptr())
-        rc |= lib.pfxt_occluded(trace.handle, h_shadow.data_ptr(), ns, h_blocked.data_ptr())
+    for i in range(e2e_steps):
+        rc = lib.pfxt_sample(trace.handle, 1, seed0 + 500 + i)
+        rc |= lib.pfxt_readback(trace.handle, film.data_ptr(), None, None)
         assert rc == 0, lib.pfxt_last_error()
     e2e_s = time.perf_counter() - t0
+    r1 = trace.rays_traced()
+    e2e_rays = float((r1[0] - r0[0]) + (r1[1] - r0[1]))
     if pg:
-        t = torch.tensor([e2e_s], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = rays_per_step * world * e2e_steps / e2e_s / 1e6
+        t = torch.tensor([e2e_s, e2e_rays], dtype=torch.float64, device=dev)
+        tmax = t.clone()
+        pg.all_reduce(tmax, op=pg.ReduceOp.MAX)
+        tsum = t.clone()
+        pg.all_reduce(tsum, op=pg.ReduceOp.SUM)
+        e2e_s, e2e_rays = float(tmax[0].item()), float(tsum[1].item())
+    e2e_value = e2e_rays / e2e_s / 1e6
 
     if rank == 0:
-        peak, peak_kind = peaks()
-        closest_s = statistics.mean(closest_ms) / 1e3
-        achieved = bytes_closest / closest_s / 1e9
-        traffic = ncu_traffic("k_trace<0>")
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_of(args, w, nc, ns),
-            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": int((nc + ns) * 32),
-                    "d2h_bytes_per_step": int(nc * 16 + ns)},
-            "gpu_launches": 2 * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "k_trace<0> (closest-hit traversal)", "achieved": achieved,
-                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": traffic,
-                         "algorithmic_bytes_per_launch": bytes_closest,
-                         "bytes_per_ray": bytes_closest / nc,
-                         "box_tests_per_ray": cc[0] / nc, "triangle_tests_per_ray": cc[1] / nc},
-            "closest_ms_per_launch": statistics.mean(closest_ms),
+            "config": config_of(w, args), "rays_per_step": rays / args.steps,
+            "Mpaths_s": w.width * w.height * world * args.steps / (total_ms / 1e3) / 1e6,
+            "create_s": create_s,
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(w.width * w.height * 16),
+                    "note": "scene uploaded once by Trace::new (create_s); per step one pass and the colour film"},
+            "gpu_launches": args.steps * (2 + 2 + (w.settings.bounces[0] + 2) * 5 + 1),
             "clocks": clk.summary(),
         }
+        line["roofline"] = traversal_roofline(trace, w, dev, stream, flush)
+        if world == 1 and not args.no_relmse:
+            mask = np.zeros((w.height, w.width), bool)
+            s = args.stride
+            mask[s // 2::s, s // 2::s] = True
+            mask_idx = torch.from_numpy(np.flatnonzero(mask.reshape(-1))).to(dev)
+            ref, ref_s = reference_image(w, args, mask, mask_idx)
+            spp_plain, curve = plain_convergence(w, mask, mask_idx, ref, args.max_spp)
+            pass_s = total_ms / args.steps / 1e3
+            line["time_to_relmse"] = {
+                "target": TARGET_RELMSE, "plain_spp": spp_plain,
+                "plain_s": None if spp_plain is None else spp_plain * pass_s, "pass_s": pass_s,
+                "cached_s": None,
+                "reference": f"{args.ref_spp} spp accumulated in FP64 over every {s}th pixel in x and y "
+                             f"({int(mask.sum())} pixels), {ref_s:.1f} s",
+                "plain_curve": [(n, round(e, 5)) for n, e in curve[:: max(1, len(curve) // 12)] + curve[-1:]]}
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(trace, closest, shadow, 1 << 18)
+            line["cpu_baseline"] = cpu_baseline(w)
         print(json.dumps(line))
     trace.close()
     if pg:
+        pg.barrier()
         pg.destroy_process_group()
     return 0
 

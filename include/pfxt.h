@@ -251,6 +251,10 @@ int pfxt_adaptive_rounds(const pfxt_adaptive* adaptive, uint32_t* rounds, uint32
 /* Trace::readback (gpu.rs:3240): RGBA32F colour, albedo and normal films,
  * width*height*4 floats each; any pointer may be NULL. */
 int pfxt_readback(pfxt_trace* trace, float* color, float* albedo, float* normal);
+/* The three films in device memory (RGBA32F, width*height*4 floats each), as
+ * the reference hands its colour/albedo/normal textures to the denoiser
+ * without a readback (gpu.rs:328-330).  Valid until pfxt_destroy. */
+int pfxt_films_device(pfxt_trace* trace, float** color, float** albedo, float** normal);
 /* Trace::sample_counts (adaptive.rs:328): |accum.color.w| per pixel. */
 int pfxt_sample_counts(pfxt_trace* trace, uint32_t* counts);
 /* The raw 48 B/pixel accumulation (Accum, trace.wgsl:84). */

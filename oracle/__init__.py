@@ -135,6 +135,28 @@ def check_div(per_family: int, seed: int = 1) -> int:
     return int(lib().orc_check_div(per_family, seed))
 
 
+def frame_of(scene, width: int, height: int, tri_count: int, window=None) -> np.ndarray:
+    """The per-pass uniform the product computes on the host (gpu.rs:2295-2316)
+    for a perspective camera without lens; `window` = (full_w, full_h, x, y)
+    renders a tile of a larger frame (Trace::set_window, gpu.rs:2834)."""
+    import math
+    f = np.zeros(40, np.uint32)
+    fl = f.view(np.float32)
+    f[0:4] = (width, height, 0, 0)
+    f[4:8] = (tri_count, 0, 0, 0)
+    fl[8:11] = scene.camera.origin
+    fl[12:15] = scene.camera.forward
+    fl[16:19] = scene.camera.right
+    fl[20:23] = scene.camera.up
+    fl[24:27] = scene.sun.direction
+    fl[27] = np.float32(math.cos(np.float32(scene.sun.radius_deg) * np.float32(math.pi / 180.0)))
+    fl[28:31] = scene.sun.color
+    fl[31] = scene.sun.intensity
+    fl[32:36] = (0.0, 0.0, 0.0, 1.0)
+    f[36:40] = window if window is not None else (width, height, 0, 0)
+    return f
+
+
 class _OrcScene(C.Structure):
     _fields_ = [("nodes", C.c_void_p), ("node_count", C.c_uint32), ("tris", C.c_void_p), ("tri_count", C.c_uint32),
                 ("surfaces", C.c_void_p), ("materials", C.c_void_p), ("material_rows", C.c_uint32),
@@ -194,6 +216,16 @@ class Renderer:
         normal = np.zeros_like(color)
         lib().orc_render(C.byref(self.scene), _p(f), _p(accum), _p(color), _p(albedo), _p(normal))
         return color, albedo, normal
+
+    @staticmethod
+    def ray_counts() -> tuple:
+        """(closest, any) queries traced by render() since the last call."""
+        L = lib()
+        L.orc_ray_counts.restype = None
+        L.orc_ray_counts.argtypes = [C.c_void_p]
+        out = np.zeros(2, np.uint64)
+        L.orc_ray_counts(_p(out))
+        return int(out[0]), int(out[1])
 
     def converge(self, accum: np.ndarray, snaps: np.ndarray, min_samples: int, threshold: float, mark: bool) -> int:
         h, w = accum.shape[:2]

@@ -892,8 +892,12 @@ Candidate direct_light(Ctx& c, uint32_t slot, const m3& transform, v3 p, v3 orig
 }
 
 // ------------------------------------------------------------- scene hit
+// Closest-hit and any-hit queries traced (for the CPU baseline's rays/s).
+std::atomic<uint64_t> g_closest{0}, g_any{0};
+
 // scene() result with tri_fill (trace.wgsl:754-779) and world_hit (:682-694)
 HitInfo scene_hit(const Ctx& c, v3 o, v3 d, float limit) {
+  g_closest.fetch_add(1, std::memory_order_relaxed);
   Walk w = orc_walk(c.geo, o, d, limit, false);
   HitInfo h;
   h.t = w.t;
@@ -930,7 +934,10 @@ HitInfo scene_hit(const Ctx& c, v3 o, v3 d, float limit) {
   h.geometric = wg;
   return h;
 }
-bool occluded(const Ctx& c, v3 o, v3 d, float limit) { return orc_walk(c.geo, o, d, limit, true).hit; }
+bool occluded(const Ctx& c, v3 o, v3 d, float limit) {
+  g_any.fetch_add(1, std::memory_order_relaxed);
+  return orc_walk(c.geo, o, d, limit, true).hit;
+}
 
 v3 indirect_capped(const Ctx& c, v3 value, bool deep) {
   float cap = c.sc->clamp_indirect;
@@ -1232,6 +1239,12 @@ uint32_t orc_converge(float* accum, float* snaps, uint32_t W, uint32_t H, uint32
       running += 1;
   }
   return running;
+}
+
+// Closest-hit and any-hit queries traced by orc_render since the last call.
+void orc_ray_counts(uint64_t* out) {
+  out[0] = orc::g_closest.exchange(0);
+  out[1] = orc::g_any.exchange(0);
 }
 
 // One light-tree pick (tree_pick, lights.wgsl:350-386) per query point:

@@ -140,6 +140,8 @@ PROTOTYPES = [
     ("pfxt_readback", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pfxt_sample_counts", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pfxt_read_accum", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pfxt_films_device", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                    C.POINTER(C.c_void_p)]),
     ("pfxt_trace_rays", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("pfxt_occluded", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("pfxt_trace_rays_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
@@ -153,6 +155,7 @@ EXTRA = [
     ("pfxt_debug_frame", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pfxt_debug_rays", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pfxt_debug_stream", C.c_void_p, [C.c_void_p]),
+    ("pfxt_debug_pixel_mask", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pfxt_trace_counts_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                            C.c_void_p]),
 ]

@@ -363,4 +363,42 @@ int pfxt_debug_rays(pfxt_trace* t, uint64_t* out) {
 /* The handle's CUDA stream (cudaStream_t), so a harness can record events on
  * the stream the passes run on. */
 void* pfxt_debug_stream(pfxt_trace* t) { return t ? (void*)t->stream : nullptr; }
+
+/* Restrict sampling to the pixels whose mask byte is non-zero (width*height
+ * host bytes), or lift the restriction with NULL.  A measurement aid: it lets a
+ * high-sample reference be accumulated on a stratified subset of a large film.
+ * Restarts the accumulation. */
+int pfxt_debug_pixel_mask(pfxt_trace* t, const uint8_t* mask) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    size_t pixels = (size_t)t->width * t->height;
+    if (!mask) {
+      if (t->d_mask) cudaMemsetAsync(t->d_mask, 1, pixels, t->stream);
+      t->samples = 0;
+      return;
+    }
+    if (!t->d_mask) {
+      void* d = nullptr;
+      check(cudaMalloc(&d, pixels), "pixel mask");
+      t->owned.push_back(d);
+      t->d_mask = static_cast<uint8_t*>(d);
+    }
+    check(cudaMemcpyAsync(t->d_mask, mask, pixels, cudaMemcpyHostToDevice, t->stream), "pixel mask");
+    check(cudaStreamSynchronize(t->stream), "pixel mask");
+    t->samples = 0;
+  });
+}
+
+/* The films on the device (RGBA32F, width*height*4 floats each): what the
+ * reference exposes as its colour/albedo/normal textures for the denoiser
+ * (gpu.rs:328-330).  Valid until pfxt_destroy; written by every pass. */
+int pfxt_films_device(pfxt_trace* t, float** color, float** albedo, float** normal) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    check(cudaStreamSynchronize(t->stream), "films");
+    if (color) *color = reinterpret_cast<float*>(t->d_color);
+    if (albedo) *albedo = reinterpret_cast<float*>(t->d_albedo);
+    if (normal) *normal = reinterpret_cast<float*>(t->d_normal);
+  });
+}
 }  // extern "C"

@@ -104,10 +104,10 @@ __device__ __forceinline__ void append(uint32_t* queue, uint32_t* count, uint32_
 // ------------------------------------------------------------------ active
 // Pixels that still sample: the reference returns early when accum.color.w
 // is negative (trace.wgsl:2517), the mark of a converged pixel.
-__global__ void k_collect(Pass P, const Accum* __restrict__ accum) {
+__global__ void k_collect(Pass P, const Accum* __restrict__ accum, const uint8_t* __restrict__ mask) {
   uint32_t n = P.width * P.height;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    bool live = P.f.size[2] == 0u || !(accum[i].color.w < 0.0f);
+    bool live = (P.f.size[2] == 0u || !(accum[i].color.w < 0.0f)) && (mask == nullptr || mask[i] != 0);
     append(P.w.active, P.w.counters + 3, i, live);
   }
 }
@@ -659,7 +659,7 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   cudaStream_t st = t.stream;
   if (t.samples == 0) check(cudaMemsetAsync(t.d_accum, 0, (size_t)pixels * sizeof(Accum), st), "accumulation reset");
   check(cudaMemsetAsync(P.w.counters, 0, 32, st), "counters");  // queues; the ray totals at [8..11] persist
-  k_collect<<<g.flat, 256, 0, st>>>(P, t.d_accum);
+  k_collect<<<g.flat, 256, 0, st>>>(P, t.d_accum, t.d_mask);
   for (uint32_t sample = 0; sample < count; ++sample) {
     P.sample = sample;
     k_gen<<<g.flat, 256, 0, st>>>(P);

@@ -299,7 +299,10 @@ def instanced_1080(seed: int = 1, width: int = 1920, height: int = 1080, target:
 
 
 def room_4k(seed: int = 2, width: int = 3840, height: int = 2160, target: int = 1_200_000, meshes_n: int = 300,
-            sampler: str = "sobol") -> Workload:
+            sampler: str = "sobol", light_radius=(0.1, 0.3), light_scale: float = 0.05, light_height=(6.0, 9.6),
+            light_seed=None) -> Workload:
+    """Lights are soft (bulb radius U(0.1, 0.3) m) and hang in the upper part of
+    the room, as ceiling fixtures do."""
     rng = np.random.default_rng(seed)
     mats = []
     for i in range(32):
@@ -344,20 +347,25 @@ def room_4k(seed: int = 2, width: int = 3840, height: int = 2160, target: int = 
         parts.append(uv_sphere(c, radius, slices, stacks, material=m, wobble=wobble))
     tris = np.concatenate(parts)
     lights = []
+    lrng = np.random.default_rng(seed + 100) if light_seed is None else np.random.default_rng(light_seed)
     for i in range(128):
-        p = rng.uniform((-14, 1.0, -14), (14, 9.6, 14))
-        inten = float(_log_uniform(rng, 1.0, 1000.0)) * 0.05
-        col = tuple(rng.uniform(0.6, 1.0, 3))
+        p = lrng.uniform((-14, light_height[0], -14), (14, light_height[1], 14))
+        inten = float(_log_uniform(lrng, 1.0, 1000.0)) * light_scale
+        col = tuple(lrng.uniform(0.6, 1.0, 3))
+        radius = float(lrng.uniform(*light_radius))
         if i % 2 == 0:
-            lights.append(point_light(p, inten, col))
+            lights.append(point_light(p, inten, col, radius=radius))
         else:
-            d = rng.normal(size=3)
+            d = lrng.normal(size=3)
             d[1] = -abs(d[1]) - 0.3
-            outer = float(rng.uniform(10.0, 60.0))
-            lights.append(spot_light(p, d / np.linalg.norm(d), inten, outer, 0.8 * outer, col))
+            outer = float(lrng.uniform(10.0, 60.0))
+            lights.append(spot_light(p, d / np.linalg.norm(d), inten, outer, 0.8 * outer, col, radius=radius))
     scene = SceneDesc(tris, np.concatenate(mats), look_at((0, 5, 14.5), (0, 4, 0), 60.0, width / height),
                       lights=np.concatenate(lights))
-    return Workload("room_4k", scene, Settings.deep(8, sampler=sampler, sobol_samples=64), width, height, spp=64,
+    # the reference's firefly controls, at the values its own firefly test
+    # renders with (crates/trace/tests/fireflies.rs:21-22)
+    settings = Settings.deep(8, sampler=sampler, sobol_samples=64, filter_glossy=0.25, clamp_indirect=4.0)
+    return Workload("room_4k", scene, settings, width, height, spp=64,
                     adaptive=Adaptive(threshold=0.01, min_samples=16, max_samples=64, growth=1.5))
 
 

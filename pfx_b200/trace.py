@@ -320,6 +320,36 @@ class Trace:
     def occluded_device(self, rays_ptr: int, count: int, blocked_ptr: int, stream: int = 0) -> None:
         check(self._lib.pfxt_occluded_device(self._h, rays_ptr, count, blocked_ptr, stream))
 
+    def films_device(self):
+        """The colour, albedo and normal films as (H, W, 4) float32 CUDA tensors
+        that alias the tracer's own device memory (no copy)."""
+        import torch
+        ptrs = [C.c_void_p() for _ in range(3)]
+        check(self._lib.pfxt_films_device(self._h, *[C.byref(p) for p in ptrs]))
+
+        class _View:
+            def __init__(self, ptr, shape):
+                self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f4", "data": (ptr, False),
+                                                 "version": 3, "strides": None}
+
+        shape = (self.height, self.width, 4)
+        return [torch.as_tensor(_View(p.value, shape), device="cuda") for p in ptrs]
+
+    def set_pixel_mask(self, mask) -> None:
+        """Sample only the pixels where `mask` (H, W) is true; None lifts it.
+        Restarts the accumulation."""
+        if mask is None:
+            check(self._lib.pfxt_debug_pixel_mask(self._h, None))
+            return
+        m = np.ascontiguousarray(np.asarray(mask, bool).astype(np.uint8).reshape(self.height, self.width))
+        check(self._lib.pfxt_debug_pixel_mask(self._h, m.ctypes.data))
+
+    def rays_traced(self) -> tuple:
+        """(closest-hit, any-hit) queries traced by the sampling passes so far."""
+        out = np.zeros(2, np.uint64)
+        check(self._lib.pfxt_debug_rays(self._h, out.ctypes.data))
+        return int(out[0]), int(out[1])
+
     def frame(self) -> np.ndarray:
         """The base per-pass uniform (10 x 16 bytes: size, counts, origin, forward,
         right, up, sun_dir, sun_color, lens, window)."""

@@ -69,6 +69,32 @@ def test_room_with_glass_and_metals(gpu):
     assert exact > 0.99
 
 
+@pytest.mark.parametrize("sampler", ["pcg", "sobol"])
+def test_firefly_controls(gpu, sampler):
+    # CLAMP_INDIRECT and FILTER_GLOSSY (trace.wgsl:1872-1875, 2377-2379)
+    w = synth.small("room_4k", (40, 24), sampler=sampler)
+    w.settings = Settings.deep(8, sampler=sampler, sobol_samples=64, filter_glossy=0.25, clamp_indirect=2.0)
+    got, exact = render_both(w, 4, [21])
+    assert exact > 0.99
+
+
+@pytest.mark.parametrize("sampler", ["pcg", "sobol"])
+def test_masked_pixels_match_the_full_frame(gpu, sampler):
+    # a pixel's samples depend on the pixel, the sample index and the seed only
+    w = synth.small("room_4k", (64, 40), sampler=sampler)
+    full = Trace(w.scene, w.settings, w.width, w.height)
+    part = Trace(w.scene, w.settings, w.width, w.height)
+    mask = np.zeros((w.height, w.width), bool)
+    mask[3::5, 2::7] = True
+    part.set_pixel_mask(mask)
+    for seed in (5, 6, 7):
+        full.sample(2, seed)
+        part.sample(2, seed)
+    a, b = full.read_accum(), part.read_accum()
+    assert np.array_equal(a[mask], b[mask])
+    assert not b[~mask].any()
+
+
 def test_furnace_and_determinism(gpu):
     # gpu.rs:3787-3830
     scene = synth.furnace()
