@@ -288,6 +288,95 @@ int pfxt_occluded_device(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count
 int pfxt_occluded_noalloc(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count, uint8_t* blocked,
                           void* stream);
 
+/* ------------------------------------------------------------ radiance cache
+ *
+ * A neural radiance cache: a 16-level hash-grid encoding (2 FP16 features per
+ * level) of the position plus one-blob direction/normal and the surface's
+ * albedos, into an MLP of two 64-wide ReLU layers and an RGB output, BF16
+ * operands on the tensor cores with FP32 accumulation and FP32 master
+ * weights, trained online with Adam.  The reference has no cache: none of
+ * these entry points has a counterpart in pfx.  Attached to a tracer, paths
+ * end into the cache at vertex `query_bounce` (the vertex after that many
+ * scattering events) and a fraction of paths continue to make the training
+ * targets; where the measured bias of the cache in a cell of a 16^3 grid
+ * exceeds `error_bound`, paths continue as plain paths. */
+typedef struct pfxt_cache pfxt_cache;
+
+typedef struct pfxt_cache_settings {
+  uint32_t log2_entries;    /* table entries per level = 2^log2_entries (10..22; 19) */
+  uint32_t base_resolution; /* grid resolution of the coarsest level (16) */
+  uint32_t max_resolution;  /* grid resolution of the finest level (2048) */
+  uint32_t batch;           /* training records per step, a multiple of 128 (65536) */
+  uint32_t steps;           /* training steps per sampling pass, at most (4) */
+  uint32_t seed;            /* parameter initialisation */
+  uint32_t query_bounce;    /* the path vertex that ends into the cache (2) */
+  uint32_t record_bounces;  /* training records from vertices 0..record_bounces (3) */
+  float learning_rate;      /* Adam (1e-2) */
+  float beta1, beta2, epsilon; /* Adam (0.9, 0.99, 1e-15) */
+  float train_fraction;     /* fraction of paths that make training targets (0.01) */
+  float error_bound;        /* relative bias of a cell above which its paths stay plain (0.1) */
+  float lo[3], hi[3];       /* bounds of the grid; pfxt_set_cache sets them to the scene's */
+} pfxt_cache_settings;
+
+/* One cache query (80 B): the hit point and what the network reads of it. */
+typedef struct pfxt_cache_query {
+  float position[3];
+  float roughness;
+  float direction[3];       /* towards the previous vertex (outgoing), unit */
+  float transmission;
+  float normal[3];          /* shading normal, unit */
+  float pad0;
+  float diffuse[3];
+  float pad1;
+  float specular[3];
+  float pad2;
+} pfxt_cache_query;
+
+/* One training record (96 B): a query and the radiance the path carried. */
+typedef struct pfxt_cache_record {
+  pfxt_cache_query query;
+  float target[3];
+  float weight; /* 1 */
+} pfxt_cache_record;
+
+typedef struct pfxt_cache_stats {
+  uint64_t steps;          /* Adam steps taken */
+  float loss;              /* relative L2 loss of the last step */
+  uint32_t records;        /* training records made by the last pass */
+  uint32_t queries;        /* paths that ended into the cache in the last pass */
+  uint32_t training_paths; /* training paths of the last pass */
+  uint32_t cells_ok;       /* cells where paths may end into the cache */
+  uint32_t pad;
+} pfxt_cache_stats;
+
+/* Fills the defaults above. */
+int pfxt_cache_defaults(pfxt_cache_settings* settings);
+/* Creates a cache on the current CUDA device with seeded parameters. */
+int pfxt_cache_create(const pfxt_cache_settings* settings, pfxt_cache** out);
+void pfxt_cache_destroy(pfxt_cache* cache);
+/* Attaches the cache to a tracer (NULL detaches); sets the grid bounds to the
+ * scene's and restarts the accumulation.  The cache must outlive the
+ * attachment and belong to the tracer's device. */
+int pfxt_set_cache(pfxt_trace* trace, pfxt_cache* cache);
+int pfxt_cache_get_stats(pfxt_cache* cache, pfxt_cache_stats* stats);
+/* Network output for `count` queries (host memory): rgb[3 * k + c]. */
+int pfxt_cache_infer(pfxt_cache* cache, const pfxt_cache_query* queries, uint32_t count, float* rgb);
+/* Gradients of the mean relative L2 loss over `count` records (a multiple
+ * of 128) with the current parameters; nothing is updated.  mlp: 9216 floats
+ * (W1 64x64, W2 64x64, W3 16x64, row = output); table: 16 * 2^log2 * 2
+ * floats (NULL skips it); loss: the loss. */
+int pfxt_cache_gradients(pfxt_cache* cache, const pfxt_cache_record* records, uint32_t count, float* mlp,
+                         float* table, float* loss);
+/* count / batch training steps (Adam) over the records in order; loss: the
+ * mean loss of the steps. */
+int pfxt_cache_train(pfxt_cache* cache, const pfxt_cache_record* records, uint32_t count, float* loss);
+/* The FP32 master parameters (layouts as pfxt_cache_gradients); either may be NULL. */
+int pfxt_cache_params(pfxt_cache* cache, float* mlp, float* table);
+int pfxt_cache_set_params(pfxt_cache* cache, const float* mlp, const float* table);
+/* The encoding: per level the position scale and grid resolution, and a bit
+ * mask of the levels indexed densely (the others are hashed). */
+int pfxt_cache_encoding(pfxt_cache* cache, float scales[16], uint32_t resolutions[16], uint32_t* dense);
+
 #ifdef __cplusplus
 }
 #endif

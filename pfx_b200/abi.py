@@ -114,6 +114,19 @@ class Adaptive(C.Structure):
                 ("growth", C.c_float)]
 
 
+class CacheSettings(C.Structure):
+    _fields_ = [("log2_entries", C.c_uint32), ("base_resolution", C.c_uint32), ("max_resolution", C.c_uint32),
+                ("batch", C.c_uint32), ("steps", C.c_uint32), ("seed", C.c_uint32), ("query_bounce", C.c_uint32),
+                ("record_bounces", C.c_uint32), ("learning_rate", C.c_float), ("beta1", C.c_float),
+                ("beta2", C.c_float), ("epsilon", C.c_float), ("train_fraction", C.c_float),
+                ("error_bound", C.c_float), ("lo", f3), ("hi", f3)]
+
+
+class CacheStats(C.Structure):
+    _fields_ = [("steps", C.c_uint64), ("loss", C.c_float), ("records", C.c_uint32), ("queries", C.c_uint32),
+                ("training_paths", C.c_uint32), ("cells_ok", C.c_uint32), ("pad", C.c_uint32)]
+
+
 OK, ERR_INVALID, ERR_REFUSED, ERR_CUDA, ERR_DEVICE = 0, 1, 2, 3, 4
 
 # (name, restype, argtypes) of every exported entry point declared in pfxt.h.
@@ -147,6 +160,18 @@ PROTOTYPES = [
     ("pfxt_trace_rays_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pfxt_occluded_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pfxt_occluded_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("pfxt_cache_defaults", C.c_int, [C.POINTER(CacheSettings)]),
+    ("pfxt_cache_create", C.c_int, [C.POINTER(CacheSettings), C.POINTER(C.c_void_p)]),
+    ("pfxt_cache_destroy", None, [C.c_void_p]),
+    ("pfxt_set_cache", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pfxt_cache_get_stats", C.c_int, [C.c_void_p, C.POINTER(CacheStats)]),
+    ("pfxt_cache_infer", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    ("pfxt_cache_gradients", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_float)]),
+    ("pfxt_cache_train", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_float)]),
+    ("pfxt_cache_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pfxt_cache_set_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pfxt_cache_encoding", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
 ]
 NOALLOC_MAX_RAYS = 1 << 20
 

@@ -36,6 +36,7 @@ SOURCES = [
     ("traverse.cu", EXACT),
     ("tracer.cu", EXACT),
     ("noalloc.cu", EXACT),
+    ("cache.cu", EXACT),
 ]
 
 HEADERS = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [REPO / "include" / "pfxt.h"]

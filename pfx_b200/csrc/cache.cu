@@ -1,0 +1,783 @@
+// Kernels and host side of the neural radiance cache (cache.h).
+//
+// Inference and training run the MLP on the 5th-generation tensor cores:
+// a CTA of 128 threads owns 128 rows (one per thread and per TMEM lane),
+// writes its rows' BF16 operands into shared memory, and one thread issues
+// tcgen05.mma (M = 128, K = 16 per instruction) with the FP32 accumulator in
+// TMEM; the epilogue reads each row back with tcgen05.ld, applies ReLU and
+// writes the next layer's operand.  Training fuses forward, loss, backward
+// and the hash-grid gradient scatter in one kernel; the weight gradients of
+// all the CTA's tiles accumulate in TMEM (dW = dH^T x H, the batch rows as
+// the K dimension, with the activation tiles read MN-major) and are added
+// to the global FP32 gradient once per CTA.  Adam then updates the FP32
+// master copies and rewrites the BF16 weights and the FP16 table.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cache.h"
+#include "pfxt_internal.h"
+#include "tracer.h"
+#include "umma.cuh"
+
+namespace pfxt {
+
+namespace {
+
+constexpr uint32_t WAIT_LIMIT = 1u << 22;  // mbarrier polls before a wait gives up
+constexpr uint32_t ERR_WAIT = 1u;
+
+// Shared memory of the inference kernel (bytes).
+constexpr uint32_t I_X = 0, I_H1 = 16384, I_H2 = 32768, I_W = 49152, I_CTRL = I_W + 18432;
+constexpr uint32_t I_SMEM = 100 * 1024;  // more than used: at most two CTAs (2 x 256 TMEM columns) per SM
+// Shared memory of the training kernel.  dY, dH2 and dH1 are read as M = 128
+// MN-major operands whose rows 64..127 (16..127 for dY) are not data: the
+// 32 KB the descriptor spans from each of them stays inside the allocation,
+// and the accumulator rows they produce are never read.
+constexpr uint32_t T_DY = 0, T_DH2 = 4096, T_DH1 = 20480, T_X = 36864, T_H1 = 53248, T_H2 = 69632, T_W = 86016,
+                   T_CTRL = T_W + 18432;
+constexpr uint32_t T_SMEM = 120 * 1024;  // one CTA (512 TMEM columns) per SM
+static_assert(T_DH1 + 32768 <= T_CTRL, "padded MN-major reads stay inside shared memory");
+// Weight tiles inside the W block: W1 (64 rows), W2 (64 rows), W3 (16 rows).
+constexpr uint32_t W_1 = 0, W_2 = 8192, W_3 = 16384;
+
+constexpr uint32_t ID_F64 = umma::idesc(128, 64, false, false);   // X x W^T, N = 64
+constexpr uint32_t ID_F16 = umma::idesc(128, 16, false, false);   // H2 x W3^T
+constexpr uint32_t ID_B64 = umma::idesc(128, 64, false, true);    // dH x W (B MN-major)
+constexpr uint32_t ID_B32 = umma::idesc(128, 32, false, true);    // dH1 x W1[:, :32]
+constexpr uint32_t ID_DW = umma::idesc(128, 64, true, true);      // dH^T x H
+
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+  return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a)) |
+         ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b)) << 16);
+}
+__device__ __forceinline__ float lo_bf(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float hi_bf(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
+
+// Row r of an R-row tile, `n` columns (a multiple of 8), as BF16.
+template <int N>
+__device__ __forceinline__ void store_row(uint8_t* tile, uint32_t r, uint32_t R, const float* x) {
+#pragma unroll
+  for (int g = 0; g < N / 8; ++g) {
+    uint4 v = make_uint4(pack2(x[8 * g], x[8 * g + 1]), pack2(x[8 * g + 2], x[8 * g + 3]),
+                         pack2(x[8 * g + 4], x[8 * g + 5]), pack2(x[8 * g + 6], x[8 * g + 7]));
+    *reinterpret_cast<uint4*>(tile + ((uint32_t)g * (R >> 3) + (r >> 3)) * 128u + (r & 7u) * 16u) = v;
+  }
+}
+// Zeroes x[c] where row r of the 128-row tile `act` is not positive (ReLU').
+__device__ __forceinline__ void relu_mask(const uint8_t* act, uint32_t r, float* x) {
+#pragma unroll
+  for (int g = 0; g < 8; ++g) {
+    uint4 v = *reinterpret_cast<const uint4*>(act + ((uint32_t)g * 16u + (r >> 3)) * 128u + (r & 7u) * 16u);
+    uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (!(lo_bf(w[j]) > 0.0f)) x[8 * g + 2 * j] = 0.0f;
+      if (!(hi_bf(w[j]) > 0.0f)) x[8 * g + 2 * j + 1] = 0.0f;
+    }
+  }
+}
+
+__device__ __forceinline__ float unit_coord(float p, float lo, float inv) {
+  float u = (p - lo) * inv;
+  return u > 0.0f ? (u < 1.0f ? u : 1.0f) : 0.0f;  // NaN -> 0
+}
+
+__device__ __forceinline__ uint32_t grid_index(const CacheGrid& g, uint32_t l, uint32_t x, uint32_t y, uint32_t z) {
+  uint32_t res = g.resolution[l];
+  uint32_t i = ((g.dense >> l) & 1u) ? x + y * res + z * res * res : (x * 1u) ^ (y * 2654435761u) ^ (z * 805459861u);
+  return i & (g.entries - 1u);
+}
+
+struct Corners {
+  uint32_t ix, iy, iz;
+  float wx, wy, wz;
+};
+__device__ __forceinline__ Corners corners(const CacheGrid& g, uint32_t l, const float u[3]) {
+  float s = g.scale[l];
+  float px = u[0] * s + 0.5f, py = u[1] * s + 0.5f, pz = u[2] * s + 0.5f;
+  float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+  return Corners{(uint32_t)fx, (uint32_t)fy, (uint32_t)fz, px - fx, py - fy, pz - fz};
+}
+__device__ __forceinline__ float corner_weight(const Corners& c, uint32_t k) {
+  float a = (k & 1u) ? c.wx : 1.0f - c.wx;
+  float b = (k & 2u) ? c.wy : 1.0f - c.wy;
+  float d = (k & 4u) ? c.wz : 1.0f - c.wz;
+  return a * b * d;
+}
+
+// Hat-function one-blob encoding of a unit vector, 4 bins per component.
+__device__ __forceinline__ void one_blob(float v, float* out) {
+  float t = (v + 1.0f) * 0.5f * 4.0f;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    float h = 1.0f - fabsf(t - ((float)i + 0.5f));
+    out[i] = h > 0.0f ? h : 0.0f;
+  }
+}
+
+// The 64 network inputs of one query (5 float4: position + roughness,
+// direction + transmission, normal, diffuse, specular).
+__device__ __forceinline__ void encode(const CacheGrid& g, const __half2* __restrict__ table, const float4* q,
+                                       float x[NRC_IN]) {
+  float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4);
+  float u[3] = {unit_coord(a.x, g.lo[0], g.inv_extent[0]), unit_coord(a.y, g.lo[1], g.inv_extent[1]),
+                unit_coord(a.z, g.lo[2], g.inv_extent[2])};
+#pragma unroll
+  for (uint32_t l = 0; l < NRC_LEVELS; ++l) {
+    Corners cn = corners(g, l, u);
+    const __half2* level = table + (size_t)l * g.entries;
+    float2 f[8];
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k)
+      f[k] = __half22float2(__ldg(level + grid_index(g, l, cn.ix + (k & 1u), cn.iy + ((k >> 1) & 1u),
+                                                        cn.iz + (k >> 2))));
+    float f0 = 0.0f, f1 = 0.0f;
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k) {
+      float w = corner_weight(cn, k);
+      f0 = f0 + w * f[k].x;
+      f1 = f1 + w * f[k].y;
+    }
+    x[2 * l] = f0;
+    x[2 * l + 1] = f1;
+  }
+  one_blob(b.x, x + 32);
+  one_blob(b.y, x + 36);
+  one_blob(b.z, x + 40);
+  one_blob(c.x, x + 44);
+  one_blob(c.y, x + 48);
+  one_blob(c.z, x + 52);
+  x[56] = a.w > 0.0f ? (a.w < 1.0f ? a.w : 1.0f) : 0.0f;
+  x[57] = d.x;
+  x[58] = d.y;
+  x[59] = d.z;
+  x[60] = e.x;
+  x[61] = e.y;
+  x[62] = e.z;
+  x[63] = b.w;
+}
+
+// Gradient of the grid features of one query into the FP32 table gradient.
+__device__ __forceinline__ void scatter_grid(const CacheGrid& g, float* __restrict__ table_g, const float4* q,
+                                             const float dx[32]) {
+  float4 a = __ldg(q);
+  float u[3] = {unit_coord(a.x, g.lo[0], g.inv_extent[0]), unit_coord(a.y, g.lo[1], g.inv_extent[1]),
+                unit_coord(a.z, g.lo[2], g.inv_extent[2])};
+#pragma unroll 4
+  for (uint32_t l = 0; l < NRC_LEVELS; ++l) {
+    float g0 = dx[2 * l], g1 = dx[2 * l + 1];
+    if (g0 == 0.0f && g1 == 0.0f) continue;
+    Corners cn = corners(g, l, u);
+    float2* level = reinterpret_cast<float2*>(table_g) + (size_t)l * g.entries;
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k) {
+      float w = corner_weight(cn, k);
+      uint32_t idx = grid_index(g, l, cn.ix + (k & 1u), cn.iy + ((k >> 1) & 1u), cn.iz + (k >> 2));
+      atomicAdd(level + idx, make_float2(w * g0, w * g1));
+    }
+  }
+}
+
+__device__ __forceinline__ void sync_tc() {
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+}
+
+__device__ __forceinline__ void copy_weights(uint8_t* sw, const uint16_t* __restrict__ weights) {
+  const uint4* src = reinterpret_cast<const uint4*>(weights);
+  uint4* dst = reinterpret_cast<uint4*>(sw);
+  for (uint32_t k = threadIdx.x; k < 18432u / 16u; k += blockDim.x) dst[k] = __ldg(src + k);
+}
+
+// End of a tensor-core kernel: after a wait that ran out, flag the error and
+// give the MMAs in flight one more bounded wait before the TMEM is freed.
+__device__ __forceinline__ void finish(bool failed, uint32_t mb, uint32_t phase, uint32_t* error, uint32_t tbase,
+                                       uint32_t cols) {
+  if (failed) {
+    if (threadIdx.x == 0) atomicOr(error, ERR_WAIT);
+    umma::mbar_wait(mb, phase ^ 1u, WAIT_LIMIT);
+  }
+  sync_tc();
+  if ((threadIdx.x >> 5) == 0) umma::tmem_free(tbase, cols);
+}
+
+// Four TMEM loads of 16 columns: this thread's row, columns col..col+63.
+__device__ __forceinline__ void ld64(uint32_t tbase, uint32_t warp, uint32_t col, float x[64]) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    float v[16];
+    umma::ld16(umma::taddr(tbase, 32u * warp, col + 16u * j), v);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[16 * j + k] = v[k];
+  }
+}
+
+// ------------------------------------------------------------------ inference
+__global__ void __launch_bounds__(128, 2)
+    k_infer(CacheGrid g, const __half2* __restrict__ table, const uint16_t* __restrict__ weights,
+            const float4* __restrict__ queries, const uint32_t* __restrict__ n_dev, uint32_t n_max,
+            const uint32_t* __restrict__ scatter, float4* __restrict__ out, uint32_t* error) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + I_CTRL);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + I_CTRL + 8);
+  const uint32_t a_x = umma::smem_addr(smem + I_X), a_h1 = umma::smem_addr(smem + I_H1),
+                 a_h2 = umma::smem_addr(smem + I_H2), a_w = umma::smem_addr(smem + I_W);
+  const uint32_t mb = umma::smem_addr(mbar);
+  copy_weights(smem + I_W, weights);
+  if (tid == 0) umma::mbar_init(mb, 1);
+  if (warp == 0) umma::tmem_alloc(slot, 256);
+  umma::fence_async_smem();
+  sync_tc();
+  const uint32_t tbase = *slot;
+  const uint32_t T0 = tbase, T1 = tbase + 64, T2 = tbase + 128;
+  uint32_t count = n_dev ? min(*n_dev, n_max) : n_max;
+  uint32_t phase = 0;
+  bool late = false;
+  for (uint32_t tile = blockIdx.x; tile * NRC_ROWS < count; tile += gridDim.x) {
+    const uint32_t row = tile * NRC_ROWS + tid;
+    float x[64];
+    if (row < count) {
+      encode(g, table, queries + (size_t)row * 5u, x);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 64; ++k) x[k] = 0.0f;
+    }
+    store_row<64>(smem + I_X, tid, 128, x);
+    umma::fence_async_smem();
+    sync_tc();
+    if (tid == 0) {
+#pragma unroll
+      for (uint32_t s = 0; s < 4; ++s)
+        umma::mma(T0, umma::desc_k(a_x, 128, s), umma::desc_k(a_w + W_1, 64, s), ID_F64, s);
+      umma::commit(mb);
+    }
+    late = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    phase ^= 1u;
+    if (__syncthreads_or(late)) break;
+    umma::fence_after();
+    ld64(tbase, warp, 0, x);
+#pragma unroll
+    for (int k = 0; k < 64; ++k) x[k] = x[k] > 0.0f ? x[k] : 0.0f;
+    store_row<64>(smem + I_H1, tid, 128, x);
+    umma::fence_async_smem();
+    sync_tc();
+    if (tid == 0) {
+#pragma unroll
+      for (uint32_t s = 0; s < 4; ++s)
+        umma::mma(T1, umma::desc_k(a_h1, 128, s), umma::desc_k(a_w + W_2, 64, s), ID_F64, s);
+      umma::commit(mb);
+    }
+    late = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    phase ^= 1u;
+    if (__syncthreads_or(late)) break;
+    umma::fence_after();
+    ld64(tbase, warp, 64, x);
+#pragma unroll
+    for (int k = 0; k < 64; ++k) x[k] = x[k] > 0.0f ? x[k] : 0.0f;
+    store_row<64>(smem + I_H2, tid, 128, x);
+    umma::fence_async_smem();
+    sync_tc();
+    if (tid == 0) {
+#pragma unroll
+      for (uint32_t s = 0; s < 4; ++s)
+        umma::mma(T2, umma::desc_k(a_h2, 128, s), umma::desc_k(a_w + W_3, 16, s), ID_F16, s);
+      umma::commit(mb);
+    }
+    late = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    phase ^= 1u;
+    if (__syncthreads_or(late)) break;
+    umma::fence_after();
+    float y[16];
+    umma::ld16(umma::taddr(tbase, 32u * warp, 128), y);
+    if (row < count) out[scatter ? scatter[row] : row] = make_float4(y[0], y[1], y[2], 0.0f);
+    sync_tc();
+  }
+  finish(late, mb, phase, error, tbase, 256);
+}
+
+// ------------------------------------------------------------------ training
+// Records: 6 float4 (the query's 5, then target rgb + weight).  dY rows are
+// the gradient of mean_rows,channels (y - t)^2 / (y^2 + 0.01) (the
+// denominator held constant), the relative L2 loss of neural radiance caching.
+__global__ void __launch_bounds__(128, 1)
+    k_train(CacheGrid g, const __half2* __restrict__ table, const uint16_t* __restrict__ weights,
+            const float4* __restrict__ records, uint32_t first, uint32_t batch, const uint32_t* __restrict__ ran,
+            float* __restrict__ mlp_g, float* __restrict__ table_g, float* __restrict__ loss,
+            float* __restrict__ cell_stats, uint32_t* error) {
+  if (*ran == 0u) return;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + T_CTRL);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + T_CTRL + 8);
+  const uint32_t a_dy = umma::smem_addr(smem + T_DY), a_dh2 = umma::smem_addr(smem + T_DH2),
+                 a_dh1 = umma::smem_addr(smem + T_DH1), a_x = umma::smem_addr(smem + T_X),
+                 a_h1 = umma::smem_addr(smem + T_H1), a_h2 = umma::smem_addr(smem + T_H2),
+                 a_w = umma::smem_addr(smem + T_W);
+  const uint32_t mb = umma::smem_addr(mbar);
+  copy_weights(smem + T_W, weights);
+  if (tid == 0) umma::mbar_init(mb, 1);
+  if (warp == 0) umma::tmem_alloc(slot, 512);
+  umma::fence_async_smem();
+  sync_tc();
+  const uint32_t tbase = *slot;
+  const uint32_t T0 = tbase, T1 = tbase + 64, T2 = tbase + 128, DW1 = tbase + 192, DW2 = tbase + 256,
+                 DW3 = tbase + 320;
+  const float scale = 1.0f / (3.0f * (float)batch);
+  const uint32_t tiles = batch / NRC_ROWS;
+  uint32_t phase = 0, done = 0;
+  bool failed = false;
+  float loss_sum = 0.0f;
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++done) {
+    const float4* rec = records + ((size_t)first + (size_t)tile * NRC_ROWS + tid) * 6u;
+    float x[64];
+    encode(g, table, rec, x);
+    store_row<64>(smem + T_X, tid, 128, x);
+    umma::fence_async_smem();
+    sync_tc();
+    // forward
+    if (tid == 0) {
+#pragma unroll
+      for (uint32_t s = 0; s < 4; ++s)
+        umma::mma(T0, umma::desc_k(a_x, 128, s), umma::desc_k(a_w + W_1, 64, s), ID_F64, s);
+      umma::commit(mb);
+    }
+    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    phase ^= 1u;
+    if (__syncthreads_or(failed)) { failed = true; break; }
+    umma::fence_after();
+    ld64(tbase, warp, 0, x);
+#pragma unroll
+    for (int k = 0; k < 64; ++k) x[k] = x[k] > 0.0f ? x[k] : 0.0f;
+    store_row<64>(smem + T_H1, tid, 128, x);
+    umma::fence_async_smem();
+    sync_tc();
+    if (tid == 0) {
+#pragma unroll
+      for (uint32_t s = 0; s < 4; ++s)
+        umma::mma(T1, umma::desc_k(a_h1, 128, s), umma::desc_k(a_w + W_2, 64, s), ID_F64, s);
+      umma::commit(mb);
+    }
+    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    phase ^= 1u;
+    if (__syncthreads_or(failed)) { failed = true; break; }
+    umma::fence_after();
+    ld64(tbase, warp, 64, x);
+#pragma unroll
+    for (int k = 0; k < 64; ++k) x[k] = x[k] > 0.0f ? x[k] : 0.0f;
+    store_row<64>(smem + T_H2, tid, 128, x);
+    umma::fence_async_smem();
+    sync_tc();
+    if (tid == 0) {
+#pragma unroll
+      for (uint32_t s = 0; s < 4; ++s)
+        umma::mma(T2, umma::desc_k(a_h2, 128, s), umma::desc_k(a_w + W_3, 16, s), ID_F16, s);
+      umma::commit(mb);
+    }
+    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    phase ^= 1u;
+    if (__syncthreads_or(failed)) { failed = true; break; }
+    umma::fence_after();
+    float y[16];
+    umma::ld16(umma::taddr(tbase, 32u * warp, 128), y);
+    // loss and dY
+    float4 t = __ldg(rec + 5);
+    float target[3] = {t.x, t.y, t.z};
+    float dy[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) dy[k] = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float d = y[c] - target[c];
+      float den = y[c] * y[c] + 0.01f;
+      loss_sum = loss_sum + d * d / den;
+      dy[c] = 2.0f * d / den * scale;
+    }
+    if (cell_stats) {
+      float4 p = __ldg(rec);
+      uint32_t cx = min((uint32_t)(unit_coord(p.x, g.lo[0], g.inv_extent[0]) * (float)NRC_CELLS), NRC_CELLS - 1u);
+      uint32_t cy = min((uint32_t)(unit_coord(p.y, g.lo[1], g.inv_extent[1]) * (float)NRC_CELLS), NRC_CELLS - 1u);
+      uint32_t cz = min((uint32_t)(unit_coord(p.z, g.lo[2], g.inv_extent[2]) * (float)NRC_CELLS), NRC_CELLS - 1u);
+      float* cs = cell_stats + 4u * ((cz * NRC_CELLS + cy) * NRC_CELLS + cx);
+      float py = 0.2126f * fmaxf(y[0], 0.0f) + 0.7152f * fmaxf(y[1], 0.0f) + 0.0722f * fmaxf(y[2], 0.0f);
+      float ty = 0.2126f * target[0] + 0.7152f * target[1] + 0.0722f * target[2];
+      atomicAdd(cs + 0, py - ty);
+      atomicAdd(cs + 1, ty);
+      atomicAdd(cs + 2, 1.0f);
+    }
+    store_row<16>(smem + T_DY, tid, 128, dy);
+    umma::fence_async_smem();
+    sync_tc();
+    // dW3 += dY^T H2 ; dH2 = dY W3
+    if (tid == 0) {
+#pragma unroll
+      for (uint32_t s = 0; s < 8; ++s)
+        umma::mma(DW3, umma::desc_mn(a_dy, 128, s), umma::desc_mn(a_h2, 128, s), ID_DW, (done | s) ? 1u : 0u);
+      umma::mma(T0, umma::desc_k(a_dy, 128, 0), umma::desc_mn(a_w + W_3, 16, 0), ID_B64, 0u);
+      umma::commit(mb);
+    }
+    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    phase ^= 1u;
+    if (__syncthreads_or(failed)) { failed = true; break; }
+    umma::fence_after();
+    ld64(tbase, warp, 0, x);
+    relu_mask(smem + T_H2, tid, x);
+    store_row<64>(smem + T_DH2, tid, 128, x);
+    umma::fence_async_smem();
+    sync_tc();
+    // dW2 += dH2^T H1 ; dH1 = dH2 W2
+    if (tid == 0) {
+#pragma unroll
+      for (uint32_t s = 0; s < 8; ++s)
+        umma::mma(DW2, umma::desc_mn(a_dh2, 128, s), umma::desc_mn(a_h1, 128, s), ID_DW, (done | s) ? 1u : 0u);
+#pragma unroll
+      for (uint32_t s = 0; s < 4; ++s)
+        umma::mma(T1, umma::desc_k(a_dh2, 128, s), umma::desc_mn(a_w + W_2, 64, s), ID_B64, s);
+      umma::commit(mb);
+    }
+    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    phase ^= 1u;
+    if (__syncthreads_or(failed)) { failed = true; break; }
+    umma::fence_after();
+    ld64(tbase, warp, 64, x);
+    relu_mask(smem + T_H1, tid, x);
+    store_row<64>(smem + T_DH1, tid, 128, x);
+    umma::fence_async_smem();
+    sync_tc();
+    // dW1 += dH1^T X ; dX = dH1 W1 (grid features only)
+    if (tid == 0) {
+#pragma unroll
+      for (uint32_t s = 0; s < 8; ++s)
+        umma::mma(DW1, umma::desc_mn(a_dh1, 128, s), umma::desc_mn(a_x, 128, s), ID_DW, (done | s) ? 1u : 0u);
+#pragma unroll
+      for (uint32_t s = 0; s < 4; ++s)
+        umma::mma(T2, umma::desc_k(a_dh1, 128, s), umma::desc_mn(a_w + W_1, 64, s), ID_B32, s);
+      umma::commit(mb);
+    }
+    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    phase ^= 1u;
+    if (__syncthreads_or(failed)) { failed = true; break; }
+    umma::fence_after();
+    float dx[32];
+    {
+      float v[16];
+      umma::ld16(umma::taddr(tbase, 32u * warp, 128), v);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) dx[k] = v[k];
+      umma::ld16(umma::taddr(tbase, 32u * warp, 144), v);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) dx[16 + k] = v[k];
+    }
+    scatter_grid(g, table_g, rec, dx);
+    sync_tc();
+  }
+  // loss: warp sums, one atomic per warp
+  for (int o = 16; o > 0; o >>= 1) loss_sum += __shfl_xor_sync(0xffffffffu, loss_sum, o);
+  if ((tid & 31u) == 0u && loss_sum != 0.0f) atomicAdd(loss, loss_sum);
+  if (!failed && done > 0u && warp < 2u) {
+    // weight gradients: TMEM lanes 0..63 hold the rows of dW1 and dW2 (dW3: lanes 0..2)
+    const uint32_t m = tid;  // output feature
+    float v[64];
+    ld64(tbase, warp, 192, v);
+    for (int k = 0; k < 64; ++k) atomicAdd(mlp_g + NRC_W1 + m * 64u + k, v[k]);
+    ld64(tbase, warp, 256, v);
+    for (int k = 0; k < 64; ++k) atomicAdd(mlp_g + NRC_W2 + m * 64u + k, v[k]);
+    ld64(tbase, warp, 320, v);
+    if (m < 3u)
+      for (int k = 0; k < 64; ++k) atomicAdd(mlp_g + NRC_W3 + m * 64u + k, v[k]);
+  }
+  finish(failed, mb, phase, error, tbase, 512);
+}
+
+// ------------------------------------------------------------------ Adam
+// step[0]: steps taken, step[1]: this step ran; beta_pow: beta1^t, beta2^t.
+__global__ void k_step(const uint32_t* count_dev, uint32_t count, uint32_t need, uint32_t* step, float* beta_pow,
+                       float b1, float b2, uint32_t advance, float* loss) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  uint32_t total = count_dev ? *count_dev : count;
+  uint32_t run = need <= total ? 1u : 0u;
+  step[1] = run;
+  loss[0] = 0.0f;
+  if (run && advance) {
+    step[0] += 1u;
+    beta_pow[0] = beta_pow[0] * b1;
+    beta_pow[1] = beta_pow[1] * b2;
+  }
+}
+
+// Lazy Adam: parameters with a zero gradient keep their value and moments.
+__global__ void k_adam(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v, float* __restrict__ g,
+                       uint32_t n, uint32_t mlp, uint16_t* __restrict__ weights, __half* __restrict__ table16,
+                       const uint32_t* __restrict__ step, const float* __restrict__ beta_pow, float lr, float b1,
+                       float b2, float eps) {
+  if (step[1] == 0u) return;
+  const float c1 = 1.0f - beta_pow[0], c2 = 1.0f - beta_pow[1];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float gi = g[i];
+    if (gi == 0.0f) continue;
+    g[i] = 0.0f;
+    float mi = b1 * m[i] + (1.0f - b1) * gi;
+    float vi = b2 * v[i] + (1.0f - b2) * (gi * gi);
+    m[i] = mi;
+    v[i] = vi;
+    float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    p[i] = pi;
+    if (mlp) {
+      uint32_t base = i < NRC_W2 ? 0u : (i < NRC_W3 ? 4096u : 8192u);
+      uint32_t R = i < NRC_W3 ? 64u : 16u;
+      uint32_t j = i - (i < NRC_W2 ? NRC_W1 : (i < NRC_W3 ? NRC_W2 : NRC_W3));
+      uint32_t off = base + ((j & 63u) >> 3) * (R >> 3) * 64u + ((j >> 6) >> 3) * 64u + ((j >> 6) & 7u) * 8u + (j & 7u);
+      weights[off] = __bfloat16_as_ushort(__float2bfloat16_rn(pi));
+    } else {
+      table16[i] = __float2half_rn(pi);
+    }
+  }
+}
+
+// Rewrites the BF16 weights and the FP16 table from the FP32 masters.
+__global__ void k_copies(const float* __restrict__ mlp, uint16_t* __restrict__ weights, const float* __restrict__ table,
+                         __half* __restrict__ table16, uint32_t table_n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < NRC_MLP + table_n; i += gridDim.x * blockDim.x) {
+    if (i < NRC_MLP) {
+      uint32_t base = i < NRC_W2 ? 0u : (i < NRC_W3 ? 4096u : 8192u);
+      uint32_t R = i < NRC_W3 ? 64u : 16u;
+      uint32_t j = i - (i < NRC_W2 ? NRC_W1 : (i < NRC_W3 ? NRC_W2 : NRC_W3));
+      uint32_t off = base + ((j & 63u) >> 3) * (R >> 3) * 64u + ((j >> 6) >> 3) * 64u + ((j >> 6) & 7u) * 8u + (j & 7u);
+      weights[off] = __bfloat16_as_ushort(__float2bfloat16_rn(mlp[i]));
+    } else {
+      uint32_t k = i - NRC_MLP;
+      table16[k] = __float2half_rn(table[k]);
+    }
+  }
+}
+
+// A cell lets paths end into the cache once it has seen 64 records and the
+// measured relative bias |sum(pred - target)| / sum(target) of the current
+// window is within the bound; the window decays by half each pass.
+__global__ void k_cells(float* __restrict__ stats, uint8_t* __restrict__ ok, float bound) {
+  uint32_t n = NRC_CELLS * NRC_CELLS * NRC_CELLS;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 s = reinterpret_cast<float4*>(stats)[i];
+    bool good = s.z >= 64.0f && fabsf(s.x) <= bound * (s.y + 1e-3f * s.z);
+    ok[i] = good ? 1u : 0u;
+    reinterpret_cast<float4*>(stats)[i] = make_float4(s.x * 0.5f, s.y * 0.5f, s.z * 0.5f, 0.0f);
+  }
+}
+
+void check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  cudaGetLastError();
+  if (e == cudaErrorMemoryAllocation) throw Refused(std::string(what) + ": out of device memory");
+  throw DeviceError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int sm_count() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms > 0 ? sms : 1;
+}
+
+void attributes() {
+  static bool done = false;
+  if (done) return;
+  check(cudaFuncSetAttribute(k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I_SMEM), "cache inference");
+  check(cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T_SMEM), "cache training");
+  done = true;
+}
+
+// PCG32 (O'Neill 2014) for the parameter initialisation.
+struct Pcg {
+  uint64_t state;
+  explicit Pcg(uint64_t seed) : state(seed * 6364136223846793005ull + 1442695040888963407ull) {}
+  uint32_t next() {
+    uint64_t old = state;
+    state = old * 6364136223846793005ull + 1442695040888963407ull;
+    uint32_t xorshifted = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xorshifted >> rot) | (xorshifted << ((32u - rot) & 31u));
+  }
+  float uniform(float a) { return ((float)(next() >> 8) * (1.0f / 16777216.0f) * 2.0f - 1.0f) * a; }
+};
+
+// Beta powers live after the step words.
+float* beta_pow(pfxt_cache& c) { return reinterpret_cast<float*>(c.d_step + 2); }
+
+}  // namespace
+
+void cache_validate(const pfxt_cache_settings& s) {
+  if (s.log2_entries < 10 || s.log2_entries > 22) throw Invalid("cache: log2_entries must be in 10..22");
+  if (s.base_resolution < 2 || s.max_resolution < s.base_resolution || s.max_resolution > (1u << 16))
+    throw Invalid("cache: resolutions must satisfy 2 <= base <= max <= 65536");
+  if (s.batch == 0 || s.batch % NRC_ROWS != 0 || s.batch > (1u << 22))
+    throw Invalid("cache: batch must be a positive multiple of 128, at most 2^22");
+  if (s.steps > 64) throw Invalid("cache: at most 64 steps per pass");
+  if (!(s.learning_rate > 0.0f) || !(s.beta1 >= 0.0f && s.beta1 < 1.0f) || !(s.beta2 >= 0.0f && s.beta2 < 1.0f) ||
+      !(s.epsilon >= 0.0f))
+    throw Invalid("cache: Adam hyper-parameters out of range");
+  if (!(s.train_fraction >= 0.0f && s.train_fraction <= 1.0f)) throw Invalid("cache: train_fraction must be in [0, 1]");
+  if (!(s.error_bound >= 0.0f)) throw Invalid("cache: error_bound must be >= 0");
+  if (s.record_bounces > 15 || s.query_bounce > 15) throw Invalid("cache: bounces above 15");
+  for (int k = 0; k < 3; ++k)
+    if (!(s.hi[k] > s.lo[k]) || !std::isfinite(s.lo[k]) || !std::isfinite(s.hi[k]))
+      throw Invalid("cache: bounds must be finite with hi > lo");
+}
+
+void cache_create(pfxt_cache& c, const pfxt_cache_settings& s) {
+  cache_validate(s);
+  c.s = s;
+  cudaGetDevice(&c.device);
+  attributes();
+  const uint32_t T = 1u << s.log2_entries;
+  c.grid.entries = T;
+  c.grid.dense = 0;
+  double growth = std::exp(std::log((double)s.max_resolution / (double)s.base_resolution) / (double)(NRC_LEVELS - 1));
+  for (uint32_t l = 0; l < NRC_LEVELS; ++l) {
+    double scale = (double)s.base_resolution * std::pow(growth, (double)l) - 1.0;
+    c.grid.scale[l] = (float)scale;
+    uint32_t res = (uint32_t)std::ceil((double)c.grid.scale[l]) + 2u;
+    c.grid.resolution[l] = res;
+    if ((uint64_t)res * res * res <= T) c.grid.dense |= 1u << l;
+  }
+  cache_set_bounds(c, s.lo, s.hi);
+  const size_t table_n = (size_t)NRC_LEVELS * T * 2u;
+  auto alloc = [&](void** p, size_t bytes, const char* what) { check(cudaMalloc(p, bytes), what); };
+  alloc((void**)&c.d_mlp, NRC_MLP * 4u, "cache parameters");
+  alloc((void**)&c.d_mlp_m, NRC_MLP * 4u, "cache parameters");
+  alloc((void**)&c.d_mlp_v, NRC_MLP * 4u, "cache parameters");
+  alloc((void**)&c.d_mlp_g, NRC_MLP * 4u, "cache parameters");
+  alloc((void**)&c.d_weights, 18432u, "cache weights");
+  alloc((void**)&c.d_table, table_n * 4u, "cache table");
+  alloc((void**)&c.d_table_m, table_n * 4u, "cache table");
+  alloc((void**)&c.d_table_v, table_n * 4u, "cache table");
+  alloc((void**)&c.d_table_g, table_n * 4u, "cache table");
+  alloc((void**)&c.d_table16, table_n * 2u, "cache table");
+  const uint32_t cells = NRC_CELLS * NRC_CELLS * NRC_CELLS;
+  alloc((void**)&c.d_cell_ok, cells, "cache cells");
+  alloc((void**)&c.d_cell_stats, cells * 16u, "cache cells");
+  alloc((void**)&c.d_loss, 16, "cache loss");
+  alloc((void**)&c.d_step, 16, "cache step");
+  alloc((void**)&c.d_error, 4, "cache error word");
+  check(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), "cache stream");
+  for (float* p : {c.d_mlp_m, c.d_mlp_v, c.d_mlp_g}) check(cudaMemset(p, 0, NRC_MLP * 4u), "cache reset");
+  for (float* p : {c.d_table_m, c.d_table_v, c.d_table_g}) check(cudaMemset(p, 0, table_n * 4u), "cache reset");
+  check(cudaMemset(c.d_cell_ok, 0, cells), "cache reset");
+  check(cudaMemset(c.d_cell_stats, 0, cells * 16u), "cache reset");
+  check(cudaMemset(c.d_loss, 0, 16), "cache reset");
+  check(cudaMemset(c.d_error, 0, 4), "cache reset");
+  uint32_t step_init[4];
+  float one = 1.0f;
+  step_init[0] = 0;
+  step_init[1] = 0;
+  std::memcpy(&step_init[2], &one, 4);
+  std::memcpy(&step_init[3], &one, 4);
+  check(cudaMemcpy(c.d_step, step_init, 16, cudaMemcpyHostToDevice), "cache step");
+  // Glorot-uniform weights (W3 rows 3..15 stay zero) and a small uniform table.
+  std::vector<float> mlp(NRC_MLP, 0.0f);
+  Pcg rng(0x9e3779b97f4a7c15ull ^ (uint64_t)s.seed);
+  float a_hidden = std::sqrt(6.0f / 128.0f), a_out = std::sqrt(6.0f / 67.0f);
+  for (uint32_t i = 0; i < NRC_W3; ++i) mlp[i] = rng.uniform(a_hidden);
+  for (uint32_t i = 0; i < 3u * NRC_HIDDEN; ++i) mlp[NRC_W3 + i] = rng.uniform(a_out);
+  std::vector<float> table(table_n);
+  for (size_t i = 0; i < table_n; ++i) table[i] = rng.uniform(1e-4f);
+  check(cudaMemcpy(c.d_mlp, mlp.data(), NRC_MLP * 4u, cudaMemcpyHostToDevice), "cache parameters");
+  check(cudaMemcpy(c.d_table, table.data(), table_n * 4u, cudaMemcpyHostToDevice), "cache table");
+  k_copies<<<sm_count() * 4, 256, 0, c.stream>>>(c.d_mlp, c.d_weights, c.d_table, (__half*)c.d_table16,
+                                                  (uint32_t)table_n);
+  check(cudaGetLastError(), "cache copies");
+  check(cudaStreamSynchronize(c.stream), "cache create");
+}
+
+void cache_release(pfxt_cache& c) {
+  for (void* p : {(void*)c.d_mlp, (void*)c.d_mlp_m, (void*)c.d_mlp_v, (void*)c.d_mlp_g, (void*)c.d_weights,
+                  (void*)c.d_table, (void*)c.d_table_m, (void*)c.d_table_v, (void*)c.d_table_g, (void*)c.d_table16,
+                  (void*)c.d_cell_ok, (void*)c.d_cell_stats, (void*)c.d_loss, (void*)c.d_step, (void*)c.d_error,
+                  c.d_stage})
+    if (p) cudaFree(p);
+  if (c.stream) cudaStreamDestroy(c.stream);
+  c.stream = nullptr;
+  c.d_stage = nullptr;
+  c.stage_bytes = 0;
+}
+
+void cache_set_bounds(pfxt_cache& c, const float lo[3], const float hi[3]) {
+  for (int k = 0; k < 3; ++k) {
+    if (!(hi[k] > lo[k]) || !std::isfinite(lo[k]) || !std::isfinite(hi[k]))
+      throw Invalid("cache: bounds must be finite with hi > lo");
+    c.grid.lo[k] = lo[k];
+    c.grid.inv_extent[k] = 1.0f / (hi[k] - lo[k]);
+    c.s.lo[k] = lo[k];
+    c.s.hi[k] = hi[k];
+  }
+}
+
+CacheView cache_view(pfxt_cache& c) {
+  CacheView v;
+  v.grid = c.grid;
+  v.table = c.d_table16;
+  v.weights = c.d_weights;
+  v.cell_ok = c.d_cell_ok;
+  v.cell_stats = c.d_cell_stats;
+  return v;
+}
+
+void cache_infer_launch(pfxt_cache& c, const float4* queries, const uint32_t* n_dev, uint32_t n,
+                        const uint32_t* scatter, float4* out, cudaStream_t stream) {
+  if (n == 0) return;
+  uint32_t tiles = (n + NRC_ROWS - 1) / NRC_ROWS;
+  uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)sm_count() * 2u);
+  k_infer<<<grid, 128, I_SMEM, stream>>>(c.grid, c.d_table16, c.d_weights, queries, n_dev, n, scatter, out,
+                                         c.d_error);
+  check(cudaGetLastError(), "cache inference");
+}
+
+void cache_train_launch(pfxt_cache& c, const float4* records, const uint32_t* count_dev, uint32_t count,
+                        uint32_t first, cudaStream_t stream, bool adam, uint32_t batch) {
+  if (batch == 0) batch = c.s.batch;
+  const uint32_t table_n = NRC_LEVELS * c.grid.entries * 2u;
+  k_step<<<1, 32, 0, stream>>>(count_dev, count, first + batch, c.d_step, beta_pow(c), c.s.beta1, c.s.beta2,
+                               adam ? 1u : 0u, c.d_loss);
+  uint32_t grid = std::min<uint32_t>(batch / NRC_ROWS, (uint32_t)sm_count());
+  k_train<<<grid, 128, T_SMEM, stream>>>(c.grid, c.d_table16, c.d_weights, records, first, batch, c.d_step + 1,
+                                         c.d_mlp_g, c.d_table_g, c.d_loss, adam ? c.d_cell_stats : nullptr,
+                                         c.d_error);
+  check(cudaGetLastError(), "cache training");
+  if (!adam) return;
+  int sms = sm_count();
+  k_adam<<<sms, 256, 0, stream>>>(c.d_mlp, c.d_mlp_m, c.d_mlp_v, c.d_mlp_g, NRC_MLP, 1u, c.d_weights, nullptr,
+                                  c.d_step, beta_pow(c), c.s.learning_rate, c.s.beta1, c.s.beta2, c.s.epsilon);
+  k_adam<<<sms * 8, 256, 0, stream>>>(c.d_table, c.d_table_m, c.d_table_v, c.d_table_g, table_n, 0u, nullptr,
+                                      (__half*)c.d_table16, c.d_step, beta_pow(c), c.s.learning_rate, c.s.beta1,
+                                      c.s.beta2, c.s.epsilon);
+  check(cudaGetLastError(), "cache Adam");
+}
+
+void cache_cells_launch(pfxt_cache& c, cudaStream_t stream) {
+  k_cells<<<16, 256, 0, stream>>>(c.d_cell_stats, c.d_cell_ok, c.s.error_bound);
+  check(cudaGetLastError(), "cache cells");
+}
+
+void cache_check_error(pfxt_cache& c) {
+  uint32_t e = 0;
+  check(cudaMemcpy(&e, c.d_error, 4, cudaMemcpyDeviceToHost), "cache error word");
+  if (e != 0u) {
+    cudaMemset(c.d_error, 0, 4);
+    throw DeviceError("cache: a tensor-core wait ran out of its limit");
+  }
+}
+
+void cache_copies(pfxt_cache& c) {
+  const uint32_t table_n = NRC_LEVELS * c.grid.entries * 2u;
+  k_copies<<<sm_count() * 4, 256, 0, c.stream>>>(c.d_mlp, c.d_weights, c.d_table, (__half*)c.d_table16, table_n);
+  check(cudaGetLastError(), "cache copies");
+}
+
+}  // namespace pfxt

@@ -12,6 +12,7 @@
 #include "pfxt.h"
 #include "pfxt_internal.h"
 #include "tracer.h"
+#include "cache.h"
 
 using namespace pfxt;
 
@@ -399,6 +400,219 @@ int pfxt_films_device(pfxt_trace* t, float** color, float** albedo, float** norm
     if (color) *color = reinterpret_cast<float*>(t->d_color);
     if (albedo) *albedo = reinterpret_cast<float*>(t->d_albedo);
     if (normal) *normal = reinterpret_cast<float*>(t->d_normal);
+  });
+}
+
+/* ------------------------------------------------------------ radiance cache */
+
+int pfxt_cache_defaults(pfxt_cache_settings* s) {
+  return guarded([&]() {
+    if (!s) throw Invalid("null argument");
+    *s = pfxt_cache_settings{};
+    s->log2_entries = 19;
+    s->base_resolution = 16;
+    s->max_resolution = 2048;
+    s->batch = 65536;
+    s->steps = 4;
+    s->seed = 1;
+    s->query_bounce = 2;
+    s->record_bounces = 3;
+    s->learning_rate = 1e-2f;
+    s->beta1 = 0.9f;
+    s->beta2 = 0.99f;
+    s->epsilon = 1e-15f;
+    s->train_fraction = 0.01f;
+    s->error_bound = 0.1f;
+    for (int k = 0; k < 3; ++k) {
+      s->lo[k] = 0.0f;
+      s->hi[k] = 1.0f;
+    }
+  });
+}
+
+int pfxt_cache_create(const pfxt_cache_settings* s, pfxt_cache** out) {
+  return guarded([&]() {
+    if (!s || !out) throw Invalid("null argument");
+    *out = nullptr;
+    cache_validate(*s);
+    ensure_device();
+    auto c = std::make_unique<pfxt_cache>();
+    try {
+      cache_create(*c, *s);
+    } catch (...) {
+      cache_release(*c);
+      throw;
+    }
+    *out = c.release();
+  });
+}
+
+void pfxt_cache_destroy(pfxt_cache* c) {
+  if (!c) return;
+  cache_release(*c);
+  delete c;
+}
+
+int pfxt_set_cache(pfxt_trace* t, pfxt_cache* c) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    check(cudaStreamSynchronize(t->stream), "set cache");
+    if (c) {
+      if (c->device != t->device) throw Invalid("the cache belongs to another device");
+      float lo[3], hi[3];
+      for (int k = 0; k < 3; ++k) {
+        float pad = 1e-3f * (t->bounds_hi[k] - t->bounds_lo[k]) + 1e-4f;
+        lo[k] = t->bounds_lo[k] - pad;
+        hi[k] = t->bounds_hi[k] + pad;
+      }
+      cache_set_bounds(*c, lo, hi);
+    }
+    t->cache = c;
+    t->samples = 0;
+  });
+}
+
+int pfxt_cache_get_stats(pfxt_cache* c, pfxt_cache_stats* out) {
+  return guarded([&]() {
+    if (!c || !out) throw Invalid("null argument");
+    std::lock_guard<std::mutex> g(c->lock);
+    check(cudaStreamSynchronize(c->stream), "cache stats");
+    uint32_t step[2];
+    check(cudaMemcpy(step, c->d_step, 8, cudaMemcpyDeviceToHost), "cache stats");
+    std::vector<uint8_t> ok(NRC_CELLS * NRC_CELLS * NRC_CELLS);
+    check(cudaMemcpy(ok.data(), c->d_cell_ok, ok.size(), cudaMemcpyDeviceToHost), "cache stats");
+    *out = pfxt_cache_stats{};
+    out->steps = step[0];
+    out->loss = c->last_loss;
+    out->records = c->last_records;
+    out->queries = c->last_queries;
+    out->training_paths = c->last_training_paths;
+    for (uint8_t v : ok) out->cells_ok += v;
+  });
+}
+
+namespace {
+// Device staging of the cache's host-buffer entry points.
+char* cache_stage(pfxt_cache& c, size_t bytes) {
+  if (bytes > c.stage_bytes) {
+    if (c.d_stage) cudaFree(c.d_stage);
+    c.d_stage = nullptr;
+    c.stage_bytes = 0;
+    check(cudaMalloc(&c.d_stage, bytes), "cache staging");
+    c.stage_bytes = bytes;
+  }
+  return static_cast<char*>(c.d_stage);
+}
+}  // namespace
+
+int pfxt_cache_infer(pfxt_cache* c, const pfxt_cache_query* q, uint32_t count, float* rgb) {
+  return guarded([&]() {
+    if (!c || (count && (!q || !rgb))) throw Invalid("null argument");
+    if (count == 0) return;
+    std::lock_guard<std::mutex> g(c->lock);
+    size_t qb = (size_t)count * sizeof(pfxt_cache_query);
+    char* d = cache_stage(*c, qb + (size_t)count * 16u);
+    float4* d_out = reinterpret_cast<float4*>(d + qb);
+    check(cudaMemcpyAsync(d, q, qb, cudaMemcpyHostToDevice, c->stream), "cache queries");
+    cache_infer_launch(*c, reinterpret_cast<const float4*>(d), nullptr, count, nullptr, d_out, c->stream);
+    std::vector<float4> out(count);
+    check(cudaMemcpyAsync(out.data(), d_out, (size_t)count * 16u, cudaMemcpyDeviceToHost, c->stream), "cache output");
+    check(cudaStreamSynchronize(c->stream), "cache inference");
+    cache_check_error(*c);
+    for (uint32_t k = 0; k < count; ++k) {
+      rgb[3 * k + 0] = out[k].x;
+      rgb[3 * k + 1] = out[k].y;
+      rgb[3 * k + 2] = out[k].z;
+    }
+  });
+}
+
+int pfxt_cache_gradients(pfxt_cache* c, const pfxt_cache_record* r, uint32_t count, float* mlp, float* table,
+                         float* loss) {
+  return guarded([&]() {
+    if (!c || !r || !mlp) throw Invalid("null argument");
+    if (count == 0 || count % NRC_ROWS != 0 || count > (1u << 22))
+      throw Invalid("records: a positive multiple of 128, at most 2^22");
+    std::lock_guard<std::mutex> g(c->lock);
+    const size_t table_n = (size_t)NRC_LEVELS * c->grid.entries * 2u;
+    size_t rb = (size_t)count * sizeof(pfxt_cache_record);
+    char* d = cache_stage(*c, rb);
+    check(cudaMemsetAsync(c->d_mlp_g, 0, NRC_MLP * 4u, c->stream), "cache gradients");
+    check(cudaMemsetAsync(c->d_table_g, 0, table_n * 4u, c->stream), "cache gradients");
+    check(cudaMemcpyAsync(d, r, rb, cudaMemcpyHostToDevice, c->stream), "cache records");
+    cache_train_launch(*c, reinterpret_cast<const float4*>(d), nullptr, count, 0, c->stream, false, count);
+    check(cudaMemcpyAsync(mlp, c->d_mlp_g, NRC_MLP * 4u, cudaMemcpyDeviceToHost, c->stream), "cache gradients");
+    if (table)
+      check(cudaMemcpyAsync(table, c->d_table_g, table_n * 4u, cudaMemcpyDeviceToHost, c->stream), "cache gradients");
+    float l = 0.0f;
+    check(cudaMemcpyAsync(&l, c->d_loss, 4, cudaMemcpyDeviceToHost, c->stream), "cache loss");
+    check(cudaMemsetAsync(c->d_mlp_g, 0, NRC_MLP * 4u, c->stream), "cache gradients");
+    check(cudaMemsetAsync(c->d_table_g, 0, table_n * 4u, c->stream), "cache gradients");
+    check(cudaStreamSynchronize(c->stream), "cache gradients");
+    cache_check_error(*c);
+    if (loss) *loss = l / (3.0f * (float)count);
+  });
+}
+
+int pfxt_cache_train(pfxt_cache* c, const pfxt_cache_record* r, uint32_t count, float* loss) {
+  return guarded([&]() {
+    if (!c || !r) throw Invalid("null argument");
+    if (count == 0 || count % c->s.batch != 0) throw Invalid("records: a positive multiple of the batch");
+    std::lock_guard<std::mutex> g(c->lock);
+    size_t rb = (size_t)count * sizeof(pfxt_cache_record);
+    char* d = cache_stage(*c, rb);
+    check(cudaMemcpyAsync(d, r, rb, cudaMemcpyHostToDevice, c->stream), "cache records");
+    double sum = 0.0;
+    uint32_t steps = count / c->s.batch;
+    for (uint32_t s = 0; s < steps; ++s) {
+      cache_train_launch(*c, reinterpret_cast<const float4*>(d), nullptr, count, s * c->s.batch, c->stream, true, 0);
+      float l = 0.0f;
+      check(cudaMemcpyAsync(&l, c->d_loss, 4, cudaMemcpyDeviceToHost, c->stream), "cache loss");
+      check(cudaStreamSynchronize(c->stream), "cache training");
+      sum += l / (3.0 * c->s.batch);
+    }
+    cache_check_error(*c);
+    c->last_loss = (float)(sum / steps);
+    if (loss) *loss = c->last_loss;
+  });
+}
+
+int pfxt_cache_params(pfxt_cache* c, float* mlp, float* table) {
+  return guarded([&]() {
+    if (!c) throw Invalid("null argument");
+    std::lock_guard<std::mutex> g(c->lock);
+    check(cudaStreamSynchronize(c->stream), "cache parameters");
+    const size_t table_n = (size_t)NRC_LEVELS * c->grid.entries * 2u;
+    if (mlp) check(cudaMemcpy(mlp, c->d_mlp, NRC_MLP * 4u, cudaMemcpyDeviceToHost), "cache parameters");
+    if (table) check(cudaMemcpy(table, c->d_table, table_n * 4u, cudaMemcpyDeviceToHost), "cache parameters");
+  });
+}
+
+int pfxt_cache_set_params(pfxt_cache* c, const float* mlp, const float* table) {
+  return guarded([&]() {
+    if (!c) throw Invalid("null argument");
+    std::lock_guard<std::mutex> g(c->lock);
+    check(cudaStreamSynchronize(c->stream), "cache parameters");
+    const size_t table_n = (size_t)NRC_LEVELS * c->grid.entries * 2u;
+    if (mlp) {
+      for (uint32_t i = 3u * NRC_HIDDEN; i < NRC_OUT * NRC_HIDDEN; ++i)
+        if (mlp[NRC_W3 + i] != 0.0f) throw Invalid("rows 3..15 of W3 must stay zero");
+      check(cudaMemcpy(c->d_mlp, mlp, NRC_MLP * 4u, cudaMemcpyHostToDevice), "cache parameters");
+    }
+    if (table) check(cudaMemcpy(c->d_table, table, table_n * 4u, cudaMemcpyHostToDevice), "cache parameters");
+    cache_copies(*c);
+    check(cudaStreamSynchronize(c->stream), "cache parameters");
+  });
+}
+
+int pfxt_cache_encoding(pfxt_cache* c, float scales[16], uint32_t resolutions[16], uint32_t* dense) {
+  return guarded([&]() {
+    if (!c) throw Invalid("null argument");
+    for (uint32_t l = 0; l < NRC_LEVELS; ++l) {
+      if (scales) scales[l] = c->grid.scale[l];
+      if (resolutions) resolutions[l] = c->grid.resolution[l];
+    }
+    if (dense) *dense = c->grid.dense;
   });
 }
 }  // extern "C"

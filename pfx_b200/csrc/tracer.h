@@ -116,6 +116,11 @@ struct pfxt_trace {
   void* d_stage = nullptr;      // staging of the host-memory ray entry points
   size_t stage_bytes = 0;
   std::vector<void*> owned;
+  // radiance cache (pfxt_set_cache)
+  float bounds_lo[3] = {0, 0, 0}, bounds_hi[3] = {0, 0, 0};  // world box of the scene root
+  pfxt_cache* cache = nullptr;
+  void* d_cache_scratch = nullptr;  // queries, predictions, training vertices and records
+  size_t cache_scratch_bytes = 0;
 };
 
 namespace pfxt {

@@ -68,6 +68,13 @@ void trace_init(pfxt_trace& t, const pfxt_buffers& b, const pfxt_scene& view, co
   t.view.tris = t.d_tris;
   t.view.insts = t.d_insts;
   t.view.root = layout.root;
+  if (b.nodes_bytes >= sizeof(GpuNode)) {
+    const GpuNode* root = static_cast<const GpuNode*>(b.nodes);
+    for (int k = 0; k < 3; ++k) {
+      t.bounds_lo[k] = root->lo[k];
+      t.bounds_hi[k] = root->hi[k];
+    }
+  }
 
   // ---- shading buffers (reference layouts)
   t.d_triangles = dev_copy(t, b.triangles, b.triangles_bytes, "triangle records");
@@ -214,6 +221,9 @@ void trace_release(pfxt_trace& t) {
   t.d_wave = nullptr;
   if (t.d_stage) cudaFree(t.d_stage);
   t.d_stage = nullptr;
+  if (t.d_cache_scratch) cudaFree(t.d_cache_scratch);
+  t.d_cache_scratch = nullptr;
+  t.cache = nullptr;
   if (t.stream) cudaStreamDestroy(t.stream);
   t.stream = nullptr;
 }
