@@ -15,7 +15,11 @@ events recorded on the tracer's own stream.
                    in x and y (a stratified 480x270 subset of the 4K frame);
                    the error is followed on those pixels alone (their values do
                    not depend on the other pixels) and the time is spp x the
-                   full-frame pass time measured above
+                   full-frame pass time measured above.  The cached tracer
+                   (radiance cache at vertex 2, trained online from an untrained
+                   start) runs full-frame passes; its time is the sum of their
+                   event-timed durations, training included, L2 flushed before
+                   each; relMSE evaluation is outside the timed regions
   roofline         the closest-hit traversal kernel on a batch with the ray mix
                    of one pass (the same traversal code as the tracer's extend
                    kernel): algorithmic bytes 32*box + 36*tri + 48 per ray over
@@ -233,6 +237,51 @@ def plain_convergence(w, mask, mask_idx, ref, max_spp):
     return (curve[-1][0] if reached else None), curve
 
 
+def cache_settings(args):
+    """The radiance cache of the 4K workload: 16 levels x 2^19 entries, 64-wide
+    MLP, 2^16 records per step, 4 steps per pass, paths end at vertex 2."""
+    from pfx_b200.cache import CacheSettings
+    s = CacheSettings()
+    if args.cache_error_bound is not None:
+        s.error_bound = args.cache_error_bound
+    if args.cache_min_roughness is not None:
+        s.min_roughness = args.cache_min_roughness
+    return s
+
+
+def cached_convergence(trace, w, mask_idx, ref, stream, flush, max_spp, cache_settings):
+    """The cached tracer on the full frame from an untrained cache: device time
+    of every sampling pass (online training included, L2 flushed before each),
+    summed until the masked pixels reach the target relMSE."""
+    import torch
+    from pfx_b200.cache import RadianceCache
+    cache = RadianceCache(cache_settings)
+    trace.set_cache(cache)  # restarts the accumulation
+    color = trace.films_device()[0].reshape(-1, 4)
+    elapsed, curve, pass_ms = 0.0, [], []
+    reached = None
+    for p in range(max_spp):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        trace.sample(1, 50_000 + p)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        pass_ms.append(ms)
+        elapsed += ms / 1e3
+        err = relmse(color[mask_idx, :3], ref)
+        curve.append((p + 1, round(elapsed, 3), err))
+        if err <= TARGET_RELMSE:
+            reached = p + 1
+            break
+    stats = cache.stats()
+    trace.set_cache(None)
+    cache.close()
+    return reached, elapsed, statistics.median(pass_ms), curve, stats
+
+
 def traversal_roofline(trace, w, dev, stream, flush):
     """Closest-hit kernel on a one-pass ray mix, timed with events on its stream."""
     import torch
@@ -300,6 +349,9 @@ def main():
     ap.add_argument("--ref-spp", type=int, default=4096)
     ap.add_argument("--stride", type=int, default=8)
     ap.add_argument("--max-spp", type=int, default=2048)
+    ap.add_argument("--max-cached-spp", type=int, default=1024)
+    ap.add_argument("--cache-error-bound", type=float, default=None)
+    ap.add_argument("--cache-min-roughness", type=float, default=None)
     ap.add_argument("--no-relmse", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -405,13 +457,21 @@ def main():
             ref, ref_s = reference_image(w, args, mask, mask_idx)
             spp_plain, curve = plain_convergence(w, mask, mask_idx, ref, args.max_spp)
             pass_s = total_ms / args.steps / 1e3
+            settings = cache_settings(args)
+            spp_c, t_c, pass_c, curve_c, stats = cached_convergence(trace, w, mask_idx, ref, stream, flush,
+                                                                    args.max_cached_spp, settings)
+            plain_s = None if spp_plain is None else spp_plain * pass_s
             line["time_to_relmse"] = {
-                "target": TARGET_RELMSE, "plain_spp": spp_plain,
-                "plain_s": None if spp_plain is None else spp_plain * pass_s, "pass_s": pass_s,
-                "cached_s": None,
+                "target": TARGET_RELMSE, "plain_spp": spp_plain, "plain_s": plain_s, "pass_s": pass_s,
+                "cached_spp": spp_c, "cached_s": t_c if spp_c else None, "cached_pass_s": pass_c / 1e3,
+                "speedup": (plain_s / t_c) if (plain_s and spp_c) else None,
                 "reference": f"{args.ref_spp} spp accumulated in FP64 over every {s}th pixel in x and y "
                              f"({int(mask.sum())} pixels), {ref_s:.1f} s",
-                "plain_curve": [(n, round(e, 5)) for n, e in curve[:: max(1, len(curve) // 12)] + curve[-1:]]}
+                "cache": {k: v for k, v in settings.__dict__.items() if k not in ("lo", "hi")},
+                "cache_stats": stats,
+                "plain_curve": [(n, round(e, 5)) for n, e in curve[:: max(1, len(curve) // 12)] + curve[-1:]],
+                "cached_curve": [(n, t, round(e, 5)) for n, t, e in
+                                 curve_c[:: max(1, len(curve_c) // 12)] + curve_c[-1:]]}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(w)
         print(json.dumps(line))

@@ -314,7 +314,8 @@ typedef struct pfxt_cache_settings {
   float learning_rate;      /* Adam (1e-2) */
   float beta1, beta2, epsilon; /* Adam (0.9, 0.99, 1e-15) */
   float train_fraction;     /* fraction of paths that make training targets (0.01) */
-  float error_bound;        /* relative bias of a cell above which its paths stay plain (0.1) */
+  float error_bound;        /* relative bias of a cell above which its paths stay plain (1) */
+  float min_roughness;      /* a vertex smoother than this, or transmissive, stays plain; 0 = any (0) */
   float lo[3], hi[3];       /* bounds of the grid; pfxt_set_cache sets them to the scene's */
 } pfxt_cache_settings;
 

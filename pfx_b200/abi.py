@@ -119,7 +119,7 @@ class CacheSettings(C.Structure):
                 ("batch", C.c_uint32), ("steps", C.c_uint32), ("seed", C.c_uint32), ("query_bounce", C.c_uint32),
                 ("record_bounces", C.c_uint32), ("learning_rate", C.c_float), ("beta1", C.c_float),
                 ("beta2", C.c_float), ("epsilon", C.c_float), ("train_fraction", C.c_float),
-                ("error_bound", C.c_float), ("lo", f3), ("hi", f3)]
+                ("error_bound", C.c_float), ("min_roughness", C.c_float), ("lo", f3), ("hi", f3)]
 
 
 class CacheStats(C.Structure):

@@ -43,7 +43,8 @@ class CacheSettings:
     beta2: float = 0.99
     epsilon: float = 1e-15
     train_fraction: float = 0.01
-    error_bound: float = 0.1
+    error_bound: float = 1.0
+    min_roughness: float = 0.0
     lo: tuple = (0.0, 0.0, 0.0)
     hi: tuple = (1.0, 1.0, 1.0)
 

@@ -559,16 +559,16 @@ __global__ void k_copies(const float* __restrict__ mlp, uint16_t* __restrict__ w
   }
 }
 
-// A cell lets paths end into the cache once it has seen 64 records and the
+// A cell lets paths end into the cache once it has seen 32 records and the
 // measured relative bias |sum(pred - target)| / sum(target) of the current
-// window is within the bound; the window decays by half each pass.
+// window is within the bound; the window decays by a quarter each pass.
 __global__ void k_cells(float* __restrict__ stats, uint8_t* __restrict__ ok, float bound) {
   uint32_t n = NRC_CELLS * NRC_CELLS * NRC_CELLS;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float4 s = reinterpret_cast<float4*>(stats)[i];
-    bool good = s.z >= 64.0f && fabsf(s.x) <= bound * (s.y + 1e-3f * s.z);
+    bool good = s.z >= 32.0f && fabsf(s.x) <= bound * (s.y + 1e-3f * s.z);
     ok[i] = good ? 1u : 0u;
-    reinterpret_cast<float4*>(stats)[i] = make_float4(s.x * 0.5f, s.y * 0.5f, s.z * 0.5f, 0.0f);
+    reinterpret_cast<float4*>(stats)[i] = make_float4(s.x * 0.75f, s.y * 0.75f, s.z * 0.75f, 0.0f);
   }
 }
 
@@ -625,6 +625,7 @@ void cache_validate(const pfxt_cache_settings& s) {
     throw Invalid("cache: Adam hyper-parameters out of range");
   if (!(s.train_fraction >= 0.0f && s.train_fraction <= 1.0f)) throw Invalid("cache: train_fraction must be in [0, 1]");
   if (!(s.error_bound >= 0.0f)) throw Invalid("cache: error_bound must be >= 0");
+  if (!(s.min_roughness >= 0.0f)) throw Invalid("cache: min_roughness must be >= 0");
   if (s.record_bounces > 15 || s.query_bounce > 15) throw Invalid("cache: bounces above 15");
   for (int k = 0; k < 3; ++k)
     if (!(s.hi[k] > s.lo[k]) || !std::isfinite(s.lo[k]) || !std::isfinite(s.hi[k]))

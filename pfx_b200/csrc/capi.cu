@@ -422,7 +422,7 @@ int pfxt_cache_defaults(pfxt_cache_settings* s) {
     s->beta2 = 0.99f;
     s->epsilon = 1e-15f;
     s->train_fraction = 0.01f;
-    s->error_bound = 0.1f;
+    s->error_bound = 1.0f;
     for (int k = 0; k < 3; ++k) {
       s->lo[k] = 0.0f;
       s->hi[k] = 1.0f;
@@ -459,6 +459,7 @@ int pfxt_set_cache(pfxt_trace* t, pfxt_cache* c) {
     check(cudaStreamSynchronize(t->stream), "set cache");
     if (c) {
       if (c->device != t->device) throw Invalid("the cache belongs to another device");
+      if (c->s.record_bounces > 7) throw Invalid("a tracer records at most vertices 0..7 for the cache");
       float lo[3], hi[3];
       for (int k = 0; k < 3; ++k) {
         float pad = 1e-3f * (t->bounds_hi[k] - t->bounds_lo[k]) + 1e-4f;

@@ -28,6 +28,7 @@
 #include <string>
 #include <vector>
 
+#include "cache.h"
 #include "kernels.h"
 #include "shade.cuh"
 #include "tracer.h"
@@ -45,6 +46,7 @@ constexpr uint32_t F_CARRIED = 0x3u;  // bits 0-1
 constexpr int F_LOBE0 = 2, F_LOBE1 = 9, F_LOBE2 = 16;  // 7 bits each
 constexpr uint32_t F_LAST = 1u << 23, F_THROUGH = 1u << 24, F_LIT = 1u << 25, F_DIFFUSED = 1u << 26;
 constexpr int F_PEND = 27;  // 4 bits: pending light-slot contributions
+constexpr uint32_t F_CACHED = 1u << 31;  // the path ended into the radiance cache
 
 struct Wave {
   float4* ray_o;   // o.xyz, previous pdf
@@ -64,12 +66,32 @@ struct Wave {
   uint32_t* counters;  // 0,1: ray queues, 2: shadow queue, 3: active paths, 4: work counter
 };
 
+// The radiance cache as the wave sees it (all null/zero when none is attached).
+struct CachePass {
+  uint32_t enabled;
+  uint32_t query_bounce;    // paths end into the cache at this vertex
+  uint32_t record_bounces;  // training paths record vertices 0..record_bounces
+  uint32_t threshold;       // a path trains when its 24-bit hash is below this
+  uint32_t tcap, rcap;      // training-path slots, training records
+  float min_roughness;      // smoother (or transmissive) vertices stay plain; 0 = any
+  uint32_t pad;
+  float4* query;            // 5 float4 per query (compact)
+  uint32_t* cqueue;         // path index of each query
+  float4* pred;             // per path: the cache's radiance
+  uint32_t* tslot;          // per path: training slot (low 24 bits) | recorded-vertex mask << 24, ~0 = none
+  float4* tvert;            // per slot and recorded vertex: 5 float4 query, throughput, result so far
+  float4* records;          // 6 float4 per training record
+  const uint8_t* cell_ok;   // fallback cells (NRC_CELLS^3)
+  float lo[3], inv[3];      // grid bounds
+};
+
 struct Pass {
   FrameParams f;
   Specialise sp;
   ShadeView v;
   SceneView s;
   Wave w;
+  CachePass c;
   uint32_t sample;     // sample index inside the pass
   uint32_t bounce;
   uint32_t cap;        // shadow slots per path
@@ -99,6 +121,18 @@ __device__ __forceinline__ void append(uint32_t* queue, uint32_t* count, uint32_
   if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(m));
   base = __shfl_sync(m, base, leader);
   queue[base + (uint32_t)__popc(m & ((1u << lane) - 1u))] = value;
+}
+
+// Warp-aggregated claim of one index from `count`; ~0 for threads that do not want one.
+__device__ __forceinline__ uint32_t claim(uint32_t* count, bool want) {
+  unsigned m = __ballot_sync(__activemask(), want);
+  if (!want) return ~0u;
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+  base = __shfl_sync(m, base, leader);
+  return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
 }
 
 // ------------------------------------------------------------------ active
@@ -161,6 +195,21 @@ __global__ void k_gen(Pass P) {
     P.w.alb[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     P.w.nrm[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     P.w.queue[0][i] = i;
+    if (P.c.enabled) {
+      // training paths: a hash of the pixel and the sample, apart from the
+      // sampler's own sequence, so the chosen paths draw exactly as the others
+      uint32_t h = pcg(stream * 9781u + pcg(P.f.counts[2] * 6529u + absolute * 3571u + 40503u));
+      uint32_t slot = claim(P.w.counters + 6, (h >> 8) < P.c.threshold);
+      P.c.tslot[i] = slot < P.c.tcap ? slot : ~0u;
+    }
+  }
+}
+
+// Before a sample's k_gen: no cache queries and no training slots yet.
+__global__ void k_cache_begin(Pass P) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    P.w.counters[5] = 0u;
+    P.w.counters[6] = 0u;
   }
 }
 
@@ -304,6 +353,56 @@ __device__ __forceinline__ v3 flush_pending(const Pass& P, uint32_t i, uint32_t 
   return result;
 }
 
+// What the radiance cache reads of a shaded hit (5 float4): position and
+// roughness, outgoing direction and transmission, normal, diffuse albedo,
+// specular albedo (F0: 4 % for dielectrics, the base colour for metals).
+__device__ __noinline__ void cache_features(float4* out, v3 p, v3 wo, v3 n, const Shaded& s) {
+  float m = s.metalness, tr = s.transmission;
+  v3 diffuse = scl3(s.base, (1.0f - m) * (1.0f - tr));
+  v3 spec = mix3(splat3(0.04f), s.base, m);
+  out[0] = make_float4(p.x, p.y, p.z, s.roughness);
+  out[1] = make_float4(wo.x, wo.y, wo.z, tr);
+  out[2] = make_float4(n.x, n.y, n.z, 0.0f);
+  out[3] = make_float4(diffuse.x, diffuse.y, diffuse.z, 0.0f);
+  out[4] = make_float4(spec.x, spec.y, spec.z, 0.0f);
+}
+
+// The fallback grid: may a path end into the cache at p?
+__device__ __forceinline__ bool cell_ok(const CachePass& c, v3 p) {
+  float q[3] = {p.x, p.y, p.z};
+  uint32_t cell[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float u = (q[k] - c.lo[k]) * c.inv[k];
+    u = u > 0.0f ? (u < 1.0f ? u : 1.0f) : 0.0f;
+    cell[k] = min((uint32_t)(u * (float)NRC_CELLS), NRC_CELLS - 1u);
+  }
+  return c.cell_ok[(cell[2] * NRC_CELLS + cell[1]) * NRC_CELLS + cell[0]] != 0u;
+}
+
+// Training records of a finished training path: for every recorded vertex,
+// the radiance the path gathered after it, divided by the throughput that
+// reached it (the path's estimate of the vertex's scattered radiance).
+__device__ __noinline__ void emit_records(const float4* __restrict__ tvert, float4* __restrict__ records,
+                                          uint32_t* count, uint32_t rcap, uint32_t vertices, uint32_t ts,
+                                          v3 result) {
+  uint32_t slot = ts & 0xFFFFFFu, mask = ts >> 24;
+  for (uint32_t b = 0; b < vertices; ++b) {
+    if (!((mask >> b) & 1u)) continue;
+    const float4* vtx = tvert + ((size_t)slot * vertices + b) * 7u;
+    float4 T = vtx[5], R = vtx[6];
+    float tx = T.x > 0.0f ? fmaxf(result.x - R.x, 0.0f) / T.x : 0.0f;
+    float ty = T.y > 0.0f ? fmaxf(result.y - R.y, 0.0f) / T.y : 0.0f;
+    float tz = T.z > 0.0f ? fmaxf(result.z - R.z, 0.0f) / T.z : 0.0f;
+    uint32_t k = atomicAdd(count, 1u);
+    if (k >= rcap) return;
+    float4* rec = records + (size_t)k * 6u;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) rec[j] = vtx[j];
+    rec[5] = make_float4(tx, ty, tz, 1.0f);
+  }
+}
+
 // DEFERRED: light-slot shadow rays go through the shadow queue (the usual
 // case); otherwise (more than CAP_MAX light slots) they are traced inline.
 template <bool DEFERRED>
@@ -364,7 +463,27 @@ __global__ void __launch_bounds__(kThreads, 4) k_shade(Pass P, uint32_t which) {
         }
         s.emission = scl3(s.emission, emitter_weight(P, hit, p, origin_point, previous_pdf));
         result = add3(result, capped(P, mul3(throughput, s.emission), bounce > 1u));
-        if (!(flags & F_LAST)) {
+        bool to_cache = false;
+        if (P.c.enabled && !(flags & F_LAST)) {
+          uint32_t ts = P.c.tslot[i];
+          if (ts != ~0u) {
+            if (bounce <= P.c.record_bounces) {
+              float4* vtx = P.c.tvert + ((size_t)(ts & 0xFFFFFFu) * (P.c.record_bounces + 1u) + bounce) * 7u;
+              cache_features(vtx, p, neg3(d), nn, s);
+              vtx[5] = make_float4(throughput.x, throughput.y, throughput.z, 0.0f);
+              vtx[6] = make_float4(result.x, result.y, result.z, 0.0f);
+              P.c.tslot[i] = ts | (1u << (24u + bounce));
+            }
+          } else if (bounce == P.c.query_bounce && cell_ok(P.c, p) &&
+                     (P.c.min_roughness <= 0.0f || (s.roughness >= P.c.min_roughness && !(s.transmission > 0.0f)))) {
+            uint32_t k = claim(P.w.counters + 5, true);
+            cache_features(P.c.query + (size_t)k * 5u, p, neg3(d), nn, s);
+            P.c.cqueue[k] = i;
+            to_cache = true;
+            flags |= F_CACHED;
+          }
+        }
+        if (!(flags & F_LAST) && !to_cache) {
           m3 transform = basis(nn);
           v3 wo = mulmtv(transform, neg3(d));
           v3 origin = spawn_point(p, nn, o, hit.t);
@@ -519,6 +638,17 @@ __global__ void k_finish(Pass P, Accum* __restrict__ accum) {
     float4 rs = P.w.res[i];
     uint32_t flags = __float_as_uint(P.w.ray_d[i].w);
     v3 result = flush_pending(P, i, flags, mk3(rs.x, rs.y, rs.z));
+    if (flags & F_CACHED) {
+      // the cache's radiance at the vertex the path ended at, through its throughput
+      float4 pr = P.c.pred[i], th = P.w.thr[i];
+      v3 radiance = mk3(fmaxf(pr.x, 0.0f), fmaxf(pr.y, 0.0f), fmaxf(pr.z, 0.0f));
+      result = add3(result, capped(P, mul3(mk3(th.x, th.y, th.z), radiance), true));
+    }
+    if (P.c.enabled) {
+      uint32_t ts = P.c.tslot[i];
+      if (ts != ~0u)
+        emit_records(P.c.tvert, P.c.records, P.w.counters + 7, P.c.rcap, P.c.record_bounces + 1u, ts, result);
+    }
     uint32_t pixel = __float_as_uint(rs.w);
     Accum a = accum[pixel];
     float4 al = P.w.alb[i], nr = P.w.nrm[i];
@@ -627,6 +757,52 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
   w.counters = reinterpret_cast<uint32_t*>(b + o_cnt);
 }
 
+// Cache scratch for `pixels` paths: queries, their path indices and
+// predictions, training slots, training vertices and records.
+CachePass ensure_cache(pfxt_trace& t, uint32_t pixels) {
+  CachePass c;
+  memset(&c, 0, sizeof(c));
+  if (!t.cache) return c;
+  pfxt_cache& k = *t.cache;
+  const pfxt_cache_settings& s = k.s;
+  c.enabled = 1u;
+  c.query_bounce = s.query_bounce;
+  c.record_bounces = s.record_bounces;
+  c.threshold = (uint32_t)std::min(16777216.0, (double)s.train_fraction * 16777216.0);
+  c.tcap = std::min<uint32_t>(pixels, (uint32_t)((double)s.train_fraction * pixels * 1.25) + 4096u);
+  c.rcap = s.steps * s.batch;
+  c.min_roughness = s.min_roughness;
+  const uint32_t vertices = s.record_bounces + 1u;
+  size_t need = 0;
+  auto add = [&](size_t bytes) {
+    size_t at = (need + 255) & ~size_t(255);
+    need = at + bytes;
+    return at;
+  };
+  size_t o_q = add(80ull * pixels), o_cq = add(4ull * pixels), o_pred = add(16ull * pixels),
+         o_ts = add(4ull * pixels), o_tv = add(112ull * c.tcap * vertices), o_rec = add(96ull * std::max(c.rcap, 1u));
+  if (need > t.cache_scratch_bytes) {
+    if (t.d_cache_scratch) cudaFree(t.d_cache_scratch);
+    t.d_cache_scratch = nullptr;
+    t.cache_scratch_bytes = 0;
+    check(cudaMalloc(&t.d_cache_scratch, need), "radiance cache scratch");
+    t.cache_scratch_bytes = need;
+  }
+  char* b = static_cast<char*>(t.d_cache_scratch);
+  c.query = reinterpret_cast<float4*>(b + o_q);
+  c.cqueue = reinterpret_cast<uint32_t*>(b + o_cq);
+  c.pred = reinterpret_cast<float4*>(b + o_pred);
+  c.tslot = reinterpret_cast<uint32_t*>(b + o_ts);
+  c.tvert = reinterpret_cast<float4*>(b + o_tv);
+  c.records = reinterpret_cast<float4*>(b + o_rec);
+  c.cell_ok = k.d_cell_ok;
+  for (int j = 0; j < 3; ++j) {
+    c.lo[j] = k.grid.lo[j];
+    c.inv[j] = k.grid.inv_extent[j];
+  }
+  return c;
+}
+
 }  // namespace
 
 static_assert(sizeof(Wave) <= sizeof(((pfxt_trace*)nullptr)->wave_layout), "wave layout storage");
@@ -655,6 +831,7 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   P.slots = slots;
   P.width = t.width;
   P.height = t.height;
+  P.c = ensure_cache(t, pixels);
   Grids& g = grids();
   cudaStream_t st = t.stream;
   if (t.samples == 0) check(cudaMemsetAsync(t.d_accum, 0, (size_t)pixels * sizeof(Accum), st), "accumulation reset");
@@ -662,6 +839,7 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   k_collect<<<g.flat, 256, 0, st>>>(P, t.d_accum, t.d_mask);
   for (uint32_t sample = 0; sample < count; ++sample) {
     P.sample = sample;
+    if (P.c.enabled) k_cache_begin<<<1, 32, 0, st>>>(P);
     k_gen<<<g.flat, 256, 0, st>>>(P);
     k_seed_counts<<<1, 32, 0, st>>>(P);
     for (uint32_t bounce = 0; bounce <= t.spec.total_bounces + 1u; ++bounce) {
@@ -673,6 +851,8 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
         k_shade<true><<<g.shade, kThreads, 0, st>>>(P, cur);
       else
         k_shade<false><<<g.shade_inline, kThreads, 0, st>>>(P, cur);
+      if (P.c.enabled && bounce == P.c.query_bounce)
+        cache_infer_launch(*t.cache, P.c.query, P.w.counters + 5, pixels, P.c.cqueue, P.c.pred, st);
       if (deferred) {
         k_rewind<<<1, 32, 0, st>>>(P);
         k_trace_queue<true><<<g.trace_any, kThreads, 0, st>>>(P, 0u);
@@ -681,8 +861,25 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
     k_finish<<<g.flat, 256, 0, st>>>(P, t.d_accum);
   }
   k_films<<<g.flat, 256, 0, st>>>(P, t.d_accum, t.d_color, t.d_albedo, t.d_normal);
+  if (P.c.enabled) {
+    // online training on this pass's records, then the fallback cells
+    for (uint32_t s = 0; s < t.cache->s.steps; ++s)
+      cache_train_launch(*t.cache, P.c.records, P.w.counters + 7, P.c.rcap, s * t.cache->s.batch, st, true, 0);
+    cache_cells_launch(*t.cache, st);
+  }
   check(cudaGetLastError(), "tracer launch");
   check(cudaStreamSynchronize(st), "tracer pass");
+  if (P.c.enabled) {
+    uint32_t c[3];
+    check(cudaMemcpy(c, P.w.counters + 5, 12, cudaMemcpyDeviceToHost), "cache counters");
+    t.cache->last_queries = c[0];
+    t.cache->last_training_paths = std::min(c[1], P.c.tcap);
+    t.cache->last_records = std::min(c[2], P.c.rcap);
+    float loss = 0.0f;
+    check(cudaMemcpy(&loss, t.cache->d_loss, 4, cudaMemcpyDeviceToHost), "cache loss");
+    t.cache->last_loss = loss / (3.0f * (float)t.cache->s.batch);
+    cache_check_error(*t.cache);
+  }
   t.samples += count;
 }
 

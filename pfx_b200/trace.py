@@ -335,6 +335,13 @@ class Trace:
         shape = (self.height, self.width, 4)
         return [torch.as_tensor(_View(p.value, shape), device="cuda") for p in ptrs]
 
+    def set_cache(self, cache) -> None:
+        """Attach a pfx_b200.cache.RadianceCache (None detaches): paths then end
+        into the cache at its query bounce and a fraction of them train it.
+        Restarts the accumulation; the cache's grid takes the scene's bounds."""
+        check(self._lib.pfxt_set_cache(self._h, None if cache is None else cache.handle))
+        self._cache = cache
+
     def set_pixel_mask(self, mask) -> None:
         """Sample only the pixels where `mask` (H, W) is true; None lifts it.
         Restarts the accumulation."""

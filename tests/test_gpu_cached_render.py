@@ -1,0 +1,53 @@
+"""The tracer with the radiance cache attached.
+
+* With every fallback cell closed (error bound 0) no path ends into the cache:
+  the image must be the plain tracer's bit for bit, while the training paths
+  still feed the cache (training paths are plain paths that also record).
+* With the cache open, paths end into it at the query bounce and the image
+  stays finite and close to the plain one."""
+import numpy as np
+import pytest
+
+from pfx_b200 import synth
+from pfx_b200.cache import CacheSettings, RadianceCache
+from pfx_b200.trace import Trace
+
+pytestmark = pytest.mark.gpu
+
+
+def small_cache(**kw):
+    base = dict(log2_entries=14, base_resolution=8, max_resolution=512, batch=256, steps=2, train_fraction=0.05)
+    base.update(kw)
+    return RadianceCache(CacheSettings(**base))
+
+
+@pytest.mark.parametrize("sampler", ["pcg", "sobol"])
+def test_closed_cells_render_the_plain_image(gpu, sampler):
+    w = synth.small("room_4k", (64, 40), sampler=sampler)
+    plain = Trace(w.scene, w.settings, w.width, w.height)
+    cached = Trace(w.scene, w.settings, w.width, w.height)
+    cache = small_cache(error_bound=0.0)
+    cached.set_cache(cache)
+    for seed in range(4):
+        plain.sample(2, seed)
+        cached.sample(2, seed)
+    assert np.array_equal(plain.read_accum(), cached.read_accum())
+    st = cache.stats()
+    assert st["queries"] == 0 and st["records"] > 0 and st["training_paths"] > 0
+    assert st["steps"] >= 4
+
+
+def test_open_cache_ends_paths(gpu):
+    w = synth.small("room_4k", (64, 40), sampler="sobol")
+    trace = Trace(w.scene, w.settings, w.width, w.height)
+    cache = small_cache(error_bound=1e30, train_fraction=0.5, batch=1024, steps=4)
+    trace.set_cache(cache)
+    for seed in range(24):
+        trace.sample(1, seed)
+    st = cache.stats()
+    assert st["cells_ok"] > 0 and st["queries"] > 0
+    out = trace.readback()
+    assert np.isfinite(out.color).all()
+    trace.set_cache(None)
+    trace.sample(1, 99)
+    assert cache.stats()["queries"] == st["queries"]  # detached: nothing more asked of it
