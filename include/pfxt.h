@@ -297,9 +297,11 @@ int pfxt_occluded_noalloc(pfxt_trace* trace, const pfxt_ray* rays, uint32_t coun
  * weights, trained online with Adam.  The reference has no cache: none of
  * these entry points has a counterpart in pfx.  Attached to a tracer, paths
  * end into the cache at vertex `query_bounce` (the vertex after that many
- * scattering events) and a fraction of paths continue to make the training
- * targets; where the measured bias of the cache in a cell of a 16^3 grid
- * exceeds `error_bound`, paths continue as plain paths. */
+ * scattering events), or at the first vertex after it that is at least
+ * `min_roughness` rough and not transmissive, `delay_bounces` vertices later
+ * at most; a fraction of paths continue to make the training targets; where
+ * the measured bias of the cache in a cell of a 16^3 grid exceeds
+ * `error_bound`, paths continue as plain paths. */
 typedef struct pfxt_cache pfxt_cache;
 
 typedef struct pfxt_cache_settings {
@@ -315,7 +317,8 @@ typedef struct pfxt_cache_settings {
   float beta1, beta2, epsilon; /* Adam (0.9, 0.99, 1e-15) */
   float train_fraction;     /* fraction of paths that make training targets (0.01) */
   float error_bound;        /* relative bias of a cell above which its paths stay plain (1) */
-  float min_roughness;      /* a vertex smoother than this, or transmissive, stays plain; 0 = any (0) */
+  float min_roughness;      /* a vertex smoother than this, or transmissive, does not end a path (0.25) */
+  uint32_t delay_bounces;   /* ... for at most this many vertices after query_bounce (2) */
   float lo[3], hi[3];       /* bounds of the grid; pfxt_set_cache sets them to the scene's */
 } pfxt_cache_settings;
 

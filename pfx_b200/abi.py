@@ -119,7 +119,8 @@ class CacheSettings(C.Structure):
                 ("batch", C.c_uint32), ("steps", C.c_uint32), ("seed", C.c_uint32), ("query_bounce", C.c_uint32),
                 ("record_bounces", C.c_uint32), ("learning_rate", C.c_float), ("beta1", C.c_float),
                 ("beta2", C.c_float), ("epsilon", C.c_float), ("train_fraction", C.c_float),
-                ("error_bound", C.c_float), ("min_roughness", C.c_float), ("lo", f3), ("hi", f3)]
+                ("error_bound", C.c_float), ("min_roughness", C.c_float), ("delay_bounces", C.c_uint32),
+                ("lo", f3), ("hi", f3)]
 
 
 class CacheStats(C.Structure):
@@ -181,6 +182,7 @@ EXTRA = [
     ("pfxt_debug_rays", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pfxt_debug_stream", C.c_void_p, [C.c_void_p]),
     ("pfxt_debug_pixel_mask", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pfxt_debug_sort", C.c_int, [C.c_void_p, C.c_uint32]),
     ("pfxt_trace_counts_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                            C.c_void_p]),
 ]

@@ -37,14 +37,15 @@ class CacheSettings:
     steps: int = 4
     seed: int = 1
     query_bounce: int = 2
-    record_bounces: int = 3
+    record_bounces: int = 4
     learning_rate: float = 1e-2
     beta1: float = 0.9
     beta2: float = 0.99
     epsilon: float = 1e-15
     train_fraction: float = 0.01
     error_bound: float = 1.0
-    min_roughness: float = 0.0
+    min_roughness: float = 0.25
+    delay_bounces: int = 2
     lo: tuple = (0.0, 0.0, 0.0)
     hi: tuple = (1.0, 1.0, 1.0)
 

@@ -626,6 +626,7 @@ void cache_validate(const pfxt_cache_settings& s) {
   if (!(s.train_fraction >= 0.0f && s.train_fraction <= 1.0f)) throw Invalid("cache: train_fraction must be in [0, 1]");
   if (!(s.error_bound >= 0.0f)) throw Invalid("cache: error_bound must be >= 0");
   if (!(s.min_roughness >= 0.0f)) throw Invalid("cache: min_roughness must be >= 0");
+  if (s.delay_bounces > 4) throw Invalid("cache: delay_bounces above 4");
   if (s.record_bounces > 15 || s.query_bounce > 15) throw Invalid("cache: bounces above 15");
   for (int k = 0; k < 3; ++k)
     if (!(s.hi[k] > s.lo[k]) || !std::isfinite(s.lo[k]) || !std::isfinite(s.hi[k]))

@@ -365,6 +365,15 @@ int pfxt_debug_rays(pfxt_trace* t, uint64_t* out) {
  * the stream the passes run on. */
 void* pfxt_debug_stream(pfxt_trace* t) { return t ? (void*)t->stream : nullptr; }
 
+/* Turn the per-bounce material sort of the shade queue on (1, the default) or
+ * off (0); the image does not change, only the time. */
+int pfxt_debug_sort(pfxt_trace* t, uint32_t on) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    t->sort_shading = on != 0u;
+  });
+}
+
 /* Restrict sampling to the pixels whose mask byte is non-zero (width*height
  * host bytes), or lift the restriction with NULL.  A measurement aid: it lets a
  * high-sample reference be accumulated on a stratified subset of a large film.
@@ -416,7 +425,9 @@ int pfxt_cache_defaults(pfxt_cache_settings* s) {
     s->steps = 4;
     s->seed = 1;
     s->query_bounce = 2;
-    s->record_bounces = 3;
+    s->record_bounces = 4;
+    s->min_roughness = 0.25f;
+    s->delay_bounces = 2;
     s->learning_rate = 1e-2f;
     s->beta1 = 0.9f;
     s->beta2 = 0.99f;

@@ -64,6 +64,11 @@ struct Wave {
   uint32_t* squeue;
   uint32_t* active;
   uint32_t* counters;  // 0,1: ray queues, 2: shadow queue, 3: active paths, 4: work counter
+  // shade queue sorted by hit material (counting sort per bounce)
+  uint32_t* keys;      // per queue entry: material key
+  uint32_t* sorted;    // the queue, grouped by key
+  uint32_t* hist;      // SORT_BINS: paths per key
+  uint32_t* cursor;    // SORT_BINS: entries handed out per key
 };
 
 // The radiance cache as the wave sees it (all null/zero when none is attached).
@@ -73,8 +78,8 @@ struct CachePass {
   uint32_t record_bounces;  // training paths record vertices 0..record_bounces
   uint32_t threshold;       // a path trains when its 24-bit hash is below this
   uint32_t tcap, rcap;      // training-path slots, training records
-  float min_roughness;      // smoother (or transmissive) vertices stay plain; 0 = any
-  uint32_t pad;
+  float min_roughness;      // smoother (or transmissive) vertices do not end paths; 0 = any
+  uint32_t query_last;      // the last vertex a path may end into the cache at
   float4* query;            // 5 float4 per query (compact)
   uint32_t* cqueue;         // path index of each query
   float4* pred;             // per path: the cache's radiance
@@ -99,6 +104,7 @@ struct Pass {
   uint32_t light_rows;
   uint32_t slots;      // 2 + light_slots()
   uint32_t width, height;
+  uint32_t bins;       // material keys + 1 (misses); 0 = the shade queue is not sorted
 };
 
 __device__ __forceinline__ uint32_t lobe_count(uint32_t f, int shift) { return (f >> shift) & 127u; }
@@ -230,6 +236,86 @@ __global__ void k_reset(Pass P, uint32_t cur) {
     P.w.counters[2] = 0u;
     P.w.counters[4] = 0u;
     reinterpret_cast<unsigned long long*>(P.w.counters + 8)[0] += P.w.counters[cur];
+  }
+  if (blockIdx.x == 0)
+    for (uint32_t b = threadIdx.x; b < P.bins; b += blockDim.x) {
+      P.w.hist[b] = 0u;
+      P.w.cursor[b] = 0u;
+    }
+}
+
+// ------------------------------------------------------------------ sort
+// The shade queue grouped by the material of each path's hit (misses last),
+// so that the warps of the shade kernel run one BSDF's code.  A counting
+// sort: block histograms into the global one, then every block reserves a
+// range per key and places its entries with shared-memory atomics.  The
+// order inside a key is arbitrary; no result depends on it.
+constexpr uint32_t SORT_BINS = 1024;
+
+__device__ __forceinline__ uint32_t material_key(const Pass& P, uint32_t i) {
+  float4 h = P.w.hit[i];
+  if (h.x >= 1e19f) return P.bins - 1u;
+  uint32_t surface = __float_as_uint(h.y), record = __float_as_uint(h.z);
+  uint4 info = __ldg(reinterpret_cast<const uint4*>(P.v.surfaces + record) + 4);
+  uint32_t material = info.y == NO_MATERIAL
+                          ? f2u(__ldg(reinterpret_cast<const float*>(P.v.triangles + surface) + 3))
+                          : info.y;
+  return min(material, P.bins - 2u);
+}
+
+// This block's share [first, last) of n queue entries.
+__device__ __forceinline__ void block_chunk(uint32_t n, uint32_t& first, uint32_t& last) {
+  uint32_t per = (n + gridDim.x - 1u) / gridDim.x;
+  first = min(n, blockIdx.x * per);
+  last = min(n, first + per);
+}
+
+__global__ void __launch_bounds__(256) k_sort_count(Pass P, uint32_t which) {
+  __shared__ uint32_t hist[SORT_BINS];
+  const uint32_t n = P.w.counters[which];
+  const uint32_t* queue = P.w.queue[which];
+  for (uint32_t b = threadIdx.x; b < P.bins; b += blockDim.x) hist[b] = 0u;
+  __syncthreads();
+  uint32_t first, last;
+  block_chunk(n, first, last);
+  for (uint32_t q = first + threadIdx.x; q < last; q += blockDim.x) {
+    uint32_t key = material_key(P, queue[q]);
+    P.w.keys[q] = key;
+    atomicAdd(&hist[key], 1u);
+  }
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b < P.bins; b += blockDim.x)
+    if (hist[b]) atomicAdd(P.w.hist + b, hist[b]);
+}
+
+__global__ void __launch_bounds__(256) k_sort_place(Pass P, uint32_t which) {
+  __shared__ uint32_t base[SORT_BINS];
+  __shared__ uint32_t local[SORT_BINS];
+  const uint32_t n = P.w.counters[which];
+  const uint32_t* queue = P.w.queue[which];
+  // exclusive scan of the global histogram (one thread: the bins are few)
+  if (threadIdx.x == 0) {
+    uint32_t run = 0u;
+    for (uint32_t b = 0; b < P.bins; ++b) {
+      base[b] = run;
+      run += P.w.hist[b];
+    }
+  }
+  for (uint32_t b = threadIdx.x; b < P.bins; b += blockDim.x) local[b] = 0u;
+  __syncthreads();
+  uint32_t first, last;
+  block_chunk(n, first, last);
+  for (uint32_t q = first + threadIdx.x; q < last; q += blockDim.x) atomicAdd(&local[P.w.keys[q]], 1u);
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b < P.bins; b += blockDim.x) {
+    uint32_t c = local[b];
+    base[b] += c ? atomicAdd(P.w.cursor + b, c) : 0u;
+    local[b] = 0u;
+  }
+  __syncthreads();
+  for (uint32_t q = first + threadIdx.x; q < last; q += blockDim.x) {
+    uint32_t key = P.w.keys[q];
+    P.w.sorted[base[key] + atomicAdd(&local[key], 1u)] = queue[q];
   }
 }
 __global__ void k_rewind(Pass P) {
@@ -408,7 +494,7 @@ __device__ __noinline__ void emit_records(const float4* __restrict__ tvert, floa
 template <bool DEFERRED>
 __global__ void __launch_bounds__(kThreads, 4) k_shade(Pass P, uint32_t which) {
   const uint32_t n = P.w.counters[which];
-  const uint32_t* queue = P.w.queue[which];
+  const uint32_t* queue = P.bins ? P.w.sorted : P.w.queue[which];
   uint32_t* next_queue = P.w.queue[which ^ 1u];
   uint32_t* next_count = P.w.counters + (which ^ 1u);
   const uint32_t bounce = P.bounce;
@@ -474,8 +560,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_shade(Pass P, uint32_t which) {
               vtx[6] = make_float4(result.x, result.y, result.z, 0.0f);
               P.c.tslot[i] = ts | (1u << (24u + bounce));
             }
-          } else if (bounce == P.c.query_bounce && cell_ok(P.c, p) &&
-                     (P.c.min_roughness <= 0.0f || (s.roughness >= P.c.min_roughness && !(s.transmission > 0.0f)))) {
+          } else if (bounce >= P.c.query_bounce && bounce <= P.c.query_last && cell_ok(P.c, p) &&
+                     (bounce == P.c.query_last || P.c.min_roughness <= 0.0f ||
+                      (s.roughness >= P.c.min_roughness && !(s.transmission > 0.0f)))) {
             uint32_t k = claim(P.w.counters + 5, true);
             cache_features(P.c.query + (size_t)k * 5u, p, neg3(d), nn, s);
             P.c.cqueue[k] = i;
@@ -726,7 +813,8 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
          o_hit = add(16ull * capacity), o_hitv = add(4ull * capacity), o_sho = add(16ull * capacity * cap),
          o_shd = add(16ull * capacity * cap), o_shc = add(16ull * capacity * cap), o_q0 = add(4ull * capacity),
          o_q1 = add(4ull * capacity), o_sq = add(4ull * capacity * cap), o_act = add(4ull * capacity),
-         o_cnt = add(64);
+         o_cnt = add(64), o_keys = add(4ull * capacity), o_sorted = add(4ull * capacity),
+         o_hist = add(4ull * SORT_BINS), o_cursor = add(4ull * SORT_BINS);
   if (need > t.wave_bytes) {
     if (t.d_wave) cudaFree(t.d_wave);
     t.d_wave = nullptr;
@@ -755,6 +843,10 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
   w.squeue = reinterpret_cast<uint32_t*>(b + o_sq);
   w.active = reinterpret_cast<uint32_t*>(b + o_act);
   w.counters = reinterpret_cast<uint32_t*>(b + o_cnt);
+  w.keys = reinterpret_cast<uint32_t*>(b + o_keys);
+  w.sorted = reinterpret_cast<uint32_t*>(b + o_sorted);
+  w.hist = reinterpret_cast<uint32_t*>(b + o_hist);
+  w.cursor = reinterpret_cast<uint32_t*>(b + o_cursor);
 }
 
 // Cache scratch for `pixels` paths: queries, their path indices and
@@ -772,6 +864,10 @@ CachePass ensure_cache(pfxt_trace& t, uint32_t pixels) {
   c.tcap = std::min<uint32_t>(pixels, (uint32_t)((double)s.train_fraction * pixels * 1.25) + 4096u);
   c.rcap = s.steps * s.batch;
   c.min_roughness = s.min_roughness;
+  // the inference runs after the shade of bounce query_last, which the bounce loop must reach
+  c.query_last = std::min(s.query_bounce + (s.min_roughness > 0.0f ? s.delay_bounces : 0u),
+                          t.spec.total_bounces + 1u);
+  c.query_bounce = std::min(c.query_bounce, c.query_last);
   const uint32_t vertices = s.record_bounces + 1u;
   size_t need = 0;
   auto add = [&](size_t bytes) {
@@ -832,6 +928,7 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   P.width = t.width;
   P.height = t.height;
   P.c = ensure_cache(t, pixels);
+  P.bins = t.sort_shading ? std::max<uint32_t>(std::min<uint32_t>(t.shade.material_count + 1u, SORT_BINS), 2u) : 0u;
   Grids& g = grids();
   cudaStream_t st = t.stream;
   if (t.samples == 0) check(cudaMemsetAsync(t.d_accum, 0, (size_t)pixels * sizeof(Accum), st), "accumulation reset");
@@ -847,11 +944,15 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
       P.bounce = bounce;
       k_reset<<<1, 32, 0, st>>>(P, cur);
       k_trace_queue<false><<<g.trace_closest, kThreads, 0, st>>>(P, cur);
+      if (P.bins) {
+        k_sort_count<<<g.flat, 256, 0, st>>>(P, cur);
+        k_sort_place<<<g.flat, 256, 0, st>>>(P, cur);
+      }
       if (deferred)
         k_shade<true><<<g.shade, kThreads, 0, st>>>(P, cur);
       else
         k_shade<false><<<g.shade_inline, kThreads, 0, st>>>(P, cur);
-      if (P.c.enabled && bounce == P.c.query_bounce)
+      if (P.c.enabled && bounce == P.c.query_last)
         cache_infer_launch(*t.cache, P.c.query, P.w.counters + 5, pixels, P.c.cqueue, P.c.pred, st);
       if (deferred) {
         k_rewind<<<1, 32, 0, st>>>(P);

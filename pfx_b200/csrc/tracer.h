@@ -110,6 +110,7 @@ struct pfxt_trace {
   uint32_t light_rows = 0;                     // rows of the light buffer (lights + tree)
   uint32_t* wave_counters = nullptr;           // queue counters and ray totals inside d_wave
   uint8_t* d_mask = nullptr;                   // optional per-pixel mask of the pixels to sample
+  bool sort_shading = true;                    // group the shade queue by material every bounce
   uint32_t* d_error = nullptr;  // device error word
   uint32_t* d_counters = nullptr;  // ring of work-sharing counters (device scratch)
   uint32_t counter_slot = 0;

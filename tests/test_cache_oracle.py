@@ -86,7 +86,7 @@ def test_bf16_rounding_is_nearest_even():
 
 def test_records_are_the_abi_layout():
     assert QUERY.itemsize == 80 and RECORD.itemsize == 96
-    assert C.sizeof(abi.CacheSettings) == 4 * 21
+    assert C.sizeof(abi.CacheSettings) == 4 * 22
     assert C.sizeof(abi.CacheStats) == 32
 
 
