@@ -104,8 +104,21 @@ struct Pass {
   uint32_t light_rows;
   uint32_t slots;      // 2 + light_slots()
   uint32_t width, height;
-  uint32_t bins;       // material keys + 1 (misses); 0 = the shade queue is not sorted
+  uint32_t bins;       // 2 x (material keys + 1 for misses); 0 = the shade queue is not sorted
 };
+
+// The fallback grid: may a path end into the cache at p?
+__device__ __forceinline__ bool cell_ok(const CachePass& c, v3 p) {
+  float q[3] = {p.x, p.y, p.z};
+  uint32_t cell[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float u = (q[k] - c.lo[k]) * c.inv[k];
+    u = u > 0.0f ? (u < 1.0f ? u : 1.0f) : 0.0f;
+    cell[k] = min((uint32_t)(u * (float)NRC_CELLS), NRC_CELLS - 1u);
+  }
+  return c.cell_ok[(cell[2] * NRC_CELLS + cell[1]) * NRC_CELLS + cell[0]] != 0u;
+}
 
 __device__ __forceinline__ uint32_t lobe_count(uint32_t f, int shift) { return (f >> shift) & 127u; }
 
@@ -246,21 +259,40 @@ __global__ void k_reset(Pass P, uint32_t cur) {
 
 // ------------------------------------------------------------------ sort
 // The shade queue grouped by the material of each path's hit (misses last),
-// so that the warps of the shade kernel run one BSDF's code.  A counting
-// sort: block histograms into the global one, then every block reserves a
-// range per key and places its entries with shared-memory atomics.  The
-// order inside a key is arbitrary; no result depends on it.
+// so that the warps of the shade kernel run one BSDF's code; at the vertices
+// where paths may end into the radiance cache, the paths that will continue
+// are further grouped apart from those that will end.  A counting sort:
+// block histograms into the global one, then every block reserves a range
+// per key and places its entries with shared-memory atomics.  The order
+// inside a key is arbitrary and the key only orders: the shade kernel makes
+// every decision itself, so no result depends on it.
 constexpr uint32_t SORT_BINS = 1024;
 
+// Key 2 * material + (1 if the path continues past a cache vertex).
 __device__ __forceinline__ uint32_t material_key(const Pass& P, uint32_t i) {
   float4 h = P.w.hit[i];
-  if (h.x >= 1e19f) return P.bins - 1u;
+  if (h.x >= 1e19f) return P.bins - 2u;
   uint32_t surface = __float_as_uint(h.y), record = __float_as_uint(h.z);
   uint4 info = __ldg(reinterpret_cast<const uint4*>(P.v.surfaces + record) + 4);
   uint32_t material = info.y == NO_MATERIAL
                           ? f2u(__ldg(reinterpret_cast<const float*>(P.v.triangles + surface) + 3))
                           : info.y;
-  return min(material, P.bins - 2u);
+  material = min(material, P.bins / 2u - 2u);
+  uint32_t cont = 0u;
+  if (P.c.enabled && P.bounce >= P.c.query_bounce && P.bounce <= P.c.query_last) {
+    cont = P.c.tslot[i] != ~0u ? 1u : 0u;
+    if (!cont) {
+      float4 o = P.w.ray_o[i], d = P.w.ray_d[i];
+      cont = cell_ok(P.c, add3(mk3(o.x, o.y, o.z), scl3(mk3(d.x, d.y, d.z), h.x))) ? 0u : 1u;
+      if (!cont && P.bounce < P.c.query_last && P.c.min_roughness > 0.0f) {
+        const float4* row = P.v.materials + (size_t)(material + 1u) * 8u;
+        float rough = fmax_(__ldg(row).w, 0.05f);
+        if (P.sp.filter_glossy > 0.0f && (__float_as_uint(d.w) & F_DIFFUSED)) rough = fmax_(rough, P.sp.filter_glossy);
+        cont = (rough >= P.c.min_roughness && !(__ldg(row + 2).y > 0.0f)) ? 0u : 1u;
+      }
+    }
+  }
+  return 2u * material + cont;
 }
 
 // This block's share [first, last) of n queue entries.
@@ -451,19 +483,6 @@ __device__ __noinline__ void cache_features(float4* out, v3 p, v3 wo, v3 n, cons
   out[2] = make_float4(n.x, n.y, n.z, 0.0f);
   out[3] = make_float4(diffuse.x, diffuse.y, diffuse.z, 0.0f);
   out[4] = make_float4(spec.x, spec.y, spec.z, 0.0f);
-}
-
-// The fallback grid: may a path end into the cache at p?
-__device__ __forceinline__ bool cell_ok(const CachePass& c, v3 p) {
-  float q[3] = {p.x, p.y, p.z};
-  uint32_t cell[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    float u = (q[k] - c.lo[k]) * c.inv[k];
-    u = u > 0.0f ? (u < 1.0f ? u : 1.0f) : 0.0f;
-    cell[k] = min((uint32_t)(u * (float)NRC_CELLS), NRC_CELLS - 1u);
-  }
-  return c.cell_ok[(cell[2] * NRC_CELLS + cell[1]) * NRC_CELLS + cell[0]] != 0u;
 }
 
 // Training records of a finished training path: for every recorded vertex,
@@ -928,7 +947,8 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   P.width = t.width;
   P.height = t.height;
   P.c = ensure_cache(t, pixels);
-  P.bins = t.sort_shading ? std::max<uint32_t>(std::min<uint32_t>(t.shade.material_count + 1u, SORT_BINS), 2u) : 0u;
+  P.bins = t.sort_shading ? 2u * std::max<uint32_t>(std::min<uint32_t>(t.shade.material_count + 1u, SORT_BINS / 2u), 2u)
+                          : 0u;
   Grids& g = grids();
   cudaStream_t st = t.stream;
   if (t.samples == 0) check(cudaMemsetAsync(t.d_accum, 0, (size_t)pixels * sizeof(Accum), st), "accumulation reset");
