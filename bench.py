@@ -62,12 +62,17 @@ def peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic(kernel: str):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary."""
+def ncu_traffic(kernel: str, rays: int):
+    """DRAM bytes (read + write) of one launch of `kernel` over `rays` rays: the
+    committed ncu capture's bytes scaled linearly by rays (an upper bound: the
+    scene's L2 misses do not grow with the ray count)."""
     p = ROOT / "profiles" / "traffic.json"
     if not p.exists():
         return None
-    return json.loads(p.read_text()).get(kernel)
+    e = json.loads(p.read_text()).get(kernel)
+    if not e:
+        return None
+    return e["dram_bytes"] * rays / e["captured_rays"]
 
 
 class Clocks:
@@ -313,7 +318,7 @@ def traversal_roofline(trace, w, dev, stream, flush):
     achieved = algorithmic / launch_s / 1e9
     return {"bound": "hbm", "kernel": "k_trace<0>: closest-hit traversal (the extend kernel's walk)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": kind,
-            "traffic": ncu_traffic("k_trace<0>"), "algorithmic_bytes_per_launch": algorithmic,
+            "traffic": ncu_traffic("k_trace<0>", n), "algorithmic_bytes_per_launch": algorithmic,
             "rays_per_launch": n, "box_tests_per_ray": c[0] / n, "triangle_tests_per_ray": c[1] / n,
             "launch_ms": statistics.mean(ms), "Mrays_s": n / launch_s / 1e6}
 
