@@ -183,6 +183,8 @@ EXTRA = [
     ("pfxt_debug_stream", C.c_void_p, [C.c_void_p]),
     ("pfxt_debug_pixel_mask", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pfxt_debug_sort", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("pfxt_debug_graphs", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("pfxt_debug_graph_captures", C.c_uint32, [C.c_void_p]),
     ("pfxt_trace_counts_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                            C.c_void_p]),
 ]

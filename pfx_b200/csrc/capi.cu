@@ -374,6 +374,18 @@ int pfxt_debug_sort(pfxt_trace* t, uint32_t on) {
   });
 }
 
+/* Replay each sampling pass from a captured CUDA graph (1, the default) or
+ * launch its kernels one by one (0); the image does not change. */
+int pfxt_debug_graphs(pfxt_trace* t, uint32_t on) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    t->use_graphs = on != 0u;
+  });
+}
+
+/* How many sampling passes have been captured as graphs so far. */
+uint32_t pfxt_debug_graph_captures(pfxt_trace* t) { return t ? t->graph_captures : 0u; }
+
 /* Restrict sampling to the pixels whose mask byte is non-zero (width*height
  * host bytes), or lift the restriction with NULL.  A measurement aid: it lets a
  * high-sample reference be accumulated on a stratified subset of a large film.
@@ -479,6 +491,7 @@ int pfxt_set_cache(pfxt_trace* t, pfxt_cache* c) {
       }
       cache_set_bounds(*c, lo, hi);
     }
+    trace_forget_graphs(*t);
     t->cache = c;
     t->samples = 0;
   });

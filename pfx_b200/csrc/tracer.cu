@@ -105,7 +105,15 @@ struct Pass {
   uint32_t slots;      // 2 + light_slots()
   uint32_t width, height;
   uint32_t bins;       // 2 x (material keys + 1 for misses); 0 = the shade queue is not sorted
+  // What changes from pass to pass lives in device memory, written by the
+  // pass's first operation, so one captured pass replays for every pass:
+  // [0] samples accumulated before the pass, [1] samples in it, [2] seed.
+  const uint32_t* vars;
 };
+
+__device__ __forceinline__ uint32_t pass_accum(const Pass& P) { return __ldg(P.vars + 0); }
+__device__ __forceinline__ uint32_t pass_count(const Pass& P) { return __ldg(P.vars + 1); }
+__device__ __forceinline__ uint32_t pass_seed(const Pass& P) { return __ldg(P.vars + 2); }
 
 // The fallback grid: may a path end into the cache at p?
 __device__ __forceinline__ bool cell_ok(const CachePass& c, v3 p) {
@@ -160,7 +168,7 @@ __device__ __forceinline__ uint32_t claim(uint32_t* count, bool want) {
 __global__ void k_collect(Pass P, const Accum* __restrict__ accum, const uint8_t* __restrict__ mask) {
   uint32_t n = P.width * P.height;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    bool live = (P.f.size[2] == 0u || !(accum[i].color.w < 0.0f)) && (mask == nullptr || mask[i] != 0);
+    bool live = (pass_accum(P) == 0u || !(accum[i].color.w < 0.0f)) && (mask == nullptr || mask[i] != 0);
     append(P.w.active, P.w.counters + 3, i, live);
   }
 }
@@ -174,9 +182,10 @@ __global__ void k_gen(Pass P) {
     uint32_t gx = pixel % P.width, gy = pixel / P.width;
     uint32_t px = gx + P.f.window[2], py = gy + P.f.window[3];
     uint32_t stream = py * P.f.window[0] + px;
-    uint32_t absolute = P.f.size[2] + P.sample;
-    uint32_t state = pcg(stream * 1973u + pcg(P.f.counts[2] * 9277u + absolute * 7919u + 26699u));
-    Rng r{hash_iqnt2d(px, py) ^ P.f.counts[2], absolute, 0u};
+    const uint32_t seed = pass_seed(P);
+    uint32_t absolute = pass_accum(P) + P.sample;
+    uint32_t state = pcg(stream * 1973u + pcg(seed * 9277u + absolute * 7919u + 26699u));
+    Rng r{hash_iqnt2d(px, py) ^ seed, absolute, 0u};
     float4 pf = sobol4(P.v, P.sp, r, 0u);
     float jx = rnd(P.sp, state, pf.x);
     float jy = rnd(P.sp, state, pf.y);
@@ -217,7 +226,7 @@ __global__ void k_gen(Pass P) {
     if (P.c.enabled) {
       // training paths: a hash of the pixel and the sample, apart from the
       // sampler's own sequence, so the chosen paths draw exactly as the others
-      uint32_t h = pcg(stream * 9781u + pcg(P.f.counts[2] * 6529u + absolute * 3571u + 40503u));
+      uint32_t h = pcg(stream * 9781u + pcg(seed * 6529u + absolute * 3571u + 40503u));
       uint32_t slot = claim(P.w.counters + 6, (h >> 8) < P.c.threshold);
       P.c.tslot[i] = slot < P.c.tcap ? slot : ~0u;
     }
@@ -536,7 +545,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_shade(Pass P, uint32_t which) {
       flags &= ~(15u << F_PEND);
       uint32_t pixel = __float_as_uint(rs.w);
       uint32_t px = pixel % P.width + P.f.window[2], py = pixel / P.width + P.f.window[3];
-      Rng r{hash_iqnt2d(px, py) ^ P.f.counts[2], P.f.size[2] + P.sample, 16u * (bounce + 1u)};
+      Rng r{hash_iqnt2d(px, py) ^ pass_seed(P), pass_accum(P) + P.sample, 16u * (bounce + 1u)};
       float4 h = P.w.hit[i];
       float reach = h.x;
       v3 origin_point = spawn_point(o, neg3(d), o, 0.0f);
@@ -773,7 +782,7 @@ __global__ void k_films(Pass P, Accum* __restrict__ accum, float4* color, float4
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t pixel = P.w.active[i];
     Accum a = accum[pixel];
-    a.color.w = (float)(P.f.size[2] + P.f.size[3]);
+    a.color.w = (float)(pass_accum(P) + pass_count(P));
     accum[pixel] = a;
     float count = fmax_(a.color.w, 1.0f);
     v3 nn = divs3(mk3(a.normal.x, a.normal.y, a.normal.z), count);
@@ -838,6 +847,7 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
     if (t.d_wave) cudaFree(t.d_wave);
     t.d_wave = nullptr;
     t.wave_bytes = 0;
+    trace_forget_graphs(t);  // captured passes name the old buffers
     check(cudaMalloc(&t.d_wave, need), "wavefront path state");
     check(cudaMemset(static_cast<char*>(t.d_wave) + o_cnt, 0, 64), "counters");
     t.wave_bytes = need;
@@ -900,6 +910,7 @@ CachePass ensure_cache(pfxt_trace& t, uint32_t pixels) {
     if (t.d_cache_scratch) cudaFree(t.d_cache_scratch);
     t.d_cache_scratch = nullptr;
     t.cache_scratch_bytes = 0;
+    trace_forget_graphs(t);
     check(cudaMalloc(&t.d_cache_scratch, need), "radiance cache scratch");
     t.cache_scratch_bytes = need;
   }
@@ -918,7 +929,21 @@ CachePass ensure_cache(pfxt_trace& t, uint32_t pixels) {
   return c;
 }
 
+// The pass variables: 16 device bytes and their pinned host mirror.
+void ensure_vars(pfxt_trace& t) {
+  if (t.d_vars) return;
+  check(cudaMalloc(&t.d_vars, 16), "pass variables");
+  check(cudaHostAlloc(&t.h_vars, 16, cudaHostAllocDefault), "pass variables");
+}
+
+void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_t pixels);
+
 }  // namespace
+
+void trace_forget_graphs(pfxt_trace& t) {
+  for (auto& e : t.graphs) cudaGraphExecDestroy(e.exec);
+  t.graphs.clear();
+}
 
 static_assert(sizeof(Wave) <= sizeof(((pfxt_trace*)nullptr)->wave_layout), "wave layout storage");
 
@@ -932,10 +957,10 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   ensure_wave(t, pixels, cap);
   Pass P;
   memset(&P, 0, sizeof(P));
-  P.f = t.base;
-  P.f.size[2] = t.samples;
-  P.f.size[3] = count;
-  P.f.counts[2] = seed;
+  P.f = t.base;  // the accumulated samples, the count and the seed travel in P.vars
+  P.f.size[2] = 0u;
+  P.f.size[3] = 0u;
+  P.f.counts[2] = 0u;
   P.sp = t.spec;
   P.v = t.shade;
   P.s = t.view;
@@ -949,9 +974,75 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   P.c = ensure_cache(t, pixels);
   P.bins = t.sort_shading ? 2u * std::max<uint32_t>(std::min<uint32_t>(t.shade.material_count + 1u, SORT_BINS / 2u), 2u)
                           : 0u;
-  Grids& g = grids();
+  ensure_vars(t);
+  P.vars = t.d_vars;
+  t.h_vars[0] = t.samples;
+  t.h_vars[1] = count;
+  t.h_vars[2] = seed;
+  t.h_vars[3] = 0u;
   cudaStream_t st = t.stream;
   if (t.samples == 0) check(cudaMemsetAsync(t.d_accum, 0, (size_t)pixels * sizeof(Accum), st), "accumulation reset");
+  if (!t.use_graphs) {
+    enqueue_pass(t, P, count, deferred, pixels);
+  } else {
+    // the launch sequence depends only on P (with the pass's variables in
+    // device memory), the sample count and the buffers: captured once, replayed
+    std::vector<unsigned char> key(sizeof(P) + 64);
+    memcpy(key.data(), &P, sizeof(P));
+    uint64_t extra[8] = {count, (uint64_t)(uintptr_t)t.d_mask, (uint64_t)(uintptr_t)t.cache, deferred ? 1u : 0u,
+                         t.cache ? (uint64_t)t.cache->s.steps : 0u, t.cache ? (uint64_t)t.cache->s.batch : 0u,
+                         (uint64_t)(uintptr_t)t.d_accum, pixels};
+    memcpy(key.data() + sizeof(P), extra, sizeof(extra));
+    cudaGraphExec_t exec = nullptr;
+    for (auto& e : t.graphs)
+      if (e.key == key) exec = e.exec;
+    if (!exec) {
+      check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "pass capture");
+      cudaGraph_t graph = nullptr;
+      try {
+        enqueue_pass(t, P, count, deferred, pixels);
+      } catch (...) {
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+      }
+      check(cudaStreamEndCapture(st, &graph), "pass capture");
+      cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      check(e, "pass graph");
+      if (t.graphs.size() >= 8) {
+        cudaGraphExecDestroy(t.graphs.front().exec);
+        t.graphs.erase(t.graphs.begin());
+      }
+      t.graphs.push_back(GraphEntry{std::move(key), exec});
+      t.graph_captures += 1u;
+    }
+    check(cudaGraphLaunch(exec, st), "pass graph launch");
+  }
+  check(cudaGetLastError(), "tracer launch");
+  check(cudaStreamSynchronize(st), "tracer pass");
+  if (P.c.enabled) {
+    uint32_t c[3];
+    check(cudaMemcpy(c, P.w.counters + 5, 12, cudaMemcpyDeviceToHost), "cache counters");
+    t.cache->last_queries = c[0];
+    t.cache->last_training_paths = std::min(c[1], P.c.tcap);
+    t.cache->last_records = std::min(c[2], P.c.rcap);
+    float loss = 0.0f;
+    check(cudaMemcpy(&loss, t.cache->d_loss, 4, cudaMemcpyDeviceToHost), "cache loss");
+    t.cache->last_loss = loss / (3.0f * (float)t.cache->s.batch);
+    cache_check_error(*t.cache);
+  }
+  t.samples += count;
+}
+
+namespace {
+
+// One pass's operations on t.stream: the variables' copy, the queues' reset,
+// the samples' bounce loops, the films, and the cache's training.
+void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_t pixels) {
+  Grids& g = grids();
+  cudaStream_t st = t.stream;
+  check(cudaMemcpyAsync(t.d_vars, t.h_vars, 16, cudaMemcpyHostToDevice, st), "pass variables");
   check(cudaMemsetAsync(P.w.counters, 0, 32, st), "counters");  // queues; the ray totals at [8..11] persist
   k_collect<<<g.flat, 256, 0, st>>>(P, t.d_accum, t.d_mask);
   for (uint32_t sample = 0; sample < count; ++sample) {
@@ -988,23 +1079,7 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
       cache_train_launch(*t.cache, P.c.records, P.w.counters + 7, P.c.rcap, s * t.cache->s.batch, st, true, 0);
     cache_cells_launch(*t.cache, st);
   }
-  check(cudaGetLastError(), "tracer launch");
-  check(cudaStreamSynchronize(st), "tracer pass");
-  if (P.c.enabled) {
-    uint32_t c[3];
-    check(cudaMemcpy(c, P.w.counters + 5, 12, cudaMemcpyDeviceToHost), "cache counters");
-    t.cache->last_queries = c[0];
-    t.cache->last_training_paths = std::min(c[1], P.c.tcap);
-    t.cache->last_records = std::min(c[2], P.c.rcap);
-    float loss = 0.0f;
-    check(cudaMemcpy(&loss, t.cache->d_loss, 4, cudaMemcpyDeviceToHost), "cache loss");
-    t.cache->last_loss = loss / (3.0f * (float)t.cache->s.batch);
-    cache_check_error(*t.cache);
-  }
-  t.samples += count;
 }
-
-namespace {
 
 // measure (converge.wgsl:9-30): the half-buffer error of every pixel against
 // its snapshot of the previous round.  snaps: 2 float4 per pixel (mean, info).

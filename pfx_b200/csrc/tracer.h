@@ -66,6 +66,12 @@ struct Accum {
   float4 color, albedo, normal;
 };
 
+// A captured sampling pass and the launch parameters it was captured with.
+struct GraphEntry {
+  std::vector<unsigned char> key;
+  cudaGraphExec_t exec;
+};
+
 }  // namespace pfxt
 
 // The handle behind the C ABI.
@@ -122,6 +128,12 @@ struct pfxt_trace {
   pfxt_cache* cache = nullptr;
   void* d_cache_scratch = nullptr;  // queries, predictions, training vertices and records
   size_t cache_scratch_bytes = 0;
+  // CUDA graphs of the sampling pass (tracer.cu)
+  uint32_t* d_vars = nullptr;  // accumulated samples, samples this pass, seed
+  uint32_t* h_vars = nullptr;  // pinned mirror, copied in by the pass's first node
+  std::vector<pfxt::GraphEntry> graphs;
+  bool use_graphs = true;
+  uint32_t graph_captures = 0;  // passes captured so far
 };
 
 namespace pfxt {
@@ -133,6 +145,8 @@ void trace_set_camera(pfxt_trace& t, const pfxt_camera& c);
 void trace_set_lens(pfxt_trace& t, const float lens[4]);
 void trace_set_window(pfxt_trace& t, const uint32_t full[2], const uint32_t origin[2]);
 void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed);
+// Drops the captured passes (their buffers or launch parameters changed).
+void trace_forget_graphs(pfxt_trace& t);
 void trace_sample_adaptive(pfxt_trace& t, const pfxt_adaptive& a, uint32_t seed, pfxt_round* rounds, uint32_t cap,
                            uint32_t* written);
 std::vector<uint32_t> adaptive_rounds(const pfxt_adaptive& a);

@@ -224,6 +224,11 @@ void trace_release(pfxt_trace& t) {
   if (t.d_cache_scratch) cudaFree(t.d_cache_scratch);
   t.d_cache_scratch = nullptr;
   t.cache = nullptr;
+  trace_forget_graphs(t);
+  if (t.d_vars) cudaFree(t.d_vars);
+  if (t.h_vars) cudaFreeHost(t.h_vars);
+  t.d_vars = nullptr;
+  t.h_vars = nullptr;
   if (t.stream) cudaStreamDestroy(t.stream);
   t.stream = nullptr;
 }

@@ -107,6 +107,28 @@ def test_material_sort_keeps_the_image(gpu):
     assert np.array_equal(a.read_accum(), b.read_accum())
 
 
+def test_graph_replay_matches_launches(gpu):
+    # a captured pass replays with each pass's seed and sample offset
+    w = synth.small("plain_512", (48, 40), sampler="sobol")
+    w.settings = Settings.deep(4, sampler="sobol", sobol_samples=16)
+    a = Trace(w.scene, w.settings, w.width, w.height)
+    b = Trace(w.scene, w.settings, w.width, w.height)
+    b._lib.pfxt_debug_graphs(b.handle, 0)
+    for t in (a, b):
+        for seed, count in ((1, 1), (2, 1), (3, 2), (4, 1)):
+            t.sample(count, seed)
+    assert np.array_equal(a.read_accum(), b.read_accum())
+    assert a._lib.pfxt_debug_graph_captures(a.handle) == 2  # one graph per sample count
+    cam = w.scene.camera
+    moved = type(cam)(tuple(np.asarray(cam.origin) + 0.25), cam.forward, cam.right, cam.up)
+    for t in (a, b):
+        t.set_camera(moved)
+        t.sample(1, 9)
+        t.sample(1, 10)
+    assert np.array_equal(a.read_accum(), b.read_accum())
+    assert a.samples() == 2
+
+
 def test_furnace_and_determinism(gpu):
     # gpu.rs:3787-3830
     scene = synth.furnace()
