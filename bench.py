@@ -358,6 +358,7 @@ def main():
     ap.add_argument("--cache-error-bound", type=float, default=None)
     ap.add_argument("--cache-min-roughness", type=float, default=None)
     ap.add_argument("--no-relmse", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -380,6 +381,9 @@ def main():
     t0 = time.perf_counter()
     trace = Trace(w.scene, w.settings, w.width, w.height)
     create_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tuning = trace.autotune(passes=3) if not args.no_autotune else trace.tuning()
+    autotune_s = time.perf_counter() - t0
     stream = torch.cuda.ExternalStream(trace._lib.pfxt_debug_stream(trace.handle), device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     seed0 = 1000 * (rank + 1)
@@ -446,11 +450,13 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_of(w, args), "rays_per_step": rays / args.steps,
             "Mpaths_s": w.width * w.height * world * args.steps / (total_ms / 1e3) / 1e6,
-            "create_s": create_s,
+            "create_s": create_s, "autotune": {**tuning, "seconds": autotune_s},
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(w.width * w.height * 16),
                     "note": "scene uploaded once by Trace::new (create_s); per step one pass and the colour film"},
-            "gpu_launches": args.steps * (2 + 2 + (w.settings.bounces[0] + 2) * 5 + 1),
+            # per pass: collect, gen, seed counts, finish, films, and per bounce reset,
+            # extend, (material sort: 2), shade, rewind, connect
+            "gpu_launches": args.steps * (5 + (w.settings.bounces[0] + 2) * (5 + (2 if tuning["sort_shading"] else 0))),
             "clocks": clk.summary(),
         }
         line["roofline"] = traversal_roofline(trace, w, dev, stream, flush)

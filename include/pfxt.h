@@ -288,6 +288,25 @@ int pfxt_occluded_device(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count
 int pfxt_occluded_noalloc(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count, uint8_t* blocked,
                           void* stream);
 
+/* ------------------------------------------------------------ launch tuning
+ * Launch choices that change how long a sampling pass takes but no value it
+ * computes.  No counterpart in the reference (wgpu sizes its own dispatches). */
+typedef struct pfxt_tuning {
+  uint32_t trace_threads; /* threads per block of the persistent traversal kernels: 64, 128 or 256 (128) */
+  uint32_t sort_shading;  /* sort the shade queue by hit material every bounce (1) */
+  uint32_t graphs;        /* replay each pass from a captured CUDA graph (1) */
+  float pass_ms;          /* from pfxt_autotune: the chosen configuration's median pass time */
+} pfxt_tuning;
+
+int pfxt_get_tuning(pfxt_trace* trace, pfxt_tuning* out);
+int pfxt_set_tuning(pfxt_trace* trace, const pfxt_tuning* tuning);
+/* Times `passes` one-sample passes (at least 2; the first of each
+ * configuration warms up and is not counted) of this tracer's scene under every
+ * traversal block size with and without the material sort, and keeps the
+ * fastest; `out` (may be NULL) receives it.  Restarts the accumulation; with a
+ * radiance cache attached, the trial passes also train it. */
+int pfxt_autotune(pfxt_trace* trace, uint32_t passes, pfxt_tuning* out);
+
 /* ------------------------------------------------------------ radiance cache
  *
  * A neural radiance cache: a 16-level hash-grid encoding (2 FP16 features per

@@ -114,6 +114,11 @@ class Adaptive(C.Structure):
                 ("growth", C.c_float)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("trace_threads", C.c_uint32), ("sort_shading", C.c_uint32), ("graphs", C.c_uint32),
+                ("pass_ms", C.c_float)]
+
+
 class CacheSettings(C.Structure):
     _fields_ = [("log2_entries", C.c_uint32), ("base_resolution", C.c_uint32), ("max_resolution", C.c_uint32),
                 ("batch", C.c_uint32), ("steps", C.c_uint32), ("seed", C.c_uint32), ("query_bounce", C.c_uint32),
@@ -161,6 +166,9 @@ PROTOTYPES = [
     ("pfxt_trace_rays_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pfxt_occluded_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pfxt_occluded_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("pfxt_get_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
+    ("pfxt_set_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
+    ("pfxt_autotune", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),
     ("pfxt_cache_defaults", C.c_int, [C.POINTER(CacheSettings)]),
     ("pfxt_cache_create", C.c_int, [C.POINTER(CacheSettings), C.POINTER(C.c_void_p)]),
     ("pfxt_cache_destroy", None, [C.c_void_p]),

@@ -424,6 +424,30 @@ int pfxt_films_device(pfxt_trace* t, float** color, float** albedo, float** norm
   });
 }
 
+/* ------------------------------------------------------------ launch tuning */
+
+int pfxt_get_tuning(pfxt_trace* t, pfxt_tuning* out) {
+  return guarded([&]() {
+    if (!t || !out) throw Invalid("null argument");
+    *out = trace_get_tuning(*t);
+  });
+}
+
+int pfxt_set_tuning(pfxt_trace* t, const pfxt_tuning* k) {
+  return guarded([&]() {
+    if (!t || !k) throw Invalid("null argument");
+    trace_set_tuning(*t, *k);
+  });
+}
+
+int pfxt_autotune(pfxt_trace* t, uint32_t passes, pfxt_tuning* out) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    pfxt_tuning k = trace_autotune(*t, passes);
+    if (out) *out = k;
+  });
+}
+
 /* ------------------------------------------------------------ radiance cache */
 
 int pfxt_cache_defaults(pfxt_cache_settings* s) {

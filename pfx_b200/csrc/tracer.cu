@@ -367,8 +367,10 @@ __global__ void k_rewind(Pass P) {
 }
 
 // ------------------------------------------------------------------ extend
-template <bool ANY>
-__global__ void __launch_bounds__(kThreads) k_trace_queue(Pass P, uint32_t which) {
+// THREADS per block is a launch choice of the autotuner: the walk is per lane
+// and the refill per warp, so the block size changes only the residency.
+template <bool ANY, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_trace_queue(Pass P, uint32_t which) {
   constexpr unsigned FULL = 0xffffffffu;
   const uint32_t* queue = ANY ? P.w.squeue : P.w.queue[which];
   const uint32_t n = ANY ? P.w.counters[2] : P.w.counters[which];
@@ -810,14 +812,19 @@ int grid_for(const void* kernel, int threads) {
   return sms * (per > 0 ? per : 1);
 }
 
+// Persistent grids of the traversal kernels for 64, 128 and 256 threads per block.
 struct Grids {
-  int trace_closest = 0, trace_any = 0, shade = 0, shade_inline = 0, flat = 0;
+  int trace_closest[3] = {0, 0, 0}, trace_any[3] = {0, 0, 0}, shade = 0, shade_inline = 0, flat = 0;
 };
 Grids& grids() {
   static Grids g;
   if (g.shade == 0) {
-    g.trace_closest = grid_for((const void*)k_trace_queue<false>, kThreads);
-    g.trace_any = grid_for((const void*)k_trace_queue<true>, kThreads);
+    g.trace_closest[0] = grid_for((const void*)k_trace_queue<false, 64>, 64);
+    g.trace_closest[1] = grid_for((const void*)k_trace_queue<false, 128>, 128);
+    g.trace_closest[2] = grid_for((const void*)k_trace_queue<false, 256>, 256);
+    g.trace_any[0] = grid_for((const void*)k_trace_queue<true, 64>, 64);
+    g.trace_any[1] = grid_for((const void*)k_trace_queue<true, 128>, 128);
+    g.trace_any[2] = grid_for((const void*)k_trace_queue<true, 256>, 256);
     g.shade = grid_for((const void*)k_shade<true>, kThreads);
     g.shade_inline = grid_for((const void*)k_shade<false>, kThreads);
     int dev = 0, sms = 0;
@@ -827,6 +834,21 @@ Grids& grids() {
   }
   return g;
 }
+
+// The traversal launches for the tuned block size (0: 64, 1: 128, 2: 256 threads).
+template <bool ANY>
+void launch_trace_queue(int sel, const Pass& P, uint32_t which, cudaStream_t st) {
+  Grids& g = grids();
+  const int* grid = ANY ? g.trace_any : g.trace_closest;
+  if (sel == 0)
+    k_trace_queue<ANY, 64><<<grid[0], 64, 0, st>>>(P, which);
+  else if (sel == 2)
+    k_trace_queue<ANY, 256><<<grid[2], 256, 0, st>>>(P, which);
+  else
+    k_trace_queue<ANY, 128><<<grid[1], 128, 0, st>>>(P, which);
+}
+
+int thread_select(uint32_t threads) { return threads == 64u ? 0 : (threads == 256u ? 2 : 1); }
 
 // Path-state buffers for `capacity` paths and `cap` slots per path.
 void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
@@ -991,7 +1013,7 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
     memcpy(key.data(), &P, sizeof(P));
     uint64_t extra[8] = {count, (uint64_t)(uintptr_t)t.d_mask, (uint64_t)(uintptr_t)t.cache, deferred ? 1u : 0u,
                          t.cache ? (uint64_t)t.cache->s.steps : 0u, t.cache ? (uint64_t)t.cache->s.batch : 0u,
-                         (uint64_t)(uintptr_t)t.d_accum, pixels};
+                         (uint64_t)(uintptr_t)t.d_accum, (uint64_t)pixels | ((uint64_t)t.trace_threads << 32)};
     memcpy(key.data() + sizeof(P), extra, sizeof(extra));
     cudaGraphExec_t exec = nullptr;
     for (auto& e : t.graphs)
@@ -1054,7 +1076,7 @@ void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_
       uint32_t cur = bounce & 1u;
       P.bounce = bounce;
       k_reset<<<1, 32, 0, st>>>(P, cur);
-      k_trace_queue<false><<<g.trace_closest, kThreads, 0, st>>>(P, cur);
+      launch_trace_queue<false>(thread_select(t.trace_threads), P, cur, st);
       if (P.bins) {
         k_sort_count<<<g.flat, 256, 0, st>>>(P, cur);
         k_sort_place<<<g.flat, 256, 0, st>>>(P, cur);
@@ -1067,7 +1089,7 @@ void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_
         cache_infer_launch(*t.cache, P.c.query, P.w.counters + 5, pixels, P.c.cqueue, P.c.pred, st);
       if (deferred) {
         k_rewind<<<1, 32, 0, st>>>(P);
-        k_trace_queue<true><<<g.trace_any, kThreads, 0, st>>>(P, 0u);
+        launch_trace_queue<true>(thread_select(t.trace_threads), P, 0u, st);
       }
     }
     k_finish<<<g.flat, 256, 0, st>>>(P, t.d_accum);

@@ -117,6 +117,8 @@ struct pfxt_trace {
   uint32_t* wave_counters = nullptr;           // queue counters and ray totals inside d_wave
   uint8_t* d_mask = nullptr;                   // optional per-pixel mask of the pixels to sample
   bool sort_shading = true;                    // group the shade queue by material every bounce
+  uint32_t trace_threads = 128;                // threads per block of the traversal kernels (64, 128, 256)
+  float tuned_pass_ms = 0.0f;                  // the autotuner's measured pass time, 0 = not tuned
   uint32_t* d_error = nullptr;  // device error word
   uint32_t* d_counters = nullptr;  // ring of work-sharing counters (device scratch)
   uint32_t counter_slot = 0;
@@ -147,6 +149,9 @@ void trace_set_window(pfxt_trace& t, const uint32_t full[2], const uint32_t orig
 void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed);
 // Drops the captured passes (their buffers or launch parameters changed).
 void trace_forget_graphs(pfxt_trace& t);
+void trace_set_tuning(pfxt_trace& t, const pfxt_tuning& k);
+pfxt_tuning trace_get_tuning(const pfxt_trace& t);
+pfxt_tuning trace_autotune(pfxt_trace& t, uint32_t passes);
 void trace_sample_adaptive(pfxt_trace& t, const pfxt_adaptive& a, uint32_t seed, pfxt_round* rounds, uint32_t cap,
                            uint32_t* written);
 std::vector<uint32_t> adaptive_rounds(const pfxt_adaptive& a);

@@ -3,9 +3,11 @@
 // sample counts (adaptive.rs:328).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "tracer.h"
 
@@ -310,6 +312,64 @@ std::vector<uint32_t> adaptive_rounds(const pfxt_adaptive& a) {
     next = std::min(next, a.max_samples);
     rounds.push_back(next);
   }
+}
+
+// ------------------------------------------------------------------ tuning
+void trace_set_tuning(pfxt_trace& t, const pfxt_tuning& k) {
+  if (k.trace_threads != 64u && k.trace_threads != 128u && k.trace_threads != 256u)
+    throw Invalid("trace_threads must be 64, 128 or 256");
+  t.trace_threads = k.trace_threads;
+  t.sort_shading = k.sort_shading != 0u;
+  t.use_graphs = k.graphs != 0u;
+}
+
+pfxt_tuning trace_get_tuning(const pfxt_trace& t) {
+  pfxt_tuning k{};
+  k.trace_threads = t.trace_threads;
+  k.sort_shading = t.sort_shading ? 1u : 0u;
+  k.graphs = t.use_graphs ? 1u : 0u;
+  k.pass_ms = t.tuned_pass_ms;
+  return k;
+}
+
+// Median device time of `passes - 1` one-sample passes after one warm-up pass.
+static float time_passes(pfxt_trace& t, uint32_t passes, uint32_t& seed) {
+  cudaEvent_t e0, e1;
+  check(cudaEventCreate(&e0), "autotune events");
+  check(cudaEventCreate(&e1), "autotune events");
+  std::vector<float> ms;
+  for (uint32_t i = 0; i < passes; ++i) {
+    check(cudaEventRecord(e0, t.stream), "autotune events");
+    trace_sample(t, 1u, seed++);
+    check(cudaEventRecord(e1, t.stream), "autotune events");
+    check(cudaEventSynchronize(e1), "autotune events");
+    float v = 0.0f;
+    check(cudaEventElapsedTime(&v, e0, e1), "autotune events");
+    if (i > 0) ms.push_back(v);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::sort(ms.begin(), ms.end());
+  return ms[ms.size() / 2];
+}
+
+pfxt_tuning trace_autotune(pfxt_trace& t, uint32_t passes) {
+  if (passes < 2 || passes > 64) throw Invalid("autotune: passes must be in 2..64");
+  pfxt_tuning best = trace_get_tuning(t);
+  best.pass_ms = INFINITY;
+  const bool graphs = t.use_graphs;
+  uint32_t seed = 0x7e000000u;
+  for (uint32_t threads : {64u, 128u, 256u})
+    for (uint32_t sort : {1u, 0u}) {
+      pfxt_tuning k{threads, sort, graphs ? 1u : 0u, 0.0f};
+      trace_set_tuning(t, k);
+      k.pass_ms = time_passes(t, passes, seed);
+      if (k.pass_ms < best.pass_ms) best = k;
+    }
+  trace_set_tuning(t, best);
+  t.tuned_pass_ms = best.pass_ms;
+  t.samples = 0;  // the trial passes are not part of the image
+  return best;
 }
 
 }  // namespace pfxt

@@ -335,6 +335,23 @@ class Trace:
         shape = (self.height, self.width, 4)
         return [torch.as_tensor(_View(p.value, shape), device="cuda") for p in ptrs]
 
+    def tuning(self) -> dict:
+        k = abi.Tuning()
+        check(self._lib.pfxt_get_tuning(self._h, C.byref(k)))
+        return {"trace_threads": k.trace_threads, "sort_shading": bool(k.sort_shading), "graphs": bool(k.graphs),
+                "pass_ms": float(k.pass_ms)}
+
+    def set_tuning(self, trace_threads: int = 128, sort_shading: bool = True, graphs: bool = True) -> None:
+        k = abi.Tuning(trace_threads, int(sort_shading), int(graphs), 0.0)
+        check(self._lib.pfxt_set_tuning(self._h, C.byref(k)))
+
+    def autotune(self, passes: int = 3) -> dict:
+        """Time passes of this scene under each launch configuration and keep the
+        fastest (restarts the accumulation)."""
+        k = abi.Tuning()
+        check(self._lib.pfxt_autotune(self._h, passes, C.byref(k)))
+        return self.tuning()
+
     def set_cache(self, cache) -> None:
         """Attach a pfx_b200.cache.RadianceCache (None detaches): paths then end
         into the cache at its query bounce and a fraction of them train it.

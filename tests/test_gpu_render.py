@@ -129,6 +129,26 @@ def test_graph_replay_matches_launches(gpu):
     assert a.samples() == 2
 
 
+def test_autotune_keeps_the_image(gpu):
+    w = synth.small("room_4k", (64, 40), sampler="sobol")
+    a = Trace(w.scene, w.settings, w.width, w.height)
+    b = Trace(w.scene, w.settings, w.width, w.height)
+    k = a.autotune(passes=2)
+    assert k["trace_threads"] in (64, 128, 256) and k["pass_ms"] > 0
+    assert a.samples() == 0  # the trial passes are not part of the image
+    for threads in (64, 256):
+        b.set_tuning(trace_threads=threads, sort_shading=threads == 64, graphs=threads == 256)
+        b.set_camera(w.scene.camera)
+        b.sample(2, 5)
+        if threads == 64:
+            first = b.read_accum()
+    a.sample(2, 5)
+    assert np.array_equal(a.read_accum(), b.read_accum())
+    assert np.array_equal(first, b.read_accum())
+    with pytest.raises(Exception):
+        b.set_tuning(trace_threads=96)
+
+
 def test_furnace_and_determinism(gpu):
     # gpu.rs:3787-3830
     scene = synth.furnace()
