@@ -129,6 +129,25 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def rank_seed(rank: int) -> int:
+    """First pass seed of a rank: every rank renders its own frame (weak scaling)."""
+    return 1000 * (rank + 1)
+
+
+def combine_ranks(pg, elapsed: float, units: float, device):
+    """(max of `elapsed` over ranks, sum of `units` over ranks): the job's time is
+    its slowest rank's, its work every rank's.  `pg` is torch.distributed or None."""
+    if pg is None:
+        return elapsed, units
+    import torch
+    t = torch.tensor([elapsed, units], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    pg.all_reduce(tmax, op=pg.ReduceOp.MAX)
+    tsum = t.clone()
+    pg.all_reduce(tsum, op=pg.ReduceOp.SUM)
+    return float(tmax[0].item()), float(tsum[1].item())
+
+
 def workload(name: str):
     from pfx_b200 import synth
     return synth.WORKLOADS[name]()
@@ -386,7 +405,7 @@ def main():
     autotune_s = time.perf_counter() - t0
     stream = torch.cuda.ExternalStream(trace._lib.pfxt_debug_stream(trace.handle), device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    seed0 = 1000 * (rank + 1)
+    seed0 = rank_seed(rank)
 
     for i in range(args.warmup):
         trace.sample(1, seed0 + i)
@@ -407,16 +426,7 @@ def main():
             step_ms.append(e0.elapsed_time(e1))
     after = trace.rays_traced()
     rays = (after[0] - before[0]) + (after[1] - before[1])
-    total_ms = sum(step_ms)
-    if pg:
-        t = torch.tensor([total_ms, float(rays)], dtype=torch.float64, device=dev)
-        tmax = t.clone()
-        pg.all_reduce(tmax, op=pg.ReduceOp.MAX)
-        tsum = t.clone()
-        pg.all_reduce(tsum, op=pg.ReduceOp.SUM)
-        total_ms, rays_all = float(tmax[0].item()), float(tsum[1].item())
-    else:
-        rays_all = float(rays)
+    total_ms, rays_all = combine_ranks(pg, sum(step_ms), float(rays), dev)
     value = rays_all / (total_ms / 1e3) / 1e6
 
     # e2e: sample + readback of the colour film through the host-buffer API
@@ -433,14 +443,7 @@ def main():
         assert rc == 0, lib.pfxt_last_error()
     e2e_s = time.perf_counter() - t0
     r1 = trace.rays_traced()
-    e2e_rays = float((r1[0] - r0[0]) + (r1[1] - r0[1]))
-    if pg:
-        t = torch.tensor([e2e_s, e2e_rays], dtype=torch.float64, device=dev)
-        tmax = t.clone()
-        pg.all_reduce(tmax, op=pg.ReduceOp.MAX)
-        tsum = t.clone()
-        pg.all_reduce(tsum, op=pg.ReduceOp.SUM)
-        e2e_s, e2e_rays = float(tmax[0].item()), float(tsum[1].item())
+    e2e_s, e2e_rays = combine_ranks(pg, e2e_s, float((r1[0] - r0[0]) + (r1[1] - r0[1])), dev)
     e2e_value = e2e_rays / e2e_s / 1e6
 
     if rank == 0:

@@ -45,6 +45,7 @@ def lib() -> C.CDLL:
             "orc_adaptive_error": (f32, [vp, f32, vp, f32]),
             "orc_falloff": (f32, [f32, f32, f32, f32]),
             "orc_check_div": (C.c_uint64, [C.c_uint64, C.c_uint64]),
+            "orc_math": (None, [C.c_int, vp, vp, vp, C.c_uint64]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -133,6 +134,18 @@ def falloff(intensity, radius, range_, distance) -> float:
 def check_div(per_family: int, seed: int = 1) -> int:
     """Mismatches between the kernels' correctly-rounded division (div_rn) and IEEE division."""
     return int(lib().orc_check_div(per_family, seed))
+
+
+MATH_FUNCTIONS = ("sin", "cos", "asin", "acos", "atan2", "exp", "log", "pow")
+
+
+def math(fn: str, x, y=None) -> np.ndarray:
+    """The transcendentals the kernels and the oracle share (pfxt_math.h), on float32 arrays."""
+    x = np.ascontiguousarray(x, np.float32)
+    yy = None if y is None else np.ascontiguousarray(y, np.float32)
+    out = np.empty_like(x)
+    lib().orc_math(MATH_FUNCTIONS.index(fn), _p(x), None if yy is None else _p(yy), _p(out), x.size)
+    return out
 
 
 def frame_of(scene, width: int, height: int, tri_count: int, window=None) -> np.ndarray:

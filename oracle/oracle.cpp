@@ -707,6 +707,26 @@ uint64_t orc_check_div(uint64_t per_family, uint64_t seed) {
   }
   return bad;
 }
+
+// The shared transcendentals over an array, for their accuracy test:
+// fn 0 sin, 1 cos, 2 asin, 3 acos, 4 atan2(x, y), 5 exp, 6 log, 7 pow(x, y).
+void orc_math(int fn, const float* x, const float* y, float* out, uint64_t n) {
+  for (uint64_t i = 0; i < n; ++i) {
+    float a = x[i], b = y ? y[i] : 0.0f, r = 0.0f;
+    switch (fn) {
+      case 0: r = sin_(a); break;
+      case 1: r = cos_(a); break;
+      case 2: r = asin_(a); break;
+      case 3: r = acos_(a); break;
+      case 4: r = atan2_(a, b); break;
+      case 5: r = exp_(a); break;
+      case 6: r = log_(a); break;
+      case 7: r = pow_(a, b); break;
+      default: break;
+    }
+    out[i] = r;
+  }
+}
 }  // extern "C"
 
 // The path integrator restatement shares this translation unit.
