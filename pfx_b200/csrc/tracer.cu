@@ -39,6 +39,11 @@ namespace pfxt {
 namespace {
 
 constexpr int kThreads = 128;
+// Resident blocks of the shade kernel per SM the compiler must allow for: it
+// sets the register budget (4: 128 registers, 2: up to 255).
+#ifndef SHADE_MIN_BLOCKS
+#define SHADE_MIN_BLOCKS 4
+#endif
 constexpr uint32_t CAP_MAX = 8u;
 
 // Path flag word (ray_d.w bits).
@@ -165,7 +170,7 @@ __device__ __forceinline__ uint32_t claim(uint32_t* count, bool want) {
 // ------------------------------------------------------------------ active
 // Pixels that still sample: the reference returns early when accum.color.w
 // is negative (trace.wgsl:2517), the mark of a converged pixel.
-__global__ void k_collect(Pass P, const Accum* __restrict__ accum, const uint8_t* __restrict__ mask) {
+__global__ void k_collect(const __grid_constant__ Pass P,const Accum* __restrict__ accum, const uint8_t* __restrict__ mask) {
   uint32_t n = P.width * P.height;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     bool live = (pass_accum(P) == 0u || !(accum[i].color.w < 0.0f)) && (mask == nullptr || mask[i] != 0);
@@ -175,7 +180,7 @@ __global__ void k_collect(Pass P, const Accum* __restrict__ accum, const uint8_t
 
 // ------------------------------------------------------------------ generate
 // main() up to the call of radiance(): seeding, pixel filter, camera ray.
-__global__ void k_gen(Pass P) {
+__global__ void k_gen(const __grid_constant__ Pass P) {
   const uint32_t n = P.w.counters[3];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t pixel = P.w.active[i];
@@ -234,14 +239,14 @@ __global__ void k_gen(Pass P) {
 }
 
 // Before a sample's k_gen: no cache queries and no training slots yet.
-__global__ void k_cache_begin(Pass P) {
+__global__ void k_cache_begin(const __grid_constant__ Pass P) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     P.w.counters[5] = 0u;
     P.w.counters[6] = 0u;
   }
 }
 
-__global__ void k_seed_counts(Pass P) {
+__global__ void k_seed_counts(const __grid_constant__ Pass P) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     P.w.counters[0] = P.w.counters[3];
     P.w.counters[1] = 0u;
@@ -252,7 +257,7 @@ __global__ void k_seed_counts(Pass P) {
 // Before a bounce: empty the next ray queue and the shadow queue, rewind the
 // work counter of the extend kernel, and count the closest-hit queries of the
 // bounce (64-bit totals at counters[8..9] closest, [10..11] any hit).
-__global__ void k_reset(Pass P, uint32_t cur) {
+__global__ void k_reset(const __grid_constant__ Pass P,uint32_t cur) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     P.w.counters[cur ^ 1u] = 0u;
     P.w.counters[2] = 0u;
@@ -311,7 +316,7 @@ __device__ __forceinline__ void block_chunk(uint32_t n, uint32_t& first, uint32_
   last = min(n, first + per);
 }
 
-__global__ void __launch_bounds__(256) k_sort_count(Pass P, uint32_t which) {
+__global__ void __launch_bounds__(256) k_sort_count(const __grid_constant__ Pass P,uint32_t which) {
   __shared__ uint32_t hist[SORT_BINS];
   const uint32_t n = P.w.counters[which];
   const uint32_t* queue = P.w.queue[which];
@@ -329,7 +334,7 @@ __global__ void __launch_bounds__(256) k_sort_count(Pass P, uint32_t which) {
     if (hist[b]) atomicAdd(P.w.hist + b, hist[b]);
 }
 
-__global__ void __launch_bounds__(256) k_sort_place(Pass P, uint32_t which) {
+__global__ void __launch_bounds__(256) k_sort_place(const __grid_constant__ Pass P,uint32_t which) {
   __shared__ uint32_t base[SORT_BINS];
   __shared__ uint32_t local[SORT_BINS];
   const uint32_t n = P.w.counters[which];
@@ -359,7 +364,7 @@ __global__ void __launch_bounds__(256) k_sort_place(Pass P, uint32_t which) {
     P.w.sorted[base[key] + atomicAdd(&local[key], 1u)] = queue[q];
   }
 }
-__global__ void k_rewind(Pass P) {
+__global__ void k_rewind(const __grid_constant__ Pass P) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     P.w.counters[4] = 0u;
     reinterpret_cast<unsigned long long*>(P.w.counters + 8)[1] += P.w.counters[2];
@@ -370,7 +375,7 @@ __global__ void k_rewind(Pass P) {
 // THREADS per block is a launch choice of the autotuner: the walk is per lane
 // and the refill per warp, so the block size changes only the residency.
 template <bool ANY, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_trace_queue(Pass P, uint32_t which) {
+__global__ void __launch_bounds__(THREADS) k_trace_queue(const __grid_constant__ Pass P,uint32_t which) {
   constexpr unsigned FULL = 0xffffffffu;
   const uint32_t* queue = ANY ? P.w.squeue : P.w.queue[which];
   const uint32_t n = ANY ? P.w.counters[2] : P.w.counters[which];
@@ -522,7 +527,7 @@ __device__ __noinline__ void emit_records(const float4* __restrict__ tvert, floa
 // DEFERRED: light-slot shadow rays go through the shadow queue (the usual
 // case); otherwise (more than CAP_MAX light slots) they are traced inline.
 template <bool DEFERRED>
-__global__ void __launch_bounds__(kThreads, 4) k_shade(Pass P, uint32_t which) {
+__global__ void __launch_bounds__(kThreads, SHADE_MIN_BLOCKS) k_shade(const __grid_constant__ Pass P,uint32_t which) {
   const uint32_t n = P.w.counters[which];
   const uint32_t* queue = P.bins ? P.w.sorted : P.w.queue[which];
   uint32_t* next_queue = P.w.queue[which ^ 1u];
@@ -749,7 +754,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_shade(Pass P, uint32_t which) {
 // ------------------------------------------------------------------ finish
 // Pending contributions of the last bounce, then Accum += (result, first
 // albedo, first normal) in sample order (trace.wgsl:2564-2567).
-__global__ void k_finish(Pass P, Accum* __restrict__ accum) {
+__global__ void k_finish(const __grid_constant__ Pass P,Accum* __restrict__ accum) {
   const uint32_t n = P.w.counters[3];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float4 rs = P.w.res[i];
@@ -779,7 +784,7 @@ __global__ void k_finish(Pass P, Accum* __restrict__ accum) {
 }
 
 // Films (trace.wgsl:2568-2578) for the pixels of this pass.
-__global__ void k_films(Pass P, Accum* __restrict__ accum, float4* color, float4* albedo, float4* normal) {
+__global__ void k_films(const __grid_constant__ Pass P,Accum* __restrict__ accum, float4* color, float4* albedo, float4* normal) {
   const uint32_t n = P.w.counters[3];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t pixel = P.w.active[i];
