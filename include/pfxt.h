@@ -295,6 +295,7 @@ typedef struct pfxt_tuning {
   uint32_t trace_threads; /* threads per block of the persistent traversal kernels: 64, 128 or 256 (128) */
   uint32_t sort_shading;  /* sort the shade queue by hit material every bounce (1) */
   uint32_t graphs;        /* replay each pass from a captured CUDA graph (1) */
+  uint32_t split_shade;   /* shade a bounce in three kernels (hit, light slots, BSDF) instead of one (1) */
   float pass_ms;          /* from pfxt_autotune: the chosen configuration's median pass time */
 } pfxt_tuning;
 
@@ -302,8 +303,8 @@ int pfxt_get_tuning(pfxt_trace* trace, pfxt_tuning* out);
 int pfxt_set_tuning(pfxt_trace* trace, const pfxt_tuning* tuning);
 /* Times `passes` one-sample passes (at least 2; the first of each
  * configuration warms up and is not counted) of this tracer's scene under every
- * traversal block size with and without the material sort, and keeps the
- * fastest; `out` (may be NULL) receives it.  Restarts the accumulation; with a
+ * traversal block size, with and without the material sort, with one shade
+ * kernel and with three, and keeps the fastest; `out` (may be NULL) receives it.  Restarts the accumulation; with a
  * radiance cache attached, the trial passes also train it. */
 int pfxt_autotune(pfxt_trace* trace, uint32_t passes, pfxt_tuning* out);
 

@@ -22,7 +22,11 @@ namespace pfxt {
 constexpr float SH_PI = 0x1.921fb6p+1f;
 
 // Heavy helpers are kept out of line (one copy each in the shading kernel).
-#define SH_CALL static __device__ __noinline__  // brdf.wgsl:1 `const PI: f32 = 3.141592653589793`
+#define SH_CALL static __device__ __noinline__
+// Small helpers: out of line as well unless a build inlines them.
+#ifndef SH_SMALL
+#define SH_SMALL SH_CALL
+#endif  // brdf.wgsl:1 `const PI: f32 = 3.141592653589793`
 
 // ------------------------------------------------------------------ random
 __device__ __forceinline__ uint32_t pcg(uint32_t v) {
@@ -92,7 +96,7 @@ __device__ __forceinline__ uint32_t hash_shuffle_256(uint32_t i0, uint32_t seed)
   }
   return i;
 }
-SH_CALL float4 sobol4(const ShadeView& v, const Specialise& sp, const Rng& r, uint32_t dimension) {
+SH_SMALL float4 sobol4(const ShadeView& v, const Specialise& sp, const Rng& r, uint32_t dimension) {
   if (!sp.sobol) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   uint32_t L = sp.sobol_length;
   uint32_t seed = r.x;
@@ -192,7 +196,7 @@ __device__ __forceinline__ v3 beer(float distance, v3 tint, float absorption) {
 __device__ __forceinline__ float fresnel_exponent(const Shaded& s) {
   return s.fresnel_power <= 0.0f ? 5.0f : s.fresnel_power;
 }
-SH_CALL v3 reflection(const Shaded& s, float ndh_cos) {
+SH_SMALL v3 reflection(const Shaded& s, float ndh_cos) {
   float power = fresnel_exponent(s);
   v3 f0 = mix3(splat3(s.specular), s.base, clamp_(s.metalness, 0.0f, 1.0f));
   if (s.transmission > 0.0f || s.dispersion != 0.0f) {
@@ -254,7 +258,7 @@ __device__ __forceinline__ float glossy_share(const Shaded& s) {
 __device__ __forceinline__ float coat_weight_of(const Shaded& s, v3 wo) {
   return clamp_(s.clearcoat * (0.12f + 0.88f * (0.04f + 0.96f * pow_(1.0f - fmax_(wo.z, 0.0f), 5.0f))), 0.0f, 0.9f);
 }
-SH_CALL float bsdf_pdf(const Shaded& s, v3 wo, v3 wi) {
+SH_SMALL float bsdf_pdf(const Shaded& s, v3 wo, v3 wi) {
   if (wi.z <= 0.0f) return 0.0f;
   float trans = clamp_(s.transmission, 0.0f, 1.0f) * (1.0f - clamp_(s.metalness, 0.0f, 1.0f));
   float coat = coat_weight_of(s, wo);
@@ -368,7 +372,7 @@ __device__ __forceinline__ uint32_t cdf_find(const float* __restrict__ cdf, uint
 __device__ __forceinline__ v3 sky_radiance(const ShadeView& v) {
   return mk3(v.sky_radiance[0], v.sky_radiance[1], v.sky_radiance[2]);
 }
-SH_CALL float sky_pdf(const ShadeView& v, v3 direction) {
+SH_SMALL float sky_pdf(const ShadeView& v, v3 direction) {
   v3 d = normalize3(direction);
   float theta = acos_(clamp_(d.y, -1.0f, 1.0f));
   float phi = fmod_wgsl(atan2_(d.z, d.x) + 6.28318531f, 6.28318531f);
@@ -593,7 +597,7 @@ SH_CALL Candidate light_candidate(const Specialise& sp, const LightRow& light, c
 __device__ __forceinline__ float sin_from_cos(float c) { return sqrtf(fmax_(1.0f - c * c, 0.0f)); }
 
 // tree_importance (lights.wgsl:204-237) -> (max, min)
-SH_CALL float2 tree_importance(v3 n, v3 to, float cos_u, v3 axis, float theta_o, float theta_e,
+SH_SMALL float2 tree_importance(v3 n, v3 to, float cos_u, v3 axis, float theta_o, float theta_e,
                                                   float far, float near, float energy) {
   float sin_u = sin_from_cos(cos_u);
   float cos_i = dot3(to, n);
@@ -625,7 +629,7 @@ SH_CALL float2 tree_importance(v3 n, v3 to, float cos_u, v3 axis, float theta_o,
   float cos_max_out = cos_t_plus_u * cos_o - sin_from_cos(cos_t_plus_u) * sin_o;
   return make_float2(most, abs_(cos_max_i * energy * cos_max_out / (far * far)));
 }
-SH_CALL float2 node_importance(const LightRow& node, v3 p, v3 n) {
+SH_SMALL float2 node_importance(const LightRow& node, v3 p, v3 n) {
   v3 lo = f3of(node.a), hi = f3of(node.b);
   v3 centroid = scl3(add3(lo, hi), 0.5f);
   v3 extent = sub3(hi, centroid);
@@ -640,7 +644,7 @@ SH_CALL float2 node_importance(const LightRow& node, v3 p, v3 n) {
   return tree_importance(n, divs3(to, fmax_(reach, 1e-30f)), cos_u, f3of(node.c), node.c.w, node.d.x, distance,
                          distance, node.a.w);
 }
-SH_CALL float2 emitter_importance(const LightRow& light, v3 p, v3 n) {
+SH_SMALL float2 emitter_importance(const LightRow& light, v3 p, v3 n) {
   v3 to = sub3(f3of(light.a), p);
   float near = length3(to);
   if (near >= light.b.w || near <= 1e-6f) return make_float2(0.0f, 0.0f);

@@ -74,6 +74,9 @@ struct Wave {
   uint32_t* sorted;    // the queue, grouped by key
   uint32_t* hist;      // SORT_BINS: paths per key
   uint32_t* cursor;    // SORT_BINS: entries handed out per key
+  // split shade: the paths that scatter this bounce (count at counters[12]) and their surfaces
+  uint32_t* lit;
+  float4* surf;        // 9 float4 per path
 };
 
 // The radiance cache as the wave sees it (all null/zero when none is attached).
@@ -262,6 +265,7 @@ __global__ void k_reset(const __grid_constant__ Pass P,uint32_t cur) {
     P.w.counters[cur ^ 1u] = 0u;
     P.w.counters[2] = 0u;
     P.w.counters[4] = 0u;
+    P.w.counters[12] = 0u;
     reinterpret_cast<unsigned long long*>(P.w.counters + 8)[0] += P.w.counters[cur];
   }
   if (blockIdx.x == 0)
@@ -751,6 +755,342 @@ __global__ void __launch_bounds__(kThreads, SHADE_MIN_BLOCKS) k_shade(const __gr
   }
 }
 
+// ------------------------------------------------------------------ split shade
+// The same bounce body in three kernels, for an instruction cache that the
+// whole body overflows: k_shade_hit (emission, light hits, the cache), then,
+// for the paths that scatter, k_shade_lights (the light slots) and
+// k_shade_bsdf (the BSDF sample, Russian roulette, the next ray).  The shaded
+// surface travels between them in 9 float4 per path; every expression is the
+// fused kernel's, in the same order, so the results are identical.
+
+__device__ __forceinline__ void store_surface(float4* out, v3 p, float t, v3 nn, bool entering, v3 geometric,
+                                              const Shaded& s) {
+  out[0] = make_float4(p.x, p.y, p.z, t);
+  out[1] = make_float4(nn.x, nn.y, nn.z, entering ? 1.0f : 0.0f);
+  out[2] = make_float4(geometric.x, geometric.y, geometric.z, s.roughness);
+  out[3] = make_float4(s.base.x, s.base.y, s.base.z, s.metalness);
+  out[4] = make_float4(s.specular, s.clearcoat, s.clearcoat_roughness, s.sheen);
+  out[5] = make_float4(s.transmission, s.ior, s.dispersion, s.thickness);
+  out[6] = make_float4(s.subsurface, s.subsurface_tint.x, s.subsurface_tint.y, s.subsurface_tint.z);
+  out[7] = make_float4(s.absorption, s.emission.x, s.emission.y, s.emission.z);
+  out[8] = make_float4(s.fresnel_power, 0.0f, 0.0f, 0.0f);
+}
+
+struct Surface {
+  v3 p, nn, geometric;
+  float t;
+  bool entering;
+  Shaded s;
+};
+
+__device__ __forceinline__ Surface load_surface_record(const float4* in) {
+  float4 a = in[0], b = in[1], c = in[2], e = in[3], f = in[4], g = in[5], h = in[6], k = in[7], m = in[8];
+  Surface S;
+  S.p = mk3(a.x, a.y, a.z);
+  S.t = a.w;
+  S.nn = mk3(b.x, b.y, b.z);
+  S.entering = b.w != 0.0f;
+  S.geometric = mk3(c.x, c.y, c.z);
+  S.s.roughness = c.w;
+  S.s.base = mk3(e.x, e.y, e.z);
+  S.s.metalness = e.w;
+  S.s.specular = f.x;
+  S.s.clearcoat = f.y;
+  S.s.clearcoat_roughness = f.z;
+  S.s.sheen = f.w;
+  S.s.transmission = g.x;
+  S.s.ior = g.y;
+  S.s.dispersion = g.z;
+  S.s.thickness = g.w;
+  S.s.subsurface = h.x;
+  S.s.subsurface_tint = mk3(h.y, h.z, h.w);
+  S.s.absorption = k.x;
+  S.s.emission = mk3(k.y, k.z, k.w);
+  S.s.fresnel_power = m.x;
+  return S;
+}
+
+__global__ void __launch_bounds__(kThreads) k_shade_hit(const __grid_constant__ Pass P, uint32_t which) {
+  const uint32_t n = P.w.counters[which];
+  const uint32_t* queue = P.bins ? P.w.sorted : P.w.queue[which];
+  const uint32_t bounce = P.bounce;
+  const Specialise& sp = P.sp;
+  const ShadeView& V = P.v;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    uint32_t qi = base + threadIdx.x;
+    bool active = qi < n;
+    bool lit = false;
+    uint32_t i = active ? queue[qi] : 0u;
+    if (active) {
+      float4 ro = P.w.ray_o[i], rd = P.w.ray_d[i], th = P.w.thr[i], rs = P.w.res[i];
+      v3 o = mk3(ro.x, ro.y, ro.z), d = mk3(rd.x, rd.y, rd.z);
+      float previous_pdf = ro.w;
+      uint32_t flags = __float_as_uint(rd.w);
+      v3 throughput = mk3(th.x, th.y, th.z);
+      v3 result = flush_pending(P, i, flags, mk3(rs.x, rs.y, rs.z));
+      flags &= ~(15u << F_PEND);
+      uint32_t pixel = __float_as_uint(rs.w);
+      float4 h = P.w.hit[i];
+      float reach = h.x;
+      v3 origin_point = spawn_point(o, neg3(d), o, 0.0f);
+      result = add3(result, capped(P, mul3(throughput, light_hits(V, o, d, reach, origin_point, previous_pdf)),
+                                   bounce > 1u));
+      if (h.x >= 1e19f) {
+        if (!(bounce == 0u && P.f.forward[3] > 0.0f)) {
+          float pdf = sky_pdf(V, d);
+          float weight = (bounce > 0u && previous_pdf > 0.0f) ? previous_pdf / (previous_pdf + pdf) : 1.0f;
+          result = add3(result, capped(P, scl3(mul3(throughput, sky_radiance(V)), weight), bounce > 1u));
+        }
+      } else {
+        HitInfo hit = fill_hit(P, h, P.w.hit_v[i]);
+        v3 p = add3(o, scl3(d, hit.t));
+        v3 nn = dot3(hit.n, d) > 0.0f ? neg3(hit.n) : hit.n;
+        Shaded s = load_surface(V, hit.material);
+        v3 geometric = dot3(hit.geometric, d) > 0.0f ? neg3(hit.geometric) : hit.geometric;
+        if (dot3(nn, geometric) < 0.05f) nn = normalize3(add3(nn, scl3(geometric, 0.1f)));
+        s.roughness = fmax_(s.roughness, 0.05f);
+        s.clearcoat_roughness = fmax_(s.clearcoat_roughness, 0.05f);
+        if (sp.filter_glossy > 0.0f && (flags & F_DIFFUSED)) {
+          s.roughness = fmax_(s.roughness, sp.filter_glossy);
+          s.clearcoat_roughness = fmax_(s.clearcoat_roughness, sp.filter_glossy);
+        }
+        if (bounce == 0u) {
+          P.w.alb[i] = make_float4(s.base.x, s.base.y, s.base.z, 1.0f);
+          P.w.nrm[i] = make_float4(nn.x, nn.y, nn.z, 1.0f);
+        }
+        s.emission = scl3(s.emission, emitter_weight(P, hit, p, origin_point, previous_pdf));
+        result = add3(result, capped(P, mul3(throughput, s.emission), bounce > 1u));
+        bool to_cache = false;
+        if (P.c.enabled && !(flags & F_LAST)) {
+          uint32_t ts = P.c.tslot[i];
+          if (ts != ~0u) {
+            if (bounce <= P.c.record_bounces) {
+              float4* vtx = P.c.tvert + ((size_t)(ts & 0xFFFFFFu) * (P.c.record_bounces + 1u) + bounce) * 7u;
+              cache_features(vtx, p, neg3(d), nn, s);
+              vtx[5] = make_float4(throughput.x, throughput.y, throughput.z, 0.0f);
+              vtx[6] = make_float4(result.x, result.y, result.z, 0.0f);
+              P.c.tslot[i] = ts | (1u << (24u + bounce));
+            }
+          } else if (bounce >= P.c.query_bounce && bounce <= P.c.query_last && cell_ok(P.c, p) &&
+                     (bounce == P.c.query_last || P.c.min_roughness <= 0.0f ||
+                      (s.roughness >= P.c.min_roughness && !(s.transmission > 0.0f)))) {
+            uint32_t k = claim(P.w.counters + 5, true);
+            cache_features(P.c.query + (size_t)k * 5u, p, neg3(d), nn, s);
+            P.c.cqueue[k] = i;
+            to_cache = true;
+            flags |= F_CACHED;
+          }
+        }
+        if (!(flags & F_LAST) && !to_cache) {
+          store_surface(P.w.surf + (size_t)i * 9u, p, hit.t, nn, dot3(hit.n, d) < 0.0f, geometric, s);
+          lit = true;
+        }
+      }
+      P.w.ray_d[i] = make_float4(d.x, d.y, d.z, __uint_as_float(flags));
+      P.w.res[i] = make_float4(result.x, result.y, result.z, __uint_as_float(pixel));
+    }
+    append(P.w.lit, P.w.counters + 12, i, active && lit);
+  }
+}
+
+template <bool DEFERRED>
+__global__ void __launch_bounds__(kThreads) k_shade_lights(const __grid_constant__ Pass P) {
+  const uint32_t n = P.w.counters[12];
+  const uint32_t bounce = P.bounce;
+  const Specialise& sp = P.sp;
+  const ShadeView& V = P.v;
+  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n; qi += gridDim.x * blockDim.x) {
+    const uint32_t i = P.w.lit[qi];
+    float4 ro = P.w.ray_o[i], rd = P.w.ray_d[i], th = P.w.thr[i], rs = P.w.res[i];
+    v3 o = mk3(ro.x, ro.y, ro.z), d = mk3(rd.x, rd.y, rd.z);
+    uint32_t flags = __float_as_uint(rd.w);
+    v3 throughput = mk3(th.x, th.y, th.z);
+    uint32_t state = __float_as_uint(th.w);
+    v3 result = mk3(rs.x, rs.y, rs.z);
+    uint32_t pixel = __float_as_uint(rs.w);
+    uint32_t px = pixel % P.width + P.f.window[2], py = pixel / P.width + P.f.window[3];
+    Rng r{hash_iqnt2d(px, py) ^ pass_seed(P), pass_accum(P) + P.sample, 16u * (bounce + 1u)};
+    const Surface S = load_surface_record(P.w.surf + (size_t)i * 9u);
+    const Shaded& s = S.s;
+    const v3 p = S.p, geometric = S.geometric;
+    m3 transform = basis(S.nn);
+    v3 wo = mulmtv(transform, neg3(d));
+    v3 origin = spawn_point(p, S.nn, o, S.t);
+    uint32_t pending = 0u;
+    for (uint32_t k = 0u; k < P.slots; ++k) {
+      float4 u = sobol4(V, sp, r, light_dim(k));
+      v3 local = mk3(0.0f, 0.0f, 1.0f), direction = mk3(0.0f, 0.0f, 1.0f), strength = splat3(0.0f);
+      float limit = 1e19f, pdf = 0.0f;
+      float lit_roughness = s.roughness;
+      if (k == 0u) {
+        if (P.f.sun_color[3] <= 0.0f) continue;
+        direction = normalize3(mk3(P.f.sun_dir[0], P.f.sun_dir[1], P.f.sun_dir[2]));
+        if (P.f.sun_dir[3] < 1.0f) {
+          float height = 1.0f - rnd(sp, state, u.x) * (1.0f - P.f.sun_dir[3]);
+          float radius = sqrtf(fmax_(0.0f, 1.0f - height * height));
+          float phi = 2.0f * SH_PI * rnd(sp, state, u.y);
+          m3 orient = basis(direction);
+          direction = normalize3(mulmv(orient, mk3(radius * cos_(phi), radius * sin_(phi), height)));
+        }
+        local = mulmtv(transform, direction);
+        if (local.z <= 0.0f) continue;
+        strength = scl3(mk3(P.f.sun_color[0], P.f.sun_color[1], P.f.sun_color[2]), P.f.sun_color[3] * 1.0f);
+      } else if (k == 1u) {
+        if (V.sky_width == 0u) continue;
+        float ux = rnd(sp, state, u.x);
+        float uy = rnd(sp, state, u.y);
+        SkySample light = sky_sample(V, ux, uy);
+        direction = light.direction;
+        local = mulmtv(transform, direction);
+        if (local.z <= 0.0f) continue;
+        strength = scl3(sky_radiance(V), 1.0f);
+        pdf = light.pdf;
+        if (!(pdf > 0.0f)) continue;
+      } else {
+        uint32_t slot = k - 2u;
+        Candidate picked;
+        if (slot > V.looped) {
+          float2 pk = tree_pick(V, P.light_rows, p, transform.c2, rnd(sp, state, u.z), nullptr);
+          if (!(pk.y > 0.0f)) {
+            picked = candidate_none();
+          } else {
+            picked = light_candidate(sp, load_light(V, f2u(pk.x)), transform, p, origin, geometric, state, u);
+            picked.scale = divs3(picked.scale, pk.y);
+          }
+        } else if (slot > 0u) {
+          picked = light_candidate(sp, load_light(V, slot - 1u), transform, p, origin, geometric, state, u);
+        } else if (V.emitter_count == 0u) {
+          picked = candidate_none();
+        } else {
+          picked = emitter_candidate(V, sp, transform, p, origin, state, u);
+        }
+        if (picked.limit < 0.0f) continue;
+        local = picked.wi;
+        direction = picked.direction;
+        strength = picked.scale;
+        pdf = picked.pdf;
+        limit = picked.limit;
+        lit_roughness = fmax_(s.roughness, picked.roughness);
+      }
+      if (pdf > 0.0f) {
+        float bsdf = bsdf_pdf(s, wo, local);
+        if (k == 1u) {
+          strength = divs3(strength, pdf + bsdf);
+        } else {
+          float ratio = bsdf / pdf;
+          strength = divs3(strength, pdf * (1.0f + ratio * ratio));
+        }
+      }
+      Shaded lit = s;
+      lit.roughness = lit_roughness;
+      v3 term = mul3(scl3(scl3(mul3(throughput, bsdf_eval(lit, wo, local)), pdf > 0.0f ? glossy_share(s) : 1.0f),
+                          local.z),
+                     strength);
+      term = capped(P, term, bounce > 0u);
+      if (term.x == 0.0f && term.y == 0.0f && term.z == 0.0f) continue;  // adds nothing, traces nothing
+      if (!DEFERRED) {
+        if (limit > 0.0f && traverse<true>(P.s, origin, direction, limit).hit) continue;
+        result = add3(result, term);
+        continue;
+      }
+      uint32_t slot_index = i * P.cap + pending;
+      P.w.sh_c[slot_index] = make_float4(term.x, term.y, term.z, 0.0f);
+      P.w.sh_o[slot_index] = make_float4(origin.x, origin.y, origin.z, limit);
+      P.w.sh_d[slot_index] = make_float4(direction.x, direction.y, direction.z, __uint_as_float(limit > 0.0f ? 0u : 1u));
+      if (limit > 0.0f) {
+        uint32_t at = atomicAdd(P.w.counters + 2, 1u);
+        P.w.squeue[at] = slot_index;
+      }
+      pending += 1u;
+    }
+    P.w.ray_d[i] = make_float4(d.x, d.y, d.z, __uint_as_float(flags | (pending << F_PEND)));
+    P.w.thr[i] = make_float4(throughput.x, throughput.y, throughput.z, __uint_as_float(state));
+    if (!DEFERRED) P.w.res[i] = make_float4(result.x, result.y, result.z, __uint_as_float(pixel));
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_shade_bsdf(const __grid_constant__ Pass P, uint32_t which) {
+  const uint32_t n = P.w.counters[12];
+  uint32_t* next_queue = P.w.queue[which ^ 1u];
+  uint32_t* next_count = P.w.counters + (which ^ 1u);
+  const uint32_t bounce = P.bounce;
+  const Specialise& sp = P.sp;
+  const ShadeView& V = P.v;
+  const uint32_t TOTAL = sp.total_bounces;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    uint32_t qi = base + threadIdx.x;
+    bool active = qi < n;
+    bool cont = false;
+    uint32_t i = active ? P.w.lit[qi] : 0u;
+    if (active) {
+      float4 ro = P.w.ray_o[i], rd = P.w.ray_d[i], th = P.w.thr[i];
+      v3 o = mk3(ro.x, ro.y, ro.z), d = mk3(rd.x, rd.y, rd.z);
+      float previous_pdf = ro.w;
+      uint32_t flags = __float_as_uint(rd.w);
+      const uint32_t pending = (flags >> F_PEND) & 15u;
+      v3 throughput = mk3(th.x, th.y, th.z);
+      uint32_t state = __float_as_uint(th.w);
+      uint32_t pixel = __float_as_uint(P.w.res[i].w);
+      uint32_t px = pixel % P.width + P.f.window[2], py = pixel / P.width + P.f.window[3];
+      Rng r{hash_iqnt2d(px, py) ^ pass_seed(P), pass_accum(P) + P.sample, 16u * (bounce + 1u)};
+      const Surface S = load_surface_record(P.w.surf + (size_t)i * 9u);
+      const Shaded& s = S.s;
+      const v3 p = S.p;
+      m3 transform = basis(S.nn);
+      v3 wo = mulmtv(transform, neg3(d));
+      bool entering = S.entering;
+      // BSDF sampling and the next ray (trace.wgsl:2472-2500)
+      uint32_t carried = flags & F_CARRIED;
+      BsdfSample sample = sample_bsdf(sp, s, wo, entering, carried, state, sobol4(V, sp, r, 3u));
+      v3 wi = sample.dir;
+      uint32_t l0 = lobe_count(flags, F_LOBE0) + (sample.lobe == 0u ? 1u : 0u);
+      uint32_t l1 = lobe_count(flags, F_LOBE1) + (sample.lobe == 1u ? 1u : 0u);
+      uint32_t l2 = lobe_count(flags, F_LOBE2) + (sample.lobe == 2u ? 1u : 0u);
+      bool diffused = (flags & F_DIFFUSED) || sample.lobe == 0u;
+      bool last = bounce >= TOTAL || l0 > sp.diffuse_bounces || l1 > sp.glossy_bounces || l2 > sp.transmission_bounces;
+      bool lit_vertex = (flags & F_LIT) != 0u;
+      bool through = sample.pdf < -1.5f && lit_vertex;
+      lit_vertex = sample.pdf > 0.0f || through;
+      bool go = true;
+      if (sample.pdf < 0.0f) {
+        throughput = mul3(throughput, sample.weight);
+        carried = sample.channel;
+        if (sample.pdf < -1.5f)
+          throughput = mul3(throughput, mul3(mk3(sqrtf(clamp_(s.base.x, 0.0f, 1.0f)), sqrtf(clamp_(s.base.y, 0.0f, 1.0f)),
+                                                 sqrtf(clamp_(s.base.z, 0.0f, 1.0f))),
+                                             beer(s.thickness, s.subsurface_tint, s.absorption)));
+        d = normalize3(mulmv(transform, wi));
+        previous_pdf = 0.0f;
+      } else if (wi.z <= 0.0f || sample.pdf <= 0.0f) {
+        go = false;
+      } else {
+        throughput = mul3(throughput, scl3(divs3(scl3(scl3(bsdf_eval(s, wo, wi), glossy_share(s)), wi.z), sample.pdf), 1.0f));
+        d = normalize3(mulmv(transform, wi));
+        previous_pdf = sample.pdf;
+      }
+      if (go) {
+        o = spawn_point(p, d, o, S.t);
+        if (bounce >= 3u) {
+          float keep = clamp_(fmax_(throughput.x, fmax_(throughput.y, throughput.z)), 0.05f, 0.95f);
+          Rng r0 = r;
+          if (rnd(sp, state, sobol4(V, sp, r0, 0u).x) > keep)
+            go = false;
+          else
+            throughput = divs3(throughput, keep);
+        }
+      }
+      flags = (carried & F_CARRIED) | (l0 << F_LOBE0) | (l1 << F_LOBE1) | (l2 << F_LOBE2) | (last ? F_LAST : 0u) |
+              (through ? F_THROUGH : 0u) | (lit_vertex ? F_LIT : 0u) | (diffused ? F_DIFFUSED : 0u);
+      flags |= pending << F_PEND;
+      cont = go;
+      P.w.ray_o[i] = make_float4(o.x, o.y, o.z, previous_pdf);
+      P.w.ray_d[i] = make_float4(d.x, d.y, d.z, __uint_as_float(flags));
+      P.w.thr[i] = make_float4(throughput.x, throughput.y, throughput.z, __uint_as_float(state));
+    }
+    append(next_queue, next_count, i, active && cont);
+  }
+}
+
 // ------------------------------------------------------------------ finish
 // Pending contributions of the last bounce, then Accum += (result, first
 // albedo, first normal) in sample order (trace.wgsl:2564-2567).
@@ -820,6 +1160,7 @@ int grid_for(const void* kernel, int threads) {
 // Persistent grids of the traversal kernels for 64, 128 and 256 threads per block.
 struct Grids {
   int trace_closest[3] = {0, 0, 0}, trace_any[3] = {0, 0, 0}, shade = 0, shade_inline = 0, flat = 0;
+  int shade_hit = 0, shade_lights = 0, shade_lights_inline = 0, shade_bsdf = 0;
 };
 Grids& grids() {
   static Grids g;
@@ -832,6 +1173,10 @@ Grids& grids() {
     g.trace_any[2] = grid_for((const void*)k_trace_queue<true, 256>, 256);
     g.shade = grid_for((const void*)k_shade<true>, kThreads);
     g.shade_inline = grid_for((const void*)k_shade<false>, kThreads);
+    g.shade_hit = grid_for((const void*)k_shade_hit, kThreads);
+    g.shade_lights = grid_for((const void*)k_shade_lights<true>, kThreads);
+    g.shade_lights_inline = grid_for((const void*)k_shade_lights<false>, kThreads);
+    g.shade_bsdf = grid_for((const void*)k_shade_bsdf, kThreads);
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -869,7 +1214,8 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
          o_shd = add(16ull * capacity * cap), o_shc = add(16ull * capacity * cap), o_q0 = add(4ull * capacity),
          o_q1 = add(4ull * capacity), o_sq = add(4ull * capacity * cap), o_act = add(4ull * capacity),
          o_cnt = add(64), o_keys = add(4ull * capacity), o_sorted = add(4ull * capacity),
-         o_hist = add(4ull * SORT_BINS), o_cursor = add(4ull * SORT_BINS);
+         o_hist = add(4ull * SORT_BINS), o_cursor = add(4ull * SORT_BINS), o_lit = add(4ull * capacity),
+         o_surf = add(144ull * capacity);
   if (need > t.wave_bytes) {
     if (t.d_wave) cudaFree(t.d_wave);
     t.d_wave = nullptr;
@@ -903,6 +1249,8 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
   w.sorted = reinterpret_cast<uint32_t*>(b + o_sorted);
   w.hist = reinterpret_cast<uint32_t*>(b + o_hist);
   w.cursor = reinterpret_cast<uint32_t*>(b + o_cursor);
+  w.lit = reinterpret_cast<uint32_t*>(b + o_lit);
+  w.surf = reinterpret_cast<float4*>(b + o_surf);
 }
 
 // Cache scratch for `pixels` paths: queries, their path indices and
@@ -1018,7 +1366,8 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
     memcpy(key.data(), &P, sizeof(P));
     uint64_t extra[8] = {count, (uint64_t)(uintptr_t)t.d_mask, (uint64_t)(uintptr_t)t.cache, deferred ? 1u : 0u,
                          t.cache ? (uint64_t)t.cache->s.steps : 0u, t.cache ? (uint64_t)t.cache->s.batch : 0u,
-                         (uint64_t)(uintptr_t)t.d_accum, (uint64_t)pixels | ((uint64_t)t.trace_threads << 32)};
+                         (uint64_t)(uintptr_t)t.d_accum,
+                         (uint64_t)pixels | ((uint64_t)t.trace_threads << 32) | ((uint64_t)t.split_shade << 48)};
     memcpy(key.data() + sizeof(P), extra, sizeof(extra));
     cudaGraphExec_t exec = nullptr;
     for (auto& e : t.graphs)
@@ -1086,10 +1435,18 @@ void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_
         k_sort_count<<<g.flat, 256, 0, st>>>(P, cur);
         k_sort_place<<<g.flat, 256, 0, st>>>(P, cur);
       }
-      if (deferred)
+      if (t.split_shade) {
+        k_shade_hit<<<g.shade_hit, kThreads, 0, st>>>(P, cur);
+        if (deferred)
+          k_shade_lights<true><<<g.shade_lights, kThreads, 0, st>>>(P);
+        else
+          k_shade_lights<false><<<g.shade_lights_inline, kThreads, 0, st>>>(P);
+        k_shade_bsdf<<<g.shade_bsdf, kThreads, 0, st>>>(P, cur);
+      } else if (deferred) {
         k_shade<true><<<g.shade, kThreads, 0, st>>>(P, cur);
-      else
+      } else {
         k_shade<false><<<g.shade_inline, kThreads, 0, st>>>(P, cur);
+      }
       if (P.c.enabled && bounce == P.c.query_last)
         cache_infer_launch(*t.cache, P.c.query, P.w.counters + 5, pixels, P.c.cqueue, P.c.pred, st);
       if (deferred) {

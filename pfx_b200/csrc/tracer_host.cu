@@ -321,6 +321,7 @@ void trace_set_tuning(pfxt_trace& t, const pfxt_tuning& k) {
   t.trace_threads = k.trace_threads;
   t.sort_shading = k.sort_shading != 0u;
   t.use_graphs = k.graphs != 0u;
+  t.split_shade = k.split_shade != 0u;
 }
 
 pfxt_tuning trace_get_tuning(const pfxt_trace& t) {
@@ -328,6 +329,7 @@ pfxt_tuning trace_get_tuning(const pfxt_trace& t) {
   k.trace_threads = t.trace_threads;
   k.sort_shading = t.sort_shading ? 1u : 0u;
   k.graphs = t.use_graphs ? 1u : 0u;
+  k.split_shade = t.split_shade ? 1u : 0u;
   k.pass_ms = t.tuned_pass_ms;
   return k;
 }
@@ -360,12 +362,13 @@ pfxt_tuning trace_autotune(pfxt_trace& t, uint32_t passes) {
   const bool graphs = t.use_graphs;
   uint32_t seed = 0x7e000000u;
   for (uint32_t threads : {64u, 128u, 256u})
-    for (uint32_t sort : {1u, 0u}) {
-      pfxt_tuning k{threads, sort, graphs ? 1u : 0u, 0.0f};
-      trace_set_tuning(t, k);
-      k.pass_ms = time_passes(t, passes, seed);
-      if (k.pass_ms < best.pass_ms) best = k;
-    }
+    for (uint32_t sort : {1u, 0u})
+      for (uint32_t split : {1u, 0u}) {
+        pfxt_tuning k{threads, sort, graphs ? 1u : 0u, split, 0.0f};
+        trace_set_tuning(t, k);
+        k.pass_ms = time_passes(t, passes, seed);
+        if (k.pass_ms < best.pass_ms) best = k;
+      }
   trace_set_tuning(t, best);
   t.tuned_pass_ms = best.pass_ms;
   t.samples = 0;  // the trial passes are not part of the image

@@ -107,6 +107,18 @@ def test_material_sort_keeps_the_image(gpu):
     assert np.array_equal(a.read_accum(), b.read_accum())
 
 
+@pytest.mark.parametrize("name", ["room_4k", "instanced_1080"])
+def test_split_shade_matches_the_fused_kernel(gpu, name):
+    w = synth.small(name, (64, 40), sampler="sobol")
+    a = Trace(w.scene, w.settings, w.width, w.height)
+    b = Trace(w.scene, w.settings, w.width, w.height)
+    b.set_tuning(split_shade=False)
+    for t in (a, b):
+        t.sample(2, 7)
+        t.sample(1, 8)
+    assert np.array_equal(a.read_accum(), b.read_accum())
+
+
 def test_graph_replay_matches_launches(gpu):
     # a captured pass replays with each pass's seed and sample offset
     w = synth.small("plain_512", (48, 40), sampler="sobol")
