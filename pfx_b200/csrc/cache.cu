@@ -34,8 +34,11 @@ constexpr uint32_t WAIT_LIMIT = 1u << 22;  // mbarrier polls before a wait gives
 constexpr uint32_t ERR_WAIT = 1u;
 
 // Shared memory of the inference kernel (bytes).
-constexpr uint32_t I_X = 0, I_H1 = 16384, I_H2 = 32768, I_W = 49152, I_CTRL = I_W + 18432;
-constexpr uint32_t I_SMEM = 100 * 1024;  // more than used: at most two CTAs (2 x 256 TMEM columns) per SM
+// The second hidden layer's operand reuses the input tile (whose MMA has
+// completed by then); the output layer's accumulator reuses the first's.
+constexpr uint32_t I_X = 0, I_H1 = 16384, I_H2 = I_X, I_W = 32768, I_CTRL = I_W + 18432;
+constexpr uint32_t I_SMEM = 52 * 1024;  // four CTAs (4 x 128 TMEM columns) per SM
+constexpr uint32_t I_TMEM = 128;
 // Shared memory of the training kernel.  dY, dH2 and dH1 are read as M = 128
 // MN-major operands whose rows 64..127 (16..127 for dY) are not data: the
 // 32 KB the descriptor spans from each of them stays inside the allocation,
@@ -221,7 +224,7 @@ __device__ __forceinline__ void ld64(uint32_t tbase, uint32_t warp, uint32_t col
 }
 
 // ------------------------------------------------------------------ inference
-__global__ void __launch_bounds__(128, 2)
+__global__ void __launch_bounds__(128, 4)
     k_infer(CacheGrid g, const __half2* __restrict__ table, const uint16_t* __restrict__ weights,
             const float4* __restrict__ queries, const uint32_t* __restrict__ n_dev, uint32_t n_max,
             const uint32_t* __restrict__ scatter, float4* __restrict__ out, uint32_t* error) {
@@ -234,11 +237,11 @@ __global__ void __launch_bounds__(128, 2)
   const uint32_t mb = umma::smem_addr(mbar);
   copy_weights(smem + I_W, weights);
   if (tid == 0) umma::mbar_init(mb, 1);
-  if (warp == 0) umma::tmem_alloc(slot, 256);
+  if (warp == 0) umma::tmem_alloc(slot, I_TMEM);
   umma::fence_async_smem();
   sync_tc();
   const uint32_t tbase = *slot;
-  const uint32_t T0 = tbase, T1 = tbase + 64, T2 = tbase + 128;
+  const uint32_t T0 = tbase, T1 = tbase + 64, T2 = tbase;  // T2: the output layer over T0's columns 0..15
   uint32_t count = n_dev ? min(*n_dev, n_max) : n_max;
   uint32_t phase = 0;
   bool late = false;
@@ -297,11 +300,11 @@ __global__ void __launch_bounds__(128, 2)
     if (__syncthreads_or(late)) break;
     umma::fence_after();
     float y[16];
-    umma::ld16(umma::taddr(tbase, 32u * warp, 128), y);
+    umma::ld16(umma::taddr(tbase, 32u * warp, 0), y);
     if (row < count) out[scatter ? scatter[row] : row] = make_float4(y[0], y[1], y[2], 0.0f);
     sync_tc();
   }
-  finish(late, mb, phase, error, tbase, 256);
+  finish(late, mb, phase, error, tbase, I_TMEM);
 }
 
 // ------------------------------------------------------------------ training
@@ -735,7 +738,7 @@ void cache_infer_launch(pfxt_cache& c, const float4* queries, const uint32_t* n_
                         const uint32_t* scatter, float4* out, cudaStream_t stream) {
   if (n == 0) return;
   uint32_t tiles = (n + NRC_ROWS - 1) / NRC_ROWS;
-  uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)sm_count() * 2u);
+  uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)sm_count() * 4u);
   k_infer<<<grid, 128, I_SMEM, stream>>>(c.grid, c.d_table16, c.d_weights, queries, n_dev, n, scatter, out,
                                          c.d_error);
   check(cudaGetLastError(), "cache inference");
