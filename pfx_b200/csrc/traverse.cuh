@@ -68,32 +68,76 @@ __device__ __forceinline__ TRay make_tray(v3 o, v3 d) {
   return t;
 }
 
-// Slab test of one box: true when the ray's geometry passes (degenerate axes
-// inside the slab, entry <= exit); `near` receives max(0, entries).
-__device__ __forceinline__ bool box_geometry(float lx, float ly, float lz, float hx, float hy, float hz,
-                                             const TRay& ray, float& near) {
+// Slab test of one box with IEEE division throughout: the rare case in which
+// a Markstein quotient below could be off by one rounding.
+static __device__ __noinline__ bool box_geometry_ieee(float lx, float ly, float lz, float hx, float hy, float hz,
+                                               const TRay& ray, float& near) {
   float n = 0.0f, f = INFINITY;
   if (fabsf(ray.d.x) < 1e-12f) {
     if (ray.o.x < lx || ray.o.x > hx) return false;
   } else {
-    float a = div_rn(lx - ray.o.x, ray.d.x, ray.r.x), b = div_rn(hx - ray.o.x, ray.d.x, ray.r.x);
+    float a = (lx - ray.o.x) / ray.d.x, b = (hx - ray.o.x) / ray.d.x;
     n = fmaxf(n, fminf(a, b));
     f = fminf(f, fmaxf(a, b));
   }
   if (fabsf(ray.d.y) < 1e-12f) {
     if (ray.o.y < ly || ray.o.y > hy) return false;
   } else {
-    float a = div_rn(ly - ray.o.y, ray.d.y, ray.r.y), b = div_rn(hy - ray.o.y, ray.d.y, ray.r.y);
+    float a = (ly - ray.o.y) / ray.d.y, b = (hy - ray.o.y) / ray.d.y;
     n = fmaxf(n, fminf(a, b));
     f = fminf(f, fmaxf(a, b));
   }
   if (fabsf(ray.d.z) < 1e-12f) {
     if (ray.o.z < lz || ray.o.z > hz) return false;
   } else {
-    float a = div_rn(lz - ray.o.z, ray.d.z, ray.r.z), b = div_rn(hz - ray.o.z, ray.d.z, ray.r.z);
+    float a = (lz - ray.o.z) / ray.d.z, b = (hz - ray.o.z) / ray.d.z;
     n = fmaxf(n, fminf(a, b));
     f = fminf(f, fmaxf(a, b));
   }
+  near = n;
+  return !(n > f);
+}
+
+// x / d by Markstein's correction from r = RN(1/d), correctly rounded unless
+// `bad` is raised (the guard of div_rn, gathered instead of branched on).
+__device__ __forceinline__ float quotient(float x, float d, float r, bool& bad) {
+  float q = x * r;
+  float e = fmaf(-q, d, x);
+  float q2 = fmaf(e, r, q);
+  bad |= !(fabsf(x) >= 0x1p-96f) || !(fabsf(q2) >= 0x1p-100f) || !(fabsf(q2) <= 0x1p+120f);
+  return q2;
+}
+
+// Slab test of one box: true when the ray's geometry passes (degenerate axes
+// inside the slab, entry <= exit); `near` receives max(0, entries).  The six
+// quotients equal IEEE division's (the reference divides); where one might
+// not, the box is tested again with IEEE division.
+__device__ __forceinline__ bool box_geometry(float lx, float ly, float lz, float hx, float hy, float hz,
+                                             const TRay& ray, float& near) {
+  float n = 0.0f, f = INFINITY;
+  bool bad = false;
+  if (fabsf(ray.d.x) < 1e-12f) {
+    if (ray.o.x < lx || ray.o.x > hx) return false;
+  } else {
+    float a = quotient(lx - ray.o.x, ray.d.x, ray.r.x, bad), b = quotient(hx - ray.o.x, ray.d.x, ray.r.x, bad);
+    n = fmaxf(n, fminf(a, b));
+    f = fminf(f, fmaxf(a, b));
+  }
+  if (fabsf(ray.d.y) < 1e-12f) {
+    if (ray.o.y < ly || ray.o.y > hy) return false;
+  } else {
+    float a = quotient(ly - ray.o.y, ray.d.y, ray.r.y, bad), b = quotient(hy - ray.o.y, ray.d.y, ray.r.y, bad);
+    n = fmaxf(n, fminf(a, b));
+    f = fminf(f, fmaxf(a, b));
+  }
+  if (fabsf(ray.d.z) < 1e-12f) {
+    if (ray.o.z < lz || ray.o.z > hz) return false;
+  } else {
+    float a = quotient(lz - ray.o.z, ray.d.z, ray.r.z, bad), b = quotient(hz - ray.o.z, ray.d.z, ray.r.z, bad);
+    n = fmaxf(n, fminf(a, b));
+    f = fminf(f, fmaxf(a, b));
+  }
+  if (bad) return box_geometry_ieee(lx, ly, lz, hx, hy, hz, ray, near);
   near = n;
   return !(n > f);
 }
