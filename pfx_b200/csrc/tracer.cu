@@ -384,8 +384,7 @@ __global__ void __launch_bounds__(THREADS) k_trace_queue(const __grid_constant__
   const uint32_t* queue = ANY ? P.w.squeue : P.w.queue[which];
   const uint32_t n = ANY ? P.w.counters[2] : P.w.counters[which];
   uint32_t* counter = P.w.counters + 4;
-  uint32_t sref[REF_STACK];
-  float snear[REF_STACK];
+  LaneStack<0> st;  // local memory: a shared-memory top measured slower (more registers, fewer warps)
   Walker<ANY, false> w;
   const int lane = threadIdx.x & 31;
   uint32_t idx = 0, item = 0;
@@ -413,8 +412,8 @@ __global__ void __launch_bounds__(THREADS) k_trace_queue(const __grid_constant__
     }
     if (__all_sync(FULL, retired)) break;
     if (have) {
-      w.inner_phase(P.s, sref, snear);
-      if (!w.done) w.leaf_phase(P.s, sref, snear);
+      w.inner_phase(P.s, st);
+      if (!w.done) w.leaf_phase(P.s, st);
       if (w.done) {
         if (ANY) {
           reinterpret_cast<float*>(P.w.sh_d + item)[3] = __uint_as_float(w.hit.hit ? 0u : 1u);

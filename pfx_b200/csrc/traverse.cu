@@ -37,8 +37,7 @@ __global__ void __launch_bounds__(kThreads) k_trace(SceneView s, const pfxt_ray*
   constexpr bool ANY = (MODE == 1 || MODE == 3);
   constexpr bool COUNT = (MODE >= 2);
   constexpr unsigned FULL = 0xffffffffu;
-  uint32_t sref[REF_STACK];
-  float snear[REF_STACK];
+  LaneStack<0> st;  // local memory: a shared-memory top measured slower (more registers, fewer warps)
   Walker<ANY, COUNT> w;
   const int lane = threadIdx.x & 31;
   uint32_t idx = 0;
@@ -66,8 +65,8 @@ __global__ void __launch_bounds__(kThreads) k_trace(SceneView s, const pfxt_ray*
     }
     if (__all_sync(FULL, retired)) break;
     if (have) {
-      w.inner_phase(s, sref, snear);
-      if (!w.done) w.leaf_phase(s, sref, snear);
+      w.inner_phase(s, st);
+      if (!w.done) w.leaf_phase(s, st);
       if (w.done) {
         if (MODE == 0) {
           reinterpret_cast<uint4*>(out)[idx] =

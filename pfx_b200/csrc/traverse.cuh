@@ -151,7 +151,55 @@ __device__ __forceinline__ v3 to_object(const float4& r0, const float4& r1, cons
   return o;
 }
 
-// One query's traversal state.  The stack lives in the caller (local memory).
+// The traversal stack of one lane.  With SHORT > 0 its first SHORT entries
+// live in shared memory, one column per lane (entry k of lane t at word
+// k * lanes + t, so a warp's accesses fall in distinct banks), and the rest
+// in local memory; with SHORT == 0 all of it is local.  Only where entries
+// are kept differs: the walk pushes and pops exactly the same entries.
+constexpr int SHORT_STACK = 16;
+
+template <int SHORT>
+struct LaneStack {
+  uint32_t* sh_ref;
+  float* sh_near;
+  uint32_t lanes;
+  uint32_t lref[REF_STACK - SHORT];
+  float lnear[REF_STACK - SHORT];
+  __device__ __forceinline__ void put(int k, uint32_t r, float n) {
+    if (k < SHORT) {
+      sh_ref[k * lanes] = r;
+      sh_near[k * lanes] = n;
+    } else {
+      lref[k - SHORT] = r;
+      lnear[k - SHORT] = n;
+    }
+  }
+  __device__ __forceinline__ void get(int k, uint32_t& r, float& n) const {
+    if (k < SHORT) {
+      r = sh_ref[k * lanes];
+      n = sh_near[k * lanes];
+    } else {
+      r = lref[k - SHORT];
+      n = lnear[k - SHORT];
+    }
+  }
+};
+
+template <>
+struct LaneStack<0> {
+  uint32_t lref[REF_STACK];
+  float lnear[REF_STACK];
+  __device__ __forceinline__ void put(int k, uint32_t r, float n) {
+    lref[k] = r;
+    lnear[k] = n;
+  }
+  __device__ __forceinline__ void get(int k, uint32_t& r, float& n) const {
+    r = lref[k];
+    n = lnear[k];
+  }
+};
+
+// One query's traversal state; the stack is the caller's.
 template <bool ANY, bool COUNT>
 struct Walker {
   v3 o, d;      // world ray
@@ -183,14 +231,14 @@ struct Walker {
     counts.boxes = counts.tris = 0u;
   }
 
-  __device__ __forceinline__ void pop(const uint32_t* sref, const float* snear) {
+  template <class Stack>
+  __device__ __forceinline__ void pop(const Stack& st) {
     if (top == 0) {
       done = true;
       return;
     }
     --top;
-    ref = sref[top];
-    near_cur = snear[top];
+    st.get(top, ref, near_cur);
     if (COUNT && ref != STACK_SENTINEL) counts.boxes += 1u;
   }
 
@@ -200,17 +248,18 @@ struct Walker {
 
   // Walk inner nodes until the current entry is a leaf that passes its
   // near check, or the traversal is finished.
-  __device__ __forceinline__ void inner_phase(const SceneView& s, uint32_t* sref, float* snear) {
+  template <class Stack>
+  __device__ __forceinline__ void inner_phase(const SceneView& s, Stack& st) {
     while (!done) {
       if (ref == STACK_SENTINEL) {
         ray = make_tray(o, d);
         base = record = word = 0u;
         inv_det = 1.0f;
-        pop(sref, snear);
+        pop(st);
         continue;
       }
       if (!(near_cur <= hit.t)) {
-        pop(sref, snear);
+        pop(st);
         continue;
       }
       if ((ref & REF_LEAF) == 0u) {
@@ -223,29 +272,27 @@ struct Walker {
         bool ok1 = has1 && box_geometry(q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, ray, n1) && n1 <= hit.t;
         if (COUNT) counts.boxes += 1u;  // the left child, popped next by the reference
         if ((ok1 || (COUNT && has1)) && top < (int)REF_STACK) {
-          sref[top] = q3.y;
-          snear[top] = ok1 ? n1 : INFINITY;
+          st.put(top, q3.y, ok1 ? n1 : INFINITY);
           ++top;
         }
         if (ok0) {
           ref = q3.x;
           near_cur = n0;
         } else {
-          pop(sref, snear);
+          pop(st);
         }
         continue;
       }
       if ((ref & REF_INST) == REF_INST) {
         if (top >= (int)REF_STACK) {  // refused at creation; never taken
-          pop(sref, snear);
+          pop(st);
           continue;
         }
         const float4* p = reinterpret_cast<const float4*>(s.insts + (ref & 0x3fffffffu));
         float4 r0 = __ldg(p + 0), r1 = __ldg(p + 1), r2 = __ldg(p + 2);
         uint4 m = __ldg(reinterpret_cast<const uint4*>(p + 3));
         float4 m2 = __ldg(p + 4);
-        sref[top] = STACK_SENTINEL;
-        snear[top] = -INFINITY;
+        st.put(top, STACK_SENTINEL, -INFINITY);
         ++top;
         base = m.y;
         record = m.z;
@@ -261,7 +308,8 @@ struct Walker {
   }
 
   // Test the triangles of the held leaf, then move to the next entry.
-  __device__ __forceinline__ void leaf_phase(const SceneView& s, uint32_t* sref, float* snear) {
+  template <class Stack>
+  __device__ __forceinline__ void leaf_phase(const SceneView& s, Stack& st) {
     uint32_t first = ref & LEAF_FIRST_MASK;
     uint32_t n = ((ref >> LEAF_FIRST_BITS) & 15u) + 1u;
     bool skip = ANY ? ((word & CASTS_NO_SHADOW) != 0u) : ((word & SHADOW_ONLY) != 0u);
@@ -304,15 +352,16 @@ struct Walker {
         }
       }
     }
-    pop(sref, snear);
+    pop(st);
   }
 
   // Run to completion (one query, no work sharing).
-  __device__ __forceinline__ void run(const SceneView& s, uint32_t* sref, float* snear) {
+  template <class Stack>
+  __device__ __forceinline__ void run(const SceneView& s, Stack& st) {
     while (!done) {
-      inner_phase(s, sref, snear);
+      inner_phase(s, st);
       if (done) break;
-      leaf_phase(s, sref, snear);
+      leaf_phase(s, st);
     }
   }
 };
@@ -320,11 +369,10 @@ struct Walker {
 // Single-query helpers used by shading code.
 template <bool ANY>
 __device__ __forceinline__ TraceHit traverse(const SceneView& s, v3 o, v3 d, float limit) {
-  uint32_t sref[REF_STACK];
-  float snear[REF_STACK];
+  LaneStack<0> st;
   Walker<ANY, false> w;
   w.start(s, o, d, limit);
-  w.run(s, sref, snear);
+  w.run(s, st);
   return w.hit;
 }
 
