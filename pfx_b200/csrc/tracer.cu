@@ -379,7 +379,8 @@ __global__ void k_rewind(const __grid_constant__ Pass P) {
 // THREADS per block is a launch choice of the autotuner: the walk is per lane
 // and the refill per warp, so the block size changes only the residency.
 template <bool ANY, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_trace_queue(const __grid_constant__ Pass P,uint32_t which) {
+__global__ void __launch_bounds__(THREADS, TRACE_WARPS_PER_SM * 32 / THREADS) k_trace_queue(const __grid_constant__ Pass P,
+                                                                                       uint32_t which) {
   constexpr unsigned FULL = 0xffffffffu;
   const uint32_t* queue = ANY ? P.w.squeue : P.w.queue[which];
   const uint32_t n = ANY ? P.w.counters[2] : P.w.counters[which];

@@ -32,7 +32,7 @@ __device__ __forceinline__ void load_ray(const pfxt_ray* __restrict__ rays, uint
 // MODE 0: closest hit -> pfxt_hit; MODE 1: any hit -> u32 flag;
 // MODE 2/3: work counters of closest / any hit -> uint2.
 template <int MODE>
-__global__ void __launch_bounds__(kThreads) k_trace(SceneView s, const pfxt_ray* __restrict__ rays, uint32_t n,
+__global__ void __launch_bounds__(kThreads, TRACE_WARPS_PER_SM * 32 / kThreads) k_trace(SceneView s, const pfxt_ray* __restrict__ rays, uint32_t n,
                                                     void* __restrict__ out, uint32_t* __restrict__ counter) {
   constexpr bool ANY = (MODE == 1 || MODE == 3);
   constexpr bool COUNT = (MODE >= 2);

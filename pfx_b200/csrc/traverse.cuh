@@ -158,6 +158,13 @@ __device__ __forceinline__ v3 to_object(const float4& r0, const float4& r1, cons
 // are kept differs: the walk pushes and pops exactly the same entries.
 constexpr int SHORT_STACK = 16;
 
+// Resident warps per SM the traversal kernels are compiled for: it sets their
+// register budget.  32 warps (64 registers, a few bytes of spill) measured
+// faster than 24 (72 registers) and 36 (56 registers, more spills).
+#ifndef TRACE_WARPS_PER_SM
+#define TRACE_WARPS_PER_SM 32
+#endif
+
 template <int SHORT>
 struct LaneStack {
   uint32_t* sh_ref;
