@@ -615,12 +615,13 @@ __global__ void __launch_bounds__(kThreads, SHADE_MIN_BLOCKS) k_shade(const __gr
           v3 origin = spawn_point(p, nn, o, hit.t);
           bool entering = dot3(hit.n, d) < 0.0f;
           for (uint32_t k = 0u; k < P.slots; ++k) {
-            float4 u = sobol4(V, sp, r, light_dim(k));
+            float4 u;  // the slot's Sobol sample, looked up once the slot is known to be live
             v3 local = mk3(0.0f, 0.0f, 1.0f), direction = mk3(0.0f, 0.0f, 1.0f), strength = splat3(0.0f);
             float limit = 1e19f, pdf = 0.0f;
             float lit_roughness = s.roughness;
             if (k == 0u) {
               if (P.f.sun_color[3] <= 0.0f) continue;
+              u = sobol4(V, sp, r, light_dim(k));
               direction = normalize3(mk3(P.f.sun_dir[0], P.f.sun_dir[1], P.f.sun_dir[2]));
               if (P.f.sun_dir[3] < 1.0f) {
                 float height = 1.0f - rnd(sp, state, u.x) * (1.0f - P.f.sun_dir[3]);
@@ -634,8 +635,11 @@ __global__ void __launch_bounds__(kThreads, SHADE_MIN_BLOCKS) k_shade(const __gr
               strength = scl3(mk3(P.f.sun_color[0], P.f.sun_color[1], P.f.sun_color[2]), P.f.sun_color[3] * 1.0f);
             } else if (k == 1u) {
               if (V.sky_width == 0u) continue;
+              u = sobol4(V, sp, r, light_dim(k));
               float ux = rnd(sp, state, u.x);
               float uy = rnd(sp, state, u.y);
+              // a black sky adds nothing (its sample is drawn all the same)
+              if (V.sky_radiance[0] == 0.0f && V.sky_radiance[1] == 0.0f && V.sky_radiance[2] == 0.0f) continue;
               SkySample light = sky_sample(V, ux, uy);
               direction = light.direction;
               local = mulmtv(transform, direction);
@@ -645,6 +649,8 @@ __global__ void __launch_bounds__(kThreads, SHADE_MIN_BLOCKS) k_shade(const __gr
               if (!(pdf > 0.0f)) continue;
             } else {
               uint32_t slot = k - 2u;
+              if (slot == 0u && V.emitter_count == 0u) continue;  // no emissive triangles
+              u = sobol4(V, sp, r, light_dim(k));
               Candidate picked;
               if (slot > V.looped) {
                 float2 pk = tree_pick(V, P.light_rows, p, transform.c2, rnd(sp, state, u.z), nullptr);
@@ -918,12 +924,13 @@ __global__ void __launch_bounds__(kThreads) k_shade_lights(const __grid_constant
     v3 origin = spawn_point(p, S.nn, o, S.t);
     uint32_t pending = 0u;
     for (uint32_t k = 0u; k < P.slots; ++k) {
-      float4 u = sobol4(V, sp, r, light_dim(k));
+      float4 u;  // the slot's Sobol sample, looked up once the slot is known to be live
       v3 local = mk3(0.0f, 0.0f, 1.0f), direction = mk3(0.0f, 0.0f, 1.0f), strength = splat3(0.0f);
       float limit = 1e19f, pdf = 0.0f;
       float lit_roughness = s.roughness;
       if (k == 0u) {
         if (P.f.sun_color[3] <= 0.0f) continue;
+        u = sobol4(V, sp, r, light_dim(k));
         direction = normalize3(mk3(P.f.sun_dir[0], P.f.sun_dir[1], P.f.sun_dir[2]));
         if (P.f.sun_dir[3] < 1.0f) {
           float height = 1.0f - rnd(sp, state, u.x) * (1.0f - P.f.sun_dir[3]);
@@ -937,8 +944,11 @@ __global__ void __launch_bounds__(kThreads) k_shade_lights(const __grid_constant
         strength = scl3(mk3(P.f.sun_color[0], P.f.sun_color[1], P.f.sun_color[2]), P.f.sun_color[3] * 1.0f);
       } else if (k == 1u) {
         if (V.sky_width == 0u) continue;
+        u = sobol4(V, sp, r, light_dim(k));
         float ux = rnd(sp, state, u.x);
         float uy = rnd(sp, state, u.y);
+        // a black sky adds nothing (its sample is drawn all the same)
+        if (V.sky_radiance[0] == 0.0f && V.sky_radiance[1] == 0.0f && V.sky_radiance[2] == 0.0f) continue;
         SkySample light = sky_sample(V, ux, uy);
         direction = light.direction;
         local = mulmtv(transform, direction);
@@ -948,6 +958,8 @@ __global__ void __launch_bounds__(kThreads) k_shade_lights(const __grid_constant
         if (!(pdf > 0.0f)) continue;
       } else {
         uint32_t slot = k - 2u;
+        if (slot == 0u && V.emitter_count == 0u) continue;  // no emissive triangles
+        u = sobol4(V, sp, r, light_dim(k));
         Candidate picked;
         if (slot > V.looped) {
           float2 pk = tree_pick(V, P.light_rows, p, transform.c2, rnd(sp, state, u.z), nullptr);
