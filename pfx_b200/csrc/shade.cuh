@@ -438,6 +438,19 @@ __device__ __forceinline__ LightRow load_light(const ShadeView& v, uint32_t i) {
   l.d = __ldg(p + 3);
   return l;
 }
+// The trigonometry of a light-tree row's cones, which its importance needs at
+// every visit, computed once per row by the same functions (k_light_trig):
+// node  = (cos theta_o, sin theta_o, cos(theta_o + theta_e), cos(theta_e - theta_o))
+//         of a tree node (theta_o = c.w, theta_e = d.x);
+// light = (theta_e, cos theta_e, cos 0, sin 0) of a light (theta_o = 0; a
+//         spot's theta_e = acos(-d.y / d.x), otherwise pi / 2).
+struct RowTrig {
+  float4 node, light;
+};
+__device__ __forceinline__ RowTrig load_trig(const ShadeView& v, uint32_t i) {
+  return RowTrig{__ldg(v.light_trig + 2u * i), __ldg(v.light_trig + 2u * i + 1u)};
+}
+
 __device__ __forceinline__ v3 f3of(float4 q) { return mk3(q.x, q.y, q.z); }
 __device__ __forceinline__ float mis_power(float chosen, float other) {
   if (chosen <= 0.0f) return 0.0f;
@@ -597,8 +610,9 @@ SH_CALL Candidate light_candidate(const Specialise& sp, const LightRow& light, c
 __device__ __forceinline__ float sin_from_cos(float c) { return sqrtf(fmax_(1.0f - c * c, 0.0f)); }
 
 // tree_importance (lights.wgsl:204-237) -> (max, min)
+// trig = (cos theta_o, sin theta_o, cos(theta_o + theta_e), cos(theta_e - theta_o)).
 SH_SMALL float2 tree_importance(v3 n, v3 to, float cos_u, v3 axis, float theta_o, float theta_e,
-                                                  float far, float near, float energy) {
+                                                  float far, float near, float energy, float4 trig) {
   float sin_u = sin_from_cos(cos_u);
   float cos_i = dot3(to, n);
   float sin_i = sin_from_cos(cos_i);
@@ -612,24 +626,24 @@ SH_SMALL float2 tree_importance(v3 n, v3 to, float cos_u, v3 axis, float theta_o
     sin_t = sin_from_cos(cos_t);
   }
   float cos_t_minus_u = cos_t * cos_u + sin_t * sin_u;
-  float cos_o = cos_(theta_o);
-  float sin_o = sin_(theta_o);
+  float cos_o = trig.x;
+  float sin_o = trig.y;
   float cos_min_out;
   if (cos_t >= cos_u || cos_t_minus_u >= cos_o) {
     cos_min_out = 1.0f;
-  } else if (theta_o + theta_e > SH_PI || cos_t_minus_u > cos_(theta_o + theta_e)) {
+  } else if (theta_o + theta_e > SH_PI || cos_t_minus_u > trig.z) {
     cos_min_out = cos_t_minus_u * cos_o + sin_from_cos(cos_t_minus_u) * sin_o;
   } else {
     return make_float2(0.0f, 0.0f);
   }
   float most = abs_(cos_min_i * energy * cos_min_out / (near * near));
   float cos_t_plus_u = cos_t * cos_u - sin_t * sin_u;
-  if (theta_e - theta_o < 0.0f || cos_t < 0.0f || cos_u < 0.0f || cos_t_plus_u < cos_(theta_e - theta_o))
+  if (theta_e - theta_o < 0.0f || cos_t < 0.0f || cos_u < 0.0f || cos_t_plus_u < trig.w)
     return make_float2(most, 0.0f);
   float cos_max_out = cos_t_plus_u * cos_o - sin_from_cos(cos_t_plus_u) * sin_o;
   return make_float2(most, abs_(cos_max_i * energy * cos_max_out / (far * far)));
 }
-SH_SMALL float2 node_importance(const LightRow& node, v3 p, v3 n) {
+SH_SMALL float2 node_importance(const LightRow& node, float4 trig, v3 p, v3 n) {
   v3 lo = f3of(node.a), hi = f3of(node.b);
   v3 centroid = scl3(add3(lo, hi), 0.5f);
   v3 extent = sub3(hi, centroid);
@@ -642,9 +656,10 @@ SH_SMALL float2 node_importance(const LightRow& node, v3 p, v3 n) {
   if (reach * reach > radius2) cos_u = sqrtf(fmax_(1.0f - radius2 / (reach * reach), 0.0f));
   float distance = fmax_(fmax_(0.5f * sqrtf(radius2), reach), 1e-6f);
   return tree_importance(n, divs3(to, fmax_(reach, 1e-30f)), cos_u, f3of(node.c), node.c.w, node.d.x, distance,
-                         distance, node.a.w);
+                         distance, node.a.w, trig);
 }
-SH_SMALL float2 emitter_importance(const LightRow& light, v3 p, v3 n) {
+// trig: the light's RowTrig::light.
+SH_SMALL float2 emitter_importance(const LightRow& light, float4 trig, v3 p, v3 n) {
   v3 to = sub3(f3of(light.a), p);
   float near = length3(to);
   if (near >= light.b.w || near <= 1e-6f) return make_float2(0.0f, 0.0f);
@@ -653,18 +668,23 @@ SH_SMALL float2 emitter_importance(const LightRow& light, v3 p, v3 n) {
   float far = sqrtf(radius * radius + near * near);
   float cos_u = near / far;
   float energy = (light.b.x + light.b.y + light.b.z) / 3.0f;
+  const float4 cones = make_float4(trig.z, trig.w, trig.y, trig.y);  // theta_o = 0
   if (f2u(light.a.w) == 1u) {
-    float theta_e = acos_(clamp_(-light.d.y / light.d.x, -1.0f, 1.0f));
+    float theta_e = trig.x;
     float cos_min_out = cos_(fmax_(0.0f, acos_(clamp_(dot3(f3of(light.c), neg3(toward)), -1.0f, 1.0f)) - acos_(cos_u)));
     float along = clamp_(cos_min_out * light.d.x + light.d.y, 0.0f, 1.0f);
     energy = energy * (along * along);
-    return tree_importance(n, toward, cos_u, f3of(light.c), 0.0f, theta_e, far, near, energy);
+    return tree_importance(n, toward, cos_u, f3of(light.c), 0.0f, theta_e, far, near, energy, cones);
   }
-  return tree_importance(n, toward, cos_u, neg3(toward), 0.0f, SH_PI / 2.0f, far, near, energy);
+  return tree_importance(n, toward, cos_u, neg3(toward), 0.0f, trig.x, far, near, energy, cones);
 }
-__device__ __forceinline__ float2 child_importance(const ShadeView& v, const LightRow& node, v3 p, v3 n) {
-  if (f2u(node.d.y) == 1u) return emitter_importance(load_light(v, f2u(node.d.z)), p, n);
-  return node_importance(node, p, n);
+__device__ __forceinline__ float2 child_importance(const ShadeView& v, uint32_t row, v3 p, v3 n) {
+  LightRow node = load_light(v, row);
+  if (f2u(node.d.y) == 1u) {
+    uint32_t light = f2u(node.d.z);
+    return emitter_importance(load_light(v, light), load_trig(v, light).light, p, n);
+  }
+  return node_importance(node, load_trig(v, row).node, p, n);
 }
 
 // tree_leaf (lights.wgsl:276-349): (selected row, pmf)
@@ -678,7 +698,7 @@ SH_CALL float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 
   uint32_t has = 0u;
   for (uint32_t i = 0u; i < count; ++i) {
     int32_t index = (int32_t)(first + i);
-    float2 importance = emitter_importance(load_light(v, first + i), p, n);
+    float2 importance = emitter_importance(load_light(v, first + i), load_trig(v, first + i).light, p, n);
     float weight = sample_max ? importance.x : importance.y;
     float other = sample_max ? importance.y : importance.x;
     if (weight > 0.0f) {
@@ -735,7 +755,8 @@ SH_CALL float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 
       }
       chosen_min = 1.0f;
       total_min = valid;
-      chosen_max = emitter_importance(load_light(v, (uint32_t)selected), p, n).x;
+      chosen_max =
+          emitter_importance(load_light(v, (uint32_t)selected), load_trig(v, (uint32_t)selected).light, p, n).x;
     }
   }
   return make_float2((float)selected, 0.5f * (chosen_max / total_max + chosen_min / total_min));
@@ -760,8 +781,8 @@ SH_CALL float2 tree_pick(const ShadeView& v, uint32_t rows, v3 p, v3 n, float st
     uint32_t left = at + 1u;
     uint32_t right = f2u(node.d.z);
     if (right >= rows) break;
-    float2 l = child_importance(v, load_light(v, left), p, n);
-    float2 r = child_importance(v, load_light(v, right), p, n);
+    float2 l = child_importance(v, left, p, n);
+    float2 r = child_importance(v, right, p, n);
     float total_max = l.x + r.x;
     if (total_max == 0.0f) return make_float2(0.0f, 0.0f);
     float total_min = l.y + r.y;

@@ -1327,6 +1327,33 @@ void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_
 
 }  // namespace
 
+namespace {
+// RowTrig of every light row (shade.cuh), by the functions and expressions the
+// importance of a row used to evaluate at each visit.
+__global__ void k_light_trig(const __grid_constant__ ShadeView V, uint32_t rows, float4* __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+    LightRow r = load_light(V, i);
+    float theta_o = r.c.w, theta_e = r.d.x;
+    out[2u * i] = make_float4(cos_(theta_o), sin_(theta_o), cos_(theta_o + theta_e), cos_(theta_e - theta_o));
+    float cone = f2u(r.a.w) == 1u ? acos_(clamp_(-r.d.y / r.d.x, -1.0f, 1.0f)) : SH_PI / 2.0f;
+    out[2u * i + 1u] = make_float4(cone, cos_(cone), cos_(0.0f), sin_(0.0f));
+  }
+}
+}  // namespace
+
+void light_trig_init(pfxt_trace& t) {
+  uint32_t rows = std::max<uint32_t>(t.light_rows, 1u);
+  void* d = nullptr;
+  check(cudaMalloc(&d, (size_t)rows * 32u), "light-row trigonometry");
+  t.owned.push_back(d);
+  t.shade.light_trig = static_cast<const float4*>(d);
+  if (t.light_rows) {
+    k_light_trig<<<(t.light_rows + 127u) / 128u, 128, 0, t.stream>>>(t.shade, t.light_rows, static_cast<float4*>(d));
+    check(cudaGetLastError(), "light-row trigonometry");
+  }
+  check(cudaStreamSynchronize(t.stream), "light-row trigonometry");
+}
+
 void trace_forget_graphs(pfxt_trace& t) {
   for (auto& e : t.graphs) cudaGraphExecDestroy(e.exec);
   t.graphs.clear();

@@ -50,6 +50,7 @@ struct ShadeView {
   const GpuEmitter* __restrict__ emitters;
   const float* __restrict__ emitter_cdf;
   const GpuLight* __restrict__ lights;
+  const float4* __restrict__ light_trig;  // 2 float4 per light row: its cones' trigonometry (shade.cuh RowTrig)
   const float* __restrict__ sky_rows;
   const float* __restrict__ sky_columns;
   const float4* __restrict__ sobol;
@@ -148,6 +149,8 @@ void trace_set_camera(pfxt_trace& t, const pfxt_camera& c);
 void trace_set_lens(pfxt_trace& t, const float lens[4]);
 void trace_set_window(pfxt_trace& t, const uint32_t full[2], const uint32_t origin[2]);
 void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed);
+// The light rows' cone trigonometry (ShadeView::light_trig), once per tracer.
+void light_trig_init(pfxt_trace& t);
 // Drops the captured passes (their buffers or launch parameters changed).
 void trace_forget_graphs(pfxt_trace& t);
 void trace_set_tuning(pfxt_trace& t, const pfxt_tuning& k);

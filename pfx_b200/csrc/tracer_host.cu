@@ -212,6 +212,8 @@ void trace_init(pfxt_trace& t, const pfxt_buffers& b, const pfxt_scene& view, co
   sp.sobol_length = sp.sobol ? b.sobol_length : 256u;
   sp.clamp_indirect = s.clamp_indirect;
   sp.filter_glossy = s.filter_glossy;
+
+  light_trig_init(t);
 }
 
 void trace_release(pfxt_trace& t) {
