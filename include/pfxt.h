@@ -296,6 +296,7 @@ typedef struct pfxt_tuning {
   uint32_t sort_shading;  /* sort the shade queue by hit material every bounce (1) */
   uint32_t graphs;        /* replay each pass from a captured CUDA graph (1) */
   uint32_t split_shade;   /* shade a bounce in three kernels (hit, light slots, BSDF) instead of one (1) */
+  uint32_t sort_rays;     /* sort the rays of every bounce after the first by direction and origin (0) */
   float pass_ms;          /* from pfxt_autotune: the chosen configuration's median pass time */
 } pfxt_tuning;
 

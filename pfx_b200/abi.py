@@ -116,7 +116,7 @@ class Adaptive(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("trace_threads", C.c_uint32), ("sort_shading", C.c_uint32), ("graphs", C.c_uint32),
-                ("split_shade", C.c_uint32), ("pass_ms", C.c_float)]
+                ("split_shade", C.c_uint32), ("sort_rays", C.c_uint32), ("pass_ms", C.c_float)]
 
 
 class CacheSettings(C.Structure):

@@ -77,6 +77,8 @@ struct Wave {
   // split shade: the paths that scatter this bounce (count at counters[12]) and their surfaces
   uint32_t* lit;
   float4* surf;        // 9 float4 per path
+  uint32_t* rhist;     // RAY_BINS: the extend queue's histogram by ray key
+  uint32_t* rcursor;
 };
 
 // The radiance cache as the wave sees it (all null/zero when none is attached).
@@ -113,6 +115,8 @@ struct Pass {
   uint32_t slots;      // 2 + light_slots()
   uint32_t width, height;
   uint32_t bins;       // 2 x (material keys + 1 for misses); 0 = the shade queue is not sorted
+  uint32_t ray_bins;   // RAY_BINS when the extend queue of bounces after the first is sorted by ray key, else 0
+  float scene_lo[3], scene_inv[3];  // the scene box, for the ray key's origin cell
   // What changes from pass to pass lives in device memory, written by the
   // pass's first operation, so one captured pass replays for every pass:
   // [0] samples accumulated before the pass, [1] samples in it, [2] seed.
@@ -268,11 +272,16 @@ __global__ void k_reset(const __grid_constant__ Pass P,uint32_t cur) {
     P.w.counters[12] = 0u;
     reinterpret_cast<unsigned long long*>(P.w.counters + 8)[0] += P.w.counters[cur];
   }
-  if (blockIdx.x == 0)
+  if (blockIdx.x == 0) {
     for (uint32_t b = threadIdx.x; b < P.bins; b += blockDim.x) {
       P.w.hist[b] = 0u;
       P.w.cursor[b] = 0u;
     }
+    for (uint32_t b = threadIdx.x; b < P.ray_bins; b += blockDim.x) {
+      P.w.rhist[b] = 0u;
+      P.w.rcursor[b] = 0u;
+    }
+  }
 }
 
 // ------------------------------------------------------------------ sort
@@ -320,46 +329,73 @@ __device__ __forceinline__ void block_chunk(uint32_t n, uint32_t& first, uint32_
   last = min(n, first + per);
 }
 
-__global__ void __launch_bounds__(256) k_sort_count(const __grid_constant__ Pass P,uint32_t which) {
+// The extend queue of the bounces after the first grouped by ray: direction
+// octant x a 4 x 4 x 4 cell of the origin in the scene box, so that a warp's
+// rays walk the same parts of the tree.
+constexpr uint32_t RAY_BINS = 512;
+
+__device__ __forceinline__ uint32_t ray_key(const Pass& P, uint32_t i) {
+  float4 o = P.w.ray_o[i], d = P.w.ray_d[i];
+  float q[3] = {o.x, o.y, o.z};
+  uint32_t cell = 0u;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float u = (q[k] - P.scene_lo[k]) * P.scene_inv[k];
+    u = u > 0.0f ? (u < 1.0f ? u : 1.0f) : 0.0f;
+    cell = cell * 4u + min((uint32_t)(u * 4.0f), 3u);
+  }
+  uint32_t octant = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+  return octant * 64u + cell;
+}
+
+// RAYS: the extend queue by ray_key (RAY_BINS); otherwise the shade queue by material_key (P.bins).
+template <bool RAYS>
+__global__ void __launch_bounds__(256) k_sort_count(const __grid_constant__ Pass P, uint32_t which) {
   __shared__ uint32_t hist[SORT_BINS];
   const uint32_t n = P.w.counters[which];
   const uint32_t* queue = P.w.queue[which];
-  for (uint32_t b = threadIdx.x; b < P.bins; b += blockDim.x) hist[b] = 0u;
+  const uint32_t bins = RAYS ? P.ray_bins : P.bins;
+  for (uint32_t b = threadIdx.x; b < bins; b += blockDim.x) hist[b] = 0u;
   __syncthreads();
   uint32_t first, last;
   block_chunk(n, first, last);
   for (uint32_t q = first + threadIdx.x; q < last; q += blockDim.x) {
-    uint32_t key = material_key(P, queue[q]);
+    uint32_t key = RAYS ? ray_key(P, queue[q]) : material_key(P, queue[q]);
     P.w.keys[q] = key;
     atomicAdd(&hist[key], 1u);
   }
   __syncthreads();
-  for (uint32_t b = threadIdx.x; b < P.bins; b += blockDim.x)
-    if (hist[b]) atomicAdd(P.w.hist + b, hist[b]);
+  uint32_t* global = RAYS ? P.w.rhist : P.w.hist;
+  for (uint32_t b = threadIdx.x; b < bins; b += blockDim.x)
+    if (hist[b]) atomicAdd(global + b, hist[b]);
 }
 
-__global__ void __launch_bounds__(256) k_sort_place(const __grid_constant__ Pass P,uint32_t which) {
+template <bool RAYS>
+__global__ void __launch_bounds__(256) k_sort_place(const __grid_constant__ Pass P, uint32_t which) {
   __shared__ uint32_t base[SORT_BINS];
   __shared__ uint32_t local[SORT_BINS];
   const uint32_t n = P.w.counters[which];
   const uint32_t* queue = P.w.queue[which];
+  const uint32_t bins = RAYS ? P.ray_bins : P.bins;
+  const uint32_t* global = RAYS ? P.w.rhist : P.w.hist;
+  uint32_t* cursor = RAYS ? P.w.rcursor : P.w.cursor;
   // exclusive scan of the global histogram (one thread: the bins are few)
   if (threadIdx.x == 0) {
     uint32_t run = 0u;
-    for (uint32_t b = 0; b < P.bins; ++b) {
+    for (uint32_t b = 0; b < bins; ++b) {
       base[b] = run;
-      run += P.w.hist[b];
+      run += global[b];
     }
   }
-  for (uint32_t b = threadIdx.x; b < P.bins; b += blockDim.x) local[b] = 0u;
+  for (uint32_t b = threadIdx.x; b < bins; b += blockDim.x) local[b] = 0u;
   __syncthreads();
   uint32_t first, last;
   block_chunk(n, first, last);
   for (uint32_t q = first + threadIdx.x; q < last; q += blockDim.x) atomicAdd(&local[P.w.keys[q]], 1u);
   __syncthreads();
-  for (uint32_t b = threadIdx.x; b < P.bins; b += blockDim.x) {
+  for (uint32_t b = threadIdx.x; b < bins; b += blockDim.x) {
     uint32_t c = local[b];
-    base[b] += c ? atomicAdd(P.w.cursor + b, c) : 0u;
+    base[b] += c ? atomicAdd(cursor + b, c) : 0u;
     local[b] = 0u;
   }
   __syncthreads();
@@ -382,7 +418,7 @@ template <bool ANY, int THREADS>
 __global__ void __launch_bounds__(THREADS, TRACE_WARPS_PER_SM * 32 / THREADS) k_trace_queue(const __grid_constant__ Pass P,
                                                                                        uint32_t which) {
   constexpr unsigned FULL = 0xffffffffu;
-  const uint32_t* queue = ANY ? P.w.squeue : P.w.queue[which];
+  const uint32_t* queue = ANY ? P.w.squeue : ((P.ray_bins && P.bounce > 0u) ? P.w.sorted : P.w.queue[which]);
   const uint32_t n = ANY ? P.w.counters[2] : P.w.counters[which];
   uint32_t* counter = P.w.counters + 4;
   LaneStack<0> st;  // local memory: a shared-memory top measured slower (more registers, fewer warps)
@@ -1227,7 +1263,7 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
          o_q1 = add(4ull * capacity), o_sq = add(4ull * capacity * cap), o_act = add(4ull * capacity),
          o_cnt = add(64), o_keys = add(4ull * capacity), o_sorted = add(4ull * capacity),
          o_hist = add(4ull * SORT_BINS), o_cursor = add(4ull * SORT_BINS), o_lit = add(4ull * capacity),
-         o_surf = add(144ull * capacity);
+         o_surf = add(144ull * capacity), o_rhist = add(4ull * RAY_BINS), o_rcursor = add(4ull * RAY_BINS);
   if (need > t.wave_bytes) {
     if (t.d_wave) cudaFree(t.d_wave);
     t.d_wave = nullptr;
@@ -1263,6 +1299,8 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
   w.cursor = reinterpret_cast<uint32_t*>(b + o_cursor);
   w.lit = reinterpret_cast<uint32_t*>(b + o_lit);
   w.surf = reinterpret_cast<float4*>(b + o_surf);
+  w.rhist = reinterpret_cast<uint32_t*>(b + o_rhist);
+  w.rcursor = reinterpret_cast<uint32_t*>(b + o_rcursor);
 }
 
 // Cache scratch for `pixels` paths: queries, their path indices and
@@ -1386,6 +1424,12 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   P.width = t.width;
   P.height = t.height;
   P.c = ensure_cache(t, pixels);
+  P.ray_bins = t.sort_rays ? RAY_BINS : 0u;
+  for (int k = 0; k < 3; ++k) {
+    float extent = t.bounds_hi[k] - t.bounds_lo[k];
+    P.scene_lo[k] = t.bounds_lo[k];
+    P.scene_inv[k] = extent > 0.0f ? 1.0f / extent : 0.0f;
+  }
   P.bins = t.sort_shading ? 2u * std::max<uint32_t>(std::min<uint32_t>(t.shade.material_count + 1u, SORT_BINS / 2u), 2u)
                           : 0u;
   ensure_vars(t);
@@ -1469,10 +1513,14 @@ void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_
       uint32_t cur = bounce & 1u;
       P.bounce = bounce;
       k_reset<<<1, 32, 0, st>>>(P, cur);
+      if (P.ray_bins && bounce > 0u) {
+        k_sort_count<true><<<g.flat, 256, 0, st>>>(P, cur);
+        k_sort_place<true><<<g.flat, 256, 0, st>>>(P, cur);
+      }
       launch_trace_queue<false>(thread_select(t.trace_threads), P, cur, st);
       if (P.bins) {
-        k_sort_count<<<g.flat, 256, 0, st>>>(P, cur);
-        k_sort_place<<<g.flat, 256, 0, st>>>(P, cur);
+        k_sort_count<false><<<g.flat, 256, 0, st>>>(P, cur);
+        k_sort_place<false><<<g.flat, 256, 0, st>>>(P, cur);
       }
       if (t.split_shade) {
         k_shade_hit<<<g.shade_hit, kThreads, 0, st>>>(P, cur);

@@ -120,6 +120,7 @@ struct pfxt_trace {
   bool sort_shading = true;                    // group the shade queue by material every bounce
   uint32_t trace_threads = 128;                // threads per block of the traversal kernels (64, 128, 256)
   bool split_shade = true;                     // shade in three kernels (hit, lights, BSDF) or one
+  bool sort_rays = false;                      // group the extend queue of later bounces by ray
   float tuned_pass_ms = 0.0f;                  // the autotuner's measured pass time, 0 = not tuned
   uint32_t* d_error = nullptr;  // device error word
   uint32_t* d_counters = nullptr;  // ring of work-sharing counters (device scratch)

@@ -324,6 +324,7 @@ void trace_set_tuning(pfxt_trace& t, const pfxt_tuning& k) {
   t.sort_shading = k.sort_shading != 0u;
   t.use_graphs = k.graphs != 0u;
   t.split_shade = k.split_shade != 0u;
+  t.sort_rays = k.sort_rays != 0u;
 }
 
 pfxt_tuning trace_get_tuning(const pfxt_trace& t) {
@@ -332,6 +333,7 @@ pfxt_tuning trace_get_tuning(const pfxt_trace& t) {
   k.sort_shading = t.sort_shading ? 1u : 0u;
   k.graphs = t.use_graphs ? 1u : 0u;
   k.split_shade = t.split_shade ? 1u : 0u;
+  k.sort_rays = t.sort_rays ? 1u : 0u;
   k.pass_ms = t.tuned_pass_ms;
   return k;
 }
@@ -365,12 +367,13 @@ pfxt_tuning trace_autotune(pfxt_trace& t, uint32_t passes) {
   uint32_t seed = 0x7e000000u;
   for (uint32_t threads : {64u, 128u, 256u})
     for (uint32_t sort : {1u, 0u})
-      for (uint32_t split : {1u, 0u}) {
-        pfxt_tuning k{threads, sort, graphs ? 1u : 0u, split, 0.0f};
-        trace_set_tuning(t, k);
-        k.pass_ms = time_passes(t, passes, seed);
-        if (k.pass_ms < best.pass_ms) best = k;
-      }
+      for (uint32_t split : {1u, 0u})
+        for (uint32_t rays : {0u, 1u}) {
+          pfxt_tuning k{threads, sort, graphs ? 1u : 0u, split, rays, 0.0f};
+          trace_set_tuning(t, k);
+          k.pass_ms = time_passes(t, passes, seed);
+          if (k.pass_ms < best.pass_ms) best = k;
+        }
   trace_set_tuning(t, best);
   t.tuned_pass_ms = best.pass_ms;
   t.samples = 0;  // the trial passes are not part of the image

@@ -339,11 +339,11 @@ class Trace:
         k = abi.Tuning()
         check(self._lib.pfxt_get_tuning(self._h, C.byref(k)))
         return {"trace_threads": k.trace_threads, "sort_shading": bool(k.sort_shading), "graphs": bool(k.graphs),
-                "split_shade": bool(k.split_shade), "pass_ms": float(k.pass_ms)}
+                "split_shade": bool(k.split_shade), "sort_rays": bool(k.sort_rays), "pass_ms": float(k.pass_ms)}
 
     def set_tuning(self, trace_threads: int = 128, sort_shading: bool = True, graphs: bool = True,
-                   split_shade: bool = True) -> None:
-        k = abi.Tuning(trace_threads, int(sort_shading), int(graphs), int(split_shade), 0.0)
+                   split_shade: bool = True, sort_rays: bool = False) -> None:
+        k = abi.Tuning(trace_threads, int(sort_shading), int(graphs), int(split_shade), int(sort_rays), 0.0)
         check(self._lib.pfxt_set_tuning(self._h, C.byref(k)))
 
     def autotune(self, passes: int = 3) -> dict:

@@ -112,7 +112,7 @@ def test_split_shade_matches_the_fused_kernel(gpu, name):
     w = synth.small(name, (64, 40), sampler="sobol")
     a = Trace(w.scene, w.settings, w.width, w.height)
     b = Trace(w.scene, w.settings, w.width, w.height)
-    b.set_tuning(split_shade=False)
+    b.set_tuning(split_shade=False, sort_rays=True)
     for t in (a, b):
         t.sample(2, 7)
         t.sample(1, 8)
