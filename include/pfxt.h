@@ -288,6 +288,32 @@ int pfxt_occluded_device(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count
 int pfxt_occluded_noalloc(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count, uint8_t* blocked,
                           void* stream);
 
+/* ------------------------------------------------------------ checkpoints
+ * The reference's checkpoint byte layout (crates/trace/src/checkpoint.rs:8-158):
+ * "PFXCKPT1", the key's length (u64) and bytes, width, height, samples (u32),
+ * the 48 B/pixel accumulation, the colour, albedo and normal films (16 B/pixel
+ * each), then u32 0xffffffff, or a round count, the rounds (u32 samples, u64
+ * active) and 32 B/pixel adaptive snapshots; all little-endian. */
+typedef struct pfxt_checkpoint_info {
+  uint32_t width, height, samples;
+  uint32_t rounds; /* adaptive rounds recorded; 0xffffffff when none */
+} pfxt_checkpoint_info;
+
+/* Trace::save + Saved::write_to (checkpoint.rs:82-104, 161-172): the
+ * accumulation and films under `key`, without adaptive rounds.  With bytes ==
+ * NULL, *written receives the size needed; otherwise capacity must hold it. */
+int pfxt_save(pfxt_trace* trace, const char* key, void* bytes, size_t capacity, size_t* written);
+/* Saved::read_from + Trace::restore (checkpoint.rs:106-158, 174-203): refuses a
+ * checkpoint of another key or size, cut short or running past its end; the
+ * adaptive part is read and checked but, as in the reference, not restored. */
+int pfxt_restore(pfxt_trace* trace, const char* key, const void* bytes, size_t length);
+/* Saved::read_from alone, on the host: checks a checkpoint and describes it. */
+int pfxt_checkpoint_read(const char* key, const void* bytes, size_t length, pfxt_checkpoint_info* out);
+
+/* Trace::set_projection (gpu.rs:2872-2890): PFXT_PROJECTION_*, the
+ * orthographic width and height; restarts the accumulation. */
+int pfxt_set_projection(pfxt_trace* trace, uint32_t projection, const float ortho[2]);
+
 /* ------------------------------------------------------------ launch tuning
  * Launch choices that change how long a sampling pass takes but no value it
  * computes.  No counterpart in the reference (wgpu sizes its own dispatches). */

@@ -114,6 +114,10 @@ class Adaptive(C.Structure):
                 ("growth", C.c_float)]
 
 
+class CheckpointInfo(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("samples", C.c_uint32), ("rounds", C.c_uint32)]
+
+
 class Tuning(C.Structure):
     _fields_ = [("trace_threads", C.c_uint32), ("sort_shading", C.c_uint32), ("graphs", C.c_uint32),
                 ("split_shade", C.c_uint32), ("sort_rays", C.c_uint32), ("pass_ms", C.c_float)]
@@ -166,6 +170,10 @@ PROTOTYPES = [
     ("pfxt_trace_rays_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pfxt_occluded_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pfxt_occluded_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("pfxt_save", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    ("pfxt_restore", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]),
+    ("pfxt_checkpoint_read", C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, C.POINTER(CheckpointInfo)]),
+    ("pfxt_set_projection", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_float)]),
     ("pfxt_get_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     ("pfxt_set_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     ("pfxt_autotune", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),

@@ -424,6 +424,127 @@ int pfxt_films_device(pfxt_trace* t, float** color, float** albedo, float** norm
   });
 }
 
+/* ------------------------------------------------------------ checkpoints */
+
+namespace {
+constexpr char CKPT_MAGIC[8] = {'P', 'F', 'X', 'C', 'K', 'P', 'T', '1'};
+constexpr uint64_t CKPT_ACCUM = 48, CKPT_TEXEL = 16, CKPT_SNAP = 32;
+
+// Saved::read_from (checkpoint.rs:106-158): where each part of a checkpoint lies.
+struct Checkpoint {
+  uint32_t width = 0, height = 0, samples = 0, rounds = 0xffffffffu;
+  const uint8_t* accum = nullptr;
+  const uint8_t* films[3] = {nullptr, nullptr, nullptr};
+};
+
+Checkpoint read_checkpoint(const char* key, const void* bytes, size_t length) {
+  if (!key || (!bytes && length)) throw Invalid("null argument");
+  const uint8_t* p = static_cast<const uint8_t*>(bytes);
+  uint64_t left = length;
+  auto take = [&](uint64_t n) {
+    if (n > left) throw Invalid("the checkpoint is cut short: failed to fill whole buffer");
+    const uint8_t* at = p;
+    p += n;
+    left -= n;
+    return at;
+  };
+  auto word = [&]() {
+    uint32_t v;
+    memcpy(&v, take(4), 4);
+    return v;
+  };
+  auto longword = [&]() {
+    uint64_t v;
+    memcpy(&v, take(8), 8);
+    return v;
+  };
+  if (memcmp(take(8), CKPT_MAGIC, 8) != 0) throw Invalid("not a pfx checkpoint");
+  const uint64_t key_length = strlen(key);
+  if (longword() != key_length) throw Invalid("the checkpoint was made by another render");
+  if (memcmp(take(key_length), key, key_length) != 0) throw Invalid("the checkpoint was made by another render");
+  Checkpoint c;
+  c.width = word();
+  c.height = word();
+  c.samples = word();
+  const uint64_t pixels = (uint64_t)c.width * c.height;
+  if (pixels > (1ull << 40)) throw Invalid("the checkpoint is too large");
+  c.accum = take(pixels * CKPT_ACCUM);
+  for (auto& film : c.films) film = take(pixels * CKPT_TEXEL);
+  c.rounds = word();
+  if (c.rounds != 0xffffffffu) {
+    for (uint32_t r = 0; r < c.rounds; ++r) {
+      word();
+      longword();
+    }
+    take(pixels * CKPT_SNAP);
+  }
+  if (left != 0) throw Invalid("the checkpoint runs on past its end");
+  return c;
+}
+}  // namespace
+
+int pfxt_checkpoint_read(const char* key, const void* bytes, size_t length, pfxt_checkpoint_info* out) {
+  return guarded([&]() {
+    Checkpoint c = read_checkpoint(key, bytes, length);
+    if (out) *out = pfxt_checkpoint_info{c.width, c.height, c.samples, c.rounds};
+  });
+}
+
+int pfxt_save(pfxt_trace* t, const char* key, void* bytes, size_t capacity, size_t* written) {
+  return guarded([&]() {
+    if (!t || !key || !written) throw Invalid("null argument");
+    const uint64_t key_length = strlen(key);
+    const uint64_t pixels = (uint64_t)t->width * t->height;
+    const uint64_t need = 8 + 8 + key_length + 12 + pixels * (CKPT_ACCUM + 3 * CKPT_TEXEL) + 4;
+    *written = (size_t)need;
+    if (!bytes) return;
+    if (capacity < need) throw Invalid("the buffer is smaller than the checkpoint");
+    uint8_t* p = static_cast<uint8_t*>(bytes);
+    auto put = [&](const void* src, size_t n) {
+      memcpy(p, src, n);
+      p += n;
+    };
+    put(CKPT_MAGIC, 8);
+    put(&key_length, 8);
+    put(key, key_length);
+    uint32_t head[3] = {t->width, t->height, t->samples};
+    put(head, 12);
+    check(cudaStreamSynchronize(t->stream), "checkpoint");
+    check(cudaMemcpy(p, t->d_accum, pixels * CKPT_ACCUM, cudaMemcpyDeviceToHost), "checkpoint");
+    p += pixels * CKPT_ACCUM;
+    for (const float4* film : {t->d_color, t->d_albedo, t->d_normal}) {
+      check(cudaMemcpy(p, film, pixels * CKPT_TEXEL, cudaMemcpyDeviceToHost), "checkpoint");
+      p += pixels * CKPT_TEXEL;
+    }
+    uint32_t none = 0xffffffffu;
+    put(&none, 4);
+  });
+}
+
+int pfxt_restore(pfxt_trace* t, const char* key, const void* bytes, size_t length) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    Checkpoint c = read_checkpoint(key, bytes, length);
+    if (c.width != t->width || c.height != t->height)
+      throw Invalid("the checkpoint is " + std::to_string(c.width) + "x" + std::to_string(c.height) +
+                    " and the trace " + std::to_string(t->width) + "x" + std::to_string(t->height));
+    const uint64_t pixels = (uint64_t)t->width * t->height;
+    check(cudaStreamSynchronize(t->stream), "restore");
+    check(cudaMemcpy(t->d_accum, c.accum, pixels * CKPT_ACCUM, cudaMemcpyHostToDevice), "restore");
+    float4* films[3] = {t->d_color, t->d_albedo, t->d_normal};
+    for (int k = 0; k < 3; ++k)
+      check(cudaMemcpy(films[k], c.films[k], pixels * CKPT_TEXEL, cudaMemcpyHostToDevice), "restore");
+    t->samples = c.samples;
+  });
+}
+
+int pfxt_set_projection(pfxt_trace* t, uint32_t projection, const float ortho[2]) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    trace_set_projection(*t, projection, ortho);
+  });
+}
+
 /* ------------------------------------------------------------ launch tuning */
 
 int pfxt_get_tuning(pfxt_trace* t, pfxt_tuning* out) {

@@ -36,7 +36,9 @@
 // Out-of-line on the device: the transcendentals are called from many sites of
 // the shading kernel, and one shared copy keeps its code in the instruction
 // cache.
+#ifndef PFXT_HDN
 #define PFXT_HDN static __host__ __device__ __noinline__
+#endif
 #else
 #define PFXT_HD static inline
 #define PFXT_HDN static inline

@@ -154,6 +154,7 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed);
 void light_trig_init(pfxt_trace& t);
 // Drops the captured passes (their buffers or launch parameters changed).
 void trace_forget_graphs(pfxt_trace& t);
+void trace_set_projection(pfxt_trace& t, uint32_t projection, const float ortho[2]);
 void trace_set_tuning(pfxt_trace& t, const pfxt_tuning& k);
 pfxt_tuning trace_get_tuning(const pfxt_trace& t);
 pfxt_tuning trace_autotune(pfxt_trace& t, uint32_t passes);

@@ -316,6 +316,34 @@ std::vector<uint32_t> adaptive_rounds(const pfxt_adaptive& a) {
   }
 }
 
+// Trace::set_projection (gpu.rs:2872-2890) with Projection::valid, fits and
+// place (gpu.rs:191-218).
+void trace_set_projection(pfxt_trace& t, uint32_t projection, const float ortho[2]) {
+  if (projection > PFXT_PROJECTION_EQUIRECT) throw Invalid("invalid projection");
+  if (projection == PFXT_PROJECTION_ORTHOGRAPHIC &&
+      (!ortho || !std::isfinite(ortho[0]) || !std::isfinite(ortho[1]) || !(ortho[0] > 0.0f) || !(ortho[1] > 0.0f)))
+    throw Invalid("invalid projection");
+  if (projection != PFXT_PROJECTION_PERSPECTIVE) {
+    const float* axes[] = {t.base.forward, t.base.right, t.base.up};
+    for (auto a : axes)
+      if (!(a[0] * a[0] + a[1] * a[1] + a[2] * a[2] > 1e-12f))
+        throw Invalid("an orthographic or equirect camera needs forward, right and up");
+  }
+  float kind = 0.0f, half_width = 0.0f, half_height = 0.0f;
+  if (projection == PFXT_PROJECTION_ORTHOGRAPHIC) {
+    kind = 1.0f;
+    half_width = ortho[0] * 0.5f;
+    half_height = ortho[1] * 0.5f;
+  } else if (projection == PFXT_PROJECTION_EQUIRECT) {
+    kind = 2.0f;
+  }
+  t.base.origin[3] = kind;
+  t.base.right[3] = half_width;
+  t.base.up[3] = half_height;
+  t.projection = projection;
+  t.samples = 0;
+}
+
 // ------------------------------------------------------------------ tuning
 void trace_set_tuning(pfxt_trace& t, const pfxt_tuning& k) {
   if (k.trace_threads != 64u && k.trace_threads != 128u && k.trace_threads != 256u)

@@ -296,6 +296,24 @@ class Trace:
         lens = abi.f4(shift[0], shift[1], aperture, focus_distance)
         check(self._lib.pfxt_set_lens(self._h, lens))
 
+    def set_projection(self, projection: str = "perspective", width: float = 0.0, height: float = 0.0) -> None:
+        """Trace::set_projection (gpu.rs:2872): "perspective", "orthographic" (width,
+        height) or "equirect"; restarts the accumulation."""
+        kind = {"perspective": 0, "orthographic": 1, "equirect": 2}[projection]
+        check(self._lib.pfxt_set_projection(self._h, kind, (C.c_float * 2)(width, height)))
+
+    def save(self, key: str) -> bytes:
+        """Trace::save + Saved::write_to (checkpoint.rs): the checkpoint bytes."""
+        need = C.c_size_t()
+        check(self._lib.pfxt_save(self._h, key.encode(), None, 0, C.byref(need)))
+        buf = (C.c_uint8 * need.value)()
+        check(self._lib.pfxt_save(self._h, key.encode(), buf, need.value, C.byref(need)))
+        return bytes(buf)
+
+    def restore(self, key: str, data: bytes) -> None:
+        """Saved::read_from + Trace::restore (checkpoint.rs)."""
+        check(self._lib.pfxt_restore(self._h, key.encode(), data, len(data)))
+
     def set_window(self, full, origin) -> None:
         f = (C.c_uint32 * 2)(*full)
         o = (C.c_uint32 * 2)(*origin)
