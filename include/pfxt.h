@@ -314,6 +314,29 @@ int pfxt_checkpoint_read(const char* key, const void* bytes, size_t length, pfxt
  * orthographic width and height; restarts the accumulation. */
 int pfxt_set_projection(pfxt_trace* trace, uint32_t projection, const float ortho[2]);
 
+/* ------------------------------------------------------- moving instances
+ * Trace::move_instances (gpu.rs:2433-2530) on the host buffers of a built
+ * scene: new column-major 4x4 transforms (16 floats each) for its first `count`
+ * instances.  Moved instances get new surface records and emitter vertices and
+ * the top-level BVH is laid again; every buffer keeps its size and address.
+ * *moved (may be NULL) is 1 when any transform differed bit for bit. */
+int pfxt_scene_move_instances(pfxt_scene_blobs* blobs, const float* transforms, uint32_t count, uint32_t* moved);
+/* Trace::builds (gpu.rs:2356, Builds gpu.rs:400-403): bottom-level BVHs built
+ * (the world's and one per distinct mesh) and top-level BVHs laid (1 for a
+ * scene with instances, one more per move). */
+int pfxt_scene_builds(const pfxt_scene_blobs* blobs, uint32_t* bottom, uint32_t* top);
+/* Trace::set_instance_transforms (gpu.rs:2422-2431): the same on the blobs the
+ * trace was created from, then the moved buffers are uploaded (finish_tops,
+ * gpu.rs:2533-2540) and the accumulation restarts when anything moved. */
+int pfxt_set_instance_transforms(pfxt_trace* trace, pfxt_scene_blobs* blobs, const float* transforms, uint32_t count,
+                                 uint32_t* moved);
+/* Trace::finish_tops (gpu.rs:2533-2546) for a host that moves instances in
+ * buffers it packs itself: uploads the nodes, surface records, emitters and
+ * emitter CDF of `buffers` (the same sizes as at pfxt_create; the triangles
+ * are read only to lay the traversal nodes again) and restarts the
+ * accumulation. */
+int pfxt_finish_tops(pfxt_trace* trace, const pfxt_buffers* buffers);
+
 /* ------------------------------------------------------------ launch tuning
  * Launch choices that change how long a sampling pass takes but no value it
  * computes.  No counterpart in the reference (wgpu sizes its own dispatches). */

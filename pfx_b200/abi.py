@@ -174,6 +174,11 @@ PROTOTYPES = [
     ("pfxt_restore", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]),
     ("pfxt_checkpoint_read", C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, C.POINTER(CheckpointInfo)]),
     ("pfxt_set_projection", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_float)]),
+    ("pfxt_scene_move_instances", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
+    ("pfxt_scene_builds", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    ("pfxt_finish_tops", C.c_int, [C.c_void_p, C.POINTER(Buffers)]),
+    ("pfxt_set_instance_transforms", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                               C.POINTER(C.c_uint32)]),
     ("pfxt_get_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     ("pfxt_set_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     ("pfxt_autotune", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(Tuning)]),

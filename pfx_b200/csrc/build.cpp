@@ -870,6 +870,82 @@ uint32_t stack_need(const std::vector<GpuNode>& nodes, uint32_t index, int guard
 
 }  // namespace
 
+// Levels::meshes / placed / world (levels.rs:11-48) and the emitter candidates
+// with the light counts (gpu.rs:530-540): what moving an instance rewrites.
+struct Placing {
+  struct Mesh {
+    std::vector<pfxt_triangle> triangles;  // local space, BVH order: slot first + j
+    uint32_t root, first;
+    Bounds bounds;
+  };
+  struct Placed {
+    uint32_t mesh, base, record;
+    float transform[16];
+    Bounds bounds;
+    float inverse[12];
+  };
+  std::vector<Mesh> meshes;
+  std::vector<int> placed_index;  // per instance: index into `placed`, -1 for an empty mesh
+  std::vector<Placed> placed;
+  bool world = false;
+  Bounds world_bounds;
+  uint32_t world_root = 0;
+  uint32_t top_len = 0;
+  std::vector<Candidate> candidates;
+  size_t looped = 0, tree = 0;
+};
+
+namespace {
+
+// Levels::top (levels.rs:393-470) with `room` = 0, written over nodes
+// [0, top_len): the instance BVH over the world and every placed instance,
+// leaves patched to enter their group, then one inverse-rows node per group.
+void lay_top(const Placing& s, GpuNode* out) {
+  struct Group {
+    Bounds bounds;
+    uint32_t root, base, record;
+    const float* inverse;  // null for the world group
+  };
+  std::vector<Group> groups;
+  if (s.world) groups.push_back(Group{s.world_bounds, s.world_root, 0u, 0u, nullptr});
+  for (const auto& p : s.placed) groups.push_back(Group{p.bounds, s.meshes[p.mesh].root, p.base, p.record, p.inverse});
+  if (groups.empty()) return;
+  std::vector<Bounds> boxes;
+  for (auto& g : groups) boxes.push_back(g.bounds);
+  Bvh top = bvh_over(boxes, INSTANCE_LEAVES);
+  uint32_t tree = (uint32_t)top.nodes.size();
+  if ((size_t)tree + groups.size() != s.top_len) throw Invalid("the instance BVH does not fill its nodes");
+  size_t at = 0;
+  for (auto node : top.nodes) {
+    if (node.count > 0) {
+      uint32_t index = top.order[node.first];
+      const Group& g = groups[index];
+      node.first = g.root;
+      node.count = g.base;
+      node.lo[3] = bits2f(g.record);
+      node.pad[0] = INSTANCE_LEAF;
+      node.pad[1] = g.inverse ? tree + index : 0u;
+    }
+    out[at++] = node;
+  }
+  for (auto& g : groups) {
+    static const float identity[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
+    const float* r = g.inverse ? g.inverse : identity;
+    GpuNode n{};
+    for (int k = 0; k < 4; ++k) {
+      n.lo[k] = r[k];
+      n.hi[k] = r[4 + k];
+    }
+    n.first = f2bits(r[8]);
+    n.count = f2bits(r[9]);
+    n.pad[0] = f2bits(r[10]);
+    n.pad[1] = f2bits(r[11]);
+    out[at++] = n;
+  }
+}
+
+}  // namespace
+
 // ======================================================================
 SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings) {
   auto out = std::make_unique<SceneBlobs>();
@@ -1051,89 +1127,50 @@ SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings) 
       placed.push_back(p);
     }
     slots = next;
-    // Levels::top (levels.rs:393-470) with `room` = 0.
-    struct Group {
-      Bounds bounds;
-      uint32_t root, base, record;
-      bool has_inverse;
-      float inverse[12];
-    };
-    std::vector<Group> groups;
-    bool world = !world_bvh.nodes.empty();
-    size_t group_count = (world ? 1 : 0) + placed.size();
-    size_t top_len = group_count == 0 ? 0 : 3 * group_count - 1;
-    uint32_t offset = (uint32_t)top_len;
-    uint32_t world_root = 0;
-    if (world) {
-      world_root = offset;
+    // Node offsets of the world and mesh BVHs after the top (levels.rs:361-375).
+    auto state = std::make_shared<Placing>();
+    Placing& s = *state;
+    s.world = !world_bvh.nodes.empty();
+    size_t group_count = (s.world ? 1 : 0) + placed.size();
+    s.top_len = group_count == 0 ? 0u : (uint32_t)(3 * group_count - 1);
+    uint32_t offset = s.top_len;
+    if (s.world) {
+      s.world_root = offset;
+      for (int k = 0; k < 3; ++k) {
+        s.world_bounds.lo[k] = world_bvh.nodes[0].lo[k];
+        s.world_bounds.hi[k] = world_bvh.nodes[0].hi[k];
+      }
       offset += (uint32_t)world_bvh.nodes.size();
     }
     for (auto& mesh : meshes) {
       mesh.root = offset;
       offset += (uint32_t)mesh.nodes.size();
+      s.meshes.push_back(Placing::Mesh{mesh.triangles, mesh.root, mesh.first, mesh.bounds});
     }
-    if (world) {
-      Group g;
-      for (int k = 0; k < 3; ++k) {
-        g.bounds.lo[k] = world_bvh.nodes[0].lo[k];
-        g.bounds.hi[k] = world_bvh.nodes[0].hi[k];
-      }
-      g.root = world_root;
-      g.base = 0;
-      g.record = 0;
-      g.has_inverse = false;
-      groups.push_back(g);
+    s.placed_index = placed_index;
+    for (uint32_t i = 0; i < scene.instance_count; ++i) {
+      if (placed_index[i] < 0) continue;
+      const Placed& p = placed[placed_index[i]];
+      Placing::Placed q;
+      q.mesh = p.mesh;
+      q.base = p.base;
+      q.record = p.record;
+      memcpy(q.transform, scene.instances[i].transform, sizeof(q.transform));
+      q.bounds = p.bounds;
+      memcpy(q.inverse, p.inverse, sizeof(q.inverse));
+      s.placed.push_back(q);
     }
-    for (auto& p : placed) {
-      Group g;
-      g.bounds = p.bounds;
-      g.root = meshes[p.mesh].root;
-      g.base = p.base;
-      g.record = p.record;
-      g.has_inverse = true;
-      memcpy(g.inverse, p.inverse, sizeof(g.inverse));
-      groups.push_back(g);
-    }
-    if (!groups.empty()) {
-      std::vector<Bounds> boxes;
-      for (auto& g : groups) boxes.push_back(g.bounds);
-      Bvh top = bvh_over(boxes, INSTANCE_LEAVES);
-      uint32_t tree = (uint32_t)top.nodes.size();
-      for (auto node : top.nodes) {
-        if (node.count > 0) {
-          uint32_t index = top.order[node.first];
-          const Group& g = groups[index];
-          node.first = g.root;
-          node.count = g.base;
-          node.lo[3] = bits2f(g.record);
-          node.pad[0] = INSTANCE_LEAF;
-          node.pad[1] = g.has_inverse ? tree + index : 0u;
-        }
-        nodes.push_back(node);
-      }
-      for (auto& g : groups) {
-        static const float identity[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
-        const float* r = g.has_inverse ? g.inverse : identity;
-        GpuNode n{};
-        for (int k = 0; k < 4; ++k) {
-          n.lo[k] = r[k];
-          n.hi[k] = r[4 + k];
-        }
-        n.first = f2bits(r[8]);
-        n.count = f2bits(r[9]);
-        n.pad[0] = f2bits(r[10]);
-        n.pad[1] = f2bits(r[11]);
-        nodes.push_back(n);
-      }
-    }
-    nodes.resize(top_len);
+    nodes.resize(s.top_len);
+    lay_top(s, nodes.data());
+    out->placing = std::move(state);
+    out->top_builds = 1;
     auto shifted = [&](const std::vector<GpuNode>& src, uint32_t off) {
       for (auto n : src) {
         if (n.count == 0) n.first += off;
         nodes.push_back(n);
       }
     };
-    if (world) shifted(world_bvh.nodes, world_root);
+    if (s.world) shifted(world_bvh.nodes, s.world_root);
     for (auto& mesh : meshes) shifted(mesh.nodes, mesh.root);
   }
 
@@ -1235,6 +1272,11 @@ SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings) 
   // ---- lights and the emitter list (gpu.rs:1011-1013)
   TreeLaid laid = tree_lay(scene.lights, scene.light_count);
   build_emitters(cands, laid.looped, laid.tree, out->emitters, out->emitter_cdf);
+  if (out->placing) {
+    out->placing->candidates = cands;
+    out->placing->looped = laid.looped;
+    out->placing->tree = laid.tree;
+  }
   out->lights = std::move(laid.rows);
   out->materials = std::move(hot);
   out->nodes = std::move(nodes);
@@ -1269,10 +1311,86 @@ SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings) 
   }
 
   out->triangle_count = slots;
+  out->bottom_builds = (uint32_t)meshes.size() + (scene.triangle_count > 0 ? 1u : 0u);
   out->light_count = scene.light_count;
   out->emitter_count = (uint32_t)cands.size();
   out->max_depth = out->nodes.empty() ? 0 : std::max<uint32_t>(1u, stack_need(out->nodes, 0, 0));
   return out.release();
+}
+
+// Trace::move_instances (gpu.rs:2433-2530).  Every transform is checked first;
+// an instance moves when any of its 16 floats differs bit for bit.  A moved
+// instance gets its inverse rows and world box (levels.rs:114-127), its
+// surface record's forward and inverse rows and inverse determinant, and its
+// emitter candidates' world vertices; the candidate list itself stays as built,
+// so the emitter list is rebuilt from it when one of them moved.  The top-level
+// BVH is then laid again over the new boxes, as finish_tops writes it
+// (gpu.rs:2533-2540).
+bool move_instances(SceneBlobs& b, const float* transforms, size_t count) {
+  Placing* s = b.placing.get();
+  if (!s) {
+    if (count == 0) return false;
+    throw Invalid("this trace has no instances to move");
+  }
+  if (count > s->placed_index.size())
+    throw Invalid("the trace has " + std::to_string(s->placed_index.size()) + " instances and " +
+                  std::to_string(count) + " transforms were given");
+  if (count > 0 && !transforms) throw Invalid("null argument");
+  std::vector<Pose> poses(count);
+  for (size_t i = 0; i < count; ++i) {
+    std::string err;
+    if (!pose_new(transforms + 16 * i, &poses[i], &err)) throw Invalid(err);
+  }
+  auto moved = [&](const Placing::Placed& p, const float* t) {
+    for (int k = 0; k < 16; ++k)
+      if (f2bits(p.transform[k]) != f2bits(t[k])) return true;
+    return false;
+  };
+  bool any = false;
+  for (size_t i = 0; i < count && !any; ++i)
+    any = s->placed_index[i] >= 0 && moved(s->placed[s->placed_index[i]], transforms + 16 * i);
+  if (!any) return false;
+  bool emitters_moved = false;
+  for (size_t i = 0; i < count; ++i) {
+    if (s->placed_index[i] < 0) continue;
+    Placing::Placed& p = s->placed[s->placed_index[i]];
+    const float* t = transforms + 16 * i;
+    if (!moved(p, t)) continue;
+    const Pose& pose = poses[i];
+    const Placing::Mesh& mesh = s->meshes[p.mesh];
+    memcpy(p.transform, t, sizeof(p.transform));
+    pose_inverse_rows(pose, p.inverse);
+    p.bounds = placed_bounds(pose, mesh.bounds);
+    for (auto& c : s->candidates) {
+      if (c.record != p.record) continue;
+      const pfxt_triangle& local = mesh.triangles[c.slot - mesh.first];
+      for (int v = 0; v < 3; ++v) {
+        V3 w = pose_point(pose, local.v[v]);
+        for (int k = 0; k < 3; ++k) c.vertices[v][k] = w[k];
+      }
+      emitters_moved = true;
+    }
+    GpuSurface& sf = b.surfaces[p.record];
+    sf.info[3] = f2bits(pose_inverse_determinant(pose));
+    float rows[12];
+    pose_rows(pose, rows);
+    memcpy(sf.forward, rows, sizeof(rows));
+    memcpy(sf.inverse, p.inverse, sizeof(p.inverse));
+  }
+  if (emitters_moved) {
+    std::vector<GpuEmitter> entries;
+    std::vector<float> cdf;
+    build_emitters(s->candidates, s->looped, s->tree, entries, cdf);
+    if (entries.size() != b.emitters.size() || cdf.size() != b.emitter_cdf.size())
+      throw Invalid("the emitter list changed size");
+    // in place: the buffers handed out by pfxt_scene_buffers keep pointing here
+    std::copy(entries.begin(), entries.end(), b.emitters.begin());
+    std::copy(cdf.begin(), cdf.end(), b.emitter_cdf.begin());
+  }
+  lay_top(*s, b.nodes.data());
+  b.max_depth = std::max<uint32_t>(1u, stack_need(b.nodes, 0, 0));
+  b.top_builds += 1;
+  return true;
 }
 
 }  // namespace pfxt

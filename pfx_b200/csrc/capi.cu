@@ -545,6 +545,62 @@ int pfxt_set_projection(pfxt_trace* t, uint32_t projection, const float ortho[2]
   });
 }
 
+/* ------------------------------------------------------- moving instances */
+
+// The radiance cache's grid box: the scene root's box, padded by 1e-3 of its
+// extent (plus 1e-4) so that surface points on the box still hash inside.
+static void bind_cache_bounds(const pfxt_trace& t, pfxt_cache& c) {
+  float lo[3], hi[3];
+  for (int k = 0; k < 3; ++k) {
+    float pad = 1e-3f * (t.bounds_hi[k] - t.bounds_lo[k]) + 1e-4f;
+    lo[k] = t.bounds_lo[k] - pad;
+    hi[k] = t.bounds_hi[k] + pad;
+  }
+  cache_set_bounds(c, lo, hi);
+}
+
+int pfxt_scene_move_instances(pfxt_scene_blobs* h, const float* transforms, uint32_t count, uint32_t* moved) {
+  return guarded([&]() {
+    if (!h) throw Invalid("null argument");
+    bool any = move_instances(*h->blobs, transforms, count);
+    if (moved) *moved = any ? 1u : 0u;
+  });
+}
+
+int pfxt_scene_builds(const pfxt_scene_blobs* h, uint32_t* bottom, uint32_t* top) {
+  return guarded([&]() {
+    if (!h || !bottom || !top) throw Invalid("null argument");
+    *bottom = h->blobs->bottom_builds;
+    *top = h->blobs->top_builds;
+  });
+}
+
+int pfxt_finish_tops(pfxt_trace* t, const pfxt_buffers* b) {
+  return guarded([&]() {
+    if (!t || !b) throw Invalid("null argument");
+    if (b->max_depth > REF_STACK) throw Invalid("the BVH needs more than the 64-entry traversal stack");
+    if (b->nodes_bytes % sizeof(GpuNode) || b->triangles_bytes % sizeof(GpuTriangle))
+      throw Invalid("scene buffers have invalid sizes");
+    trace_move_scene(*t, *b);
+    if (t->cache) bind_cache_bounds(*t, *t->cache);
+  });
+}
+
+int pfxt_set_instance_transforms(pfxt_trace* t, pfxt_scene_blobs* h, const float* transforms, uint32_t count,
+                                 uint32_t* moved) {
+  return guarded([&]() {
+    if (!t || !h) throw Invalid("null argument");
+    if (moved) *moved = 0u;
+    if (!move_instances(*h->blobs, transforms, count)) return;
+    if (h->blobs->max_depth > REF_STACK) throw Invalid("the BVH needs more than the 64-entry traversal stack");
+    pfxt_buffers b;
+    if (pfxt_scene_buffers(h, &b) != PFXT_OK) throw Invalid(pfxt_last_error());
+    trace_move_scene(*t, b);
+    if (t->cache) bind_cache_bounds(*t, *t->cache);
+    if (moved) *moved = 1u;
+  });
+}
+
 /* ------------------------------------------------------------ launch tuning */
 
 int pfxt_get_tuning(pfxt_trace* t, pfxt_tuning* out) {
@@ -628,13 +684,7 @@ int pfxt_set_cache(pfxt_trace* t, pfxt_cache* c) {
     if (c) {
       if (c->device != t->device) throw Invalid("the cache belongs to another device");
       if (c->s.record_bounces > 7) throw Invalid("a tracer records at most vertices 0..7 for the cache");
-      float lo[3], hi[3];
-      for (int k = 0; k < 3; ++k) {
-        float pad = 1e-3f * (t->bounds_hi[k] - t->bounds_lo[k]) + 1e-4f;
-        lo[k] = t->bounds_lo[k] - pad;
-        hi[k] = t->bounds_hi[k] + pad;
-      }
-      cache_set_bounds(*c, lo, hi);
+      bind_cache_bounds(*t, *c);
     }
     trace_forget_graphs(*t);
     t->cache = c;

@@ -2,6 +2,7 @@
 // libpfxtrace.  Not part of the C ABI.
 #pragma once
 #include <array>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -21,6 +22,10 @@ struct Refused : std::runtime_error {
   explicit Refused(const std::string& m) : std::runtime_error(m) {}
 };
 
+// Levels and emitter candidates of a built scene, kept for moving instances
+// afterwards (the `placing` state of Trace, gpu.rs:530-540); build.cpp.
+struct Placing;
+
 // The packed buffers of one scene (SceneBuffers, gpu.rs:412-436).
 struct SceneBlobs {
   std::vector<GpuTriangle> triangles;
@@ -39,9 +44,19 @@ struct SceneBlobs {
   uint32_t sobol_length = 0;
   uint32_t triangle_count = 0, light_count = 0, emitter_count = 0;
   uint32_t max_depth = 0;
+  std::shared_ptr<Placing> placing;  // null when the scene has no instances
+  // Builds (gpu.rs:400-403): bottom-level BVHs built (the world's and one per
+  // distinct mesh) and top-level BVHs laid (1 with instances, +1 per move).
+  uint32_t bottom_builds = 0, top_builds = 0;
 };
 
 SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings);
+
+// Trace::move_instances (gpu.rs:2433-2530) on the host buffers: new transforms
+// for the first `count` instances (16 floats each, column-major).  Rewrites the
+// moved instances' surface records, their emitters and the top-level BVH in
+// place (no buffer changes size) and returns whether anything moved.
+bool move_instances(SceneBlobs& blobs, const float* transforms, size_t count);
 
 // Thread-local last error of the C ABI.
 void set_error(const std::string& message);

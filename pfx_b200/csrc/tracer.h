@@ -96,6 +96,7 @@ struct pfxt_trace {
   void* d_surfaces = nullptr;
   void* d_emitters = nullptr;
   void* d_emitter_cdf = nullptr;
+  size_t surfaces_bytes = 0, emitters_bytes = 0, emitter_cdf_bytes = 0;  // as uploaded
   void* d_lights = nullptr;
   void* d_sky_rows = nullptr;
   void* d_sky_columns = nullptr;
@@ -155,6 +156,9 @@ void light_trig_init(pfxt_trace& t);
 // Drops the captured passes (their buffers or launch parameters changed).
 void trace_forget_graphs(pfxt_trace& t);
 void trace_set_projection(pfxt_trace& t, uint32_t projection, const float ortho[2]);
+// Uploads the node, surface and emitter buffers of a scene whose instances
+// moved (Trace::finish_tops, gpu.rs:2533) and lays the traversal nodes again.
+void trace_move_scene(pfxt_trace& t, const pfxt_buffers& b);
 void trace_set_tuning(pfxt_trace& t, const pfxt_tuning& k);
 pfxt_tuning trace_get_tuning(const pfxt_trace& t);
 pfxt_tuning trace_autotune(pfxt_trace& t, uint32_t passes);

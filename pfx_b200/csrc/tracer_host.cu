@@ -85,6 +85,9 @@ void trace_init(pfxt_trace& t, const pfxt_buffers& b, const pfxt_scene& view, co
   t.d_surfaces = dev_copy(t, b.surfaces, b.surfaces_bytes, "surfaces");
   t.d_emitters = dev_copy(t, b.emitters, b.emitters_bytes, "emitters");
   t.d_emitter_cdf = dev_copy(t, b.emitter_cdf, b.emitter_cdf_bytes, "emitter cdf");
+  t.surfaces_bytes = b.surfaces_bytes;
+  t.emitters_bytes = b.emitters_bytes;
+  t.emitter_cdf_bytes = b.emitter_cdf_bytes;
   t.d_lights = dev_copy(t, b.lights, b.lights_bytes, "lights");
   t.d_sky_rows = dev_copy(t, b.sky_rows, (size_t)b.sky_height * 4, "sky rows");
   t.d_sky_columns = dev_copy(t, b.sky_columns, (size_t)b.sky_width * b.sky_height * 4, "sky columns");
@@ -252,6 +255,52 @@ void trace_set_camera(pfxt_trace& t, const pfxt_camera& c) {
     t.base.right[k] = c.right[k];
     t.base.up[k] = c.up[k];
   }
+  t.samples = 0;
+}
+
+void trace_move_scene(pfxt_trace& t, const pfxt_buffers& b) {
+  if (b.surfaces_bytes != t.surfaces_bytes || b.emitters_bytes != t.emitters_bytes ||
+      b.emitter_cdf_bytes != t.emitter_cdf_bytes || b.nodes_bytes < sizeof(GpuNode))
+    throw Invalid("the moved scene does not match the trace's buffers");
+  TraversalLayout layout = make_layout(b);
+  check(cudaStreamSynchronize(t.stream), "move instances");
+  // New traversal buffers first, so that a failed allocation leaves the trace as it was.
+  size_t kept = t.owned.size();
+  void* fresh[3] = {nullptr, nullptr, nullptr};
+  try {
+    fresh[0] = dev_copy(t, layout.wide.data(), layout.wide.size() * sizeof(WideNode), "nodes");
+    fresh[1] = dev_copy(t, layout.tris.data(), layout.tris.size() * sizeof(TravTri), "triangles");
+    fresh[2] = dev_copy(t, layout.insts.data(), layout.insts.size() * sizeof(InstRec), "instances");
+  } catch (...) {
+    for (size_t i = kept; i < t.owned.size(); ++i) cudaFree(t.owned[i]);
+    t.owned.resize(kept);
+    throw;
+  }
+  void* stale[3] = {t.d_wide, t.d_tris, t.d_insts};
+  for (void* p : stale) {
+    auto it = std::find(t.owned.begin(), t.owned.end(), p);
+    if (it != t.owned.end()) {
+      t.owned.erase(it);
+      cudaFree(p);
+    }
+  }
+  t.d_wide = static_cast<WideNode*>(fresh[0]);
+  t.d_tris = static_cast<TravTri*>(fresh[1]);
+  t.d_insts = static_cast<InstRec*>(fresh[2]);
+  t.view.wide = t.d_wide;
+  t.view.tris = t.d_tris;
+  t.view.insts = t.d_insts;
+  t.view.root = layout.root;
+  check(cudaMemcpy(t.d_surfaces, b.surfaces, b.surfaces_bytes, cudaMemcpyHostToDevice), "surfaces");
+  check(cudaMemcpy(t.d_emitters, b.emitters, b.emitters_bytes, cudaMemcpyHostToDevice), "emitters");
+  if (b.emitter_cdf_bytes)
+    check(cudaMemcpy(t.d_emitter_cdf, b.emitter_cdf, b.emitter_cdf_bytes, cudaMemcpyHostToDevice), "emitter cdf");
+  const GpuNode* root = static_cast<const GpuNode*>(b.nodes);
+  for (int k = 0; k < 3; ++k) {
+    t.bounds_lo[k] = root->lo[k];
+    t.bounds_hi[k] = root->hi[k];
+  }
+  trace_forget_graphs(t);
   t.samples = 0;
 }
 

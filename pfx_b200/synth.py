@@ -22,7 +22,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import abi
-from .trace import INSTANCE, LIGHT, MATERIAL, TRIANGLE, Adaptive, Camera, SceneDesc, Settings
+from .trace import INSTANCE, LIGHT, MATERIAL, TRIANGLE, Adaptive, Camera, SceneDesc, Settings, Sun
 
 F32 = np.float32
 
@@ -432,6 +432,57 @@ def furnace() -> SceneDesc:
     ico["v"] = ico["v"] + np.array([0.0, 0.0, -3.0], F32)
     cam = Camera((0.0, 0.0, 0.0), (0.0, 0.0, -1.0), (1.0, 0.0, 0.0), (0.0, 1.0, 0.0))
     return SceneDesc(ico, material((1.0, 1.0, 1.0), 1.0, specular=0.0), cam, sky=(1.0, 1.0, 1.0))
+
+
+IDENTITY = np.eye(4, dtype=F32)
+
+
+def placed(at, turn: float, scale: float) -> np.ndarray:
+    """A turn about +y, a uniform scale and a translation as a column-major 4x4
+    (the `placed` helper of crates/trace/tests/instances.rs:89-97)."""
+    s, c = math.sin(turn), math.cos(turn)
+    return np.array([[c * scale, 0.0, -s * scale, 0.0], [0.0, scale, 0.0, 0.0], [s * scale, 0.0, c * scale, 0.0],
+                     [at[0], at[1], at[2], 1.0]], F32)
+
+
+def staged_poses(moved: bool) -> list:
+    """The two sets of placements of crates/trace/tests/instances.rs:137-157:
+    floor, two balls and an emissive panel."""
+    if moved:
+        return [IDENTITY, placed((0.5, 0.45, -0.2), 0.9, 0.9), placed((-0.9, 0.35, 0.6), -0.4, 0.7),
+                placed((-0.3, 1.6, -0.5), 0.6, 1.0)]
+    return [IDENTITY, placed((-0.4, 0.5, 0.0), 0.0, 1.0), placed((0.8, 0.5, 0.4), 0.3, 1.0),
+            placed((0.0, 1.8, -0.8), 0.0, 1.0)]
+
+
+def staged(transforms, size=(96, 64), world: bool = False, empty: bool = False) -> Workload:
+    """The instanced stage of crates/trace/tests/instances.rs:159-197: a floor,
+    one ball mesh placed twice (red and grey), an emissive panel, a dim sky and
+    a sun.  `world` adds a back wall as world triangles; `empty` appends an
+    instance of an empty mesh (never placed)."""
+    lambert = lambda base: material(base, 1.0, specular=0.0)  # noqa: E731
+    mats = np.concatenate([lambert((0.6, 0.6, 0.6)), lambert((0.8, 0.2, 0.1)),
+                           material((0.0, 0.0, 0.0), 1.0, specular=0.0, emission=(6.0, 5.0, 4.0))])
+    floor = quad((0, 0, 0), (3, 0, 0), (0, 0, 3), 0)
+    panel = quad((0, 0, 0), (0.4, 0, 0), (0, 0, 0.4), 2)
+    meshes = [floor, uv_sphere((0, 0, 0), 0.5, 32, 16, 1), uv_sphere((0, 0, 0), 0.5, 32, 16, 0), panel,
+              np.zeros(0, TRIANGLE)]
+    inst = np.zeros(4 + int(empty), INSTANCE)
+    inst["mesh"][:4] = [0, 1, 2, 3]
+    if empty:
+        inst["mesh"][4] = 4
+        inst["transform"][4] = IDENTITY.reshape(16)
+    inst["two_sided"] = 1
+    inst["casts_shadow"] = 1
+    for i, t in enumerate(transforms[:4]):
+        inst["transform"][i] = np.asarray(t, F32).reshape(16)
+    wall = quad((0, 1.5, -3), (3, 0, 0), (0, 1.5, 0), 0) if world else np.zeros(0, TRIANGLE)
+    w, h = size
+    cam = look_at((0.0, 2.0, 4.0), (0.0, 0.4, 0.0), 2.0 * math.degrees(math.atan(0.5)), w / h)
+    d = np.array([0.4, 1.0, 0.3])
+    scene = SceneDesc(wall, mats, cam, meshes=meshes, instances=inst, sky=(0.08, 0.09, 0.1),
+                      sun=Sun(tuple(map(float, d / np.linalg.norm(d))), (1.0, 0.95, 0.9), 2.0))
+    return Workload("staged", scene, Settings.deep(4, sampler="pcg"), w, h, spp=8)
 
 
 def small(name: str, size=(64, 48), sampler: str = "pcg") -> Workload:

@@ -213,6 +213,22 @@ class SceneBuffers:
         check(self._lib.pfxt_scene_order(self._h, C.byref(p), C.byref(n)))
         return np.ctypeslib.as_array(p, (n.value,)).copy() if n.value else np.zeros(0, np.uint32)
 
+    def move_instances(self, transforms) -> bool:
+        """Trace::move_instances (gpu.rs:2433-2530) on these host buffers: new
+        column-major 4x4 transforms for the first len(transforms) instances.
+        Returns whether any instance moved."""
+        t = _transforms(transforms)
+        moved = C.c_uint32()
+        check(self._lib.pfxt_scene_move_instances(self._h, t.ctypes.data if t.size else None, len(t),
+                                                  C.byref(moved)))
+        return bool(moved.value)
+
+    def builds(self) -> tuple:
+        """Trace::builds (gpu.rs:2356): (bottom-level BVHs built, top-level BVHs laid)."""
+        bottom, top = C.c_uint32(), C.c_uint32()
+        check(self._lib.pfxt_scene_builds(self._h, C.byref(bottom), C.byref(top)))
+        return int(bottom.value), int(top.value)
+
     def sky(self):
         b = self.buffers
         rows = np.ctypeslib.as_array((C.c_float * b.sky_height).from_address(b.sky_rows)).copy()
@@ -301,6 +317,26 @@ class Trace:
         height) or "equirect"; restarts the accumulation."""
         kind = {"perspective": 0, "orthographic": 1, "equirect": 2}[projection]
         check(self._lib.pfxt_set_projection(self._h, kind, (C.c_float * 2)(width, height)))
+
+    def set_instance_transforms(self, transforms) -> bool:
+        """Trace::set_instance_transforms (gpu.rs:2422-2431): new column-major 4x4
+        transforms for the first len(transforms) instances; the accumulation
+        restarts when any of them moved.  Returns whether any moved."""
+        t = _transforms(transforms)
+        moved = C.c_uint32()
+        check(self._lib.pfxt_set_instance_transforms(self._h, self.scene_buffers._h,
+                                                     t.ctypes.data if t.size else None, len(t), C.byref(moved)))
+        return bool(moved.value)
+
+    def finish_tops(self, buffers: SceneBuffers | None = None) -> None:
+        """Trace::finish_tops (gpu.rs:2533): upload host buffers whose instances
+        were moved (SceneBuffers.move_instances) and restart the accumulation."""
+        b = buffers if buffers is not None else self.scene_buffers
+        check(self._lib.pfxt_finish_tops(self._h, C.byref(b.buffers)))
+
+    def builds(self) -> tuple:
+        """Trace::builds (gpu.rs:2356): (bottom-level BVHs built, top-level BVHs laid)."""
+        return self.scene_buffers.builds()
 
     def save(self, key: str) -> bytes:
         """Trace::save + Saved::write_to (checkpoint.rs): the checkpoint bytes."""
@@ -402,6 +438,13 @@ class Trace:
 
     def counts_device(self, rays_ptr: int, count: int, any_hit: bool, counts_ptr: int, stream: int = 0) -> None:
         check(self._lib.pfxt_trace_counts_device(self._h, rays_ptr, count, 1 if any_hit else 0, counts_ptr, stream))
+
+
+def _transforms(transforms) -> np.ndarray:
+    """Transforms as contiguous (n, 16) float32: each a column-major 4x4, given
+    either flat (16 values) or as 4 columns of 4 (detail.rs Transform)."""
+    t = np.ascontiguousarray(np.asarray(transforms, np.float32).reshape(-1, 16))
+    return t
 
 
 def make_rays(origins: np.ndarray, directions: np.ndarray, tmax) -> np.ndarray:

@@ -1,0 +1,83 @@
+"""Moving instances on the host buffers (Trace::move_instances,
+crates/trace/src/gpu.rs:2433-2530; Levels::top, levels.rs:426-470), on the
+stage of the reference's own test crates/trace/tests/instances.rs.
+
+Moving every instance of a built scene to new transforms leaves the buffers
+bit for bit equal to a scene built with those transforms; moving nothing
+changes nothing; a partial list moves only its prefix; the reference's error
+cases keep their messages."""
+import numpy as np
+import pytest
+
+from pfx_b200 import synth
+from pfx_b200.trace import SceneBuffers, TraceError
+
+MOVED = ["nodes", "surfaces", "emitters", "emitter_cdf"]
+KEPT = ["triangles", "uv", "materials", "lights"]
+
+
+def built(poses, **kw):
+    w = synth.staged(poses, **kw)
+    return SceneBuffers(w.scene, w.settings)
+
+
+def arrays(b):
+    return {n: b.array(n) for n in MOVED + KEPT}
+
+
+@pytest.mark.parametrize("world, empty", [(False, False), (True, True)])
+def test_moved_buffers_equal_a_fresh_build(world, empty):
+    kept = built(synth.staged_poses(False), world=world, empty=empty)
+    fresh = built(synth.staged_poses(True), world=world, empty=empty)
+    before = arrays(kept)
+    # the emissive panel moves too, so its emitter rows change with the nodes
+    assert all(not np.array_equal(before[n], fresh.array(n)) for n in MOVED)
+    assert kept.builds() == fresh.builds() == (3 + int(world), 1)
+    assert kept.move_instances(synth.staged_poses(True))
+    after = arrays(kept)
+    for n in MOVED + KEPT:
+        assert np.array_equal(after[n], fresh.array(n)), n
+    # Trace::builds: the bottom levels are kept, one more top (instances.rs:245-246)
+    assert kept.builds() == (3 + int(world), 2)
+
+
+def test_the_same_transforms_move_nothing():
+    kept = built(synth.staged_poses(False), empty=True)
+    before = arrays(kept)
+    assert not kept.move_instances(synth.staged_poses(False))
+    assert not kept.move_instances([])
+    # an empty mesh's instance is never placed, so its transform is ignored
+    assert not kept.move_instances(synth.staged_poses(False) + [synth.placed((5, 5, 5), 1.0, 2.0)])
+    after = arrays(kept)
+    assert all(np.array_equal(before[n], after[n]) for n in before)
+    assert kept.builds() == (3, 1)
+
+
+def test_a_prefix_moves_only_its_instances():
+    """set_instance_transforms(&pose(true)[..2]) (instances.rs:267-270)."""
+    kept = built(synth.staged_poses(False))
+    mixed = synth.staged_poses(True)[:2] + synth.staged_poses(False)[2:]
+    fresh = built(mixed)
+    assert kept.move_instances(synth.staged_poses(True)[:2])
+    for n in MOVED:
+        assert np.array_equal(kept.array(n), fresh.array(n)), n
+    assert kept.builds() == (3, 2)
+
+
+def test_reference_errors():
+    kept = built(synth.staged_poses(False))
+    with pytest.raises(TraceError, match="the trace has 4 instances and 5 transforms were given"):
+        kept.move_instances([synth.IDENTITY] * 5)
+    bad = synth.staged_poses(True)
+    bad[3] = bad[3].copy()
+    bad[3][3, 0] = np.inf
+    before = arrays(kept)
+    with pytest.raises(TraceError, match="instance transform is not finite"):
+        kept.move_instances(bad)
+    # nothing moved on an error, even the instances before the bad transform
+    assert all(np.array_equal(before[n], kept.array(n)) for n in before)
+    plain = synth.small("plain_512", (16, 16))
+    lone = SceneBuffers(plain.scene, plain.settings)
+    assert not lone.move_instances([])
+    with pytest.raises(TraceError, match="this trace has no instances to move"):
+        lone.move_instances([synth.IDENTITY])
