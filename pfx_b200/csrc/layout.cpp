@@ -13,6 +13,7 @@
 // whose child 0 is the root, so that the root box is tested exactly as the
 // reference tests it after popping index 0 (or after entering an instance).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <unordered_map>
 
@@ -145,6 +146,17 @@ TraversalLayout make_layout(const pfxt_buffers& b) {
     // the top level itself: world leaves (base 0) must stay inside the triangles
     if (builder.reach_of[builder.out.root] > builder.tri_count)
       throw Invalid("a BVH leaf reaches past the triangles");
+  }
+  // The box test needs no range check on its quotients when every box
+  // coordinate is 0 or of magnitude in [2^-70, 2^79] (traverse.cuh,
+  // BOUNDED_TINY and BOUNDED_COORD); NaN coordinates fail this too.
+  builder.out.small = true;
+  for (const WideNode& w : builder.out.wide) {
+    const float* f = &w.b0[0];
+    for (int k = 0; k < 12; ++k) {
+      float a = std::fabs(f[k]);
+      if (!(a == 0.0f || (a >= 0x1p-70f && a <= 0x1p+79f))) builder.out.small = false;
+    }
   }
   const GpuTriangle* tris = (const GpuTriangle*)b.triangles;
   size_t count = b.triangles_bytes / sizeof(GpuTriangle);

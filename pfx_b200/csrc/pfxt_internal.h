@@ -67,6 +67,7 @@ struct TraversalLayout {
   std::vector<TravTri> tris;
   std::vector<InstRec> insts;
   uint32_t root = REF_NONE;  // wide node whose child 0 is the scene root
+  bool small = false;        // every box coordinate 0 or within 2^-70..2^79 in magnitude (SceneView::small)
 };
 TraversalLayout make_layout(const pfxt_buffers& buffers);
 

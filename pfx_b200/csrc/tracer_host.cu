@@ -70,6 +70,7 @@ void trace_init(pfxt_trace& t, const pfxt_buffers& b, const pfxt_scene& view, co
   t.view.tris = t.d_tris;
   t.view.insts = t.d_insts;
   t.view.root = layout.root;
+  t.view.small = layout.small ? 1u : 0u;
   if (b.nodes_bytes >= sizeof(GpuNode)) {
     const GpuNode* root = static_cast<const GpuNode*>(b.nodes);
     for (int k = 0; k < 3; ++k) {
@@ -291,6 +292,7 @@ void trace_move_scene(pfxt_trace& t, const pfxt_buffers& b) {
   t.view.tris = t.d_tris;
   t.view.insts = t.d_insts;
   t.view.root = layout.root;
+  t.view.small = layout.small ? 1u : 0u;
   check(cudaMemcpy(t.d_surfaces, b.surfaces, b.surfaces_bytes, cudaMemcpyHostToDevice), "surfaces");
   check(cudaMemcpy(t.d_emitters, b.emitters, b.emitters_bytes, cudaMemcpyHostToDevice), "emitters");
   if (b.emitter_cdf_bytes)

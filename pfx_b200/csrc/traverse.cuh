@@ -5,8 +5,8 @@
 // (:1096-1168, tri_blocks :1076-1095).  Both walk the reference's tree in the
 // reference's order (left child first, right child when the left subtree is
 // done), test the same fp32 boxes with the same slab arithmetic (the quotients
-// (lo - o)/d are computed correctly rounded by div_rn, so they equal the
-// reference's divisions bit for bit), and run the same Moller-Trumbore test
+// (lo - o)/d are correctly rounded, so they equal the reference's divisions
+// bit for bit), and run the same Moller-Trumbore test
 // with the same operation order, so the hit slot, record and distance are
 // bit-identical to the CPU oracle's.  Clip planes, cutouts, alpha, sprites,
 // motion and analytic shapes are outside this library's scope; the scenes it
@@ -38,6 +38,7 @@ struct SceneView {
   const TravTri* __restrict__ tris;
   const InstRec* __restrict__ insts;
   uint32_t root;
+  uint32_t small;  // 1 when every box coordinate is 0 or in [BOUNDED_TINY, BOUNDED_COORD] in magnitude
 };
 
 struct TraceHit {
@@ -54,22 +55,46 @@ struct TraceCounts {
   uint32_t tris;
 };
 
+// The Markstein quotients of the box test below are the correctly rounded
+// (lo - o)/d whenever nothing in them underflows or overflows.  That holds for
+// every box of a "bounded" ray, with no check per quotient:
+//  * box coordinates and ray origin components are 0 or of magnitude in
+//    [2^-70, 2^79], so a numerator x = lo - o is 0 (exact) or of magnitude in
+//    [2^-93, 2^80] (a nonzero difference of two such values is a multiple of
+//    the smaller one's ulp, at least 2^-93);
+//  * direction components are degenerate (below 1e-12, never divided by) or of
+//    magnitude in [1e-12, 16], so a nonzero quotient lies in [2^-97, 2^120],
+//    and the residual x - q d, a multiple of ulp(q) ulp(d) >= 2^-141, is exact.
+// Box coordinates are checked once per scene (SceneView::small); origins and
+// directions per ray, in world space and in every instance's space.
+constexpr float BOUNDED_COORD = 0x1p+79f;
+constexpr float BOUNDED_TINY = 0x1p-70f;
+constexpr float BOUNDED_DIR = 16.0f;
+
 // A ray in the space it is being traversed in, with the per-axis reciprocal
-// used by div_rn (only read on axes with |d| >= 1e-12).
+// used by the quotients (only read on axes with |d| >= 1e-12).  The boxes of
+// a ray that is not `bounded` are all tested with IEEE division.
 struct TRay {
   v3 o, d, r;
+  bool bounded;
 };
 
-__device__ __forceinline__ TRay make_tray(v3 o, v3 d) {
+__device__ __forceinline__ bool bounded_axis(float o, float d) {
+  float ao = fabsf(o), ad = fabsf(d);
+  return (ao == 0.0f || (ao >= BOUNDED_TINY && ao <= BOUNDED_COORD)) && (ad <= BOUNDED_DIR || ad < 1e-12f);
+}
+
+__device__ __forceinline__ TRay make_tray(v3 o, v3 d, uint32_t small) {
   TRay t;
   t.o = o;
   t.d = d;
   t.r = mk3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+  t.bounded = small != 0u && bounded_axis(o.x, d.x) && bounded_axis(o.y, d.y) && bounded_axis(o.z, d.z);
   return t;
 }
 
-// Slab test of one box with IEEE division throughout: the rare case in which
-// a Markstein quotient below could be off by one rounding.
+// Slab test of one box with IEEE division throughout, for rays that are not
+// bounded (see above).
 static __device__ __noinline__ bool box_geometry_ieee(float lx, float ly, float lz, float hx, float hy, float hz,
                                                const TRay& ray, float& near) {
   float n = 0.0f, f = INFINITY;
@@ -98,46 +123,46 @@ static __device__ __noinline__ bool box_geometry_ieee(float lx, float ly, float 
   return !(n > f);
 }
 
-// x / d by Markstein's correction from r = RN(1/d), correctly rounded unless
-// `bad` is raised (the guard of div_rn, gathered instead of branched on).
-__device__ __forceinline__ float quotient(float x, float d, float r, bool& bad) {
+// x / d by Markstein's correction from r = RN(1/d) (Markstein 1990; Cornea,
+// Harrison and Tang, "Scientific Computing on Itanium-based Systems", 2002,
+// ch. 8): with q = RN(x r) the residual fma(-q, d, x) is exact and
+// RN(q + e r) is the correctly rounded quotient, provided nothing underflows
+// or overflows, which a bounded ray guarantees.
+__device__ __forceinline__ float quotient(float x, float d, float r) {
   float q = x * r;
   float e = fmaf(-q, d, x);
-  float q2 = fmaf(e, r, q);
-  bad |= !(fabsf(x) >= 0x1p-96f) || !(fabsf(q2) >= 0x1p-100f) || !(fabsf(q2) <= 0x1p+120f);
-  return q2;
+  return fmaf(e, r, q);
 }
 
 // Slab test of one box: true when the ray's geometry passes (degenerate axes
 // inside the slab, entry <= exit); `near` receives max(0, entries).  The six
-// quotients equal IEEE division's (the reference divides); where one might
-// not, the box is tested again with IEEE division.
+// quotients equal IEEE division's (the reference divides); the boxes of a ray
+// that is not bounded are tested with IEEE division instead.
 __device__ __forceinline__ bool box_geometry(float lx, float ly, float lz, float hx, float hy, float hz,
                                              const TRay& ray, float& near) {
+  if (!ray.bounded) return box_geometry_ieee(lx, ly, lz, hx, hy, hz, ray, near);
   float n = 0.0f, f = INFINITY;
-  bool bad = false;
   if (fabsf(ray.d.x) < 1e-12f) {
     if (ray.o.x < lx || ray.o.x > hx) return false;
   } else {
-    float a = quotient(lx - ray.o.x, ray.d.x, ray.r.x, bad), b = quotient(hx - ray.o.x, ray.d.x, ray.r.x, bad);
+    float a = quotient(lx - ray.o.x, ray.d.x, ray.r.x), b = quotient(hx - ray.o.x, ray.d.x, ray.r.x);
     n = fmaxf(n, fminf(a, b));
     f = fminf(f, fmaxf(a, b));
   }
   if (fabsf(ray.d.y) < 1e-12f) {
     if (ray.o.y < ly || ray.o.y > hy) return false;
   } else {
-    float a = quotient(ly - ray.o.y, ray.d.y, ray.r.y, bad), b = quotient(hy - ray.o.y, ray.d.y, ray.r.y, bad);
+    float a = quotient(ly - ray.o.y, ray.d.y, ray.r.y), b = quotient(hy - ray.o.y, ray.d.y, ray.r.y);
     n = fmaxf(n, fminf(a, b));
     f = fminf(f, fmaxf(a, b));
   }
   if (fabsf(ray.d.z) < 1e-12f) {
     if (ray.o.z < lz || ray.o.z > hz) return false;
   } else {
-    float a = quotient(lz - ray.o.z, ray.d.z, ray.r.z, bad), b = quotient(hz - ray.o.z, ray.d.z, ray.r.z, bad);
+    float a = quotient(lz - ray.o.z, ray.d.z, ray.r.z), b = quotient(hz - ray.o.z, ray.d.z, ray.r.z);
     n = fmaxf(n, fminf(a, b));
     f = fminf(f, fmaxf(a, b));
   }
-  if (bad) return box_geometry_ieee(lx, ly, lz, hx, hy, hz, ray, near);
   near = n;
   return !(n > f);
 }
@@ -224,7 +249,7 @@ struct Walker {
   __device__ __forceinline__ void start(const SceneView& s, v3 wo, v3 wd, float lim) {
     o = wo;
     d = wd;
-    ray = make_tray(wo, wd);
+    ray = make_tray(wo, wd, s.small);
     limit = lim;
     base = record = word = 0u;
     inv_det = 1.0f;
@@ -259,7 +284,7 @@ struct Walker {
   __device__ __forceinline__ void inner_phase(const SceneView& s, Stack& st) {
     while (!done) {
       if (ref == STACK_SENTINEL) {
-        ray = make_tray(o, d);
+        ray = make_tray(o, d, s.small);
         base = record = word = 0u;
         inv_det = 1.0f;
         pop(st);
@@ -305,7 +330,7 @@ struct Walker {
         record = m.z;
         word = m.w;
         inv_det = m2.x;
-        if (__float_as_uint(m2.y) != 0u) ray = make_tray(to_object(r0, r1, r2, o, 1.0f), to_object(r0, r1, r2, d, 0.0f));
+        if (__float_as_uint(m2.y) != 0u) ray = make_tray(to_object(r0, r1, r2, o, 1.0f), to_object(r0, r1, r2, d, 0.0f), s.small);
         ref = m.x;
         near_cur = -INFINITY;
         continue;

@@ -87,3 +87,24 @@ def test_empty_and_degenerate_batches(gpu):
     d = np.array([[0, 0, -1], [0, -1, 0], [0, 0, 1], [1, 0, 0]], np.float32)
     compare_closest(trace, make_rays(o, d, 1e20))
     compare_any(trace, make_rays(o, d, 1e20))
+
+
+@pytest.mark.parametrize("scale", [1e-3, 40.0, 1e6])
+def test_unnormalised_directions(gpu, scale):
+    """Directions longer than 16, origins beyond 2^79 or tiny nonzero origin
+    components make a ray unbounded: its boxes are tested with IEEE division.
+    Bounded rays use the unchecked Markstein quotients.  Both equal the
+    oracle's divisions bit for bit."""
+    w = synth.plain_512()
+    trace = Trace(w.scene, w.settings, 64, 64)
+    rng = np.random.default_rng(12)
+    batch = synth.random_rays((-12, 0.01, -12), (12, 21, 12), 20_000, rng)
+    batch["direction"] = batch["direction"] * np.float32(scale)
+    compare_closest(trace, batch)
+    compare_any(trace, make_rays(batch["origin"], batch["direction"], 2.0 / scale))
+    far = batch[:64].copy()
+    far["origin"] = far["origin"] + np.float32(1e24)
+    compare_closest(trace, far)
+    tiny = batch[:256].copy()  # an origin component below 2^-70 (but not 0)
+    tiny["origin"][:, 0] = np.float32(1e-25)
+    compare_closest(trace, tiny)
