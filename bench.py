@@ -279,6 +279,12 @@ def cached_convergence(trace, w, mask_idx, ref, stream, flush, max_spp, cache_se
     summed until the masked pixels reach the target relMSE."""
     import torch
     from pfx_b200.cache import RadianceCache
+    # the launch choices of the cached pass, tuned on a cache that is then dropped
+    scratch = RadianceCache(cache_settings)
+    trace.set_cache(scratch)
+    tuning = trace.autotune(passes=3)
+    trace.set_cache(None)
+    scratch.close()
     cache = RadianceCache(cache_settings)
     trace.set_cache(cache)  # restarts the accumulation
     color = trace.films_device()[0].reshape(-1, 4)
@@ -303,6 +309,7 @@ def cached_convergence(trace, w, mask_idx, ref, stream, flush, max_spp, cache_se
     stats = cache.stats()
     trace.set_cache(None)
     cache.close()
+    stats["tuning"] = tuning
     return reached, elapsed, statistics.median(pass_ms), curve, stats
 
 

@@ -735,10 +735,11 @@ CacheView cache_view(pfxt_cache& c) {
 }
 
 void cache_infer_launch(pfxt_cache& c, const float4* queries, const uint32_t* n_dev, uint32_t n,
-                        const uint32_t* scatter, float4* out, cudaStream_t stream) {
+                        const uint32_t* scatter, float4* out, cudaStream_t stream, uint32_t ctas_per_sm) {
   if (n == 0) return;
   uint32_t tiles = (n + NRC_ROWS - 1) / NRC_ROWS;
-  uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)sm_count() * 4u);
+  ctas_per_sm = std::min<uint32_t>(std::max<uint32_t>(ctas_per_sm, 1u), 4u);
+  uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)sm_count() * ctas_per_sm);
   k_infer<<<grid, 128, I_SMEM, stream>>>(c.grid, c.d_table16, c.d_weights, queries, n_dev, n, scatter, out,
                                          c.d_error);
   check(cudaGetLastError(), "cache inference");

@@ -86,8 +86,10 @@ void cache_set_bounds(pfxt_cache& c, const float lo[3], const float hi[3]);
 CacheView cache_view(pfxt_cache& c);
 // Inference over `n` queries (5 float4 each) on `stream`; out[k] = rgb.
 // `n_dev`, if set, is read on the device instead of `n` (an upper bound).
+// `ctas_per_sm` (1..4) sizes the persistent grid: fewer leave room on every SM
+// for kernels that run beside the inference.
 void cache_infer_launch(pfxt_cache& c, const float4* queries, const uint32_t* n_dev, uint32_t n, const uint32_t* scatter,
-                        float4* out, cudaStream_t stream);
+                        float4* out, cudaStream_t stream, uint32_t ctas_per_sm = 4);
 // One training step over records [first, first + batch) of `records`
 // (6 float4 each) when at least first + batch exist (`count_dev` on the
 // device, or `count` when it is null); then Adam.

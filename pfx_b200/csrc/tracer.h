@@ -137,6 +137,10 @@ struct pfxt_trace {
   // CUDA graphs of the sampling pass (tracer.cu)
   uint32_t* d_vars = nullptr;  // accumulated samples, samples this pass, seed
   uint32_t* h_vars = nullptr;  // pinned mirror, copied in by the pass's first node
+  // The cache inference runs on `side`, forked from `stream` after the last
+  // query bounce and joined before the accumulation, beside the later bounces.
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   std::vector<pfxt::GraphEntry> graphs;
   bool use_graphs = true;
   uint32_t graph_captures = 0;  // passes captured so far

@@ -237,6 +237,14 @@ void trace_release(pfxt_trace& t) {
   if (t.h_vars) cudaFreeHost(t.h_vars);
   t.d_vars = nullptr;
   t.h_vars = nullptr;
+  if (t.side) {
+    cudaStreamSynchronize(t.side);
+    cudaStreamDestroy(t.side);
+  }
+  if (t.fork_ev) cudaEventDestroy(t.fork_ev);
+  if (t.join_ev) cudaEventDestroy(t.join_ev);
+  t.side = nullptr;
+  t.fork_ev = t.join_ev = nullptr;
   if (t.stream) cudaStreamDestroy(t.stream);
   t.stream = nullptr;
 }
