@@ -63,13 +63,14 @@ struct TraceCounts {
 //    [2^-93, 2^80] (a nonzero difference of two such values is a multiple of
 //    the smaller one's ulp, at least 2^-93);
 //  * direction components are degenerate (below 1e-12, never divided by) or of
-//    magnitude in [1e-12, 16], so a nonzero quotient lies in [2^-97, 2^120],
-//    and the residual x - q d, a multiple of ulp(q) ulp(d) >= 2^-141, is exact.
+//    magnitude in [1e-12, 2^20], so a nonzero quotient lies in [2^-113, 2^120]
+//    (normal, with margin), and the residual x - q d, a multiple of
+//    ulp(q) ulp(d) >= 2^-141 (q d is within a few ulps of x), is exact.
 // Box coordinates are checked once per scene (SceneView::small); origins and
 // directions per ray, in world space and in every instance's space.
 constexpr float BOUNDED_COORD = 0x1p+79f;
 constexpr float BOUNDED_TINY = 0x1p-70f;
-constexpr float BOUNDED_DIR = 16.0f;
+constexpr float BOUNDED_DIR = 0x1p+20f;
 
 // A ray in the space it is being traversed in, with the per-axis reciprocal
 // used by the quotients (only read on axes with |d| >= 1e-12).  The boxes of

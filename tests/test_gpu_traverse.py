@@ -89,12 +89,12 @@ def test_empty_and_degenerate_batches(gpu):
     compare_any(trace, make_rays(o, d, 1e20))
 
 
-@pytest.mark.parametrize("scale", [1e-3, 40.0, 1e6])
+@pytest.mark.parametrize("scale", [1e-3, 40.0, 1e6, 1e7])
 def test_unnormalised_directions(gpu, scale):
-    """Directions longer than 16, origins beyond 2^79 or tiny nonzero origin
-    components make a ray unbounded: its boxes are tested with IEEE division.
-    Bounded rays use the unchecked Markstein quotients.  Both equal the
-    oracle's divisions bit for bit."""
+    """Direction components above 2^20, origins beyond 2^79 or tiny nonzero
+    origin components make a ray unbounded: it is walked again with IEEE
+    division.  Bounded rays use the unchecked Markstein quotients.  Both equal
+    the oracle's divisions bit for bit."""
     w = synth.plain_512()
     trace = Trace(w.scene, w.settings, 64, 64)
     rng = np.random.default_rng(12)
