@@ -52,6 +52,9 @@ constexpr int kThreads = 128;
 #define SHADE_LIGHTS_MIN_BLOCKS 12
 #endif
 constexpr uint32_t CAP_MAX = 8u;
+// Pass variables in device memory: samples so far, samples this pass, seed, 0,
+// then the camera's origin, forward, right and up as four float4.
+constexpr size_t PASS_VAR_BYTES = 16 + 64;
 
 // Path flag word (ray_d.w bits).
 constexpr uint32_t F_CARRIED = 0x3u;  // bits 0-1
@@ -133,6 +136,12 @@ struct Pass {
 __device__ __forceinline__ uint32_t pass_accum(const Pass& P) { return __ldg(P.vars + 0); }
 __device__ __forceinline__ uint32_t pass_count(const Pass& P) { return __ldg(P.vars + 1); }
 __device__ __forceinline__ uint32_t pass_seed(const Pass& P) { return __ldg(P.vars + 2); }
+// Camera origin, forward, right and up (xyz) of this pass, after the counters:
+// outside the captured launch parameters, so a moving camera replays one graph.
+__device__ __forceinline__ v3 pass_camera(const Pass& P, int k) {
+  float4 c = __ldg(reinterpret_cast<const float4*>(P.vars) + 1 + k);
+  return mk3(c.x, c.y, c.z);
+}
 
 // The fallback grid: may a path end into the cache at p?
 __device__ __forceinline__ bool cell_ok(const CachePass& c, v3 p) {
@@ -211,10 +220,7 @@ __global__ void k_gen(const __grid_constant__ Pass P) {
     float ndc_x = ((float)px + jx) / (float)P.f.window[0] * 2.0f - 1.0f;
     float ndc_y = ((float)py + jy) / (float)P.f.window[1] * 2.0f - 1.0f;
     uint32_t kind = f2u(rint_(P.f.origin[3]));
-    v3 cam_o = mk3(P.f.origin[0], P.f.origin[1], P.f.origin[2]);
-    v3 cam_f = mk3(P.f.forward[0], P.f.forward[1], P.f.forward[2]);
-    v3 cam_r = mk3(P.f.right[0], P.f.right[1], P.f.right[2]);
-    v3 cam_u = mk3(P.f.up[0], P.f.up[1], P.f.up[2]);
+    v3 cam_o = pass_camera(P, 0), cam_f = pass_camera(P, 1), cam_r = pass_camera(P, 2), cam_u = pass_camera(P, 3);
     v3 direction = normalize3(add3(add3(cam_f, scl3(cam_r, ndc_x + P.f.lens[0])), scl3(cam_u, -ndc_y + P.f.lens[1])));
     v3 origin = cam_o;
     if (kind == 1u) {
@@ -1360,8 +1366,8 @@ CachePass ensure_cache(pfxt_trace& t, uint32_t pixels) {
 // The pass variables: 16 device bytes and their pinned host mirror.
 void ensure_vars(pfxt_trace& t) {
   if (t.d_vars) return;
-  check(cudaMalloc(&t.d_vars, 16), "pass variables");
-  check(cudaHostAlloc(&t.h_vars, 16, cudaHostAllocDefault), "pass variables");
+  check(cudaMalloc(&t.d_vars, PASS_VAR_BYTES), "pass variables");
+  check(cudaHostAlloc(&t.h_vars, PASS_VAR_BYTES, cudaHostAllocDefault), "pass variables");
   check(cudaStreamCreateWithFlags(&t.side, cudaStreamNonBlocking), "side stream");
   check(cudaEventCreateWithFlags(&t.fork_ev, cudaEventDisableTiming), "side stream events");
   check(cudaEventCreateWithFlags(&t.join_ev, cudaEventDisableTiming), "side stream events");
@@ -1415,10 +1421,11 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   ensure_wave(t, pixels, cap);
   Pass P;
   memset(&P, 0, sizeof(P));
-  P.f = t.base;  // the accumulated samples, the count and the seed travel in P.vars
+  P.f = t.base;  // the accumulated samples, the count, the seed and the camera travel in P.vars
   P.f.size[2] = 0u;
   P.f.size[3] = 0u;
   P.f.counts[2] = 0u;
+  for (int k = 0; k < 3; ++k) P.f.origin[k] = P.f.forward[k] = P.f.right[k] = P.f.up[k] = 0.0f;
   P.sp = t.spec;
   P.v = t.shade;
   P.s = t.view;
@@ -1444,6 +1451,14 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   t.h_vars[1] = count;
   t.h_vars[2] = seed;
   t.h_vars[3] = 0u;
+  {
+    const float* rows[4] = {t.base.origin, t.base.forward, t.base.right, t.base.up};
+    float* cam = reinterpret_cast<float*>(t.h_vars + 4);
+    for (int r = 0; r < 4; ++r) {
+      for (int k = 0; k < 3; ++k) cam[4 * r + k] = rows[r][k];
+      cam[4 * r + 3] = 0.0f;
+    }
+  }
   cudaStream_t st = t.stream;
   if (t.samples == 0) check(cudaMemsetAsync(t.d_accum, 0, (size_t)pixels * sizeof(Accum), st), "accumulation reset");
   if (!t.use_graphs) {
@@ -1507,7 +1522,7 @@ namespace {
 void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_t pixels) {
   Grids& g = grids();
   cudaStream_t st = t.stream;
-  check(cudaMemcpyAsync(t.d_vars, t.h_vars, 16, cudaMemcpyHostToDevice, st), "pass variables");
+  check(cudaMemcpyAsync(t.d_vars, t.h_vars, PASS_VAR_BYTES, cudaMemcpyHostToDevice, st), "pass variables");
   check(cudaMemsetAsync(P.w.counters, 0, 32, st), "counters");  // queues; the ray totals at [8..11] persist
   k_collect<<<g.flat, 256, 0, st>>>(P, t.d_accum, t.d_mask);
   bool inferred = false;

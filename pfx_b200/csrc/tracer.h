@@ -135,7 +135,7 @@ struct pfxt_trace {
   void* d_cache_scratch = nullptr;  // queries, predictions, training vertices and records
   size_t cache_scratch_bytes = 0;
   // CUDA graphs of the sampling pass (tracer.cu)
-  uint32_t* d_vars = nullptr;  // accumulated samples, samples this pass, seed
+  uint32_t* d_vars = nullptr;  // accumulated samples, samples this pass, seed, camera (tracer.cu)
   uint32_t* h_vars = nullptr;  // pinned mirror, copied in by the pass's first node
   // The cache inference runs on `side`, forked from `stream` after the last
   // query bounce and joined before the accumulation, beside the later bounces.
