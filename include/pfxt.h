@@ -245,6 +245,26 @@ uint32_t pfxt_samples(const pfxt_trace* trace);
  * per-pixel convergence test between them; writes up to `cap` rounds. */
 int pfxt_sample_adaptive(pfxt_trace* trace, const pfxt_adaptive* adaptive, uint32_t seed,
                          pfxt_round* rounds, uint32_t cap, uint32_t* written);
+/* Keeper (checkpoint.rs:30-34) as callbacks: `resume` (NULL for none) is the
+ * checkpoint Keeper::resume hands back; `due(user, samples)` is Keeper::due,
+ * nonzero when a checkpoint is due after `samples` samples (NULL: never);
+ * `keep(user, bytes, length)` is Keeper::keep, handed a checkpoint in the
+ * pfxt_save layout with the adaptive rounds and snapshots (the bytes live for
+ * the call only); it returns 0 when the checkpoint is kept. */
+typedef struct pfxt_keeper {
+  void* user;
+  const void* resume;
+  size_t resume_length;
+  int (*due)(void* user, uint32_t samples);
+  int (*keep)(void* user, const void* bytes, size_t length);
+} pfxt_keeper;
+/* Trace::sample_adaptive_kept (adaptive.rs:136-325): pfxt_sample_adaptive,
+ * resumed from `keeper->resume` when given (its rounds are written first) and,
+ * with a keeper that can be due, one sample at a time with a checkpoint under
+ * `key` offered after each.  The rounds and the image equal an uninterrupted
+ * pfxt_sample_adaptive's. */
+int pfxt_sample_adaptive_kept(pfxt_trace* trace, const pfxt_adaptive* adaptive, uint32_t seed, const char* key,
+                              const pfxt_keeper* keeper, pfxt_round* rounds, uint32_t cap, uint32_t* written);
 /* Adaptive::rounds (adaptive.rs:46-63). */
 int pfxt_adaptive_rounds(const pfxt_adaptive* adaptive, uint32_t* rounds, uint32_t cap,
                          uint32_t* written);

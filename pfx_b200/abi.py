@@ -118,6 +118,15 @@ class CheckpointInfo(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("samples", C.c_uint32), ("rounds", C.c_uint32)]
 
 
+KEEPER_DUE = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint32)
+KEEPER_KEEP = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t)
+
+
+class Keeper(C.Structure):
+    _fields_ = [("user", C.c_void_p), ("resume", C.c_void_p), ("resume_length", C.c_size_t),
+                ("due", KEEPER_DUE), ("keep", KEEPER_KEEP)]
+
+
 class Tuning(C.Structure):
     _fields_ = [("trace_threads", C.c_uint32), ("sort_shading", C.c_uint32), ("graphs", C.c_uint32),
                 ("split_shade", C.c_uint32), ("sort_rays", C.c_uint32), ("pass_ms", C.c_float)]
@@ -158,6 +167,8 @@ PROTOTYPES = [
     ("pfxt_samples", C.c_uint32, [C.c_void_p]),
     ("pfxt_sample_adaptive", C.c_int, [C.c_void_p, C.POINTER(Adaptive), C.c_uint32, C.POINTER(Round), C.c_uint32,
                                        C.POINTER(C.c_uint32)]),
+    ("pfxt_sample_adaptive_kept", C.c_int, [C.c_void_p, C.POINTER(Adaptive), C.c_uint32, C.c_char_p,
+                                            C.POINTER(Keeper), C.POINTER(Round), C.c_uint32, C.POINTER(C.c_uint32)]),
     ("pfxt_adaptive_rounds", C.c_int, [C.POINTER(Adaptive), C.POINTER(C.c_uint32), C.c_uint32,
                                        C.POINTER(C.c_uint32)]),
     ("pfxt_readback", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -435,6 +435,8 @@ struct Checkpoint {
   uint32_t width = 0, height = 0, samples = 0, rounds = 0xffffffffu;
   const uint8_t* accum = nullptr;
   const uint8_t* films[3] = {nullptr, nullptr, nullptr};
+  const uint8_t* round_bytes = nullptr;  // `rounds` x (u32 samples, u64 active)
+  const uint8_t* snaps = nullptr;        // 32 B per pixel when rounds are present
 };
 
 Checkpoint read_checkpoint(const char* key, const void* bytes, size_t length) {
@@ -472,11 +474,12 @@ Checkpoint read_checkpoint(const char* key, const void* bytes, size_t length) {
   for (auto& film : c.films) film = take(pixels * CKPT_TEXEL);
   c.rounds = word();
   if (c.rounds != 0xffffffffu) {
+    c.round_bytes = p;
     for (uint32_t r = 0; r < c.rounds; ++r) {
       word();
       longword();
     }
-    take(pixels * CKPT_SNAP);
+    c.snaps = take(pixels * CKPT_SNAP);
   }
   if (left != 0) throw Invalid("the checkpoint runs on past its end");
   return c;
@@ -490,51 +493,114 @@ int pfxt_checkpoint_read(const char* key, const void* bytes, size_t length, pfxt
   });
 }
 
+namespace {
+
+// Saved::write_to (checkpoint.rs:82-104) of the trace's accumulation and films,
+// with the adaptive rounds reached and the snapshots when `reached` is given.
+uint64_t checkpoint_size(const pfxt_trace& t, const char* key, const std::vector<pfxt_round>* reached) {
+  const uint64_t pixels = (uint64_t)t.width * t.height;
+  uint64_t need = 8 + 8 + strlen(key) + 12 + pixels * (CKPT_ACCUM + 3 * CKPT_TEXEL) + 4;
+  if (reached) need += reached->size() * 12 + pixels * CKPT_SNAP;
+  return need;
+}
+
+void write_checkpoint(pfxt_trace& t, const char* key, const std::vector<pfxt_round>* reached, uint8_t* p) {
+  const uint64_t key_length = strlen(key);
+  const uint64_t pixels = (uint64_t)t.width * t.height;
+  auto put = [&](const void* src, size_t n) {
+    memcpy(p, src, n);
+    p += n;
+  };
+  put(CKPT_MAGIC, 8);
+  put(&key_length, 8);
+  put(key, key_length);
+  uint32_t head[3] = {t.width, t.height, t.samples};
+  put(head, 12);
+  check(cudaStreamSynchronize(t.stream), "checkpoint");
+  check(cudaMemcpy(p, t.d_accum, pixels * CKPT_ACCUM, cudaMemcpyDeviceToHost), "checkpoint");
+  p += pixels * CKPT_ACCUM;
+  for (const float4* film : {t.d_color, t.d_albedo, t.d_normal}) {
+    check(cudaMemcpy(p, film, pixels * CKPT_TEXEL, cudaMemcpyDeviceToHost), "checkpoint");
+    p += pixels * CKPT_TEXEL;
+  }
+  if (!reached) {
+    uint32_t none = 0xffffffffu;
+    put(&none, 4);
+    return;
+  }
+  uint32_t count = (uint32_t)reached->size();
+  put(&count, 4);
+  for (const pfxt_round& r : *reached) {
+    put(&r.samples, 4);
+    put(&r.active, 8);
+  }
+  check(cudaMemcpy(p, t.d_snaps, pixels * CKPT_SNAP, cudaMemcpyDeviceToHost), "checkpoint");
+}
+
+// Trace::restore (checkpoint.rs:188-203): the accumulation, the films and the count.
+void restore_checkpoint(pfxt_trace& t, const Checkpoint& c) {
+  if (c.width != t.width || c.height != t.height)
+    throw Invalid("the checkpoint is " + std::to_string(c.width) + "x" + std::to_string(c.height) +
+                  " and the trace " + std::to_string(t.width) + "x" + std::to_string(t.height));
+  const uint64_t pixels = (uint64_t)t.width * t.height;
+  check(cudaStreamSynchronize(t.stream), "restore");
+  check(cudaMemcpy(t.d_accum, c.accum, pixels * CKPT_ACCUM, cudaMemcpyHostToDevice), "restore");
+  float4* films[3] = {t.d_color, t.d_albedo, t.d_normal};
+  for (int k = 0; k < 3; ++k)
+    check(cudaMemcpy(films[k], c.films[k], pixels * CKPT_TEXEL, cudaMemcpyHostToDevice), "restore");
+  t.samples = c.samples;
+}
+
+}  // namespace
+
 int pfxt_save(pfxt_trace* t, const char* key, void* bytes, size_t capacity, size_t* written) {
   return guarded([&]() {
     if (!t || !key || !written) throw Invalid("null argument");
-    const uint64_t key_length = strlen(key);
-    const uint64_t pixels = (uint64_t)t->width * t->height;
-    const uint64_t need = 8 + 8 + key_length + 12 + pixels * (CKPT_ACCUM + 3 * CKPT_TEXEL) + 4;
+    const uint64_t need = checkpoint_size(*t, key, nullptr);
     *written = (size_t)need;
     if (!bytes) return;
     if (capacity < need) throw Invalid("the buffer is smaller than the checkpoint");
-    uint8_t* p = static_cast<uint8_t*>(bytes);
-    auto put = [&](const void* src, size_t n) {
-      memcpy(p, src, n);
-      p += n;
-    };
-    put(CKPT_MAGIC, 8);
-    put(&key_length, 8);
-    put(key, key_length);
-    uint32_t head[3] = {t->width, t->height, t->samples};
-    put(head, 12);
-    check(cudaStreamSynchronize(t->stream), "checkpoint");
-    check(cudaMemcpy(p, t->d_accum, pixels * CKPT_ACCUM, cudaMemcpyDeviceToHost), "checkpoint");
-    p += pixels * CKPT_ACCUM;
-    for (const float4* film : {t->d_color, t->d_albedo, t->d_normal}) {
-      check(cudaMemcpy(p, film, pixels * CKPT_TEXEL, cudaMemcpyDeviceToHost), "checkpoint");
-      p += pixels * CKPT_TEXEL;
-    }
-    uint32_t none = 0xffffffffu;
-    put(&none, 4);
+    write_checkpoint(*t, key, nullptr, static_cast<uint8_t*>(bytes));
   });
 }
 
 int pfxt_restore(pfxt_trace* t, const char* key, const void* bytes, size_t length) {
   return guarded([&]() {
     if (!t) throw Invalid("null argument");
-    Checkpoint c = read_checkpoint(key, bytes, length);
-    if (c.width != t->width || c.height != t->height)
-      throw Invalid("the checkpoint is " + std::to_string(c.width) + "x" + std::to_string(c.height) +
-                    " and the trace " + std::to_string(t->width) + "x" + std::to_string(t->height));
-    const uint64_t pixels = (uint64_t)t->width * t->height;
-    check(cudaStreamSynchronize(t->stream), "restore");
-    check(cudaMemcpy(t->d_accum, c.accum, pixels * CKPT_ACCUM, cudaMemcpyHostToDevice), "restore");
-    float4* films[3] = {t->d_color, t->d_albedo, t->d_normal};
-    for (int k = 0; k < 3; ++k)
-      check(cudaMemcpy(films[k], c.films[k], pixels * CKPT_TEXEL, cudaMemcpyHostToDevice), "restore");
-    t->samples = c.samples;
+    restore_checkpoint(*t, read_checkpoint(key, bytes, length));
+  });
+}
+
+int pfxt_sample_adaptive_kept(pfxt_trace* t, const pfxt_adaptive* a, uint32_t seed, const char* key,
+                              const pfxt_keeper* keeper, pfxt_round* rounds, uint32_t cap, uint32_t* written) {
+  return guarded([&]() {
+    if (!t || !a || !key || !written) throw Invalid("null argument");
+    AdaptiveKeeping keeping;
+    if (keeper && keeper->resume) {
+      Checkpoint c = read_checkpoint(key, keeper->resume, keeper->resume_length);
+      if (c.rounds == 0xffffffffu) throw Invalid("the checkpoint holds no adaptive rounds for this render");
+      restore_checkpoint(*t, c);
+      const uint64_t pixels = (uint64_t)t->width * t->height;
+      check(cudaMemcpy(t->d_snaps, c.snaps, pixels * CKPT_SNAP, cudaMemcpyHostToDevice), "restore");
+      for (uint32_t r = 0; r < c.rounds; ++r) {
+        pfxt_round round{0u, 0u, 0u};
+        memcpy(&round.samples, c.round_bytes + 12 * r, 4);
+        memcpy(&round.active, c.round_bytes + 12 * r + 4, 8);
+        keeping.resumed.push_back(round);
+      }
+      keeping.resuming = true;
+    }
+    if (keeper && keeper->due) {
+      if (!keeper->keep) throw Invalid("a keeper that is due must keep");
+      keeping.due = [&](uint32_t samples) { return keeper->due(keeper->user, samples) != 0; };
+      keeping.keep = [&](const std::vector<pfxt_round>& reached) {
+        std::vector<uint8_t> bytes((size_t)checkpoint_size(*t, key, &reached));
+        write_checkpoint(*t, key, &reached, bytes.data());
+        if (keeper->keep(keeper->user, bytes.data(), bytes.size()) != 0)
+          throw Invalid("the keeper could not keep the checkpoint");
+      };
+    }
+    trace_sample_adaptive(*t, *a, seed, rounds, cap, written, &keeping);
   });
 }
 

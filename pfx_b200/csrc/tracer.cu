@@ -1651,22 +1651,42 @@ __global__ void k_mark(Accum* __restrict__ accum, const float4* __restrict__ sna
 
 // Trace::sample_adaptive_kept without a keeper (adaptive.rs:136-325).
 void trace_sample_adaptive(pfxt_trace& t, const pfxt_adaptive& a, uint32_t seed, pfxt_round* rounds, uint32_t cap,
-                           uint32_t* written) {
+                           uint32_t* written, const AdaptiveKeeping* keeping) {
   bool valid = std::isfinite(a.threshold) && a.threshold > 0.0f && a.min_samples >= 2u &&
                a.max_samples >= a.min_samples && std::isfinite(a.growth) && a.growth > 1.0f;
   if (!valid)
     throw Invalid("adaptive sampling needs a positive threshold, a growth over 1 and at least 2 samples");
-  t.samples = 0;
   uint32_t pixels = t.width * t.height;
   cudaStream_t st = t.stream;
-  check(cudaMemsetAsync(t.d_snaps, 0, (size_t)pixels * 32, st), "snapshots");
   std::vector<uint32_t> targets = adaptive_rounds(a);
+  std::vector<pfxt_round> reached;
+  if (keeping && keeping->resuming) {
+    // the caller restored the accumulation, the films, the snapshots and the sample count
+    if (keeping->resumed.size() >= targets.size())
+      throw Invalid("the checkpoint holds no adaptive rounds for this render");
+    reached = keeping->resumed;
+  } else {
+    t.samples = 0;
+    check(cudaMemsetAsync(t.d_snaps, 0, (size_t)pixels * 32, st), "snapshots");
+  }
   Grids& g = grids();
   uint32_t n = 0;
-  for (size_t step = 0; step < targets.size(); ++step) {
+  for (const pfxt_round& r : reached) {
+    if (rounds && n < cap) rounds[n] = r;
+    ++n;
+  }
+  for (size_t step = reached.size(); step < targets.size(); ++step) {
     uint32_t target = targets[step];
     uint32_t count = target > t.samples ? target - t.samples : 0u;
-    trace_sample(t, count, seed);
+    if (keeping && keeping->due) {
+      // one sample at a time, offering a checkpoint after each (adaptive.rs:258-277)
+      for (uint32_t s = 0; s < count; ++s) {
+        trace_sample(t, 1u, seed);
+        if (keeping->due(t.samples)) keeping->keep(reached);
+      }
+    } else {
+      trace_sample(t, count, seed);
+    }
     check(cudaMemsetAsync(t.d_running, 0, 4, st), "running count");
     k_measure<<<g.flat, 256, 0, st>>>(t.d_accum, t.d_snaps, t.width, t.height);
     if (step > 0) k_mark<<<g.flat, 256, 0, st>>>(t.d_accum, t.d_snaps, t.width, t.height, a.min_samples, a.threshold,
@@ -1675,11 +1695,9 @@ void trace_sample_adaptive(pfxt_trace& t, const pfxt_adaptive& a, uint32_t seed,
     check(cudaMemcpyAsync(&running, t.d_running, 4, cudaMemcpyDeviceToHost, st), "running count");
     check(cudaStreamSynchronize(st), "convergence");
     uint64_t active = step > 0 ? (uint64_t)running : (uint64_t)pixels;
-    if (rounds && n < cap) {
-      rounds[n].samples = target;
-      rounds[n].pad = 0;
-      rounds[n].active = active;
-    }
+    pfxt_round round{target, 0u, active};
+    reached.push_back(round);
+    if (rounds && n < cap) rounds[n] = round;
     ++n;
     if (active == 0) break;
   }

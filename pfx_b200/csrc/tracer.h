@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -166,8 +167,18 @@ void trace_move_scene(pfxt_trace& t, const pfxt_buffers& b);
 void trace_set_tuning(pfxt_trace& t, const pfxt_tuning& k);
 pfxt_tuning trace_get_tuning(const pfxt_trace& t);
 pfxt_tuning trace_autotune(pfxt_trace& t, uint32_t passes);
+// What Trace::sample_adaptive_kept adds (adaptive.rs:136-277): the rounds a
+// resumed render had reached (its accumulation, films and snapshots are
+// restored by the caller), and a keeper asked after every sample whether a
+// checkpoint is due and handed the rounds reached so far when one is.
+struct AdaptiveKeeping {
+  std::vector<pfxt_round> resumed;
+  bool resuming = false;
+  std::function<bool(uint32_t samples)> due;                        // empty: no keeper
+  std::function<void(const std::vector<pfxt_round>& reached)> keep;
+};
 void trace_sample_adaptive(pfxt_trace& t, const pfxt_adaptive& a, uint32_t seed, pfxt_round* rounds, uint32_t cap,
-                           uint32_t* written);
+                           uint32_t* written, const AdaptiveKeeping* keeping = nullptr);
 std::vector<uint32_t> adaptive_rounds(const pfxt_adaptive& a);
 void trace_readback(pfxt_trace& t, float* color, float* albedo, float* normal);
 void trace_sample_counts(pfxt_trace& t, uint32_t* counts);

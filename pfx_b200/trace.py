@@ -287,6 +287,45 @@ class Trace:
         return Converged([Round(int(rounds[i].samples), int(rounds[i].active)) for i in range(n.value)],
                          self.width * self.height)
 
+    def sample_adaptive_kept(self, adaptive: Adaptive, seed: int, key: str, keeper) -> Converged:
+        """Trace::sample_adaptive_kept (adaptive.rs:136-325).  `keeper` mirrors the
+        Keeper trait (checkpoint.rs:30-34): keeper.resume() -> checkpoint bytes or
+        None, keeper.due(samples) -> bool, keeper.keep(bytes) (raise to refuse).
+        Checkpoints are taken under `key` in the layout of Trace.save, with the
+        adaptive rounds and snapshots."""
+        cap = 4096
+        rounds = (abi.Round * cap)()
+        n = C.c_uint32()
+        resume = keeper.resume()
+        failure = []
+
+        def due(_user, samples):
+            try:
+                return 1 if keeper.due(int(samples)) else 0
+            except Exception as e:  # noqa: BLE001 - carried back to the caller below
+                failure.append(e)
+                return 0
+
+        def keep(_user, ptr, length):
+            try:
+                keeper.keep(C.string_at(ptr, length))
+                return 0
+            except Exception as e:  # noqa: BLE001
+                failure.append(e)
+                return 1
+
+        k = abi.Keeper(None, None, 0, abi.KEEPER_DUE(due), abi.KEEPER_KEEP(keep))
+        if resume is not None:
+            buf = C.create_string_buffer(bytes(resume), len(resume))
+            k.resume, k.resume_length = C.cast(buf, C.c_void_p), len(resume)
+        rc = self._lib.pfxt_sample_adaptive_kept(self._h, C.byref(adaptive.c()), seed, key.encode(), C.byref(k),
+                                                 rounds, cap, C.byref(n))
+        if failure:
+            raise failure[0]
+        check(rc)
+        return Converged([Round(int(rounds[i].samples), int(rounds[i].active)) for i in range(n.value)],
+                         self.width * self.height)
+
     # ---------------------------------------------------------- readback
     def readback(self) -> Output:
         shape = (self.height, self.width, 4)
