@@ -239,6 +239,14 @@ int pfxt_set_window(pfxt_trace* trace, const uint32_t full[2], const uint32_t or
 
 /* Trace::sample (gpu.rs:2942): `count` more samples per pixel with `seed`. */
 int pfxt_sample(pfxt_trace* trace, uint32_t count, uint32_t seed);
+/* Trace::sample_paced (gpu.rs:2951-3110): the same samples taken one pass at a
+ * time, `between(user, ms)` called after each with the pass's device time (the
+ * reference reports each settled slice to `between`; it slices passes to keep
+ * a display responsive, which a compute GPU does not need).  The image equals
+ * pfxt_sample's.  *wall_ms (may be NULL) receives the host time of the call. */
+typedef void (*pfxt_between)(void* user, double milliseconds);
+int pfxt_sample_paced(pfxt_trace* trace, uint32_t count, uint32_t seed, pfxt_between between, void* user,
+                      double* wall_ms);
 /* Trace::samples (gpu.rs:3233). */
 uint32_t pfxt_samples(const pfxt_trace* trace);
 /* Trace::sample_adaptive (adaptive.rs:112-325): rounds of samples with the

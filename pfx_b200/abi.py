@@ -118,6 +118,7 @@ class CheckpointInfo(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("samples", C.c_uint32), ("rounds", C.c_uint32)]
 
 
+BETWEEN = C.CFUNCTYPE(None, C.c_void_p, C.c_double)
 KEEPER_DUE = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint32)
 KEEPER_KEEP = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t)
 
@@ -165,6 +166,8 @@ PROTOTYPES = [
     ("pfxt_set_window", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     ("pfxt_sample", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     ("pfxt_samples", C.c_uint32, [C.c_void_p]),
+    ("pfxt_sample_paced", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, BETWEEN, C.c_void_p,
+                                    C.POINTER(C.c_double)]),
     ("pfxt_sample_adaptive", C.c_int, [C.c_void_p, C.POINTER(Adaptive), C.c_uint32, C.POINTER(Round), C.c_uint32,
                                        C.POINTER(C.c_uint32)]),
     ("pfxt_sample_adaptive_kept", C.c_int, [C.c_void_p, C.POINTER(Adaptive), C.c_uint32, C.c_char_p,

@@ -2,6 +2,7 @@
 // the blocking host-memory entry points.  Kernels live in the other .cu files.
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -290,6 +291,38 @@ int pfxt_sample(pfxt_trace* t, uint32_t count, uint32_t seed) {
   return guarded([&]() {
     if (!t) throw Invalid("null argument");
     trace_sample(*t, count, seed);
+  });
+}
+
+int pfxt_sample_paced(pfxt_trace* t, uint32_t count, uint32_t seed, pfxt_between between, void* user,
+                      double* wall_ms) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    if ((uint64_t)t->samples + count > 0xffffffffull) throw Invalid("sample count overflow");
+    auto start = std::chrono::steady_clock::now();
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    check(cudaEventCreate(&ev[0]), "pass timing");
+    cudaError_t e = cudaEventCreate(&ev[1]);
+    if (e != cudaSuccess) cudaEventDestroy(ev[0]);
+    check(e, "pass timing");
+    try {
+      for (uint32_t i = 0; i < count; ++i) {  // one slice per sample, as Pacer slices a pass
+        check(cudaEventRecord(ev[0], t->stream), "pass timing");
+        trace_sample(*t, 1u, seed);
+        check(cudaEventRecord(ev[1], t->stream), "pass timing");
+        check(cudaEventSynchronize(ev[1]), "pass timing");
+        float ms = 0.0f;
+        check(cudaEventElapsedTime(&ms, ev[0], ev[1]), "pass timing");
+        if (between) between(user, (double)ms);
+      }
+    } catch (...) {
+      cudaEventDestroy(ev[0]);
+      cudaEventDestroy(ev[1]);
+      throw;
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (wall_ms) *wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - start).count();
   });
 }
 

@@ -173,6 +173,14 @@ class Converged:
 
 
 @dataclass
+class Stats:
+    """Stats (crates/gpu/src/pace.rs:66-70): device milliseconds of each pass and
+    the host time of the whole call."""
+    milliseconds: list
+    wall_ms: float
+
+
+@dataclass
 class Output:
     color: np.ndarray
     albedo: np.ndarray
@@ -275,6 +283,27 @@ class Trace:
     # ---------------------------------------------------------- sampling
     def sample(self, count: int, seed: int) -> None:
         check(self._lib.pfxt_sample(self._h, count, seed))
+
+    def sample_paced(self, count: int, seed: int, between=None) -> Stats:
+        """Trace::sample_paced (gpu.rs:2951): the samples one pass at a time,
+        `between(ms)` after each with its device time; the image equals
+        sample(count, seed)'s."""
+        ms, failure = [], []
+
+        def hook(_user, t):
+            ms.append(float(t))
+            if between is not None:
+                try:
+                    between(float(t))
+                except Exception as e:  # noqa: BLE001 - carried back to the caller below
+                    failure.append(e)
+
+        wall = C.c_double()
+        rc = self._lib.pfxt_sample_paced(self._h, count, seed, abi.BETWEEN(hook), None, C.byref(wall))
+        if failure:
+            raise failure[0]
+        check(rc)
+        return Stats(ms, float(wall.value))
 
     def samples(self) -> int:
         return int(self._lib.pfxt_samples(self._h))

@@ -190,3 +190,17 @@ def test_adaptive_rounds_match_the_oracle(gpu):
     counts = trace.sample_counts()
     assert counts.max() <= adaptive.max_samples and counts.min() >= 1
     assert 0 < conv.mean_samples() <= adaptive.max_samples
+
+
+def test_paced_sampling_equals_one_call(gpu):
+    """Trace::sample_paced (gpu.rs:2951): one pass per sample, `between` told
+    each pass's device time; the image equals sample(count)'s bit for bit."""
+    w = synth.small("plain_512", (48, 32), sampler="sobol")
+    whole = Trace(w.scene, w.settings, w.width, w.height)
+    whole.sample(3, 17)
+    paced = Trace(w.scene, w.settings, w.width, w.height)
+    seen = []
+    stats = paced.sample_paced(3, 17, seen.append)
+    assert len(seen) == 3 and stats.milliseconds == seen and all(m > 0.0 for m in seen)
+    assert stats.wall_ms > 0.0 and paced.samples() == 3
+    assert np.array_equal(paced.read_accum(), whole.read_accum())
