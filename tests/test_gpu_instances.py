@@ -81,3 +81,18 @@ def test_a_move_under_the_radiance_cache(gpu):
     assert trace.samples() == 4
     assert np.isfinite(trace.readback().color).all()
     assert cache.stats()["steps"] >= 8
+
+
+def test_the_reference_stage_moves_like_a_fresh_stage(gpu):
+    """moved_instances_trace_as_a_fresh_stage (instances.rs:214-254) on the
+    reference's own stage built with pfx_b200.stage (indexed meshes, one ball
+    mesh placed with two materials), 96 x 64, 8 samples with seed 11."""
+    from test_stage import staged as reference_stage
+    kept = reference_stage(synth.staged_poses(False)).trace(96, 64)
+    before = traced(kept)
+    assert kept.set_instance_transforms(synth.staged_poses(True))
+    moved = traced(kept)
+    expected = traced(reference_stage(synth.staged_poses(True)).trace(96, 64))
+    assert not np.array_equal(before, moved)
+    assert np.array_equal(moved.view(np.uint32), expected.view(np.uint32))
+    assert kept.builds() == (3, 2)
