@@ -213,7 +213,9 @@ __device__ __forceinline__ v3 ggx_spec(float ndv, float ndl, float ndh, float a2
   float g = smith_g1(ndv, a2) * smith_g1(ndl, a2);
   return divs3(scl3(scl3(fresnel, ggx_d(ndh, a2)), g), 4.0f * ndv * ndl);
 }
-SH_CALL v3 bsdf_eval(const Shaded& s, v3 wo, v3 wi) {
+// `roughness` stands for s.roughness: a light slot evaluates the lobe widened
+// to the light's own roughness without copying the whole Shaded record.
+SH_CALL v3 bsdf_eval(const Shaded& s, v3 wo, v3 wi, float roughness) {
   float ndv = wo.z;
   if (ndv <= 1e-5f) return splat3(0.0f);
   float ndl = wi.z;
@@ -235,7 +237,7 @@ SH_CALL v3 bsdf_eval(const Shaded& s, v3 wo, v3 wi) {
   float ndh = fmax_(h.z, 0.0f);
   float vdh = fmax_(dot3(wo, h), 0.0f);
   v3 fresnel = reflection(s, vdh);
-  float a = alpha_rough(s.roughness);
+  float a = alpha_rough(roughness);
   v3 spec = ggx_spec(ndv, ndl, ndh, a * a, fresnel);
   v3 transmitted = sub3(splat3(1.0f), fresnel);
   float body = (1.0f - metal) * (1.0f - trans) * (1.0f - sss);

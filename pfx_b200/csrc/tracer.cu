@@ -733,9 +733,8 @@ __global__ void __launch_bounds__(kThreads, SHADE_MIN_BLOCKS) k_shade(const __gr
                 strength = divs3(strength, pdf * (1.0f + ratio * ratio));
               }
             }
-            Shaded lit = s;
-            lit.roughness = lit_roughness;
-            v3 term = mul3(scl3(scl3(mul3(throughput, bsdf_eval(lit, wo, local)), pdf > 0.0f ? glossy_share(s) : 1.0f),
+            v3 term = mul3(scl3(scl3(mul3(throughput, bsdf_eval(s, wo, local, lit_roughness)),
+                                     pdf > 0.0f ? glossy_share(s) : 1.0f),
                                 local.z),
                            strength);
             term = capped(P, term, bounce > 0u);
@@ -778,7 +777,7 @@ __global__ void __launch_bounds__(kThreads, SHADE_MIN_BLOCKS) k_shade(const __gr
           } else if (wi.z <= 0.0f || sample.pdf <= 0.0f) {
             go = false;
           } else {
-            throughput = mul3(throughput, scl3(divs3(scl3(scl3(bsdf_eval(s, wo, wi), glossy_share(s)), wi.z), sample.pdf), 1.0f));
+            throughput = mul3(throughput, scl3(divs3(scl3(scl3(bsdf_eval(s, wo, wi, s.roughness), glossy_share(s)), wi.z), sample.pdf), 1.0f));
             d = normalize3(mulmv(transform, wi));
             previous_pdf = sample.pdf;
           }
@@ -1040,9 +1039,8 @@ __global__ void __launch_bounds__(kThreads, SHADE_LIGHTS_MIN_BLOCKS) k_shade_lig
           strength = divs3(strength, pdf * (1.0f + ratio * ratio));
         }
       }
-      Shaded lit = s;
-      lit.roughness = lit_roughness;
-      v3 term = mul3(scl3(scl3(mul3(throughput, bsdf_eval(lit, wo, local)), pdf > 0.0f ? glossy_share(s) : 1.0f),
+      v3 term = mul3(scl3(scl3(mul3(throughput, bsdf_eval(s, wo, local, lit_roughness)),
+                               pdf > 0.0f ? glossy_share(s) : 1.0f),
                           local.z),
                      strength);
       term = capped(P, term, bounce > 0u);
@@ -1121,7 +1119,7 @@ __global__ void __launch_bounds__(kThreads) k_shade_bsdf(const __grid_constant__
       } else if (wi.z <= 0.0f || sample.pdf <= 0.0f) {
         go = false;
       } else {
-        throughput = mul3(throughput, scl3(divs3(scl3(scl3(bsdf_eval(s, wo, wi), glossy_share(s)), wi.z), sample.pdf), 1.0f));
+        throughput = mul3(throughput, scl3(divs3(scl3(scl3(bsdf_eval(s, wo, wi, s.roughness), glossy_share(s)), wi.z), sample.pdf), 1.0f));
         d = normalize3(mulmv(transform, wi));
         previous_pdf = sample.pdf;
       }
