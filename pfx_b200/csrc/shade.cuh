@@ -531,9 +531,11 @@ __device__ __forceinline__ void shadow_ray(v3 origin, v3 aim, bool shadow, v3& d
   limit = l;
 }
 
-// light_candidate (lights.wgsl:145-200)
-SH_CALL Candidate light_candidate(const Specialise& sp, const LightRow& light, const m3& transform,
-                                                     v3 p, v3 origin, v3 geometric, uint32_t& state, float4 u) {
+// light_candidate (lights.wgsl:145-200) of light row `row`, loaded here so that
+// the caller holds no copy of the row in memory across the call.
+SH_CALL Candidate light_candidate(const Specialise& sp, const ShadeView& v, uint32_t row, const m3& transform,
+                                  v3 p, v3 origin, v3 geometric, uint32_t& state, float4 u) {
+  const LightRow light = load_light(v, row);
   Candidate out = candidate_none();
   bool shadow = light.d.w > 0.5f;
   uint32_t kind = f2u(light.a.w);

@@ -706,11 +706,11 @@ __global__ void __launch_bounds__(kThreads, SHADE_MIN_BLOCKS) k_shade(const __gr
                 if (!(pk.y > 0.0f)) {
                   picked = candidate_none();
                 } else {
-                  picked = light_candidate(sp, load_light(V, f2u(pk.x)), transform, p, origin, geometric, state, u);
+                  picked = light_candidate(sp, V, f2u(pk.x), transform, p, origin, geometric, state, u);
                   picked.scale = divs3(picked.scale, pk.y);
                 }
               } else if (slot > 0u) {
-                picked = light_candidate(sp, load_light(V, slot - 1u), transform, p, origin, geometric, state, u);
+                picked = light_candidate(sp, V, slot - 1u, transform, p, origin, geometric, state, u);
               } else if (V.emitter_count == 0u) {
                 picked = candidate_none();
               } else {
@@ -1012,11 +1012,11 @@ __global__ void __launch_bounds__(kThreads, SHADE_LIGHTS_MIN_BLOCKS) k_shade_lig
           if (!(pk.y > 0.0f)) {
             picked = candidate_none();
           } else {
-            picked = light_candidate(sp, load_light(V, f2u(pk.x)), transform, p, origin, geometric, state, u);
+            picked = light_candidate(sp, V, f2u(pk.x), transform, p, origin, geometric, state, u);
             picked.scale = divs3(picked.scale, pk.y);
           }
         } else if (slot > 0u) {
-          picked = light_candidate(sp, load_light(V, slot - 1u), transform, p, origin, geometric, state, u);
+          picked = light_candidate(sp, V, slot - 1u, transform, p, origin, geometric, state, u);
         } else if (V.emitter_count == 0u) {
           picked = candidate_none();
         } else {
