@@ -6,6 +6,8 @@ Moving every instance of a built scene to new transforms leaves the buffers
 bit for bit equal to a scene built with those transforms; moving nothing
 changes nothing; a partial list moves only its prefix; the reference's error
 cases keep their messages."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -81,3 +83,23 @@ def test_reference_errors():
     assert not lone.move_instances([])
     with pytest.raises(TraceError, match="this trace has no instances to move"):
         lone.move_instances([synth.IDENTITY])
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_many_random_moves_equal_fresh_builds(seed):
+    """The instanced workload (boxes and icospheres from 8 clusters): moving
+    every instance to a random pose gives a fresh build's buffers, bit for bit."""
+    rng = np.random.default_rng(seed)
+    w = synth.instanced_1080(target=20_000)
+    n = len(w.scene.instances)
+    poses = np.stack([synth.transform_matrix(float(rng.uniform(0.2, 5.0)), synth.random_rotation(rng),
+                                             rng.uniform(-60, 60, 3)) for _ in range(n)])
+    kept = SceneBuffers(w.scene, w.settings)
+    assert kept.move_instances(poses)
+    moved = w.scene.instances.copy()
+    moved["transform"] = poses
+    fresh_scene = dataclasses.replace(w.scene, instances=moved)
+    fresh = SceneBuffers(fresh_scene, w.settings)
+    for name in MOVED + KEPT:
+        assert np.array_equal(kept.array(name), fresh.array(name)), name
+    assert kept.builds() == (fresh.builds()[0], 2)
