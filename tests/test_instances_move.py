@@ -103,3 +103,17 @@ def test_many_random_moves_equal_fresh_builds(seed):
     for name in MOVED + KEPT:
         assert np.array_equal(kept.array(name), fresh.array(name)), name
     assert kept.builds() == (fresh.builds()[0], 2)
+
+
+def test_a_move_keeps_the_emitter_list_a_fresh_build_would_shrink():
+    """move_instances rewrites the vertices of the emitter candidates it built
+    with and keeps the list (gpu.rs:2484-2499): an emissive panel shrunk below
+    the 1e-12 area cutoff stays an emitter, where a fresh build would drop it."""
+    kept = built(synth.staged_poses(False))
+    count = kept.buffers.emitter_count
+    poses = synth.staged_poses(False)
+    poses[3] = synth.placed((0.0, 1.8, -0.8), 0.0, 1e-7)
+    assert kept.move_instances(poses)
+    assert kept.buffers.emitter_count == count
+    assert np.frombuffer(kept.array("emitters")[:4].tobytes(), np.float32)[0] == count  # the header's count
+    assert built(poses).buffers.emitter_count < count
