@@ -355,7 +355,9 @@ int pfxt_scene_move_instances(pfxt_scene_blobs* blobs, const float* transforms, 
 int pfxt_scene_builds(const pfxt_scene_blobs* blobs, uint32_t* bottom, uint32_t* top);
 /* Trace::set_instance_transforms (gpu.rs:2422-2431): the same on the blobs the
  * trace was created from, then the moved buffers are uploaded (finish_tops,
- * gpu.rs:2533-2540) and the accumulation restarts when anything moved. */
+ * gpu.rs:2533-2540) and the accumulation restarts when anything moved.  If the
+ * upload fails (an error after the blobs moved), the blobs hold the new poses
+ * and the trace the old ones: pfxt_finish_tops with the blobs' buffers retries. */
 int pfxt_set_instance_transforms(pfxt_trace* trace, pfxt_scene_blobs* blobs, const float* transforms, uint32_t count,
                                  uint32_t* moved);
 /* Trace::finish_tops (gpu.rs:2533-2546) for a host that moves instances in

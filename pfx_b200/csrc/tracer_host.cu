@@ -271,6 +271,21 @@ void trace_move_scene(pfxt_trace& t, const pfxt_buffers& b) {
   if (b.surfaces_bytes != t.surfaces_bytes || b.emitters_bytes != t.emitters_bytes ||
       b.emitter_cdf_bytes != t.emitter_cdf_bytes || b.nodes_bytes < sizeof(GpuNode))
     throw Invalid("the moved scene does not match the trace's buffers");
+  // The same index checks as at creation for what is uploaded again (the
+  // traversal layout checks the nodes and instance records itself).
+  {
+    const GpuSurface* sf = static_cast<const GpuSurface*>(b.surfaces);
+    const uint32_t surfaces = (uint32_t)(b.surfaces_bytes / sizeof(GpuSurface));
+    for (uint32_t r = 0; r < surfaces; ++r)
+      if (sf[r].info[1] != NO_MATERIAL && sf[r].info[1] >= t.shade.material_count)
+        throw Invalid("an instance record names a missing material");
+    const GpuEmitter* em = static_cast<const GpuEmitter*>(b.emitters);
+    if (f2u(em[0].a[0]) != t.shade.emitter_count || f2u(em[0].a[1]) != t.shade.looped ||
+        f2u(em[0].a[3]) != t.shade.tree)
+      throw Invalid("the moved emitter list does not match the trace's");
+    for (uint32_t e = 1; e <= t.shade.emitter_count; ++e)
+      if (f2u(em[e].b[3]) >= surfaces) throw Invalid("an emitter names a missing instance record");
+  }
   TraversalLayout layout = make_layout(b);
   check(cudaStreamSynchronize(t.stream), "move instances");
   // New traversal buffers first, so that a failed allocation leaves the trace as it was.
