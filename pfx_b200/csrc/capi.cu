@@ -608,10 +608,14 @@ int pfxt_sample_adaptive_kept(pfxt_trace* t, const pfxt_adaptive* a, uint32_t se
                               const pfxt_keeper* keeper, pfxt_round* rounds, uint32_t cap, uint32_t* written) {
   return guarded([&]() {
     if (!t || !a || !key || !written) throw Invalid("null argument");
+    if (!adaptive_valid(*a))
+      throw Invalid("adaptive sampling needs a positive threshold, a growth over 1 and at least 2 samples");
     AdaptiveKeeping keeping;
     if (keeper && keeper->resume) {
       Checkpoint c = read_checkpoint(key, keeper->resume, keeper->resume_length);
-      if (c.rounds == 0xffffffffu) throw Invalid("the checkpoint holds no adaptive rounds for this render");
+      // checked before anything is restored, as the reference checks (adaptive.rs:236-243)
+      if (c.rounds == 0xffffffffu || c.rounds >= adaptive_rounds(*a).size())
+        throw Invalid("the checkpoint holds no adaptive rounds for this render");
       restore_checkpoint(*t, c);
       const uint64_t pixels = (uint64_t)t->width * t->height;
       check(cudaMemcpy(t->d_snaps, c.snaps, pixels * CKPT_SNAP, cudaMemcpyHostToDevice), "restore");

@@ -1650,9 +1650,7 @@ __global__ void k_mark(Accum* __restrict__ accum, const float4* __restrict__ sna
 // Trace::sample_adaptive_kept without a keeper (adaptive.rs:136-325).
 void trace_sample_adaptive(pfxt_trace& t, const pfxt_adaptive& a, uint32_t seed, pfxt_round* rounds, uint32_t cap,
                            uint32_t* written, const AdaptiveKeeping* keeping) {
-  bool valid = std::isfinite(a.threshold) && a.threshold > 0.0f && a.min_samples >= 2u &&
-               a.max_samples >= a.min_samples && std::isfinite(a.growth) && a.growth > 1.0f;
-  if (!valid)
+  if (!adaptive_valid(a))
     throw Invalid("adaptive sampling needs a positive threshold, a growth over 1 and at least 2 samples");
   uint32_t pixels = t.width * t.height;
   cudaStream_t st = t.stream;

@@ -179,6 +179,7 @@ struct AdaptiveKeeping {
 };
 void trace_sample_adaptive(pfxt_trace& t, const pfxt_adaptive& a, uint32_t seed, pfxt_round* rounds, uint32_t cap,
                            uint32_t* written, const AdaptiveKeeping* keeping = nullptr);
+bool adaptive_valid(const pfxt_adaptive& a);
 std::vector<uint32_t> adaptive_rounds(const pfxt_adaptive& a);
 void trace_readback(pfxt_trace& t, float* color, float* albedo, float* normal);
 void trace_sample_counts(pfxt_trace& t, uint32_t* counts);

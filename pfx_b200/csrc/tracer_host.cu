@@ -376,6 +376,11 @@ void trace_sample_counts(pfxt_trace& t, uint32_t* counts) {
 }
 
 // Adaptive::rounds (adaptive.rs:46-63).
+bool adaptive_valid(const pfxt_adaptive& a) {  // Adaptive::valid (adaptive.rs:28-33)
+  return std::isfinite(a.threshold) && a.threshold > 0.0f && a.min_samples >= 2u && a.max_samples >= a.min_samples &&
+         std::isfinite(a.growth) && a.growth > 1.0f;
+}
+
 std::vector<uint32_t> adaptive_rounds(const pfxt_adaptive& a) {
   std::vector<uint32_t> rounds{std::max(a.min_samples / 2u, 1u)};
   for (;;) {
