@@ -1361,7 +1361,8 @@ CachePass ensure_cache(pfxt_trace& t, uint32_t pixels) {
   return c;
 }
 
-// The pass variables: 16 device bytes and their pinned host mirror.
+// The pass variables (PASS_VAR_BYTES: counters, seed, camera) and their pinned
+// host mirror, and the side stream and events of the cache inference.
 void ensure_vars(pfxt_trace& t) {
   if (t.d_vars) return;
   check(cudaMalloc(&t.d_vars, PASS_VAR_BYTES), "pass variables");
