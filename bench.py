@@ -494,7 +494,7 @@ def main():
                 "plain_curve": [(n, round(e, 5)) for n, e in curve[:: max(1, len(curve) // 12)] + curve[-1:]],
                 "cached_curve": [(n, t, round(e, 5)) for n, t, e in
                                  curve_c[:: max(1, len(curve_c) // 12)] + curve_c[-1:]]}
-        if not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline:  # the host baseline is timed at N=1 only
             line["cpu_baseline"] = cpu_baseline(w)
         print(json.dumps(line))
     trace.close()
