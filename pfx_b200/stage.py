@@ -9,8 +9,9 @@ meshes placed by instances, turned into the tracer's scene.
 As in the reference, every placement becomes an instance whose triangles carry
 the placement's material; placements of the same mesh with the same material
 share one triangle list (and so one bottom-level BVH), and the staged scene has
-no world triangles.  The parts of a stage this tracer does not render (alpha
-cutouts, clip planes, content images and text, motion, image-based skies) are
+no world triangles.  Vertex alpha below a placement's cutoff is cut out of the
+geometry as the reference cuts it.  The parts of a stage this tracer does not
+render (clip planes, content images and text, motion, image-based skies) are
 refused with an error instead of being dropped.
 """
 from __future__ import annotations
@@ -99,17 +100,53 @@ def _check_mesh(mesh: Mesh) -> None:
         raise _invalid("mesh index is outside the vertex buffer")
 
 
-def _triangles(mesh: Mesh, material: int) -> np.ndarray:
-    """triangles (stage.rs:736-768) for a mesh without alpha: one triangle per
-    index triple, corners in index order, with the placement's material."""
+def _cut(corners: list, cutoff: np.float32) -> list:
+    """cut / cut_at (stage.rs:770-820): the corners of a triangle clipped to
+    where the vertex alpha is at least `cutoff` (interpolated linearly along
+    each edge, in f32 as the reference does); all three kept when all pass."""
+    if all(c[3] >= cutoff for c in corners):
+        return corners
+    kept = []
+    for k in range(3):
+        a, b = corners[k], corners[(k + 1) % 3]
+        inside_a, inside_b = a[3] >= cutoff, b[3] >= cutoff
+        if inside_a:
+            kept.append(a)
+        if inside_a != inside_b:
+            t = (cutoff - a[3]) / (b[3] - a[3])
+            kept.append(tuple([x + (y - x) * t for x, y in zip(a[:3], b[:3])]) + (cutoff,))
+    return kept
+
+
+def _triangles(mesh: Mesh, material: int, cutoff: float) -> np.ndarray:
+    """triangles (stage.rs:736-768): one triangle per index triple, corners in
+    index order, with the placement's material; where vertex alpha is given,
+    each triangle is first clipped to alpha >= cutoff and the kept polygon
+    fanned from its first corner."""
     _check_mesh(mesh)
-    if mesh.alpha is not None and np.any(np.asarray(mesh.alpha) < ALPHA_CUTOFF):
-        raise _invalid("mesh alpha cutouts are outside this tracer's scope")
     f = np.asarray(mesh.indices, np.int64).reshape(-1, 3)
-    out = np.zeros(len(f), TRIANGLE)
-    out["v"] = np.asarray(mesh.positions, np.float32)[f]
-    out["n"] = np.asarray(mesh.normals, np.float32)[f]
-    out["uv"] = np.asarray(mesh.uvs, np.float32)[f]
+    pos = np.asarray(mesh.positions, np.float32)
+    nrm = np.asarray(mesh.normals, np.float32)
+    uvs = np.asarray(mesh.uvs, np.float32)
+    if mesh.alpha is None or np.all(np.asarray(mesh.alpha, np.float32) >= np.float32(cutoff)):
+        out = np.zeros(len(f), TRIANGLE)
+        out["v"], out["n"], out["uv"] = pos[f], nrm[f], uvs[f]
+        out["material"] = material
+        return out
+    alpha = np.asarray(mesh.alpha, np.float32)
+    c32 = np.float32(cutoff)
+    tris = []
+    for face in f:
+        # a corner: (position, normal, uv, alpha) with float32 components
+        corners = [(pos[i], nrm[i], uvs[i], alpha[i]) for i in face]
+        kept = _cut(corners, c32)
+        for k in range(1, len(kept) - 1):
+            tris.append((kept[0], kept[k], kept[k + 1]))
+    out = np.zeros(len(tris), TRIANGLE)
+    for i, corners in enumerate(tris):
+        out[i]["v"] = [c[0] for c in corners]
+        out[i]["n"] = [c[1] for c in corners]
+        out[i]["uv"] = [c[2] for c in corners]
     out["material"] = material
     return out
 
@@ -170,7 +207,7 @@ class Stage:
             key = (p.mesh, np.float32(p.alpha_cutoff).view(np.uint32).item(), p.material)
             if key not in dressed:  # one triangle list per (mesh, cutoff, material), as `dressed`
                 dressed[key] = len(meshes)
-                meshes.append(_triangles(self.meshes[p.mesh], p.material))
+                meshes.append(_triangles(self.meshes[p.mesh], p.material, p.alpha_cutoff))
             inst[i]["mesh"] = dressed[key]
             inst[i]["transform"] = np.asarray(p.model, np.float32).reshape(16)
             inst[i]["casts_shadow"] = 1 if p.casts_shadow else 0

@@ -107,3 +107,47 @@ def test_reference_refusals():
     with pytest.raises(TraceError, match="image-based skies"):
         Stage([ok], [], materials(), Sky(2, 1, np.array([[1, 1, 1, 1], [0, 0, 0, 1]], np.float32)), Sun(),
               cam).build()
+
+
+def unit_triangle(alpha):
+    """The triangle of stage.rs's own tests (stage.rs:865-880)."""
+    p = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    return Mesh(p, np.tile([0, 0, 1], (3, 1)).astype(np.float32), np.tile([1, 0, 0, 1], (3, 1)).astype(np.float32),
+                np.array([[0, 0], [1, 0], [0, 1]], np.float32), np.array([0, 1, 2], np.uint32),
+                alpha=None if alpha is None else np.asarray(alpha, np.float32))
+
+
+def area(tri):
+    a, b, c = tri["v"].astype(np.float64)
+    e1, e2 = b - a, c - a
+    return 0.5 * abs(e1[0] * e2[1] - e1[1] * e2[0])
+
+
+def unit_stage(alphas_and_cutoffs):
+    cam = synth.look_at((0, 0, 4), (0, 0, 0), 60, 1.0)
+    meshes = [unit_triangle(a) for a, _ in alphas_and_cutoffs]
+    placements = [Placement(i, synth.IDENTITY, 0, alpha_cutoff=c) for i, (_, c) in enumerate(alphas_and_cutoffs)]
+    return Stage(meshes, placements, materials(), Sky(1, 1, np.ones((1, 4), np.float32)), Sun(), cam).build()
+
+
+def test_alpha_below_the_cutoff_is_cut_away():
+    """alpha_below_the_cutoff_is_cut_where_the_live_renderer_discards
+    (stage.rs:910-933): kept triangle counts and areas, and uv = (x, y) at every
+    kept corner."""
+    cases = [([1.0, 1.0, 1.0], 1, 0.5), ([0.0, 0.0, 0.0], 0, 0.0), ([1.0, 0.0, 0.0], 1, 0.125),
+             ([1.0, 1.0, 0.0], 2, 0.375)]
+    for alpha, count, expected in cases:
+        s = unit_stage([(alpha, 0.5)])
+        kept = s.scene.meshes[0]
+        assert len(kept) == count, alpha
+        assert abs(sum(area(t) for t in kept) - expected) < 1e-6, alpha
+        for t in kept:
+            assert np.array_equal(t["v"][:, :2], t["uv"])
+
+
+def test_one_mesh_keeps_a_polygon_for_each_cutoff():
+    """one_mesh_keeps_a_polygon_for_each_cutoff (stage.rs:1161-1193): cutoffs
+    0.25, 0.9 and the default 0.5 of one mesh give areas 0.28125, 0.005, 0.125."""
+    s = unit_stage([([1.0, 0.0, 0.0], 0.25), ([1.0, 0.0, 0.0], 0.9), ([1.0, 0.0, 0.0], 0.5)])
+    areas = [sum(area(t) for t in m) for m in s.scene.meshes]
+    assert abs(areas[0] - 0.28125) < 1e-6 and abs(areas[1] - 0.005) < 1e-6 and abs(areas[2] - 0.125) < 1e-6
