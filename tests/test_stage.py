@@ -151,3 +151,40 @@ def test_one_mesh_keeps_a_polygon_for_each_cutoff():
     s = unit_stage([([1.0, 0.0, 0.0], 0.25), ([1.0, 0.0, 0.0], 0.9), ([1.0, 0.0, 0.0], 0.5)])
     areas = [sum(area(t) for t in m) for m in s.scene.meshes]
     assert abs(areas[0] - 0.28125) < 1e-6 and abs(areas[1] - 0.005) < 1e-6 and abs(areas[2] - 0.125) < 1e-6
+
+
+def test_instances_share_a_mesh_with_their_own_material_and_transform():
+    """instances_share_a_mesh_with_their_own_material_and_transform (stage.rs:889-908)."""
+    moved = np.eye(4, dtype=np.float32)
+    moved[3] = [2.0, 0.0, -1.0, 1.0]
+    cam = synth.look_at((0, 0, 4), (0, 0, 0), 60, 1.0)
+    s = Stage([unit_triangle(None)], [Placement(0, synth.IDENTITY, 1), Placement(0, moved, 0)], materials(),
+              Sky(1, 1, np.ones((1, 4), np.float32)), Sun(), cam).build()
+    assert len(s.scene.triangles) == 0 and len(s.scene.materials) == 3
+    meshes, inst = s.scene.meshes, s.scene.instances
+    assert meshes[inst[0]["mesh"]]["material"][0] == 1 and meshes[inst[1]["mesh"]]["material"][0] == 0
+    assert np.array_equal(meshes[inst[0]["mesh"]]["uv"][0], [[0, 0], [1, 0], [0, 1]])
+    m = inst[1]["transform"].reshape(4, 4)  # column-major: row k of this array is column k
+    v1 = meshes[inst[1]["mesh"]]["v"][0][1]
+    assert np.array_equal(m[:3, :3].T @ v1 + m[3, :3], [3.0, 0.0, -1.0])
+
+
+def test_a_cutoff_outside_zero_to_one_or_a_non_finite_clip_is_refused():
+    """a_cutoff_outside_zero_to_one_or_a_non_finite_clip_is_refused (stage.rs:1195-1244)."""
+    cam = synth.look_at((0, 0, 4), (0, 0, 0), 60, 1.0)
+    sky = Sky(1, 1, np.ones((1, 4), np.float32))
+    nan_clip = np.zeros((2, 4), np.float32)
+    nan_clip[0, 0] = np.nan
+    bad = [Placement(0, synth.IDENTITY, 0, alpha_cutoff=1.1), Placement(0, synth.IDENTITY, 0, alpha_cutoff=-0.01),
+           Placement(0, synth.IDENTITY, 0, alpha_cutoff=float("nan")),
+           Placement(0, synth.IDENTITY, 0, alpha_cutoff=float("inf")), Placement(0, synth.IDENTITY, 0, clip=nan_clip)]
+    for p in bad:
+        with pytest.raises(TraceError):
+            Stage([unit_triangle(None)], [p], materials(), sky, Sun(), cam).build()
+    for cutoff in (0.0, 1.0):
+        Stage([unit_triangle(None)], [Placement(0, synth.IDENTITY, 0, alpha_cutoff=cutoff)], materials(), sky, Sun(),
+              cam).build()
+    spare = unit_triangle(None)
+    spare.indices = np.array([0, 1, 3], np.uint32)
+    with pytest.raises(TraceError, match="outside the vertex buffer"):
+        Stage([unit_triangle(None), spare], [Placement(0, synth.IDENTITY, 0)], materials(), sky, Sun(), cam).build()
