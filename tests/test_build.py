@@ -199,3 +199,77 @@ def test_black_sky_cdf_is_uniform():
     assert len(rows) == 128 and len(cols) == 256 * 128
     assert np.array_equal(rows, (np.arange(128, dtype=np.float32) + 1) / np.float32(128))
     assert np.array_equal(cols[:256], (np.arange(256, dtype=np.float32) + 1) / np.float32(256))
+
+
+def test_two_levels_find_the_hits_of_the_flattened_triangles():
+    """two_levels_find_the_hits_of_the_flattened_triangles (levels.rs:591-680):
+    a world blob, one mesh placed twice, a mesh of its own and a copy of the
+    shared mesh's triangles: three bottom-level builds (the copy shares the
+    shared mesh's by geometry), 130 slots, and the two-level walk (the oracle's
+    restatement of scene()) finds the nearest hit that brute force over the
+    flattened, transformed triangles finds."""
+    from pfx_b200.trace import INSTANCE, TRIANGLE, Camera, make_rays
+
+    state = [29]
+
+    def random():
+        state[0] = (state[0] * 1664525 + 1013904223) & 0xFFFFFFFF
+        return np.float32(state[0] >> 8) / np.float32(1 << 24)
+
+    def blob(count):
+        v = np.zeros((count, 3, 3), np.float32)
+        for i in range(count):
+            x, y, z = (random() * np.float32(2) - np.float32(1) for _ in range(3))
+            v[i, 0] = (x, y, z)
+            v[i, 1] = (x + random() * np.float32(0.4) + np.float32(0.05), y, z)
+            v[i, 2] = (x, y + random() * np.float32(0.4) + np.float32(0.05), z + np.float32(0.1))
+        return synth.triangles(v, np.tile(np.array([0, 0, 1], np.float32), (count, 3, 1)))
+
+    shared = blob(60)
+    world = blob(30)
+    poses = [synth.placed((2.0, 0.0, 0.0), 0.3, 1.0), synth.placed((-2.0, 0.5, 1.0), -1.2, 0.7),
+             synth.placed((0.0, -2.0, -1.0), 2.0, 1.5), synth.placed((1.0, 1.5, -2.0), 2.5, 0.5)]
+    own = blob(40)
+    meshes = [shared, own, shared.copy()]
+    inst = np.zeros(4, INSTANCE)
+    inst["mesh"] = [0, 0, 1, 2]
+    inst["two_sided"] = 1
+    inst["casts_shadow"] = 1
+    inst["transform"] = np.stack([p.reshape(16) for p in poses])
+    cam = Camera((0.0, 0.0, 5.0), (0.0, 0.0, -1.0), (1.0, 0.0, 0.0), (0.0, 1.0, 0.0))
+    scene = SceneDesc(world, synth.material(), cam, meshes=meshes, instances=inst)
+    sb = SceneBuffers(scene, Settings())
+    assert sb.builds()[0] == 3
+    assert sb.buffers.triangle_count == 30 + 60 + 40
+
+    flat = [world["v"].astype(np.float64)]
+    for k, mesh in enumerate([shared, shared, own, shared]):
+        m = poses[k].astype(np.float64)  # column-major rows: point' = p @ M[:3,:3] + M[3,:3]
+        flat.append(mesh["v"].astype(np.float64) @ m[:3, :3] + m[3, :3])
+    tris = np.concatenate(flat)
+    origins, dirs = [], []
+    for _ in range(3000):
+        origins.append([random() * np.float32(10) - np.float32(5) for _ in range(3)])
+        d = np.array([random() * np.float32(2) - np.float32(1) for _ in range(3)], np.float32)
+        dirs.append(d / np.float32(np.sqrt(np.float32((d * d).sum()))))
+    o, d = np.array(origins, np.float32), np.array(dirs, np.float32)
+    got = oracle.trace(sb, make_rays(o, d, 1e20))
+
+    a, e1, e2 = tris[:, 0], tris[:, 1] - tris[:, 0], tris[:, 2] - tris[:, 0]
+    for i in range(len(o)):
+        pv = np.cross(d[i].astype(np.float64), e2)
+        det = (e1 * pv).sum(1)
+        ok = np.abs(det) > 1e-12
+        inv = np.where(ok, 1.0 / np.where(ok, det, 1.0), 0.0)
+        sv = o[i].astype(np.float64) - a
+        u = (sv * pv).sum(1) * inv
+        qv = np.cross(sv, e1)
+        v = (d[i].astype(np.float64) * qv).sum(1) * inv
+        t = (e2 * qv).sum(1) * inv
+        hit = ok & (u >= 0) & (u <= 1) & (v >= 0) & (u + v <= 1) & (t > 1e-4)
+        if not hit.any():
+            assert got["hit"][i] == 0, i
+            continue
+        brute = t[hit].min()
+        assert got["hit"][i] == 1, i
+        assert abs(float(got["t"][i]) - brute) <= 1e-4 * max(brute, 1.0), (i, got["t"][i], brute)
