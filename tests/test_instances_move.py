@@ -117,3 +117,24 @@ def test_a_move_keeps_the_emitter_list_a_fresh_build_would_shrink():
     assert kept.buffers.emitter_count == count
     assert np.frombuffer(kept.array("emitters")[:4].tobytes(), np.float32)[0] == count  # the header's count
     assert built(poses).buffers.emitter_count < count
+
+
+def test_pose_checks_of_the_reference():
+    """a_tiny_scaled_instance_keeps_its_normals_and_only_a_flat_one_is_refused
+    (detail.rs:653-688) and Pose::new's refusals (detail.rs:190-221), through
+    moving an instance of the stage: tiny rotations and scales are accepted,
+    flat, zero, non-affine and non-finite transforms are refused."""
+    kept = built(synth.staged_poses(False))
+    for s in (1e-2, 1e-4, 1e-6):
+        m = np.array([[s, 0, 0, 0], [0, 0, s, 0], [0, -s, 0, 0], [0, 0, 0, 1]], np.float32)
+        assert kept.move_instances([synth.IDENTITY, m])
+    flat = np.array([[1, 0, 0, 0], [1, 1e-9, 0, 0], [0, 0, 1, 0], [0, 0, 0, 1]], np.float32)
+    zero = flat.copy()
+    zero[1] = 0.0
+    skew = synth.IDENTITY.copy()
+    skew[0, 3] = 0.5
+    bad = synth.IDENTITY.copy()
+    bad[3, 0] = np.nan
+    for m, message in ((flat, "singular"), (zero, "singular"), (skew, "not affine"), (bad, "not finite")):
+        with pytest.raises(TraceError, match=message):
+            kept.move_instances([synth.IDENTITY, m])
