@@ -138,3 +138,24 @@ def test_pose_checks_of_the_reference():
     for m, message in ((flat, "singular"), (zero, "singular"), (skew, "not affine"), (bad, "not finite")):
         with pytest.raises(TraceError, match=message):
             kept.move_instances([synth.IDENTITY, m])
+
+
+def test_instance_records_transform_positions_and_normals():
+    """transforms_instance_positions_and_normals (detail.rs:692-717) read from the
+    instance's surface record: its forward rows take the origin to (3, 4, 5) and
+    its inverse rows take the normal (1, 1, 0) to x = 0.4472136 once normalised."""
+    from pfx_b200.trace import INSTANCE, TRIANGLE, Camera, SceneDesc, Settings
+    tri = np.zeros(1, TRIANGLE)
+    tri["v"] = [[0, 0, 0], [1, 0, 0], [0, 1, 0]]  # a non-empty triangle; vertex 0 at the origin
+    tri["n"] = [[1, 1, 0]] * 3
+    inst = np.zeros(1, INSTANCE)
+    inst["transform"] = np.array([[2, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 0], [3, 4, 5, 1]], np.float32).reshape(16)
+    inst["two_sided"], inst["casts_shadow"] = 1, 1
+    cam = Camera((0.0, 0.0, 5.0), (0.0, 0.0, -1.0), (1.0, 0.0, 0.0), (0.0, 1.0, 0.0))
+    sb = SceneBuffers(SceneDesc(np.zeros(0, TRIANGLE), synth.material(), cam, meshes=[tri], instances=inst),
+                      Settings())
+    rec = sb.array("surfaces").view(np.float32).reshape(-1, 44)[1]
+    forward, inverse = rec[20:32].reshape(3, 4), rec[32:44].reshape(3, 4)
+    assert np.array_equal(forward @ np.array([0, 0, 0, 1], np.float32), [3.0, 4.0, 5.0])
+    n = inverse[:, :3].T.astype(np.float64) @ np.array([1.0, 1.0, 0.0])
+    assert abs(n[0] / np.linalg.norm(n) - 0.4472136) < 1e-6
