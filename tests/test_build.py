@@ -273,3 +273,26 @@ def test_two_levels_find_the_hits_of_the_flattened_triangles():
         brute = t[hit].min()
         assert got["hit"][i] == 1, i
         assert abs(float(got["t"][i]) - brute) <= 1e-4 * max(brute, 1.0), (i, got["t"][i], brute)
+
+
+def test_an_empty_emitter_list_keeps_its_header():
+    """empty_list_keeps_its_header (lights.rs:510-516) through the scene packing:
+    two looped lights and no emissive triangle leave one header entry
+    (0 emitters, 2 looped lights) and no CDF."""
+    lights = np.concatenate([synth.point_light((0, 2, 0), 1.0), synth.point_light((1, 2, 0), 1.0)])
+    sb = SceneBuffers(scene_of(synth.quad((0, 0, 0), (1, 0, 0), (0, 0, 1)), lights), Settings())
+    e = sb.array("emitters").view(np.float32).reshape(-1, 16)
+    assert len(e) == 1 and list(e[0, :2]) == [0.0, 2.0]
+    assert len(sb.array("emitter_cdf")) == 0
+
+
+@pytest.mark.parametrize("emission, emits", [((0.0, 0.0, 1.0), True), ((0.0, 0.0, 0.0), False),
+                                             ((1.0, -0.5, 1.0), False), ((float("nan"), 1.0, 1.0), False)])
+def test_only_positive_emission_emits(emission, emits):
+    """only_positive_emission_emits (lights.rs:518-524): a triangle becomes an
+    emitter only when no channel of its emission is negative or NaN and some
+    channel is positive."""
+    tris = synth.quad((0, 0, 0), (1, 0, 0), (0, 0, 1), 0)
+    scene = SceneDesc(tris, synth.material(emission=emission), synth.look_at((0, 0, 10), (0, 0, 0), 45, 1.0))
+    sb = SceneBuffers(scene, Settings())
+    assert (sb.buffers.emitter_count == 2) == emits
