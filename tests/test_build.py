@@ -296,3 +296,19 @@ def test_only_positive_emission_emits(emission, emits):
     scene = SceneDesc(tris, synth.material(emission=emission), synth.look_at((0, 0, 10), (0, 0, 0), 45, 1.0))
     sb = SceneBuffers(scene, Settings())
     assert (sb.buffers.emitter_count == 2) == emits
+
+
+def test_a_uniform_sky_cdf_sums_to_one():
+    """cdf_sums_to_one (sky.rs:505-529) for the uniform skies this tracer takes:
+    every row and column mass is non-negative, the masses sum to one and the
+    last row CDF value is one."""
+    w = synth.staged(synth.staged_poses(False))  # sky (0.08, 0.09, 0.1)
+    sb = SceneBuffers(w.scene, w.settings)
+    rows, cols = sb.sky()
+    h, wdt = len(rows), len(cols) // len(rows)
+    row_mass = np.diff(np.concatenate([[0.0], rows.astype(np.float64)]))
+    col = cols.astype(np.float64).reshape(h, wdt)
+    col_mass = np.diff(np.concatenate([np.zeros((h, 1)), col], 1), axis=1)
+    assert np.all(row_mass >= -1e-5) and np.all(col_mass >= -1e-5)
+    assert abs((row_mass[:, None] * col_mass).sum() - 1.0) < 1e-4
+    assert abs(rows[-1] - 1.0) < 1e-6
