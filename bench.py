@@ -155,9 +155,11 @@ def workload(name: str):
 
 def config_of(w, args, extra=None):
     c = {"workload": f"{w.name}: {w.width}x{w.height}, {w.scene.world_triangle_count} triangles, "
-                     f"{len(w.scene.lights)} point/spot lights (light tree), 32 materials, depth "
-                     f"{w.settings.bounces[0]}, {w.settings.sampler} sampler",
-         "step": "one sampling pass (1 spp, every pixel)",
+                     f"{len(w.scene.lights)} point/spot lights (light tree), {len(w.scene.materials)} materials "
+                     f"(2 glass IOR 1.5, metals), depth {w.settings.bounces[0]}, {w.settings.sampler} sampler, "
+                     f"filter_glossy {w.settings.filter_glossy:g}, clamp_indirect {w.settings.clamp_indirect:g}; "
+                     f"fixed 1 spp per step, not adaptive",
+         "step": "one sampling pass (1 spp, every pixel; adaptive stopping off)",
          "l2": "flushed before every timed step (256 MiB write)",
          "parallelism": f"independent frames x{args.gpus} (no collective on the data path)"}
     if extra:

@@ -309,9 +309,10 @@ int pfxt_occluded_device(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count
  * counter and the 32-bit flag words) lives in fixed device arrays sized for
  * PFXT_NOALLOC_MAX_RAYS rays, which every GPU that loads the library holds until
  * exit; larger batches are refused with PFXT_ERR_INVALID.  All calls share the
- * arrays: calls whose GPU work overlaps race.  The first call on a device
- * resolves the arrays' addresses (the handle's device must be current) and
- * should come before any stream capture. */
+ * arrays: calls whose GPU work overlaps race.  The handle's device must be
+ * current.  CUDA loads a library's kernels and places its device arrays
+ * lazily, on first use; pfxt_create does that for this entry point on the
+ * handle's device, so its calls load and allocate nothing. */
 #define PFXT_NOALLOC_MAX_RAYS (1u << 20)
 int pfxt_occluded_noalloc(pfxt_trace* trace, const pfxt_ray* rays, uint32_t count, uint8_t* blocked,
                           void* stream);
@@ -480,6 +481,12 @@ int pfxt_cache_set_params(pfxt_cache* cache, const float* mlp, const float* tabl
 /* The encoding: per level the position scale and grid resolution, and a bit
  * mask of the levels indexed densely (the others are hashed). */
 int pfxt_cache_encoding(pfxt_cache* cache, float scales[16], uint32_t resolutions[16], uint32_t* dense);
+/* The cache's kernels wait for their tensor-core work on an mbarrier with a
+ * bounded number of polls (default 2^22).  A wait that runs out makes the
+ * call fail with PFXT_ERR_CUDA ("a tensor-core wait ran out of its limit")
+ * after the kernel has drained the work it issued; the cache stays usable.
+ * Sets that limit (0 makes every wait run out: a way to test the error path). */
+int pfxt_cache_set_wait_limit(pfxt_cache* cache, uint32_t polls);
 
 #ifdef __cplusplus
 }

@@ -208,6 +208,7 @@ PROTOTYPES = [
     ("pfxt_cache_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pfxt_cache_set_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pfxt_cache_encoding", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
+    ("pfxt_cache_set_wait_limit", C.c_int, [C.c_void_p, C.c_uint32]),
 ]
 NOALLOC_MAX_RAYS = 1 << 20
 

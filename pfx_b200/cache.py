@@ -133,6 +133,11 @@ class RadianceCache:
         check(self._lib.pfxt_cache_encoding(self._h, scales.ctypes.data, res.ctypes.data, C.byref(dense)))
         return scales, res, int(dense.value)
 
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls before a kernel's wait for its tensor-core work gives up (the
+        call then fails and the cache stays usable); 0 makes every wait give up."""
+        check(self._lib.pfxt_cache_set_wait_limit(self._h, int(polls)))
+
     def stats(self) -> dict:
         s = abi.CacheStats()
         check(self._lib.pfxt_cache_get_stats(self._h, C.byref(s)))

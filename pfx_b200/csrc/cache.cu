@@ -30,8 +30,15 @@ namespace pfxt {
 
 namespace {
 
-constexpr uint32_t WAIT_LIMIT = 1u << 22;  // mbarrier polls before a wait gives up
+// A wait for the tensor cores that runs out of CacheGrid::wait_limit polls sets
+// ERR_WAIT; the kernel then drains the MMAs it issued with a wait of DRAIN_LIMIT
+// polls (MMAs in flight finish on working hardware, in far less), and frees its
+// TMEM only once they have.  If even the drain wait runs out, ERR_DRAIN is set
+// and the TMEM stays allocated: freeing columns that an unfinished MMA still
+// writes could corrupt another CTA's accumulator without any sign.
+constexpr uint32_t DRAIN_LIMIT = 1u << 26;
 constexpr uint32_t ERR_WAIT = 1u;
+constexpr uint32_t ERR_DRAIN = 2u;
 
 // Shared memory of the inference kernel (bytes).
 // The second hidden layer's operand reuses the input tile (whose MMA has
@@ -201,15 +208,20 @@ __device__ __forceinline__ void copy_weights(uint8_t* sw, const uint16_t* __rest
 }
 
 // End of a tensor-core kernel: after a wait that ran out, flag the error and
-// give the MMAs in flight one more bounded wait before the TMEM is freed.
+// drain the MMAs in flight (the commit of phase `phase ^ 1`) before the TMEM
+// is freed; a drain that runs out too leaves the TMEM allocated.
 __device__ __forceinline__ void finish(bool failed, uint32_t mb, uint32_t phase, uint32_t* error, uint32_t tbase,
                                        uint32_t cols) {
+  bool drained = true;
   if (failed) {
     if (threadIdx.x == 0) atomicOr(error, ERR_WAIT);
-    umma::mbar_wait(mb, phase ^ 1u, WAIT_LIMIT);
+    drained = umma::mbar_wait(mb, phase ^ 1u, DRAIN_LIMIT);
+    if (!drained && threadIdx.x == 0) atomicOr(error, ERR_DRAIN);
   }
-  sync_tc();
-  if ((threadIdx.x >> 5) == 0) umma::tmem_free(tbase, cols);
+  umma::fence_before();
+  drained = __syncthreads_and(drained);
+  umma::fence_after();
+  if (drained && (threadIdx.x >> 5) == 0) umma::tmem_free(tbase, cols);
 }
 
 // Four TMEM loads of 16 columns: this thread's row, columns col..col+63.
@@ -263,7 +275,7 @@ __global__ void __launch_bounds__(128, 4)
         umma::mma(T0, umma::desc_k(a_x, 128, s), umma::desc_k(a_w + W_1, 64, s), ID_F64, s);
       umma::commit(mb);
     }
-    late = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    late = !umma::mbar_wait(mb, phase, g.wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(late)) break;
     umma::fence_after();
@@ -279,7 +291,7 @@ __global__ void __launch_bounds__(128, 4)
         umma::mma(T1, umma::desc_k(a_h1, 128, s), umma::desc_k(a_w + W_2, 64, s), ID_F64, s);
       umma::commit(mb);
     }
-    late = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    late = !umma::mbar_wait(mb, phase, g.wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(late)) break;
     umma::fence_after();
@@ -295,7 +307,7 @@ __global__ void __launch_bounds__(128, 4)
         umma::mma(T2, umma::desc_k(a_h2, 128, s), umma::desc_k(a_w + W_3, 16, s), ID_F16, s);
       umma::commit(mb);
     }
-    late = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    late = !umma::mbar_wait(mb, phase, g.wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(late)) break;
     umma::fence_after();
@@ -353,7 +365,7 @@ __global__ void __launch_bounds__(128, 1)
         umma::mma(T0, umma::desc_k(a_x, 128, s), umma::desc_k(a_w + W_1, 64, s), ID_F64, s);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(failed)) { failed = true; break; }
     umma::fence_after();
@@ -369,7 +381,7 @@ __global__ void __launch_bounds__(128, 1)
         umma::mma(T1, umma::desc_k(a_h1, 128, s), umma::desc_k(a_w + W_2, 64, s), ID_F64, s);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(failed)) { failed = true; break; }
     umma::fence_after();
@@ -385,7 +397,7 @@ __global__ void __launch_bounds__(128, 1)
         umma::mma(T2, umma::desc_k(a_h2, 128, s), umma::desc_k(a_w + W_3, 16, s), ID_F16, s);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(failed)) { failed = true; break; }
     umma::fence_after();
@@ -427,7 +439,7 @@ __global__ void __launch_bounds__(128, 1)
       umma::mma(T0, umma::desc_k(a_dy, 128, 0), umma::desc_mn(a_w + W_3, 16, 0), ID_B64, 0u);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(failed)) { failed = true; break; }
     umma::fence_after();
@@ -446,7 +458,7 @@ __global__ void __launch_bounds__(128, 1)
         umma::mma(T1, umma::desc_k(a_dh2, 128, s), umma::desc_mn(a_w + W_2, 64, s), ID_B64, s);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(failed)) { failed = true; break; }
     umma::fence_after();
@@ -465,7 +477,7 @@ __global__ void __launch_bounds__(128, 1)
         umma::mma(T2, umma::desc_k(a_dh1, 128, s), umma::desc_mn(a_w + W_1, 64, s), ID_B32, s);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, WAIT_LIMIT);
+    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(failed)) { failed = true; break; }
     umma::fence_after();
@@ -644,6 +656,7 @@ void cache_create(pfxt_cache& c, const pfxt_cache_settings& s) {
   const uint32_t T = 1u << s.log2_entries;
   c.grid.entries = T;
   c.grid.dense = 0;
+  c.grid.wait_limit = NRC_WAIT_LIMIT;
   double growth = std::exp(std::log((double)s.max_resolution / (double)s.base_resolution) / (double)(NRC_LEVELS - 1));
   for (uint32_t l = 0; l < NRC_LEVELS; ++l) {
     double scale = (double)s.base_resolution * std::pow(growth, (double)l) - 1.0;
@@ -737,6 +750,7 @@ CacheView cache_view(pfxt_cache& c) {
 void cache_infer_launch(pfxt_cache& c, const float4* queries, const uint32_t* n_dev, uint32_t n,
                         const uint32_t* scatter, float4* out, cudaStream_t stream, uint32_t ctas_per_sm) {
   if (n == 0) return;
+  if (c.broken) throw DeviceError("cache: unusable after an undrained tensor-core wait");
   uint32_t tiles = (n + NRC_ROWS - 1) / NRC_ROWS;
   ctas_per_sm = std::min<uint32_t>(std::max<uint32_t>(ctas_per_sm, 1u), 4u);
   uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)sm_count() * ctas_per_sm);
@@ -748,6 +762,7 @@ void cache_infer_launch(pfxt_cache& c, const float4* queries, const uint32_t* n_
 void cache_train_launch(pfxt_cache& c, const float4* records, const uint32_t* count_dev, uint32_t count,
                         uint32_t first, cudaStream_t stream, bool adam, uint32_t batch) {
   if (batch == 0) batch = c.s.batch;
+  if (c.broken) throw DeviceError("cache: unusable after an undrained tensor-core wait");
   const uint32_t table_n = NRC_LEVELS * c.grid.entries * 2u;
   k_step<<<1, 32, 0, stream>>>(count_dev, count, first + batch, c.d_step, beta_pow(c), c.s.beta1, c.s.beta2,
                                adam ? 1u : 0u, c.d_loss);
@@ -776,6 +791,10 @@ void cache_check_error(pfxt_cache& c) {
   check(cudaMemcpy(&e, c.d_error, 4, cudaMemcpyDeviceToHost), "cache error word");
   if (e != 0u) {
     cudaMemset(c.d_error, 0, 4);
+    if (e & ERR_DRAIN) {
+      c.broken = true;
+      throw DeviceError("cache: the tensor cores did not finish the MMAs in flight; the cache is unusable");
+    }
     throw DeviceError("cache: a tensor-core wait ran out of its limit");
   }
 }

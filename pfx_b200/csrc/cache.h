@@ -36,7 +36,10 @@ struct CacheGrid {
   uint32_t resolution[NRC_LEVELS];
   uint32_t dense;         // bit l: level l indexes densely
   uint32_t entries;       // table entries per level (power of two)
+  uint32_t wait_limit;    // mbarrier polls before a wait for the tensor cores gives up
 };
+
+constexpr uint32_t NRC_WAIT_LIMIT = 1u << 22;  // default of CacheGrid::wait_limit
 
 // Device views the tracer needs from an attached cache.
 struct CacheView {
@@ -74,6 +77,7 @@ struct pfxt_cache {
   uint64_t steps = 0;
   float last_loss = 0.0f;
   uint32_t last_records = 0, last_queries = 0, last_training_paths = 0;
+  bool broken = false;           // a drain wait ran out: TMEM may be held, nothing runs again
   std::mutex lock;
 };
 

@@ -197,6 +197,9 @@ int pfxt_create(const pfxt_buffers* b, const pfxt_scene* view, const pfxt_settin
     ensure_device();
     auto t = std::make_unique<pfxt_trace>();
     trace_init(*t, *b, *view, *settings, width, height);
+    // load pfxt_occluded_noalloc's module and kernels now, so that it never
+    // allocates on its own first call
+    check(noalloc_prepare(t->device), "loading the no-allocation kernels");
     *out = t.release();
   });
 }
@@ -827,6 +830,14 @@ char* cache_stage(pfxt_cache& c, size_t bytes) {
   return static_cast<char*>(c.d_stage);
 }
 }  // namespace
+
+int pfxt_cache_set_wait_limit(pfxt_cache* c, uint32_t polls) {
+  return guarded([&]() {
+    if (!c) throw Invalid("null argument");
+    std::lock_guard<std::mutex> g(c->lock);
+    c->grid.wait_limit = polls;
+  });
+}
 
 int pfxt_cache_infer(pfxt_cache* c, const pfxt_cache_query* q, uint32_t count, float* rgb) {
   return guarded([&]() {

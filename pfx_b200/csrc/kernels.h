@@ -14,6 +14,13 @@ cudaError_t launch_closest(const SceneView& s, const pfxt_ray* rays, uint32_t n,
 cudaError_t launch_any(const SceneView& s, const pfxt_ray* rays, uint32_t n, uint32_t* blocked, uint32_t* counter,
                        cudaStream_t stream);
 cudaError_t launch_pack_flags(const uint32_t* flags, uint8_t* bytes, uint32_t n, cudaStream_t stream);
+// Loads the any-hit and flag-packing kernels on the current device and computes
+// the any-hit kernel's persistent grid there (CUDA loads modules lazily, on a
+// kernel's first use, which can allocate device memory).
+cudaError_t prepare_any_queries();
+// The same for the no-allocation entry point's module (noalloc.cu): resolves its
+// scratch arrays on `device`, which must be current.
+cudaError_t noalloc_prepare(int device);
 cudaError_t launch_counts(const SceneView& s, const pfxt_ray* rays, uint32_t n, bool any, uint2* counts,
                           uint32_t* counter, cudaStream_t stream);
 

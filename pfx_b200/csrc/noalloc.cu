@@ -17,8 +17,13 @@
 //     streams, two threads) race; the counter is cleared on the stream at the
 //     start of each call, the flag words are fully rewritten for the rays of
 //     the call;
-//   * the first call on a device resolves the arrays' device addresses with
-//     that device current; make it before any stream capture.
+//   * pfxt_create resolves the arrays' device addresses and loads the
+//     kernels this entry point launches, with the handle's device current.
+//     CUDA loads modules lazily, and loading this file's module is what
+//     places the arrays in device memory, so after pfxt_create a call loads
+//     nothing and allocates nothing.  A call on a device no handle was created
+//     on does that set-up itself; make such a first call before any stream
+//     capture.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -64,6 +69,18 @@ cudaError_t resolve(int device, Resolved* out) {
 }
 
 }  // namespace
+
+namespace pfxt {
+
+cudaError_t noalloc_prepare(int device) {
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  Resolved r;
+  cudaError_t e = resolve(device, &r);
+  if (e == cudaSuccess) e = prepare_any_queries();
+  return e;
+}
+
+}  // namespace pfxt
 
 extern "C" int pfxt_occluded_noalloc(pfxt_trace* t, const pfxt_ray* rays, uint32_t count, uint8_t* blocked,
                                      void* stream) {

@@ -12,6 +12,8 @@
 // phase together.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "kernels.h"
 #include "traverse.cuh"
 
@@ -88,15 +90,24 @@ __global__ void k_pack(const uint32_t* __restrict__ in, uint8_t* __restrict__ ou
   if (i < n) out[i] = in[i] ? 1 : 0;
 }
 
+constexpr int kMaxDevices = 64;
+
+// Blocks of a persistent launch on the current device (SM count x resident
+// blocks), computed once per device.  Threads that race on a device's first
+// launch compute the same number, so the relaxed store is enough.
 template <int MODE>
 int persistent_blocks() {
-  static int blocks = 0;
+  static std::atomic<int> cached[kMaxDevices];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::atomic<int>* slot = (dev >= 0 && dev < kMaxDevices) ? &cached[dev] : nullptr;
+  int blocks = slot ? slot->load(std::memory_order_relaxed) : 0;
   if (blocks == 0) {
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
+    int sms = 0, per = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<MODE>, kThreads, 0);
-    blocks = sms * (per > 0 ? per : 1);
+    blocks = (sms > 0 ? sms : 1) * (per > 0 ? per : 1);
+    if (slot) slot->store(blocks, std::memory_order_relaxed);
   }
   return blocks;
 }
@@ -129,6 +140,14 @@ cudaError_t launch_any(const SceneView& s, const pfxt_ray* rays, uint32_t n, uin
 cudaError_t launch_counts(const SceneView& s, const pfxt_ray* rays, uint32_t n, bool any, uint2* counts,
                           uint32_t* counter, cudaStream_t stream) {
   return any ? launch<3>(s, rays, n, counts, counter, stream) : launch<2>(s, rays, n, counts, counter, stream);
+}
+
+cudaError_t prepare_any_queries() {
+  persistent_blocks<1>();
+  cudaFuncAttributes attr;
+  cudaError_t e = cudaFuncGetAttributes(&attr, k_trace<1>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&attr, k_pack);
+  return e;
 }
 
 cudaError_t launch_pack_flags(const uint32_t* flags, uint8_t* bytes, uint32_t n, cudaStream_t stream) {

@@ -12,8 +12,16 @@ from .trace import make_rays
 F32 = np.float32
 
 
-def geometric_normals(buffers, slots: np.ndarray, records: np.ndarray, instances=None) -> np.ndarray:
-    """World-space geometric normals of hit triangles (slot order records)."""
+def geometric_normals(buffers, slots: np.ndarray, records: np.ndarray, instances=None, hit=None) -> np.ndarray:
+    """World-space geometric normals of hit triangles (slot order records).
+    Rows where `hit` is false (missed rays, whose slot and record mean nothing)
+    get +z."""
+    if hit is not None:
+        out = np.zeros((len(slots), 3), F32)
+        out[:, 2] = 1.0
+        if hit.any():
+            out[hit] = geometric_normals(buffers, slots[hit], records[hit], instances)
+        return out
     tri = buffers.array("triangles").view(np.float32).reshape(-1, 24)[slots]
     a, b, c = tri[:, 0:3], tri[:, 4:7], tri[:, 8:11]
     n = np.cross(b - a, c - a)
@@ -51,8 +59,9 @@ def pass_mix(trace, scene, width, height, n: int, seed: int = 0):
     cam = pixel_rays(scene.camera, width, height, half, rng)
     hits = trace.trace_rays(cam)
     ok = hits["hit"] == 1
-    p = cam["origin"] + cam["direction"] * hits["t"][:, None]
-    nrm = geometric_normals(trace.scene_buffers, hits["slot"], hits["record"].astype(np.int64), scene.instances)
+    p = cam["origin"] + cam["direction"] * np.where(ok, hits["t"], F32(0.0))[:, None]
+    nrm = geometric_normals(trace.scene_buffers, hits["slot"], hits["record"].astype(np.int64), scene.instances,
+                            hit=ok)
     nrm = np.where((nrm * cam["direction"]).sum(1, keepdims=True) > 0, -nrm, nrm)
     origin = (p + nrm * F32(1e-3) * np.maximum(1.0, np.abs(p).max(1, keepdims=True))).astype(F32)
     # cosine-weighted bounce directions

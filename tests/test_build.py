@@ -43,6 +43,16 @@ def test_world_bvh_equals_the_oracle_build_on_the_sphere_scene():
     assert np.array_equal(sb.order(), order)
 
 
+def test_world_bvh_equals_the_oracle_build_on_the_full_4k_room():
+    # the bench's scene: 1.19 M world triangles, every node and slot
+    w = synth.room_4k()
+    assert len(w.scene.triangles) > 1_000_000
+    sb = SceneBuffers(w.scene, w.settings)
+    nodes, order = oracle.bvh_build(w.scene.triangles["v"])
+    assert np.array_equal(sb.array("nodes"), nodes)
+    assert np.array_equal(sb.order(), order)
+
+
 def test_two_level_layout():
     # levels.rs:393-470: top tree of 2g-1 nodes, g inverse-row nodes, then the
     # world BVH and one BVH per distinct mesh; instance leaves carry the mesh

@@ -130,3 +130,26 @@ def test_training_learns_a_radiance_field(gpu):
     after = held_out_error()
     assert losses[-1] < 0.2 * losses[0], (losses[0], losses[-1])
     assert after < 0.2 * before, (before, after)
+
+
+def test_a_wait_that_runs_out_is_reported_and_the_cache_stays_usable(gpu):
+    """A kernel's wait for its tensor-core work gives up after a bounded number
+    of polls; with the limit at 0 every wait gives up at once.  The call then
+    fails with the cache's error (after the kernel drained the MMAs it issued
+    and freed its tensor memory), and with the limit restored the same cache
+    gives the same answers as before."""
+    from pfx_b200.abi import TraceError
+    c, enc, mlp, table, rng = make(SMALL)
+    q = random_queries(512, rng, SMALL.lo, SMALL.hi)
+    r = records(rng, SMALL.batch, SMALL)
+    before = c.infer(q)
+    g_before = c.gradients(r[:512])[0]
+    c.set_wait_limit(0)
+    with pytest.raises(TraceError, match="ran out of its limit"):
+        c.infer(q)
+    with pytest.raises(TraceError, match="ran out of its limit"):
+        c.gradients(r[:512])
+    c.set_wait_limit(1 << 22)
+    assert np.array_equal(c.infer(q), before)
+    assert rel(c.gradients(r[:512])[0], g_before) < 1e-6
+    assert c.stats()["steps"] == 0

@@ -1,0 +1,58 @@
+"""Parity on the full-size workloads the bench measures, not reduced copies:
+the 4K room (1.19 M triangles, 300 meshes, 128 lights through the light tree)
+and the instanced scene at its full 200 k triangles.
+
+  * traversal on 2^18-ray batches with the mix of one pass (camera, bounce and
+    shadow rays): hit flag, slot, record and distance bit for bit against the
+    oracle's walk, the same box and triangle tests per ray, and the any-hit
+    flags (trace.wgsl:999-1168);
+  * images of a window of the full 4K frame (Trace::set_window keeps the
+    full-frame pixel coordinates, so the window's samples are the full
+    frame's): accumulation and films within 1e-4 relative, PCG and Sobol."""
+import numpy as np
+import pytest
+
+import oracle
+from pfx_b200 import rays as raymix
+from pfx_b200 import synth
+from pfx_b200.trace import Settings, Trace
+
+from test_gpu_render import render_both
+from test_gpu_traverse import compare_any, compare_closest, device_counts
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def room():
+    return synth.room_4k()
+
+
+@pytest.mark.parametrize("name", ["room_4k", "instanced_1080"])
+def test_traversal_on_the_full_scene(gpu, room, name):
+    w = room if name == "room_4k" else synth.instanced_1080()
+    assert w.scene.world_triangle_count > (1_000_000 if name == "room_4k" else 200_000)
+    trace = Trace(w.scene, w.settings, 64, 36)
+    closest, shadow = raymix.pass_mix(trace, w.scene, w.width, w.height, 1 << 18, seed=17)
+    got, counts = compare_closest(trace, closest)
+    assert got["hit"].mean() > 0.5
+    assert int(got["slot"][got["hit"] == 1].max()) > w.scene.world_triangle_count // 2
+    blocked = compare_any(trace, shadow)
+    assert 0.02 < blocked.mean() < 0.98
+    assert np.array_equal(device_counts(trace, closest, False), counts)
+    _, scounts, overflow = oracle.trace(trace.scene_buffers, shadow, any_hit=True, counts=True)
+    assert overflow == 0
+    assert np.array_equal(device_counts(trace, shadow, True), scounts)
+    # deep walks: the batch reaches far into the traversal stack
+    assert counts[:, 0].max() > 200
+    trace.close()
+
+
+@pytest.mark.parametrize("sampler", ["pcg", "sobol"])
+def test_image_of_a_window_of_the_full_4k_room(gpu, room, sampler):
+    w = synth.Workload(room.name, room.scene, Settings.deep(8, sampler=sampler, sobol_samples=64,
+                                                            filter_glossy=0.25, clamp_indirect=4.0), 96, 54)
+    # a window below the frame's centre: shelves, glass and metal spheres
+    got, exact = render_both(w, 2, [31, 32], window=((3840, 2160), (1700, 1300)))
+    assert got[..., :3].mean() > 0.0
+    assert exact > 0.99

@@ -22,9 +22,13 @@ def assert_close(got, want, what):
     return float(np.mean(got.view(np.uint32) == want.view(np.uint32)))
 
 
-def render_both(w, spp, seeds):
+def render_both(w, spp, seeds, window=None):
+    """Trace::sample passes of `w` on the GPU and in the oracle; `window` =
+    ((full width, full height), (x, y)) renders that tile of a larger frame."""
     trace = Trace(w.scene, w.settings, w.width, w.height)
     r = oracle.Renderer(trace.scene_buffers, w.settings)
+    if window is not None:
+        trace.set_window(*window)
     frame = trace.frame()
     accum = np.zeros((w.height, w.width, 12), np.float32)
     samples = 0
@@ -204,3 +208,37 @@ def test_paced_sampling_equals_one_call(gpu):
     assert len(seen) == 3 and stats.milliseconds == seen and all(m > 0.0 for m in seen)
     assert stats.wall_ms > 0.0 and paced.samples() == 3
     assert np.array_equal(paced.read_accum(), whole.read_accum())
+
+
+@pytest.mark.parametrize("sampler", ["pcg", "sobol"])
+def test_emissive_instances_through_the_emitter_list(gpu, sampler):
+    """An emissive panel placed as an instance, a dim sky and a sun
+    (crates/trace/tests/instances.rs:159-197): emitter_candidate,
+    find_emitter and emitter_weight (lights.wgsl:12-44, 103-144) against the
+    oracle, with and without world triangles beside the instances."""
+    for world in (False, True):
+        w = synth.staged(synth.staged_poses(False), size=(48, 32), world=world)
+        w.settings = Settings.deep(4, sampler=sampler, sobol_samples=16)
+        got, exact = render_both(w, 4, [2, 3])
+        assert got[..., :3].mean() > 0.0
+        assert exact > 0.99
+
+
+@pytest.mark.parametrize("sampler", ["pcg", "sobol"])
+def test_emissive_world_triangles_and_a_uniform_sky(gpu, sampler):
+    """Emissive world triangles (two of the spheres glow) beside the rect
+    lights, under a non-black uniform sky: the emitter CDF, the sky's CDF
+    sampling and the miss MIS weight (sky.rs:441-480, trace.wgsl:2228-2236)."""
+    w = synth.small("plain_512", (48, 40), sampler=sampler)
+    mats = w.scene.materials.copy()
+    mats["emission"][5] = (4.0, 3.0, 2.0)
+    mats["emission"][9] = (0.5, 2.0, 6.0)
+    w.scene.materials = mats
+    w.scene.sky = (0.3, 0.4, 0.5)
+    w.settings = Settings.deep(4, sampler=sampler, sobol_samples=16)
+    trace = Trace(w.scene, w.settings, w.width, w.height)
+    head = trace.scene_buffers.array("emitters").view(np.float32)[:4]
+    assert head[0] > 100  # the glowing spheres' triangles are in the emitter list
+    got, exact = render_both(w, 4, [4, 5])
+    assert got[..., :3].mean() > 0.0
+    assert exact > 0.99
