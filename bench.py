@@ -177,9 +177,8 @@ def run_reference(args):
     if rank != 0:
         return 0
     import oracle
-    from pfx_b200.trace import SceneBuffers
     w = workload(args.workload)
-    sb = SceneBuffers(w.scene, w.settings)
+    sb = oracle.scene_buffers(w.scene, w.settings)  # the oracle's own packing: no product code on this arm
     r = oracle.Renderer(sb, w.settings)
     ww, wh = 160, 90
     x0, y0 = (w.width - ww) // 2, (w.height - wh) // 2
@@ -200,10 +199,12 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": config_of(w, args, {"sample": f"{ww}x{wh} centre window of the 4K frame, 1 spp per step"}),
+        "config": config_of(w, args),
         "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
-                         "sample": f"{ww}x{wh} centre window, 1 spp per step, oracle path tracer on all host "
-                                   "threads (the reference's wgpu tracer is unavailable on this box)"},
+                         "sample": f"each step a {ww}x{wh} centre window of the {w.width}x{w.height} frame at 1 spp "
+                                   "(the same scene, settings and pixels' samples as the full frame), oracle path "
+                                   "tracer on its own scene packing, all host threads; the reference's wgpu tracer "
+                                   "is unavailable on this box"},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
     return 0
@@ -354,8 +355,7 @@ def traversal_roofline(trace, w, dev, stream, flush):
 def cpu_baseline(w, budget_s=12.0):
     """The oracle path tracer on a window of the same frame, all host threads."""
     import oracle
-    from pfx_b200.trace import SceneBuffers
-    sb = SceneBuffers(w.scene, w.settings)
+    sb = oracle.scene_buffers(w.scene, w.settings)
     r = oracle.Renderer(sb, w.settings)
     ww, wh = 160, 90
     x0, y0 = (w.width - ww) // 2, (w.height - wh) // 2

@@ -27,7 +27,8 @@ def lib() -> C.CDLL:
     global _lib
     if _lib is None:
         if not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime
-                                   for p in [HERE / "oracle.cpp", HERE / "render.cpp", HERE.parent / "pfx_b200/csrc/pfxt_math.h"]
+                                   for p in [HERE / "oracle.cpp", HERE / "render.cpp", HERE / "pack.cpp",
+                                             HERE.parent / "pfx_b200/csrc/pfxt_math.h"]
                                    if p.exists()):
             build()
         L = C.CDLL(str(LIB))
@@ -46,6 +47,11 @@ def lib() -> C.CDLL:
             "orc_falloff": (f32, [f32, f32, f32, f32]),
             "orc_check_div": (C.c_uint64, [C.c_uint64, C.c_uint64]),
             "orc_math": (None, [C.c_int, vp, vp, vp, C.c_uint64]),
+            "orc_scene_build": (vp, [vp]),
+            "orc_scene_free": (None, [vp]),
+            "orc_scene_blob": (C.c_uint64, [vp, C.c_int, C.POINTER(C.c_void_p)]),
+            "orc_scene_counts": (None, [vp, vp]),
+            "orc_select_nth": (None, [vp, u32, u32, C.c_int32, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -57,6 +63,101 @@ def lib() -> C.CDLL:
 
 def _p(a: np.ndarray) -> int:
     return a.ctypes.data
+
+
+class _InMesh(C.Structure):
+    _fields_ = [("tris", C.c_void_p), ("count", C.c_uint32)]
+
+
+class _InScene(C.Structure):
+    _fields_ = [("world", C.c_void_p), ("world_count", C.c_uint32), ("meshes", C.c_void_p),
+                ("mesh_count", C.c_uint32), ("instances", C.c_void_p), ("instance_count", C.c_uint32),
+                ("materials", C.c_void_p), ("material_count", C.c_uint32), ("lights", C.c_void_p),
+                ("light_count", C.c_uint32), ("sky", C.c_float * 3), ("sky_width", C.c_uint32),
+                ("sky_height", C.c_uint32), ("sobol", C.c_uint32), ("sobol_samples", C.c_uint32)]
+
+
+class _Counts:
+    pass
+
+
+class OracleBuffers:
+    """The oracle's own SceneBuffers::build (oracle/pack.cpp, a restatement of
+    gpu.rs:566-1061, tree.rs, levels.rs, lights.rs, record.rs and sky.rs) for a
+    scene description (a pfx_b200.trace.SceneDesc: its input arrays only).
+    Offers the blob accessors the oracle's tracer reads (array, order, sky,
+    sobol and the counts in .buffers), so the oracle can trace without any
+    buffer the product made."""
+
+    NAMES = {"nodes": 0, "triangles": 1, "uv": 2, "surfaces": 3, "materials": 4, "emitters": 5, "emitter_cdf": 6,
+             "lights": 7}
+
+    def __init__(self, scene, settings):
+        world = np.ascontiguousarray(scene.triangles)
+        meshes = [np.ascontiguousarray(m) for m in scene.meshes]
+        inst = np.ascontiguousarray(scene.instances)
+        mats = np.ascontiguousarray(scene.materials)
+        lights = np.ascontiguousarray(scene.lights)
+        for a, size in ((world, 100), (inst, 80), (mats, 112), (lights, 100)):
+            assert a.dtype.itemsize == size, "input layout"
+        mesh_arr = (_InMesh * max(1, len(meshes)))()
+        for i, m in enumerate(meshes):
+            mesh_arr[i].tris, mesh_arr[i].count = (_p(m) if len(m) else None), len(m)
+        s = _InScene()
+        s.world, s.world_count = (_p(world) if len(world) else None), len(world)
+        s.meshes, s.mesh_count = C.cast(mesh_arr, C.c_void_p), len(meshes)
+        s.instances, s.instance_count = (_p(inst) if len(inst) else None), len(inst)
+        s.materials, s.material_count = _p(mats), len(mats)
+        s.lights, s.light_count = (_p(lights) if len(lights) else None), len(lights)
+        s.sky = (C.c_float * 3)(*scene.sky)
+        s.sky_width, s.sky_height = scene.sky_width, scene.sky_height
+        s.sobol = 1 if settings.sampler == "sobol" else 0
+        s.sobol_samples = settings.sobol_samples
+        h = lib().orc_scene_build(C.byref(s))
+        try:
+            self._blobs = {}
+            for name, which in list(self.NAMES.items()) + [("order", 8), ("sky_rows", 9), ("sky_columns", 10),
+                                                           ("sobol", 11)]:
+                ptr = C.c_void_p()
+                n = lib().orc_scene_blob(h, which, C.byref(ptr))
+                self._blobs[name] = (np.ctypeslib.as_array((C.c_uint8 * n).from_address(ptr.value)).copy()
+                                     if n else np.zeros(0, np.uint8))
+            counts = np.zeros(7, np.uint32)
+            lib().orc_scene_counts(h, _p(counts))
+        finally:
+            lib().orc_scene_free(h)
+        b = _Counts()
+        (b.triangle_count, b.emitter_count, b.light_count, b.sky_width, b.sky_height, b.sobol_length,
+         b.bottom_builds) = (int(x) for x in counts)
+        b.sky_radiance = tuple(float(x) for x in scene.sky)
+        b.sky_sun_probability = 0.0
+        self.buffers = b
+
+    def array(self, name: str) -> np.ndarray:
+        return self._blobs[name].copy()
+
+    def order(self) -> np.ndarray:
+        return self._blobs["order"].view(np.uint32).copy()
+
+    def sky(self):
+        return self._blobs["sky_rows"].view(np.float32).copy(), self._blobs["sky_columns"].view(np.float32).copy()
+
+    def sobol(self) -> np.ndarray:
+        return self._blobs["sobol"].view(np.float32).reshape(-1, 4).copy()
+
+
+def select_nth(keys, index: int, rounds: int = 16) -> np.ndarray:
+    """Rust's select_nth_unstable_by(index, f32::total_cmp) as the light tree
+    runs it: the original positions of `keys` in the order it leaves them."""
+    k = np.ascontiguousarray(keys, np.float32)
+    out = np.zeros(len(k), np.uint32)
+    lib().orc_select_nth(_p(k), len(k), index, rounds, _p(out))
+    return out
+
+
+def scene_buffers(scene, settings) -> OracleBuffers:
+    """The oracle's own packed buffers of `scene` (see OracleBuffers)."""
+    return OracleBuffers(scene, settings)
 
 
 def bvh_build(vertices: np.ndarray):

@@ -21,6 +21,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cfloat>
+#include <climits>
 #include <atomic>
 #include <thread>
 #include <vector>
@@ -729,5 +731,7 @@ void orc_math(int fn, const float* x, const float* y, float* out, uint64_t n) {
 }
 }  // extern "C"
 
-// The path integrator restatement shares this translation unit.
+// The path integrator restatement and the scene packing share this
+// translation unit.
 #include "render.cpp"
+#include "pack.cpp"

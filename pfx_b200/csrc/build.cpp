@@ -672,11 +672,221 @@ bool should_split(const std::vector<TreeEmitter>& em, size_t lo, size_t hi, Meas
   return min_cost < total_cost || count > TREE_LEAF;
 }
 
-// The reference partitions with Rust's select_nth_unstable_by on the split
-// axis; the within-side order that produces is specific to the Rust standard
-// library.  This builder partitions with a stable sort by (centroid, light
-// index), which puts the same set of lights on each side whenever the split
-// axis has no ties at the median, and keeps the order deterministic.
+// f32::total_cmp as a signed-integer key: -0 < +0, NaNs at the ends.
+inline int32_t total_order_key(float f) {
+  int32_t i;
+  memcpy(&i, &f, 4);
+  return i ^ (int32_t)(((uint32_t)(i >> 31)) >> 1);
+}
+
+// ------------------------------------------------- Rust's select_nth_unstable
+// The reference splits a light-tree node with slice::select_nth_unstable_by
+// (tree.rs:281).  The order it leaves on each side is the leaf's light order
+// (which tree_leaf's reservoir walk consumes) and the order the next split
+// sums its buckets in, so the exact permutation is part of the tree's bytes.
+// Restated from the selection algorithm of Rust's core library (core::slice::
+// select, Rust 1.81 and later): introselect over the partition of ipnsort
+// (Bergdoll and Peters): at most 16 rounds of median-of-3 (a recursive
+// pseudo-median from 64 elements) pivots and branchless cyclic Lomuto
+// partitions, insertion sort from 16 elements down, Alexandrescu's median of
+// medians with ninthers after 16 rounds, and the min/max shortcuts for the
+// first and last index.  `less` is a strict weak order.
+template <class T, class Less>
+struct RustSelect {
+  Less less;
+  int rounds = 16;  // partition rounds before the deterministic fallback
+
+  static constexpr size_t SMALL = 16;            // insertion sort at or below
+  static constexpr size_t PSEUDO_MEDIAN = 64;    // recursive pivot choice from here
+
+  void insertion_sort(T* v, size_t n) {
+    for (size_t i = 1; i < n; ++i) {
+      if (!less(v[i], v[i - 1])) continue;
+      T tail = v[i];
+      size_t j = i;
+      do {
+        v[j] = v[j - 1];
+        --j;
+      } while (j > 0 && less(tail, v[j - 1]));
+      v[j] = tail;
+    }
+  }
+  size_t median3(const T* v, size_t a, size_t b, size_t c) {
+    bool x = less(v[a], v[b]), y = less(v[a], v[c]);
+    if (x == y) return (less(v[b], v[c]) != x) ? c : b;
+    return a;
+  }
+  size_t median3_rec(const T* v, size_t a, size_t b, size_t c, size_t n) {
+    if (n * 8 >= PSEUDO_MEDIAN) {
+      size_t n8 = n / 8;
+      a = median3_rec(v, a, a + n8 * 4, a + n8 * 7, n8);
+      b = median3_rec(v, b, b + n8 * 4, b + n8 * 7, n8);
+      c = median3_rec(v, c, c + n8 * 4, c + n8 * 7, n8);
+    }
+    return median3(v, a, b, c);
+  }
+  size_t choose_pivot(const T* v, size_t n) {  // n >= 8
+    size_t n8 = n / 8;
+    if (n < PSEUDO_MEDIAN) return median3(v, 0, n8 * 4, n8 * 7);
+    return median3_rec(v, 0, n8 * 4, n8 * 7, n8);
+  }
+  // Branchless cyclic Lomuto partition of w[0, m) around `pivot`: the first
+  // element is lifted out, every later one is written to the front when it
+  // is less, and the lifted one is placed last.  Returns the count of less.
+  template <class L>
+  size_t lomuto_cyclic(T* w, size_t m, const T& pivot, L& lt) {
+    if (m == 0) return 0;
+    T lifted = w[0];
+    size_t gap = 0, num_lt = 0;
+    for (size_t right = 1; right < m; ++right) {
+      T r = w[right];
+      bool is_lt = lt(r, pivot);
+      w[gap] = w[num_lt];
+      w[num_lt] = r;
+      gap = right;
+      num_lt += is_lt ? 1 : 0;
+    }
+    bool is_lt = lt(lifted, pivot);
+    w[gap] = w[num_lt];
+    w[num_lt] = lifted;
+    return num_lt + (is_lt ? 1 : 0);
+  }
+  // Pivot to the front, partition the rest, pivot between the two sides.
+  template <class L>
+  size_t partition(T* v, size_t n, size_t pivot, L& lt) {
+    std::swap(v[0], v[pivot]);
+    const T p = v[0];
+    size_t num_lt = lomuto_cyclic(v + 1, n - 1, p, lt);
+    std::swap(v[0], v[num_lt]);
+    return num_lt;
+  }
+  size_t min_index(const T* v, size_t n) {
+    size_t best = 0;
+    for (size_t i = 1; i < n; ++i)
+      if (less(v[i], v[best])) best = i;
+    return best;
+  }
+  size_t max_index(const T* v, size_t n) {
+    size_t best = 0;
+    for (size_t i = 1; i < n; ++i)
+      if (less(v[best], v[i])) best = i;
+    return best;
+  }
+  size_t median_idx(const T* v, size_t a, size_t b, size_t c) {
+    if (less(v[c], v[a])) std::swap(a, c);
+    if (less(v[c], v[b])) return c;
+    if (less(v[b], v[a])) return a;
+    return b;
+  }
+  void ninther(T* v, size_t a, size_t b, size_t c, size_t d, size_t e, size_t f, size_t g, size_t h, size_t i) {
+    b = median_idx(v, a, b, c);
+    h = median_idx(v, g, h, i);
+    if (less(v[h], v[b])) std::swap(b, h);
+    if (less(v[f], v[d])) std::swap(d, f);
+    if (less(v[e], v[d])) {
+      // d stays
+    } else if (less(v[f], v[e])) {
+      d = f;
+    } else {
+      if (less(v[e], v[b]))
+        std::swap(v[e], v[b]);
+      else if (less(v[h], v[e]))
+        std::swap(v[e], v[h]);
+      return;
+    }
+    if (less(v[d], v[b]))
+      d = b;
+    else if (less(v[h], v[d]))
+      d = h;
+    std::swap(v[d], v[e]);
+  }
+  size_t median_of_ninthers(T* v, size_t n) {
+    size_t frac = n <= 1024 ? n / 12 : (n <= 128 * 1024 ? n / 64 : n / 1024);
+    size_t pivot = frac / 2;
+    size_t lo = n / 2 - pivot, hi = frac + lo;
+    size_t gap = (n - 9 * frac) / 4;
+    size_t a = lo - 4 * frac - gap, b = hi + gap;
+    for (size_t i = lo; i < hi; ++i, a += 3, b += 3) ninther(v, a, i - frac, b, a + 1, i, b + 1, a + 2, i + frac, b + 2);
+    median_of_medians(v + lo, frac, pivot);
+    return partition(v, n, lo + pivot, less);
+  }
+  void median_of_medians(T* v, size_t n, size_t k) {
+    for (;;) {
+      if (n <= SMALL) {
+        if (n >= 2) insertion_sort(v, n);
+        return;
+      }
+      if (k == n - 1) {
+        std::swap(v[max_index(v, n)], v[k]);
+        return;
+      }
+      if (k == 0) {
+        std::swap(v[min_index(v, n)], v[0]);
+        return;
+      }
+      size_t p = median_of_ninthers(v, n);
+      if (p == k) return;
+      if (p > k) {
+        n = p;
+      } else {
+        v += p + 1;
+        n -= p + 1;
+        k -= p + 1;
+      }
+    }
+  }
+  void select_loop(T* v, size_t n, size_t index) {
+    int limit = rounds;
+    bool has_ancestor = false;
+    T ancestor{};
+    for (;;) {
+      if (n <= SMALL) {
+        if (n >= 2) insertion_sort(v, n);
+        return;
+      }
+      if (limit == 0) {
+        median_of_medians(v, n, index);
+        return;
+      }
+      --limit;
+      size_t pivot = choose_pivot(v, n);
+      // A pivot equal to the left neighbour's (the previous round's) is the
+      // smallest value here: split off everything equal to it instead.
+      if (has_ancestor && !less(ancestor, v[pivot])) {
+        auto not_greater = [this](const T& a, const T& b) { return !less(b, a); };
+        size_t mid = partition(v, n, pivot, not_greater) + 1;
+        if (mid > index) return;
+        v += mid;
+        n -= mid;
+        index -= mid;
+        has_ancestor = false;
+        continue;
+      }
+      size_t mid = partition(v, n, pivot, less);
+      if (mid < index) {
+        ancestor = v[mid];
+        has_ancestor = true;
+        v += mid + 1;
+        n -= mid + 1;
+        index -= mid + 1;
+      } else if (mid > index) {
+        n = mid;
+      } else {
+        return;
+      }
+    }
+  }
+  void select_nth(T* v, size_t n, size_t index) {
+    if (index >= n) throw Invalid("select_nth: index out of range");
+    if (index == n - 1)
+      std::swap(v[max_index(v, n)], v[index]);
+    else if (index == 0)
+      std::swap(v[min_index(v, n)], v[0]);
+    else
+      select_loop(v, n, index);
+  }
+};
+
 void grow(std::vector<TreeEmitter>& em, size_t lo, size_t hi, size_t start, size_t base, size_t root,
           std::vector<GpuLight>& nodes) {  // tree.rs:263-293
   size_t at = nodes.size();
@@ -687,12 +897,11 @@ void grow(std::vector<TreeEmitter>& em, size_t lo, size_t hi, size_t start, size
   bool split = should_split(em, lo, hi, &measure, &middle, &dim);
   if (split) {
     if (dim >= 0) {
-      std::stable_sort(em.begin() + lo, em.begin() + hi, [dim](const TreeEmitter& l, const TreeEmitter& r) {
-        float a = l.centroid[dim], b = r.centroid[dim];
-        if (a < b) return true;
-        if (b < a) return false;
-        return l.index < r.index;
-      });
+      auto by_axis = [dim](const TreeEmitter& l, const TreeEmitter& r) {
+        return total_order_key(l.centroid[dim]) < total_order_key(r.centroid[dim]);
+      };
+      RustSelect<TreeEmitter, decltype(by_axis)> select{by_axis};
+      select.select_nth(em.data() + lo, hi - lo, middle);
     }
     grow(em, lo, lo + middle, start, base, root, nodes);
     size_t right_at = root + nodes.size();
@@ -745,7 +954,9 @@ void build_emitters(const std::vector<Candidate>& cands, size_t lights, size_t t
                     std::vector<float>& cdf) {  // lights.rs:391-440
   std::vector<double> powers;
   for (auto& c : cands) powers.push_back((double)triangle_area(c.vertices) * (double)luminance(c.emission));
-  double total = 0.0;
+  // Rust's f64 Iterator::sum starts from -0.0 (the additive identity): an
+  // empty list's total is -0.0
+  double total = -0.0;
   for (double p : powers) total += p;
   entries.clear();
   cdf.clear();
@@ -1201,9 +1412,13 @@ SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings) 
     for (size_t j = 0; j < mesh.triangles.size(); ++j) put(mesh.first + j, mesh.triangles[j]);
 
   // ---- instance surface records (gpu.rs:782-805)
+  // GpuSurface::of over InstanceSurface::default (gpu.rs:40-88, detail.rs:123-138):
+  // uv offset 0, uv scale 1, crop [0, 0, 1, 1]
   GpuSurface world_surface{};
   world_surface.transform[2] = 1.0f;
   world_surface.transform[3] = 1.0f;
+  world_surface.crop[2] = 1.0f;
+  world_surface.crop[3] = 1.0f;
   world_surface.info[0] = 0;
   world_surface.info[1] = NO_MATERIAL;
   world_surface.info[2] = 0;
@@ -1316,6 +1531,24 @@ SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings) 
   out->emitter_count = (uint32_t)cands.size();
   out->max_depth = out->nodes.empty() ? 0 : std::max<uint32_t>(1u, stack_need(out->nodes, 0, 0));
   return out.release();
+}
+
+// The light tree's selection on its own, for tests: sorts (key, index) pairs
+// as select_nth_unstable_by(index, total_cmp on the key) leaves them and
+// writes the original indices in their final order.  `rounds` < 16 reaches
+// the deterministic fallback sooner.
+void select_nth_for_test(const float* keys, uint32_t n, uint32_t index, int rounds, uint32_t* order) {
+  struct Item {
+    float key;
+    uint32_t at;
+  };
+  std::vector<Item> v(n);
+  for (uint32_t i = 0; i < n; ++i) v[i] = Item{keys[i], i};
+  auto by_key = [](const Item& a, const Item& b) { return total_order_key(a.key) < total_order_key(b.key); };
+  RustSelect<Item, decltype(by_key)> select{by_key};
+  select.rounds = rounds;
+  select.select_nth(v.data(), n, index);
+  for (uint32_t i = 0; i < n; ++i) order[i] = v[i].at;
 }
 
 // Trace::move_instances (gpu.rs:2433-2530).  Every transform is checked first;

@@ -419,6 +419,17 @@ int pfxt_debug_graphs(pfxt_trace* t, uint32_t on) {
   });
 }
 
+/* The light tree's selection (slice::select_nth_unstable_by with total_cmp)
+ * on `n` keys: writes the keys' original indices in the order it leaves them.
+ * `rounds` (16 as the tree runs it) caps the partition rounds before the
+ * deterministic fallback. */
+int pfxt_debug_select_nth(const float* keys, uint32_t n, uint32_t index, int32_t rounds, uint32_t* order) {
+  return guarded([&]() {
+    if (!keys || !order || index >= n) throw Invalid("select: index out of range");
+    select_nth_for_test(keys, n, index, rounds, order);
+  });
+}
+
 /* How many sampling passes have been captured as graphs so far. */
 uint32_t pfxt_debug_graph_captures(pfxt_trace* t) { return t ? t->graph_captures : 0u; }
 

@@ -58,6 +58,9 @@ SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings);
 // place (no buffer changes size) and returns whether anything moved.
 bool move_instances(SceneBlobs& blobs, const float* transforms, size_t count);
 
+// slice::select_nth_unstable_by as the light tree runs it, on bare keys (tests).
+void select_nth_for_test(const float* keys, uint32_t n, uint32_t index, int rounds, uint32_t* order);
+
 // Thread-local last error of the C ABI.
 void set_error(const std::string& message);
 

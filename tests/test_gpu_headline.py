@@ -33,14 +33,15 @@ def test_traversal_on_the_full_scene(gpu, room, name):
     w = room if name == "room_4k" else synth.instanced_1080()
     assert w.scene.world_triangle_count > (1_000_000 if name == "room_4k" else 200_000)
     trace = Trace(w.scene, w.settings, 64, 36)
+    ref = oracle.scene_buffers(w.scene, w.settings)
     closest, shadow = raymix.pass_mix(trace, w.scene, w.width, w.height, 1 << 18, seed=17)
-    got, counts = compare_closest(trace, closest)
+    got, counts = compare_closest(trace, closest, ref)
     assert got["hit"].mean() > 0.5
     assert int(got["slot"][got["hit"] == 1].max()) > w.scene.world_triangle_count // 2
-    blocked = compare_any(trace, shadow)
+    blocked = compare_any(trace, shadow, ref)
     assert 0.02 < blocked.mean() < 0.98
     assert np.array_equal(device_counts(trace, closest, False), counts)
-    _, scounts, overflow = oracle.trace(trace.scene_buffers, shadow, any_hit=True, counts=True)
+    _, scounts, overflow = oracle.trace(ref, shadow, any_hit=True, counts=True)
     assert overflow == 0
     assert np.array_equal(device_counts(trace, shadow, True), scounts)
     # deep walks: the batch reaches far into the traversal stack

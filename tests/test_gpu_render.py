@@ -2,6 +2,8 @@
 with the reference's random sequence reproduced (PCG and Sobol), every pixel of
 the accumulation and of the films must match within 1e-4 relative in FP32 (the
 tolerance of the parity contract); in practice the images are bit-identical.
+The oracle renders from its own packing of the scene (oracle.scene_buffers),
+never from the buffers the product built.
 Also the reference's furnace and determinism pins, and adaptive sampling
 rounds against the oracle."""
 import numpy as np
@@ -26,7 +28,7 @@ def render_both(w, spp, seeds, window=None):
     """Trace::sample passes of `w` on the GPU and in the oracle; `window` =
     ((full width, full height), (x, y)) renders that tile of a larger frame."""
     trace = Trace(w.scene, w.settings, w.width, w.height)
-    r = oracle.Renderer(trace.scene_buffers, w.settings)
+    r = oracle.Renderer(oracle.scene_buffers(w.scene, w.settings), w.settings)
     if window is not None:
         trace.set_window(*window)
     frame = trace.frame()
@@ -186,7 +188,7 @@ def test_adaptive_rounds_match_the_oracle(gpu):
     adaptive = Adaptive(threshold=0.05, min_samples=8, max_samples=32, growth=1.5)
     trace = Trace(w.scene, w.settings, w.width, w.height)
     conv = trace.sample_adaptive(adaptive, 11)
-    r = oracle.Renderer(trace.scene_buffers, w.settings)
+    r = oracle.Renderer(oracle.scene_buffers(w.scene, w.settings), w.settings)
     rounds, accum, _ = r.sample_adaptive(trace.frame(), w.width, w.height, adaptive, 11)
     assert [(x.samples, x.active) for x in conv.rounds] == rounds
     got = trace.read_accum()
