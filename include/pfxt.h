@@ -273,6 +273,27 @@ typedef struct pfxt_keeper {
  * pfxt_sample_adaptive's. */
 int pfxt_sample_adaptive_kept(pfxt_trace* trace, const pfxt_adaptive* adaptive, uint32_t seed, const char* key,
                               const pfxt_keeper* keeper, pfxt_round* rounds, uint32_t cap, uint32_t* written);
+/* One adaptive round in its two steps, measure then mark (converge.wgsl:9-51,
+ * run by adaptive.rs:282-307 after every round), for a frame whose 8-row
+ * strips are shared between several tracers (one per GPU, each sampling its
+ * own strips through pfxt_set_pixel_mask).  Between the two steps the caller
+ * writes into the snapshots the errors of the rows next to its strips that
+ * other tracers own (a one-row halo per strip edge), so mark's 3x3 maximum
+ * sees what a single tracer of the whole frame sees.  pfxt_adaptive_measure
+ * with `first` nonzero clears the snapshots (a new adaptive render);
+ * pfxt_adaptive_mark stops converged pixels and returns this tracer's running
+ * count; the frame's count is the sum over tracers. */
+int pfxt_adaptive_measure(pfxt_trace* trace, uint32_t first);
+int pfxt_adaptive_mark(pfxt_trace* trace, uint32_t min_samples, float threshold, uint32_t* running);
+/* The snapshots in device memory: width*height records of 8 floats (mean rgb,
+ * mean coverage, samples, error, 0, 0), the error at float 5 of a record.
+ * Valid until pfxt_destroy. */
+int pfxt_adaptive_snaps_device(pfxt_trace* trace, float** snaps);
+/* Sample only the pixels whose mask byte (width*height host bytes) is
+ * non-zero, or every pixel with NULL; restarts the accumulation.  A pixel's
+ * samples depend only on the pixel, the sample index and the seed
+ * (trace.wgsl:2503-2579), so a masked pixel's value equals the whole frame's. */
+int pfxt_set_pixel_mask(pfxt_trace* trace, const uint8_t* mask);
 /* Adaptive::rounds (adaptive.rs:46-63). */
 int pfxt_adaptive_rounds(const pfxt_adaptive* adaptive, uint32_t* rounds, uint32_t cap,
                          uint32_t* written);

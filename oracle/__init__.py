@@ -319,16 +319,24 @@ class Renderer:
         s.clamp_indirect, s.filter_glossy = settings.clamp_indirect, settings.filter_glossy
         self.scene = s
 
-    def render(self, frame: np.ndarray, accum: np.ndarray, accumulated: int, count: int, seed: int):
+    def render(self, frame: np.ndarray, accum: np.ndarray, accumulated: int, count: int, seed: int, mask=None):
         """One Trace::sample(count, seed) pass on `accum` (H, W, 12 floats,
-        updated in place); returns (color, albedo, normal) films."""
+        updated in place); returns (color, albedo, normal) films.  With `mask`
+        (H, W bools) only those pixels are reset and sampled."""
         f = np.array(frame, np.uint32).copy()
         f[2], f[3], f[6] = accumulated, count, seed
         h, w = accum.shape[:2]
         color = np.zeros((h, w, 4), np.float32)
         albedo = np.zeros_like(color)
         normal = np.zeros_like(color)
-        lib().orc_render(C.byref(self.scene), _p(f), _p(accum), _p(color), _p(albedo), _p(normal))
+        if mask is None:
+            lib().orc_render(C.byref(self.scene), _p(f), _p(accum), _p(color), _p(albedo), _p(normal))
+        else:
+            m = np.ascontiguousarray(np.asarray(mask, bool).reshape(h, w).astype(np.uint8))
+            L = lib()
+            L.orc_render_masked.restype = C.c_int
+            L.orc_render_masked.argtypes = [C.c_void_p] * 7
+            L.orc_render_masked(C.byref(self.scene), _p(f), _p(accum), _p(color), _p(albedo), _p(normal), _p(m))
         return color, albedo, normal
 
     @staticmethod
@@ -342,8 +350,18 @@ class Renderer:
         return int(out[0]), int(out[1])
 
     def converge(self, accum: np.ndarray, snaps: np.ndarray, min_samples: int, threshold: float, mark: bool) -> int:
+        """measure (converge.wgsl:9-31), then mark (:32-51) when `mark`."""
         h, w = accum.shape[:2]
         return int(lib().orc_converge(_p(accum), _p(snaps), w, h, min_samples, threshold, 1 if mark else 0))
+
+    def measure(self, accum: np.ndarray, snaps: np.ndarray) -> None:
+        h, w = accum.shape[:2]
+        lib().orc_converge(_p(accum), _p(snaps), w, h, 0, 0.0, 0)
+
+    def mark(self, accum: np.ndarray, snaps: np.ndarray, min_samples: int, threshold: float) -> int:
+        """mark alone, on errors already in `snaps`; returns the running count."""
+        h, w = accum.shape[:2]
+        return int(lib().orc_converge(_p(accum), _p(snaps), w, h, min_samples, threshold, 2))
 
     def tree_pick(self, points: np.ndarray, normals: np.ndarray, rands: np.ndarray):
         n = len(points)

@@ -1106,7 +1106,18 @@ extern "C" {
 // `accum` holds 12 floats per pixel (Accum) and is read and updated; the three
 // films (4 floats per pixel each) are written.  frame->size.z must hold the
 // samples already accumulated and size.w the samples of this pass.
+int orc_render_masked(const OrcScene* sc, const OrcFrame* fr, float* accum, float* color, float* albedo, float* normal,
+                      const uint8_t* mask);
 int orc_render(const OrcScene* sc, const OrcFrame* fr, float* accum, float* color, float* albedo, float* normal) {
+  return orc_render_masked(sc, fr, accum, color, albedo, normal, nullptr);
+}
+
+// The same pass over the pixels whose `mask` byte is non-zero (all of them when
+// `mask` is null); the others are neither reset nor sampled.  A pixel's samples
+// depend only on the pixel, so a masked pass gives the masked pixels exactly
+// the values a full pass gives them.
+int orc_render_masked(const OrcScene* sc, const OrcFrame* fr, float* accum, float* color, float* albedo, float* normal,
+                      const uint8_t* mask) {
   uint32_t W = fr->size[0], H = fr->size[1];
   orc::Ctx base;
   base.sc = sc;
@@ -1119,6 +1130,7 @@ int orc_render(const OrcScene* sc, const OrcFrame* fr, float* accum, float* colo
     uint32_t px = gx + fr->window[2], py = gy + fr->window[3];
     uint32_t stream = py * fr->window[0] + px;
     float* sum = accum + 12 * (size_t)index;
+    if (mask && !mask[index]) return;
     if (fr->size[2] == 0u)
       for (int k = 0; k < 12; ++k) sum[k] = 0.0f;
     if (sum[3] < 0.0f) return;
@@ -1193,8 +1205,10 @@ int orc_render(const OrcScene* sc, const OrcFrame* fr, float* accum, float* colo
 // mark; returns the running count (pixels still sampling).
 uint32_t orc_converge(float* accum, float* snaps, uint32_t W, uint32_t H, uint32_t min_samples, float threshold,
                       int mark_on) {
+  // mark_on: 0 measure only, 1 measure then mark, 2 mark only (the snapshots'
+  // errors were measured, and neighbours' errors filled in, by the caller)
   size_t n = (size_t)W * H;
-  for (size_t index = 0; index < n; ++index) {
+  for (size_t index = 0; index < (mark_on == 2 ? 0 : n); ++index) {
     float* sum = accum + 12 * index;
     float* snap = snaps + 8 * index;
     float count = sum[3];

@@ -209,6 +209,10 @@ PROTOTYPES = [
     ("pfxt_cache_set_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pfxt_cache_encoding", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
     ("pfxt_cache_set_wait_limit", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("pfxt_adaptive_measure", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("pfxt_adaptive_mark", C.c_int, [C.c_void_p, C.c_uint32, C.c_float, C.POINTER(C.c_uint32)]),
+    ("pfxt_adaptive_snaps_device", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("pfxt_set_pixel_mask", C.c_int, [C.c_void_p, C.c_void_p]),
 ]
 NOALLOC_MAX_RAYS = 1 << 20
 

@@ -350,6 +350,28 @@ int pfxt_sample_adaptive(pfxt_trace* t, const pfxt_adaptive* a, uint32_t seed, p
   });
 }
 
+int pfxt_adaptive_measure(pfxt_trace* t, uint32_t first) {
+  return guarded([&]() {
+    if (!t) throw Invalid("null argument");
+    trace_adaptive_measure(*t, first != 0u);
+  });
+}
+
+int pfxt_adaptive_mark(pfxt_trace* t, uint32_t min_samples, float threshold, uint32_t* running) {
+  return guarded([&]() {
+    if (!t || !running) throw Invalid("null argument");
+    if (!(threshold > 0.0f) || min_samples < 2) throw Invalid("adaptive sampling needs a positive threshold and at least 2 samples");
+    *running = trace_adaptive_mark(*t, min_samples, threshold);
+  });
+}
+
+int pfxt_adaptive_snaps_device(pfxt_trace* t, float** snaps) {
+  return guarded([&]() {
+    if (!t || !snaps) throw Invalid("null argument");
+    *snaps = reinterpret_cast<float*>(t->d_snaps);
+  });
+}
+
 int pfxt_readback(pfxt_trace* t, float* color, float* albedo, float* normal) {
   return guarded([&]() {
     if (!t) throw Invalid("null argument");
@@ -437,7 +459,9 @@ uint32_t pfxt_debug_graph_captures(pfxt_trace* t) { return t ? t->graph_captures
  * host bytes), or lift the restriction with NULL.  A measurement aid: it lets a
  * high-sample reference be accumulated on a stratified subset of a large film.
  * Restarts the accumulation. */
-int pfxt_debug_pixel_mask(pfxt_trace* t, const uint8_t* mask) {
+int pfxt_debug_pixel_mask(pfxt_trace* t, const uint8_t* mask) { return pfxt_set_pixel_mask(t, mask); }
+
+int pfxt_set_pixel_mask(pfxt_trace* t, const uint8_t* mask) {
   return guarded([&]() {
     if (!t) throw Invalid("null argument");
     size_t pixels = (size_t)t->width * t->height;

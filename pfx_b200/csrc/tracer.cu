@@ -1648,6 +1648,29 @@ __global__ void k_mark(Accum* __restrict__ accum, const float4* __restrict__ sna
 
 }  // namespace
 
+// One adaptive round split in its two kernels, for a frame whose pixels are
+// shared between tracers (one per GPU): measure, then, after the caller has
+// written the errors of neighbouring rows other tracers own into the
+// snapshots, mark.  `first` clears the snapshots (a new adaptive render).
+void trace_adaptive_measure(pfxt_trace& t, bool first) {
+  cudaStream_t st = t.stream;
+  if (first) check(cudaMemsetAsync(t.d_snaps, 0, (size_t)t.width * t.height * 32, st), "snapshots");
+  k_measure<<<grids().flat, 256, 0, st>>>(t.d_accum, t.d_snaps, t.width, t.height);
+  check(cudaGetLastError(), "measure");
+  check(cudaStreamSynchronize(st), "measure");
+}
+
+uint32_t trace_adaptive_mark(pfxt_trace& t, uint32_t min_samples, float threshold) {
+  cudaStream_t st = t.stream;
+  check(cudaMemsetAsync(t.d_running, 0, 4, st), "running count");
+  k_mark<<<grids().flat, 256, 0, st>>>(t.d_accum, t.d_snaps, t.width, t.height, min_samples, threshold, t.d_running);
+  check(cudaGetLastError(), "mark");
+  uint32_t running = 0;
+  check(cudaMemcpyAsync(&running, t.d_running, 4, cudaMemcpyDeviceToHost, st), "running count");
+  check(cudaStreamSynchronize(st), "mark");
+  return running;
+}
+
 // Trace::sample_adaptive_kept without a keeper (adaptive.rs:136-325).
 void trace_sample_adaptive(pfxt_trace& t, const pfxt_adaptive& a, uint32_t seed, pfxt_round* rounds, uint32_t cap,
                            uint32_t* written, const AdaptiveKeeping* keeping) {

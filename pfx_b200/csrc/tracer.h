@@ -180,6 +180,8 @@ struct AdaptiveKeeping {
 void trace_sample_adaptive(pfxt_trace& t, const pfxt_adaptive& a, uint32_t seed, pfxt_round* rounds, uint32_t cap,
                            uint32_t* written, const AdaptiveKeeping* keeping = nullptr);
 bool adaptive_valid(const pfxt_adaptive& a);
+void trace_adaptive_measure(pfxt_trace& t, bool first);
+uint32_t trace_adaptive_mark(pfxt_trace& t, uint32_t min_samples, float threshold);
 std::vector<uint32_t> adaptive_rounds(const pfxt_adaptive& a);
 void trace_readback(pfxt_trace& t, float* color, float* albedo, float* normal);
 void trace_sample_counts(pfxt_trace& t, uint32_t* counts);

@@ -486,10 +486,38 @@ class Trace:
         """Sample only the pixels where `mask` (H, W) is true; None lifts it.
         Restarts the accumulation."""
         if mask is None:
-            check(self._lib.pfxt_debug_pixel_mask(self._h, None))
+            check(self._lib.pfxt_set_pixel_mask(self._h, None))
             return
         m = np.ascontiguousarray(np.asarray(mask, bool).astype(np.uint8).reshape(self.height, self.width))
-        check(self._lib.pfxt_debug_pixel_mask(self._h, m.ctypes.data))
+        check(self._lib.pfxt_set_pixel_mask(self._h, m.ctypes.data))
+
+    # ---------------------------------------------------------- adaptive steps
+    def adaptive_measure(self, first: bool) -> None:
+        """measure (converge.wgsl:9-31) over the accumulation; `first` starts a
+        new adaptive render (clears the snapshots)."""
+        check(self._lib.pfxt_adaptive_measure(self._h, 1 if first else 0))
+
+    def adaptive_mark(self, min_samples: int, threshold: float) -> int:
+        """mark (converge.wgsl:32-51) on the errors in the snapshots; returns
+        this tracer's running count."""
+        n = C.c_uint32()
+        check(self._lib.pfxt_adaptive_mark(self._h, int(min_samples), float(threshold), C.byref(n)))
+        return int(n.value)
+
+    def adaptive_snaps_device(self):
+        """The (H, W, 8) float32 snapshots as a CUDA tensor aliasing the
+        tracer's memory (the error at [..., 5])."""
+        import torch
+        p = C.c_void_p()
+        check(self._lib.pfxt_adaptive_snaps_device(self._h, C.byref(p)))
+
+        class _View:
+            def __init__(self, ptr, shape):
+                self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f4", "data": (ptr, False),
+                                                 "version": 3, "strides": None}
+
+        return torch.as_tensor(_View(p.value, (self.height, self.width, 8)), device="cuda")
+
 
     def rays_traced(self) -> tuple:
         """(closest-hit, any-hit) queries traced by the sampling passes so far."""
