@@ -467,9 +467,10 @@ def main():
                     "d2h_bytes_per_step": int(w.width * w.height * 16),
                     "note": "scene uploaded once by Trace::new (create_s); per step one pass and the colour film"},
             # per pass: collect, gen, seed counts, finish, films, and per bounce reset,
-            # extend, (material sort: 2), shade (split: 3), rewind, connect
+            # extend and its retry walk, (material sort: 2), shade (split: 3), rewind,
+            # connect and its retry walk
             "gpu_launches": args.steps * (5 + (w.settings.bounces[0] + 2) * (
-                5 + (2 if tuning["sort_shading"] else 0) + (2 if tuning["split_shade"] else 0))),
+                7 + (2 if tuning["sort_shading"] else 0) + (2 if tuning["split_shade"] else 0))),
             "clocks": clk.summary(),
         }
         line["roofline"] = traversal_roofline(trace, w, dev, stream, flush)

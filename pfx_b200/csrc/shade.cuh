@@ -27,6 +27,11 @@ constexpr float SH_PI = 0x1.921fb6p+1f;
 #ifndef SH_SMALL
 #define SH_SMALL SH_CALL
 #endif  // brdf.wgsl:1 `const PI: f32 = 3.141592653589793`
+// The light-tree descent, its leaf and the light candidate: out of line unless
+// a build inlines them.
+#ifndef SH_TREE
+#define SH_TREE SH_CALL
+#endif
 
 // ------------------------------------------------------------------ random
 __device__ __forceinline__ uint32_t pcg(uint32_t v) {
@@ -533,7 +538,7 @@ __device__ __forceinline__ void shadow_ray(v3 origin, v3 aim, bool shadow, v3& d
 
 // light_candidate (lights.wgsl:145-200) of light row `row`, loaded here so that
 // the caller holds no copy of the row in memory across the call.
-SH_CALL Candidate light_candidate(const Specialise& sp, const ShadeView& v, uint32_t row, const m3& transform,
+SH_TREE Candidate light_candidate(const Specialise& sp, const ShadeView& v, uint32_t row, const m3& transform,
                                   v3 p, v3 origin, v3 geometric, uint32_t& state, float4 u) {
   const LightRow light = load_light(v, row);
   Candidate out = candidate_none();
@@ -692,7 +697,7 @@ __device__ __forceinline__ float2 child_importance(const ShadeView& v, uint32_t 
 }
 
 // tree_leaf (lights.wgsl:276-349): (selected row, pmf)
-SH_CALL float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n,
+SH_TREE float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n,
                                             float start) {
   float rand = start;
   bool sample_max = rand > 0.5f;
@@ -768,7 +773,7 @@ SH_CALL float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 
 
 // tree_pick (lights.wgsl:350-386): (light row, pmf).  The descent is bounded
 // by the number of tree rows; a malformed tree ends the descent with pmf 0.
-SH_CALL float2 tree_pick(const ShadeView& v, uint32_t rows, v3 p, v3 n, float start,
+SH_TREE float2 tree_pick(const ShadeView& v, uint32_t rows, v3 p, v3 n, float start,
                                             uint32_t* leaf_row) {
   uint32_t at = f2u((float)v.looped + (float)v.tree);
   float rand = start;

@@ -89,6 +89,9 @@ struct Wave {
   float4* surf;        // 9 float4 per path
   uint32_t* rhist;     // RAY_BINS: the extend queue's histogram by ray key
   uint32_t* rcursor;
+  // queue items the traversal handed over to the IEEE walk (rays that are not
+  // bounded), counted at counters[13] (extend) and counters[14] (connect)
+  uint32_t* retry;
 };
 
 // The radiance cache as the wave sees it (all null/zero when none is attached).
@@ -283,6 +286,7 @@ __global__ void k_reset(const __grid_constant__ Pass P,uint32_t cur) {
     P.w.counters[2] = 0u;
     P.w.counters[4] = 0u;
     P.w.counters[12] = 0u;
+    P.w.counters[13] = 0u;
     reinterpret_cast<unsigned long long*>(P.w.counters + 8)[0] += P.w.counters[cur];
   }
   if (blockIdx.x == 0) {
@@ -420,6 +424,7 @@ __global__ void __launch_bounds__(256) k_sort_place(const __grid_constant__ Pass
 __global__ void k_rewind(const __grid_constant__ Pass P) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     P.w.counters[4] = 0u;
+    P.w.counters[14] = 0u;
     reinterpret_cast<unsigned long long*>(P.w.counters + 8)[1] += P.w.counters[2];
   }
 }
@@ -435,7 +440,7 @@ __global__ void __launch_bounds__(THREADS, TRACE_WARPS_PER_SM * 32 / THREADS) k_
   const uint32_t n = ANY ? P.w.counters[2] : P.w.counters[which];
   uint32_t* counter = P.w.counters + 4;
   LaneStack<0> st;  // local memory: a shared-memory top measured slower (more registers, fewer warps)
-  Walker<ANY, false> w;
+  Walker<ANY, false, BOX_BOUNDED> w;
   const int lane = threadIdx.x & 31;
   uint32_t idx = 0, item = 0;
   bool have = false, retired = false;
@@ -465,7 +470,9 @@ __global__ void __launch_bounds__(THREADS, TRACE_WARPS_PER_SM * 32 / THREADS) k_
       w.inner_phase(P.s, st);
       if (!w.done) w.leaf_phase(P.s, st);
       if (w.done) {
-        if (ANY) {
+        if (w.retry) {
+          P.w.retry[atomicAdd(P.w.counters + (ANY ? 14 : 13), 1u)] = item;
+        } else if (ANY) {
           reinterpret_cast<float*>(P.w.sh_d + item)[3] = __uint_as_float(w.hit.hit ? 0u : 1u);
         } else {
           P.w.hit[item] = make_float4(w.hit.t, __uint_as_float(w.hit.slot), __uint_as_float(w.hit.record), w.hit.u);
@@ -473,6 +480,30 @@ __global__ void __launch_bounds__(THREADS, TRACE_WARPS_PER_SM * 32 / THREADS) k_
         }
         have = false;
       }
+    }
+  }
+}
+
+// The queue items k_trace_queue handed over (rays that are not bounded in
+// world or instance space), walked again from the start with IEEE division
+// throughout; its launch reads the count on the device, so a pass issues it
+// whether or not any ray needs it.
+template <bool ANY>
+__global__ void __launch_bounds__(128) k_trace_queue_retry(const __grid_constant__ Pass P) {
+  const uint32_t n = P.w.counters[ANY ? 14 : 13];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const uint32_t item = P.w.retry[k];
+    float4 a = ANY ? P.w.sh_o[item] : P.w.ray_o[item];
+    float4 b = ANY ? P.w.sh_d[item] : P.w.ray_d[item];
+    LaneStack<0> st;
+    Walker<ANY, false, BOX_IEEE> w;
+    w.start(P.s, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), ANY ? a.w : 1e20f);
+    w.run(P.s, st);
+    if (ANY) {
+      reinterpret_cast<float*>(P.w.sh_d + item)[3] = __uint_as_float(w.hit.hit ? 0u : 1u);
+    } else {
+      P.w.hit[item] = make_float4(w.hit.t, __uint_as_float(w.hit.slot), __uint_as_float(w.hit.record), w.hit.u);
+      P.w.hit_v[item] = w.hit.v;
     }
   }
 }
@@ -1216,6 +1247,7 @@ int grid_for(const void* kernel, int threads) {
 struct Grids {
   int trace_closest[3] = {0, 0, 0}, trace_any[3] = {0, 0, 0}, shade = 0, shade_inline = 0, flat = 0;
   int shade_hit = 0, shade_lights = 0, shade_lights_inline = 0, shade_bsdf = 0;
+  int retry = 0;  // blocks of the retry walks: one per SM (their work is rare)
 };
 Grids& grids() {
   static Grids g;
@@ -1236,6 +1268,7 @@ Grids& grids() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     g.flat = sms * 8;
+    g.retry = sms;
   }
   return g;
 }
@@ -1251,6 +1284,7 @@ void launch_trace_queue(int sel, const Pass& P, uint32_t which, cudaStream_t st)
     k_trace_queue<ANY, 256><<<grid[2], 256, 0, st>>>(P, which);
   else
     k_trace_queue<ANY, 128><<<grid[1], 128, 0, st>>>(P, which);
+  k_trace_queue_retry<ANY><<<g.retry, 128, 0, st>>>(P);
 }
 
 int thread_select(uint32_t threads) { return threads == 64u ? 0 : (threads == 256u ? 2 : 1); }
@@ -1270,7 +1304,8 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
          o_q1 = add(4ull * capacity), o_sq = add(4ull * capacity * cap), o_act = add(4ull * capacity),
          o_cnt = add(64), o_keys = add(4ull * capacity), o_sorted = add(4ull * capacity),
          o_hist = add(4ull * SORT_BINS), o_cursor = add(4ull * SORT_BINS), o_lit = add(4ull * capacity),
-         o_surf = add(144ull * capacity), o_rhist = add(4ull * RAY_BINS), o_rcursor = add(4ull * RAY_BINS);
+         o_surf = add(144ull * capacity), o_rhist = add(4ull * RAY_BINS), o_rcursor = add(4ull * RAY_BINS),
+         o_retry = add(4ull * capacity * (cap > 0 ? cap : 1));
   if (need > t.wave_bytes) {
     if (t.d_wave) cudaFree(t.d_wave);
     t.d_wave = nullptr;
@@ -1308,6 +1343,7 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
   w.surf = reinterpret_cast<float4*>(b + o_surf);
   w.rhist = reinterpret_cast<uint32_t*>(b + o_rhist);
   w.rcursor = reinterpret_cast<uint32_t*>(b + o_rcursor);
+  w.retry = reinterpret_cast<uint32_t*>(b + o_retry);
 }
 
 // Cache scratch for `pixels` paths: queries, their path indices and

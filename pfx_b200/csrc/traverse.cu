@@ -31,8 +31,14 @@ __device__ __forceinline__ void load_ray(const pfxt_ray* __restrict__ rays, uint
   d = mk3(b.x, b.y, b.z);
 }
 
+// The output word that marks a ray the first walk handed over to the IEEE
+// walk (closest hit: the `hit` field; any hit: the flag).
+constexpr uint32_t RETRY = 2u;
+
 // MODE 0: closest hit -> pfxt_hit; MODE 1: any hit -> u32 flag;
-// MODE 2/3: work counters of closest / any hit -> uint2.
+// MODE 2/3: work counters of closest / any hit -> uint2.  Modes 0 and 1 walk
+// bounded rays only (no call in the walk loop) and mark the others RETRY for
+// k_trace_retry; the counting modes walk every ray.
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, TRACE_WARPS_PER_SM * 32 / kThreads) k_trace(SceneView s, const pfxt_ray* __restrict__ rays, uint32_t n,
                                                     void* __restrict__ out, uint32_t* __restrict__ counter) {
@@ -40,7 +46,7 @@ __global__ void __launch_bounds__(kThreads, TRACE_WARPS_PER_SM * 32 / kThreads) 
   constexpr bool COUNT = (MODE >= 2);
   constexpr unsigned FULL = 0xffffffffu;
   LaneStack<0> st;  // local memory: a shared-memory top measured slower (more registers, fewer warps)
-  Walker<ANY, COUNT> w;
+  Walker<ANY, COUNT, COUNT ? BOX_EITHER : BOX_BOUNDED> w;
   const int lane = threadIdx.x & 31;
   uint32_t idx = 0;
   bool have = false, retired = false;
@@ -72,15 +78,39 @@ __global__ void __launch_bounds__(kThreads, TRACE_WARPS_PER_SM * 32 / kThreads) 
       if (w.done) {
         if (MODE == 0) {
           reinterpret_cast<uint4*>(out)[idx] =
-              make_uint4(__float_as_uint(w.hit.t), w.hit.slot, w.hit.record, w.hit.hit);
+              make_uint4(__float_as_uint(w.hit.t), w.hit.slot, w.hit.record, w.retry ? RETRY : w.hit.hit);
         } else if (MODE == 1) {
-          reinterpret_cast<uint32_t*>(out)[idx] = w.hit.hit;
+          reinterpret_cast<uint32_t*>(out)[idx] = w.retry ? RETRY : w.hit.hit;
         } else {
           reinterpret_cast<uint2*>(out)[idx] = make_uint2(w.counts.boxes, w.counts.tris);
         }
         have = false;
       }
     }
+  }
+}
+
+// The rays k_trace marked RETRY, walked again from the start with IEEE
+// division throughout (rare: a direction component above 2^20 or an origin
+// component beyond the bounded range, in world or instance space).
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) k_trace_retry(SceneView s, const pfxt_ray* __restrict__ rays, uint32_t n,
+                                                          void* __restrict__ out) {
+  constexpr bool ANY = (MODE == 1);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t marker = MODE == 0 ? reinterpret_cast<const uint4*>(out)[i].w : reinterpret_cast<const uint32_t*>(out)[i];
+    if (marker != RETRY) continue;
+    LaneStack<0> st;
+    Walker<ANY, false, BOX_IEEE> w;
+    v3 o, d;
+    float tmax;
+    load_ray(rays, i, o, d, tmax);
+    w.start(s, o, d, tmax);
+    w.run(s, st);
+    if (MODE == 0)
+      reinterpret_cast<uint4*>(out)[i] = make_uint4(__float_as_uint(w.hit.t), w.hit.slot, w.hit.record, w.hit.hit);
+    else
+      reinterpret_cast<uint32_t*>(out)[i] = w.hit.hit;
   }
 }
 
@@ -122,6 +152,10 @@ cudaError_t launch(const SceneView& s, const pfxt_ray* rays, uint32_t n, void* o
   uint32_t blocks = (uint32_t)persistent_blocks<MODE>();
   if (need < blocks) blocks = need;
   k_trace<MODE><<<blocks, kThreads, 0, stream>>>(s, rays, n, out, counter);
+  if constexpr (MODE < 2) {
+    uint32_t scan = (n + kThreads - 1) / kThreads, most = (uint32_t)persistent_blocks<MODE>();
+    k_trace_retry<MODE><<<scan < most ? scan : most, kThreads, 0, stream>>>(s, rays, n, out);
+  }
   return cudaGetLastError();
 }
 
@@ -146,6 +180,7 @@ cudaError_t prepare_any_queries() {
   persistent_blocks<1>();
   cudaFuncAttributes attr;
   cudaError_t e = cudaFuncGetAttributes(&attr, k_trace<1>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&attr, k_trace_retry<1>);
   if (e == cudaSuccess) e = cudaFuncGetAttributes(&attr, k_pack);
   return e;
 }

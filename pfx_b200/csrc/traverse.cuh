@@ -96,8 +96,8 @@ __device__ __forceinline__ TRay make_tray(v3 o, v3 d, uint32_t small) {
 
 // Slab test of one box with IEEE division throughout, for rays that are not
 // bounded (see above).
-static __device__ __noinline__ bool box_geometry_ieee(float lx, float ly, float lz, float hx, float hy, float hz,
-                                               const TRay& ray, float& near) {
+__device__ __forceinline__ bool box_geometry_ieee_inline(float lx, float ly, float lz, float hx, float hy, float hz,
+                                                         const TRay& ray, float& near) {
   float n = 0.0f, f = INFINITY;
   if (fabsf(ray.d.x) < 1e-12f) {
     if (ray.o.x < lx || ray.o.x > hx) return false;
@@ -124,6 +124,13 @@ static __device__ __noinline__ bool box_geometry_ieee(float lx, float ly, float 
   return !(n > f);
 }
 
+// The same test out of line, for walks that take both kinds of ray (the work
+// counting variant).
+static __device__ __noinline__ bool box_geometry_ieee(float lx, float ly, float lz, float hx, float hy, float hz,
+                                                      const TRay& ray, float& near) {
+  return box_geometry_ieee_inline(lx, ly, lz, hx, hy, hz, ray, near);
+}
+
 // x / d by Markstein's correction from r = RN(1/d) (Markstein 1990; Cornea,
 // Harrison and Tang, "Scientific Computing on Itanium-based Systems", 2002,
 // ch. 8): with q = RN(x r) the residual fma(-q, d, x) is exact and
@@ -135,13 +142,12 @@ __device__ __forceinline__ float quotient(float x, float d, float r) {
   return fmaf(e, r, q);
 }
 
-// Slab test of one box: true when the ray's geometry passes (degenerate axes
-// inside the slab, entry <= exit); `near` receives max(0, entries).  The six
-// quotients equal IEEE division's (the reference divides); the boxes of a ray
-// that is not bounded are tested with IEEE division instead.
-__device__ __forceinline__ bool box_geometry(float lx, float ly, float lz, float hx, float hy, float hz,
-                                             const TRay& ray, float& near) {
-  if (!ray.bounded) return box_geometry_ieee(lx, ly, lz, hx, hy, hz, ray, near);
+// Slab test of one box for a bounded ray: true when the ray's geometry passes
+// (degenerate axes inside the slab, entry <= exit); `near` receives
+// max(0, entries).  The six quotients equal IEEE division's (the reference
+// divides).
+__device__ __forceinline__ bool box_geometry_bounded(float lx, float ly, float lz, float hx, float hy, float hz,
+                                                     const TRay& ray, float& near) {
   float n = 0.0f, f = INFINITY;
   if (fabsf(ray.d.x) < 1e-12f) {
     if (ray.o.x < lx || ray.o.x > hx) return false;
@@ -166,6 +172,26 @@ __device__ __forceinline__ bool box_geometry(float lx, float ly, float lz, float
   }
   near = n;
   return !(n > f);
+}
+
+// How a walk tests boxes.
+//  BOX_EITHER:  bounded rays with the Markstein quotients, other rays with the
+//               out-of-line IEEE test (one walk for every ray; the call costs
+//               the walk loop spills, so only the counting variant uses it);
+//  BOX_BOUNDED: Markstein quotients only; a ray that is not bounded (in world
+//               space or in an instance's space) stops at once with `retry`
+//               set, and a second kernel walks it again from the start with
+//               BOX_IEEE, so the walk loop has no call;
+//  BOX_IEEE:    IEEE division throughout, inline.
+// All three give the same bits for every box they test.
+constexpr int BOX_EITHER = 0, BOX_BOUNDED = 1, BOX_IEEE = 2;
+
+template <int BOX>
+__device__ __forceinline__ bool box_test(float lx, float ly, float lz, float hx, float hy, float hz, const TRay& ray,
+                                         float& near) {
+  if (BOX == BOX_IEEE) return box_geometry_ieee_inline(lx, ly, lz, hx, hy, hz, ray, near);
+  if (BOX == BOX_EITHER && !ray.bounded) return box_geometry_ieee(lx, ly, lz, hx, hy, hz, ray, near);
+  return box_geometry_bounded(lx, ly, lz, hx, hy, hz, ray, near);
 }
 
 // to_object (trace.wgsl:449-452): (dot(lo,q), dot(hi,q), dot(rows2,q)), q=(p,w).
@@ -232,7 +258,7 @@ struct LaneStack<0> {
 };
 
 // One query's traversal state; the stack is the caller's.
-template <bool ANY, bool COUNT>
+template <bool ANY, bool COUNT, int BOX = BOX_EITHER>
 struct Walker {
   v3 o, d;      // world ray
   TRay ray;     // ray in the current space
@@ -243,6 +269,7 @@ struct Walker {
   float near_cur;
   int top;
   bool done;
+  bool retry;  // BOX_BOUNDED: the ray is not bounded; walk it again with BOX_IEEE
   TraceHit hit;
   TraceCounts counts;
 
@@ -257,6 +284,11 @@ struct Walker {
     near_cur = -INFINITY;
     top = 0;
     done = (s.root == REF_NONE);
+    retry = false;
+    if (BOX == BOX_BOUNDED && !done && !ray.bounded) {
+      retry = true;
+      done = true;
+    }
     hit.t = lim;
     hit.slot = hit.record = hit.hit = 0u;
     hit.u = hit.v = 0.0f;
@@ -299,9 +331,9 @@ struct Walker {
         float4 q0 = __ldg(p + 0), q1 = __ldg(p + 1), q2 = __ldg(p + 2);
         uint4 q3 = __ldg(reinterpret_cast<const uint4*>(p + 3));
         float n0 = 0.0f, n1 = 0.0f;
-        bool ok0 = box_geometry(q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, ray, n0) && n0 <= hit.t;
+        bool ok0 = box_test<BOX>(q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, ray, n0) && n0 <= hit.t;
         bool has1 = q3.y != REF_NONE;
-        bool ok1 = has1 && box_geometry(q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, ray, n1) && n1 <= hit.t;
+        bool ok1 = has1 && box_test<BOX>(q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, ray, n1) && n1 <= hit.t;
         if (COUNT) counts.boxes += 1u;  // the left child, popped next by the reference
         if ((ok1 || (COUNT && has1)) && top < (int)REF_STACK) {
           st.put(top, q3.y, ok1 ? n1 : INFINITY);
@@ -330,7 +362,14 @@ struct Walker {
         record = m.z;
         word = m.w;
         inv_det = m2.x;
-        if (__float_as_uint(m2.y) != 0u) ray = make_tray(to_object(r0, r1, r2, o, 1.0f), to_object(r0, r1, r2, d, 0.0f), s.small);
+        if (__float_as_uint(m2.y) != 0u) {
+          ray = make_tray(to_object(r0, r1, r2, o, 1.0f), to_object(r0, r1, r2, d, 0.0f), s.small);
+          if (BOX == BOX_BOUNDED && !ray.bounded) {
+            retry = true;
+            done = true;
+            return;
+          }
+        }
         ref = m.x;
         near_cur = -INFINITY;
         continue;
@@ -402,7 +441,7 @@ struct Walker {
 template <bool ANY>
 __device__ __forceinline__ TraceHit traverse(const SceneView& s, v3 o, v3 d, float limit) {
   LaneStack<0> st;
-  Walker<ANY, false> w;
+  Walker<ANY, false, BOX_EITHER> w;
   w.start(s, o, d, limit);
   w.run(s, st);
   return w.hit;

@@ -77,3 +77,11 @@ def test_adaptive_rounds_through_the_abi():
     from pfx_b200.trace import Adaptive
     assert Adaptive(0.01, 16, 100, 1.5).rounds() == [8, 16, 24, 36, 54, 81, 100]
     assert Adaptive(0.01, 16, 64, 1.5).rounds() == [8, 16, 24, 36, 54, 64]
+
+
+def test_the_rust_crate_declares_every_entry_point():
+    """pfx-trace-cuda/src/ffi.rs (the binding a pfx maintainer links; no Rust
+    toolchain here to compile it) declares exactly the header's functions."""
+    ffi = (HEADER.parent.parent / "pfx-trace-cuda" / "src" / "ffi.rs").read_text()
+    declared = sorted(set(re.findall(r"pub fn (pfxt_[a-z_0-9]+)\(", ffi)))
+    assert declared == declared_symbols()
