@@ -399,15 +399,28 @@ typedef struct pfxt_tuning {
   uint32_t split_shade;   /* shade a bounce in three kernels (hit, light slots, BSDF) instead of one (1) */
   uint32_t sort_rays;     /* sort the rays of every bounce after the first by direction and origin (0) */
   float pass_ms;          /* from pfxt_autotune: the chosen configuration's median pass time */
+  uint32_t shadow_queue;  /* queue capacity of the light slots' shadow rays: 1 = one queue entry per slot and
+                           * path, traced by the connect kernel; 0 = no queue, each slot's shadow ray traced
+                           * inside the light-slot kernel (1; scenes with more slots per path than the queue
+                           * holds always trace inside) */
+  uint32_t short_stack;   /* traversal stack entries per lane kept in shared memory, the rest in local memory:
+                           * 0 or 8 (0) */
+  uint32_t from_cache;    /* set by pfxt_autotune: 1 when the choice came from an earlier tuning of the same
+                           * scene, film and settings in this process */
 } pfxt_tuning;
 
 int pfxt_get_tuning(pfxt_trace* trace, pfxt_tuning* out);
 int pfxt_set_tuning(pfxt_trace* trace, const pfxt_tuning* tuning);
 /* Times `passes` one-sample passes (at least 2; the first of each
- * configuration warms up and is not counted) of this tracer's scene under every
- * traversal block size, with and without the material sort, with one shade
- * kernel and with three, and keeps the fastest; `out` (may be NULL) receives it.  Restarts the accumulation; with a
- * radiance cache attached, the trial passes also train it. */
+ * configuration warms up and is not counted) of this tracer's scene, one
+ * choice at a time with the others held at the best so far: the traversal
+ * block size, the material sort, one shade kernel or three, the ray sort, the
+ * shadow queue and the shared-memory stack entries; keeps the fastest and
+ * remembers it for this scene (a hash of its nodes, triangles, lights and
+ * materials), film size, settings and attached cache, so a later tracer of
+ * the same scene takes it without timing anything.  `out` (may be NULL)
+ * receives it.  Restarts the accumulation; with a radiance cache attached,
+ * the trial passes also train it. */
 int pfxt_autotune(pfxt_trace* trace, uint32_t passes, pfxt_tuning* out);
 
 /* ------------------------------------------------------------ radiance cache

@@ -255,6 +255,9 @@ pub struct PfxtTuning {
     pub split_shade: u32,
     pub sort_rays: u32,
     pub pass_ms: f32,
+    pub shadow_queue: u32,
+    pub short_stack: u32,
+    pub from_cache: u32,
 }
 
 #[repr(C)]

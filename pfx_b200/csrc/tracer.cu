@@ -432,14 +432,23 @@ __global__ void k_rewind(const __grid_constant__ Pass P) {
 // ------------------------------------------------------------------ extend
 // THREADS per block is a launch choice of the autotuner: the walk is per lane
 // and the refill per warp, so the block size changes only the residency.
-template <bool ANY, int THREADS>
+// SHORT entries of each lane's traversal stack live in shared memory (a tuning
+// choice: 0 or 8), the rest in local memory.
+template <bool ANY, int THREADS, int SHORT>
 __global__ void __launch_bounds__(THREADS, TRACE_WARPS_PER_SM * 32 / THREADS) k_trace_queue(const __grid_constant__ Pass P,
                                                                                        uint32_t which) {
   constexpr unsigned FULL = 0xffffffffu;
   const uint32_t* queue = ANY ? P.w.squeue : ((P.ray_bins && P.bounce > 0u) ? P.w.sorted : P.w.queue[which]);
   const uint32_t n = ANY ? P.w.counters[2] : P.w.counters[which];
   uint32_t* counter = P.w.counters + 4;
-  LaneStack<0> st;  // local memory: a shared-memory top measured slower (more registers, fewer warps)
+  __shared__ uint32_t short_ref[SHORT > 0 ? SHORT * THREADS : 1];
+  __shared__ float short_near[SHORT > 0 ? SHORT * THREADS : 1];
+  LaneStack<SHORT> st;
+  if constexpr (SHORT > 0) {
+    st.sh_ref = short_ref + threadIdx.x;
+    st.sh_near = short_near + threadIdx.x;
+    st.lanes = THREADS;
+  }
   Walker<ANY, false, BOX_BOUNDED> w;
   const int lane = threadIdx.x & 31;
   uint32_t idx = 0, item = 0;
@@ -1245,19 +1254,26 @@ int grid_for(const void* kernel, int threads) {
 
 // Persistent grids of the traversal kernels for 64, 128 and 256 threads per block.
 struct Grids {
-  int trace_closest[3] = {0, 0, 0}, trace_any[3] = {0, 0, 0}, shade = 0, shade_inline = 0, flat = 0;
+  // [threads choice (64, 128, 256)][shared-memory stack entries (0, 8)]
+  int trace_closest[3][2] = {}, trace_any[3][2] = {}, shade = 0, shade_inline = 0, flat = 0;
   int shade_hit = 0, shade_lights = 0, shade_lights_inline = 0, shade_bsdf = 0;
   int retry = 0;  // blocks of the retry walks: one per SM (their work is rare)
 };
 Grids& grids() {
   static Grids g;
   if (g.shade == 0) {
-    g.trace_closest[0] = grid_for((const void*)k_trace_queue<false, 64>, 64);
-    g.trace_closest[1] = grid_for((const void*)k_trace_queue<false, 128>, 128);
-    g.trace_closest[2] = grid_for((const void*)k_trace_queue<false, 256>, 256);
-    g.trace_any[0] = grid_for((const void*)k_trace_queue<true, 64>, 64);
-    g.trace_any[1] = grid_for((const void*)k_trace_queue<true, 128>, 128);
-    g.trace_any[2] = grid_for((const void*)k_trace_queue<true, 256>, 256);
+    g.trace_closest[0][0] = grid_for((const void*)k_trace_queue<false, 64, 0>, 64);
+    g.trace_closest[1][0] = grid_for((const void*)k_trace_queue<false, 128, 0>, 128);
+    g.trace_closest[2][0] = grid_for((const void*)k_trace_queue<false, 256, 0>, 256);
+    g.trace_any[0][0] = grid_for((const void*)k_trace_queue<true, 64, 0>, 64);
+    g.trace_any[1][0] = grid_for((const void*)k_trace_queue<true, 128, 0>, 128);
+    g.trace_any[2][0] = grid_for((const void*)k_trace_queue<true, 256, 0>, 256);
+    g.trace_closest[0][1] = grid_for((const void*)k_trace_queue<false, 64, 8>, 64);
+    g.trace_closest[1][1] = grid_for((const void*)k_trace_queue<false, 128, 8>, 128);
+    g.trace_closest[2][1] = grid_for((const void*)k_trace_queue<false, 256, 8>, 256);
+    g.trace_any[0][1] = grid_for((const void*)k_trace_queue<true, 64, 8>, 64);
+    g.trace_any[1][1] = grid_for((const void*)k_trace_queue<true, 128, 8>, 128);
+    g.trace_any[2][1] = grid_for((const void*)k_trace_queue<true, 256, 8>, 256);
     g.shade = grid_for((const void*)k_shade<true>, kThreads);
     g.shade_inline = grid_for((const void*)k_shade<false>, kThreads);
     g.shade_hit = grid_for((const void*)k_shade_hit, kThreads);
@@ -1274,17 +1290,26 @@ Grids& grids() {
 }
 
 // The traversal launches for the tuned block size (0: 64, 1: 128, 2: 256 threads).
-template <bool ANY>
-void launch_trace_queue(int sel, const Pass& P, uint32_t which, cudaStream_t st) {
+template <bool ANY, int SHORT>
+void launch_trace_queue_short(int sel, const Pass& P, uint32_t which, cudaStream_t st) {
   Grids& g = grids();
-  const int* grid = ANY ? g.trace_any : g.trace_closest;
+  const int k = SHORT > 0 ? 1 : 0;
+  const int* grid = ANY ? &g.trace_any[sel][k] : &g.trace_closest[sel][k];
   if (sel == 0)
-    k_trace_queue<ANY, 64><<<grid[0], 64, 0, st>>>(P, which);
+    k_trace_queue<ANY, 64, SHORT><<<*grid, 64, 0, st>>>(P, which);
   else if (sel == 2)
-    k_trace_queue<ANY, 256><<<grid[2], 256, 0, st>>>(P, which);
+    k_trace_queue<ANY, 256, SHORT><<<*grid, 256, 0, st>>>(P, which);
   else
-    k_trace_queue<ANY, 128><<<grid[1], 128, 0, st>>>(P, which);
-  k_trace_queue_retry<ANY><<<g.retry, 128, 0, st>>>(P);
+    k_trace_queue<ANY, 128, SHORT><<<*grid, 128, 0, st>>>(P, which);
+}
+
+template <bool ANY>
+void launch_trace_queue(int sel, uint32_t short_stack, const Pass& P, uint32_t which, cudaStream_t st) {
+  if (short_stack > 0u)
+    launch_trace_queue_short<ANY, 8>(sel, P, which, st);
+  else
+    launch_trace_queue_short<ANY, 0>(sel, P, which, st);
+  k_trace_queue_retry<ANY><<<grids().retry, 128, 0, st>>>(P);
 }
 
 int thread_select(uint32_t threads) { return threads == 64u ? 0 : (threads == 256u ? 2 : 1); }
@@ -1452,7 +1477,7 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
   uint32_t light_slots = 1u + t.shade.looped + (t.shade.tree > 0u ? 1u : 0u);
   uint32_t slots = 2u + light_slots;
   uint32_t cap = std::min(slots, CAP_MAX);
-  bool deferred = slots <= CAP_MAX;
+  bool deferred = slots <= CAP_MAX && t.shadow_queue;
   ensure_wave(t, pixels, cap);
   Pass P;
   memset(&P, 0, sizeof(P));
@@ -1506,7 +1531,8 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
     uint64_t extra[8] = {count, (uint64_t)(uintptr_t)t.d_mask, (uint64_t)(uintptr_t)t.cache, deferred ? 1u : 0u,
                          t.cache ? (uint64_t)t.cache->s.steps : 0u, t.cache ? (uint64_t)t.cache->s.batch : 0u,
                          (uint64_t)(uintptr_t)t.d_accum,
-                         (uint64_t)pixels | ((uint64_t)t.trace_threads << 32) | ((uint64_t)t.split_shade << 48)};
+                         (uint64_t)pixels | ((uint64_t)t.trace_threads << 32) | ((uint64_t)t.split_shade << 48) |
+                             ((uint64_t)t.short_stack << 52)};
     memcpy(key.data() + sizeof(P), extra, sizeof(extra));
     cudaGraphExec_t exec = nullptr;
     for (auto& e : t.graphs)
@@ -1574,7 +1600,7 @@ void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_
         k_sort_count<true><<<g.flat, 256, 0, st>>>(P, cur);
         k_sort_place<true><<<g.flat, 256, 0, st>>>(P, cur);
       }
-      launch_trace_queue<false>(thread_select(t.trace_threads), P, cur, st);
+      launch_trace_queue<false>(thread_select(t.trace_threads), t.short_stack, P, cur, st);
       if (P.bins) {
         k_sort_count<false><<<g.flat, 256, 0, st>>>(P, cur);
         k_sort_place<false><<<g.flat, 256, 0, st>>>(P, cur);
@@ -1605,7 +1631,7 @@ void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_
       }
       if (deferred) {
         k_rewind<<<1, 32, 0, st>>>(P);
-        launch_trace_queue<true>(thread_select(t.trace_threads), P, 0u, st);
+        launch_trace_queue<true>(thread_select(t.trace_threads), t.short_stack, P, 0u, st);
       }
     }
     if (inferred) check(cudaStreamWaitEvent(st, t.join_ev, 0), "inference join");

@@ -123,6 +123,9 @@ struct pfxt_trace {
   uint32_t trace_threads = 128;                // threads per block of the traversal kernels (64, 128, 256)
   bool split_shade = true;                     // shade in three kernels (hit, lights, BSDF) or one
   bool sort_rays = false;                      // group the extend queue of later bounces by ray
+  bool shadow_queue = true;                    // light slots' shadow rays through the connect queue
+  uint32_t short_stack = 0;                    // traversal stack entries per lane in shared memory (0 or 8)
+  uint64_t tune_key = 0;                       // hash of the scene's buffers, film and settings (autotune cache)
   float tuned_pass_ms = 0.0f;                  // the autotuner's measured pass time, 0 = not tuned
   uint32_t* d_error = nullptr;  // device error word
   uint32_t* d_counters = nullptr;  // ring of work-sharing counters (device scratch)

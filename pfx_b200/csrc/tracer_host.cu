@@ -3,12 +3,16 @@
 // sample counts (adaptive.rs:328).
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
 
+#include "cache.h"
 #include "tracer.h"
 
 namespace pfxt {
@@ -42,6 +46,9 @@ T* dev_alloc(pfxt_trace& t, size_t count, const char* what) {
 bool finite3(const float* p) { return std::isfinite(p[0]) && std::isfinite(p[1]) && std::isfinite(p[2]); }
 
 }  // namespace
+
+uint64_t fnv(uint64_t h, const void* data, size_t bytes);
+uint64_t tune_key_of(const pfxt_buffers& b, const Specialise& spec, uint32_t width, uint32_t height);
 
 void trace_init(pfxt_trace& t, const pfxt_buffers& b, const pfxt_scene& view, const pfxt_settings& s, uint32_t width,
                 uint32_t height) {
@@ -216,6 +223,7 @@ void trace_init(pfxt_trace& t, const pfxt_buffers& b, const pfxt_scene& view, co
   sp.sobol_length = sp.sobol ? b.sobol_length : 256u;
   sp.clamp_indirect = s.clamp_indirect;
   sp.filter_glossy = s.filter_glossy;
+  t.tune_key = tune_key_of(b, sp, width, height);
 
   light_trig_init(t);
 }
@@ -427,11 +435,14 @@ void trace_set_projection(pfxt_trace& t, uint32_t projection, const float ortho[
 void trace_set_tuning(pfxt_trace& t, const pfxt_tuning& k) {
   if (k.trace_threads != 64u && k.trace_threads != 128u && k.trace_threads != 256u)
     throw Invalid("trace_threads must be 64, 128 or 256");
+  if (k.short_stack != 0u && k.short_stack != 8u) throw Invalid("short_stack must be 0 or 8");
   t.trace_threads = k.trace_threads;
   t.sort_shading = k.sort_shading != 0u;
   t.use_graphs = k.graphs != 0u;
   t.split_shade = k.split_shade != 0u;
   t.sort_rays = k.sort_rays != 0u;
+  t.shadow_queue = k.shadow_queue != 0u;
+  t.short_stack = k.short_stack;
 }
 
 pfxt_tuning trace_get_tuning(const pfxt_trace& t) {
@@ -442,7 +453,38 @@ pfxt_tuning trace_get_tuning(const pfxt_trace& t) {
   k.split_shade = t.split_shade ? 1u : 0u;
   k.sort_rays = t.sort_rays ? 1u : 0u;
   k.pass_ms = t.tuned_pass_ms;
+  k.shadow_queue = t.shadow_queue ? 1u : 0u;
+  k.short_stack = t.short_stack;
+  k.from_cache = 0u;
   return k;
+}
+
+// FNV-1a style mixing of 8-byte words (and the bytes left over), continuing
+// from `h`: a fingerprint, not a format.
+uint64_t fnv(uint64_t h, const void* data, size_t bytes) {
+  const unsigned char* p = static_cast<const unsigned char*>(data);
+  size_t words = bytes / 8;
+  for (size_t i = 0; i < words; ++i) {
+    uint64_t w;
+    memcpy(&w, p + 8 * i, 8);
+    h = (h ^ w) * 0x100000001b3ull;
+  }
+  for (size_t i = 8 * words; i < bytes; ++i) h = (h ^ p[i]) * 0x100000001b3ull;
+  return h;
+}
+
+// The tuning key of a tracer: its scene's nodes, triangles, lights and
+// materials, its film and specialisation (set at creation; the attached cache's
+// settings are added when tuning).
+uint64_t tune_key_of(const pfxt_buffers& b, const Specialise& spec, uint32_t width, uint32_t height) {
+  uint64_t h = 0xcbf29ce484222325ull;
+  h = fnv(h, b.nodes, b.nodes_bytes);
+  h = fnv(h, b.triangles, b.triangles_bytes);
+  h = fnv(h, b.lights, b.lights_bytes);
+  h = fnv(h, b.materials, b.materials_bytes);
+  h = fnv(h, &spec, sizeof(spec));
+  uint32_t film[2] = {width, height};
+  return fnv(h, film, sizeof(film));
 }
 
 // Median device time of `passes - 1` one-sample passes after one warm-up pass.
@@ -466,24 +508,62 @@ static float time_passes(pfxt_trace& t, uint32_t passes, uint32_t& seed) {
   return ms[ms.size() / 2];
 }
 
+// Choices of earlier tunings in this process, by tuning key.
+std::mutex g_tuned_lock;
+std::map<uint64_t, pfxt_tuning> g_tuned;
+
 pfxt_tuning trace_autotune(pfxt_trace& t, uint32_t passes) {
   if (passes < 2 || passes > 64) throw Invalid("autotune: passes must be in 2..64");
+  uint64_t key = t.tune_key;
+  if (t.cache) key = fnv(fnv(key, "cache", 5), &t.cache->s, sizeof(t.cache->s));
+  {
+    std::lock_guard<std::mutex> hold(g_tuned_lock);
+    auto found = g_tuned.find(key);
+    if (found != g_tuned.end()) {
+      pfxt_tuning k = found->second;
+      k.graphs = t.use_graphs ? 1u : 0u;
+      trace_set_tuning(t, k);
+      t.tuned_pass_ms = k.pass_ms;
+      t.samples = 0;
+      k.from_cache = 1u;
+      return k;
+    }
+  }
+  // one choice at a time, the others held at the best so far
   pfxt_tuning best = trace_get_tuning(t);
-  best.pass_ms = INFINITY;
-  const bool graphs = t.use_graphs;
   uint32_t seed = 0x7e000000u;
+  trace_set_tuning(t, best);
+  best.pass_ms = time_passes(t, passes, seed);
+  auto consider = [&](pfxt_tuning k) {
+    trace_set_tuning(t, k);
+    k.pass_ms = time_passes(t, passes, seed);
+    if (k.pass_ms < best.pass_ms) best = k;
+  };
   for (uint32_t threads : {64u, 128u, 256u})
-    for (uint32_t sort : {1u, 0u})
-      for (uint32_t split : {1u, 0u})
-        for (uint32_t rays : {0u, 1u}) {
-          pfxt_tuning k{threads, sort, graphs ? 1u : 0u, split, rays, 0.0f};
-          trace_set_tuning(t, k);
-          k.pass_ms = time_passes(t, passes, seed);
-          if (k.pass_ms < best.pass_ms) best = k;
-        }
+    if (threads != best.trace_threads) {
+      pfxt_tuning k = best;
+      k.trace_threads = threads;
+      consider(k);
+    }
+  for (int knob = 0; knob < 5; ++knob) {
+    pfxt_tuning k = best;
+    switch (knob) {
+      case 0: k.sort_shading ^= 1u; break;
+      case 1: k.split_shade ^= 1u; break;
+      case 2: k.sort_rays ^= 1u; break;
+      case 3: k.shadow_queue ^= 1u; break;
+      default: k.short_stack = k.short_stack ? 0u : 8u; break;
+    }
+    consider(k);
+  }
   trace_set_tuning(t, best);
   t.tuned_pass_ms = best.pass_ms;
   t.samples = 0;  // the trial passes are not part of the image
+  best.from_cache = 0u;
+  {
+    std::lock_guard<std::mutex> hold(g_tuned_lock);
+    g_tuned[key] = best;
+  }
   return best;
 }
 

@@ -222,15 +222,13 @@ struct LaneStack {
   uint32_t* sh_ref;
   float* sh_near;
   uint32_t lanes;
-  uint32_t lref[REF_STACK - SHORT];
-  float lnear[REF_STACK - SHORT];
+  uint2 entry[REF_STACK - SHORT];  // (ref, near bits) pairs past the shared-memory top
   __device__ __forceinline__ void put(int k, uint32_t r, float n) {
     if (k < SHORT) {
       sh_ref[k * lanes] = r;
       sh_near[k * lanes] = n;
     } else {
-      lref[k - SHORT] = r;
-      lnear[k - SHORT] = n;
+      entry[k - SHORT] = make_uint2(r, __float_as_uint(n));
     }
   }
   __device__ __forceinline__ void get(int k, uint32_t& r, float& n) const {
@@ -238,8 +236,9 @@ struct LaneStack {
       r = sh_ref[k * lanes];
       n = sh_near[k * lanes];
     } else {
-      r = lref[k - SHORT];
-      n = lnear[k - SHORT];
+      uint2 e = entry[k - SHORT];
+      r = e.x;
+      n = __uint_as_float(e.y);
     }
   }
 };

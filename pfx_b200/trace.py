@@ -461,19 +461,26 @@ class Trace:
         k = abi.Tuning()
         check(self._lib.pfxt_get_tuning(self._h, C.byref(k)))
         return {"trace_threads": k.trace_threads, "sort_shading": bool(k.sort_shading), "graphs": bool(k.graphs),
-                "split_shade": bool(k.split_shade), "sort_rays": bool(k.sort_rays), "pass_ms": float(k.pass_ms)}
+                "split_shade": bool(k.split_shade), "sort_rays": bool(k.sort_rays), "pass_ms": float(k.pass_ms),
+                "shadow_queue": bool(k.shadow_queue), "short_stack": int(k.short_stack),
+                "from_cache": bool(k.from_cache)}
 
     def set_tuning(self, trace_threads: int = 128, sort_shading: bool = True, graphs: bool = True,
-                   split_shade: bool = True, sort_rays: bool = False) -> None:
-        k = abi.Tuning(trace_threads, int(sort_shading), int(graphs), int(split_shade), int(sort_rays), 0.0)
+                   split_shade: bool = True, sort_rays: bool = False, shadow_queue: bool = True,
+                   short_stack: int = 0) -> None:
+        k = abi.Tuning(trace_threads, int(sort_shading), int(graphs), int(split_shade), int(sort_rays), 0.0,
+                       int(shadow_queue), int(short_stack), 0)
         check(self._lib.pfxt_set_tuning(self._h, C.byref(k)))
 
     def autotune(self, passes: int = 3) -> dict:
-        """Time passes of this scene under each launch configuration and keep the
-        fastest (restarts the accumulation)."""
+        """Time passes of this scene under each launch choice and keep the
+        fastest, or take an earlier tuning of the same scene (restarts the
+        accumulation)."""
         k = abi.Tuning()
         check(self._lib.pfxt_autotune(self._h, passes, C.byref(k)))
-        return self.tuning()
+        out = self.tuning()
+        out["from_cache"] = bool(k.from_cache)
+        return out
 
     def set_cache(self, cache) -> None:
         """Attach a pfx_b200.cache.RadianceCache (None detaches): paths then end

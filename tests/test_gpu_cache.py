@@ -16,6 +16,11 @@ pytestmark = pytest.mark.gpu
 
 SMALL = CacheSettings(log2_entries=12, base_resolution=4, max_resolution=256, batch=1024, steps=1, seed=3,
                       lo=(-1.0, -2.0, -3.0), hi=(2.0, 1.0, 4.0))
+# the bench's cache: 2^19 entries per level, resolutions 16..2048 (hashed fine
+# levels), with a smaller batch so the FP64 oracle finishes in seconds
+FULL = CacheSettings(log2_entries=19, base_resolution=16, max_resolution=2048, batch=2048, steps=1, seed=4,
+                     lo=(-15.0, 0.0, -15.0), hi=(15.0, 10.0, 15.0))
+CONFIGS = pytest.mark.parametrize("settings", [SMALL, FULL], ids=["reduced", "bench"])
 
 
 def make(settings, table_scale=1.0, seed=5):
@@ -52,9 +57,10 @@ def test_encoding_geometry(gpu):
     assert dense & 1 and not (dense >> 15) & 1  # both kinds of level are exercised
 
 
-def test_inference_matches_oracle(gpu):
-    c, enc, mlp, table, rng = make(SMALL)
-    q = random_queries(1000, rng, SMALL.lo, SMALL.hi)  # a ragged last tile
+@CONFIGS
+def test_inference_matches_oracle(gpu, settings):
+    c, enc, mlp, table, rng = make(settings)
+    q = random_queries(3000, rng, settings.lo, settings.hi)  # a ragged last tile
     got = c.infer(q)
     want = oc.infer(mlp, table, enc, q)
     assert np.isfinite(got).all()
@@ -65,9 +71,10 @@ def test_inference_matches_oracle(gpu):
     assert np.isfinite(c.infer(q2)).all()
 
 
-def test_gradients_match_oracle(gpu):
-    c, enc, mlp, table, rng = make(SMALL)
-    r = records(rng, 512, SMALL)
+@CONFIGS
+def test_gradients_match_oracle(gpu, settings):
+    c, enc, mlp, table, rng = make(settings)
+    r = records(rng, 2048, settings)
     g_mlp, g_tab, loss = c.gradients(r)
     w_mlp, w_tab, w_loss = oc.gradients(mlp, table, enc, r)
     assert abs(loss - w_loss) <= 1e-3 * w_loss
@@ -81,8 +88,9 @@ def test_gradients_match_oracle(gpu):
     assert np.all(g_tab[w_tab == 0.0] == 0.0)
 
 
-def test_adam_step_matches_oracle(gpu):
-    s = CacheSettings(**{**SMALL.__dict__, "epsilon": 1e-4, "learning_rate": 1e-3})
+@CONFIGS
+def test_adam_step_matches_oracle(gpu, settings):
+    s = CacheSettings(**{**settings.__dict__, "epsilon": 1e-4, "learning_rate": 1e-3})
     c, enc, mlp, table, rng = make(s)
     r = records(rng, s.batch, s)
     c.train(r)

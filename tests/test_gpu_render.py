@@ -152,19 +152,30 @@ def test_autotune_keeps_the_image(gpu):
     a = Trace(w.scene, w.settings, w.width, w.height)
     b = Trace(w.scene, w.settings, w.width, w.height)
     k = a.autotune(passes=2)
-    assert k["trace_threads"] in (64, 128, 256) and k["pass_ms"] > 0
+    assert k["trace_threads"] in (64, 128, 256) and k["pass_ms"] > 0 and k["short_stack"] in (0, 8)
     assert a.samples() == 0  # the trial passes are not part of the image
-    for threads in (64, 256):
-        b.set_tuning(trace_threads=threads, sort_shading=threads == 64, graphs=threads == 256)
+    images = []
+    for threads, queue, short in ((64, True, 8), (256, False, 0), (128, False, 8)):
+        b.set_tuning(trace_threads=threads, sort_shading=threads == 64, graphs=threads == 256, shadow_queue=queue,
+                     short_stack=short)
         b.set_camera(w.scene.camera)
         b.sample(2, 5)
-        if threads == 64:
-            first = b.read_accum()
+        images.append(b.read_accum())
     a.sample(2, 5)
-    assert np.array_equal(a.read_accum(), b.read_accum())
-    assert np.array_equal(first, b.read_accum())
+    for img in images:  # block size, sorts, shadow queue and shared stack change no value
+        assert np.array_equal(a.read_accum(), img)
     with pytest.raises(Exception):
         b.set_tuning(trace_threads=96)
+    with pytest.raises(Exception):
+        b.set_tuning(short_stack=4)
+    # the same scene, film and settings again: the choice comes from the first tuning
+    c = Trace(w.scene, w.settings, w.width, w.height)
+    again = c.autotune(passes=2)
+    assert again["from_cache"] and not k["from_cache"]
+    assert {x: again[x] for x in ("trace_threads", "short_stack", "shadow_queue")} == \
+        {x: k[x] for x in ("trace_threads", "short_stack", "shadow_queue")}
+    other = Trace(w.scene, w.settings, w.width + 8, w.height)  # another film: tuned anew
+    assert not other.autotune(passes=2)["from_cache"]
 
 
 def test_furnace_and_determinism(gpu):
