@@ -372,6 +372,23 @@ def cpu_baseline(w, budget_s=12.0):
             "sample": f"{ww}x{wh} centre window of the 4K frame, {spp} x 1 spp, oracle path tracer on all host threads"}
 
 
+def clip_line(frames: int):
+    """The batched clip workload (1280x720, 16 spp per frame, shots over rooms
+    of 10k/100k/400k/1M triangles, the camera moving every frame): `frames`
+    frames split evenly over the four shots, device time of the sampling calls."""
+    from pfx_b200 import clip
+    shots = clip.clip_shots(frames, (1280, 720))
+    res = clip.render(shots, spp=16)
+    device_s = sum(r.device_s for r in res)
+    rays = sum(r.rays for r in res)
+    return {"workload": f"clip: 1280x720, 16 spp per frame, {frames} frames over shots of "
+                        f"{', '.join(str(r.triangles) for r in res)} triangles (the 240-frame clip's shots, "
+                        f"{frames // len(res)} frames each)",
+            "frames_per_s": frames / device_s, "Mrays_s": rays / device_s / 1e6, "device_s": device_s,
+            "ms_per_frame": [round(1e3 * r.device_s / r.frames, 2) for r in res],
+            "graph_captures": [r.graph_captures for r in res]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -388,6 +405,7 @@ def main():
     ap.add_argument("--no-relmse", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--clip-frames", type=int, default=48, help="frames of the clip line (0: none)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -497,6 +515,8 @@ def main():
                 "plain_curve": [(n, round(e, 5)) for n, e in curve[:: max(1, len(curve) // 12)] + curve[-1:]],
                 "cached_curve": [(n, t, round(e, 5)) for n, t, e in
                                  curve_c[:: max(1, len(curve_c) // 12)] + curve_c[-1:]]}
+        if world == 1 and args.clip_frames > 0:
+            line["clip"] = clip_line(args.clip_frames)
         if world == 1 and not args.no_cpu_baseline:  # the host baseline is timed at N=1 only
             line["cpu_baseline"] = cpu_baseline(w)
         print(json.dumps(line))

@@ -36,6 +36,7 @@ SOURCES = [
     ("traverse.cu", EXACT),
     ("tracer.cu", EXACT),
     ("noalloc.cu", EXACT),
+    ("bvh_gpu.cu", EXACT),
     ("cache.cu", EXACT),
 ]
 

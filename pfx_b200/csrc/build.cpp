@@ -5,6 +5,7 @@
 // arithmetic in the reference's own order, so the packed bytes are the ones the
 // reference would upload for the same scene.
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <cmath>
 #include <cstring>
@@ -199,19 +200,46 @@ struct BvhBuilder {
 struct Bvh {
   std::vector<GpuNode> nodes;
   std::vector<uint32_t> order;
+  bool gpu = false;  // built on the GPU
 };
 
 Bvh bvh_over(const std::vector<Bounds>& boxes, Leaves leaves) {
   BvhBuilder b(boxes, leaves);
-  return Bvh{std::move(b.nodes), std::move(b.order)};
+  return Bvh{std::move(b.nodes), std::move(b.order), false};
 }
+
+// Triangle BVHs of at least this many triangles are built on the GPU when one
+// is present; smaller ones take longer to launch than to build on the host.
+constexpr size_t GPU_BVH_MIN = 1u << 16;
+std::atomic<int> g_gpu_bvh{1};
 
 Bvh bvh_triangles(const pfxt_triangle* tris, size_t n) {  // bvh.rs:95-105
   std::vector<Bounds> boxes(n);
+  // no -0.0 and no NaN: the GPU's minima and maxima are then order-free
+  auto plain_value = [](float v) { return !std::isnan(v) && !(v == 0.0f && std::signbit(v)); };
+  bool plain = true;
   for (size_t i = 0; i < n; ++i) {
     Bounds b = Bounds::empty();
     for (int c = 0; c < 3; ++c) b.point(tris[i].v[c]);
     boxes[i] = b;
+    for (int k = 0; k < 3; ++k) plain = plain && plain_value(b.lo[k]) && plain_value(b.hi[k]);
+  }
+  if (plain && n >= GPU_BVH_MIN && n <= 0xffffffffu && g_gpu_bvh.load() && gpu_bvh_available()) {
+    try {
+      std::vector<float> flat(6 * n);
+      for (size_t i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+          flat[6 * i + k] = boxes[i].lo[k];
+          flat[6 * i + 3 + k] = boxes[i].hi[k];
+        }
+      Bvh out;
+      gpu_bvh_build(flat.data(), (uint32_t)n, (uint32_t)TRIANGLE_LEAVES.size, (uint32_t)TRIANGLE_LEAVES.most,
+                    out.nodes, out.order);
+      out.gpu = true;
+      return out;
+    } catch (const std::exception&) {
+      // the host build gives the same bytes
+    }
   }
   return bvh_over(boxes, TRIANGLE_LEAVES);
 }
@@ -1220,6 +1248,7 @@ SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings) 
 
   // ---- levels::lay (levels.rs:225-383)
   Bvh world_bvh = bvh_triangles(scene.triangles, scene.triangle_count);
+  if (world_bvh.gpu) out->gpu_builds += 1;
   struct Mesh {
     uint32_t source;
     std::vector<pfxt_triangle> triangles;  // BVH order
@@ -1300,6 +1329,7 @@ SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings) 
         mesh_index = (size_t)found;
       } else {
         Bvh bvh = bvh_triangles(src.triangles, src.count);
+        if (bvh.gpu) out->gpu_builds += 1;
         Mesh mesh;
         mesh.source = in.mesh;
         mesh.bounds = Bounds::empty();
@@ -1532,6 +1562,8 @@ SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings) 
   out->max_depth = out->nodes.empty() ? 0 : std::max<uint32_t>(1u, stack_need(out->nodes, 0, 0));
   return out.release();
 }
+
+int set_gpu_bvh(int on) { return g_gpu_bvh.exchange(on ? 1 : 0); }
 
 // The light tree's selection on its own, for tests: sorts (key, index) pairs
 // as select_nth_unstable_by(index, total_cmp on the key) leaves them and

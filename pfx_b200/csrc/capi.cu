@@ -452,6 +452,15 @@ int pfxt_debug_select_nth(const float* keys, uint32_t n, uint32_t index, int32_t
   });
 }
 
+/* Large triangle BVHs on the GPU (1, the default, when a device is present) or
+ * always on the host (0); returns the previous setting.  The bytes are the same. */
+int pfxt_debug_gpu_bvh(int32_t on) { return set_gpu_bvh(on); }
+
+/* How many of a built scene's bottom-level BVHs were built on the GPU. */
+uint32_t pfxt_debug_scene_gpu_builds(const pfxt_scene_blobs* b) {
+  return b && b->blobs ? b->blobs->gpu_builds : 0u;
+}
+
 /* How many sampling passes have been captured as graphs so far. */
 uint32_t pfxt_debug_graph_captures(pfxt_trace* t) { return t ? t->graph_captures : 0u; }
 

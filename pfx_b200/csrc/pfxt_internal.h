@@ -48,6 +48,7 @@ struct SceneBlobs {
   // Builds (gpu.rs:400-403): bottom-level BVHs built (the world's and one per
   // distinct mesh) and top-level BVHs laid (1 with instances, +1 per move).
   uint32_t bottom_builds = 0, top_builds = 0;
+  uint32_t gpu_builds = 0;  // bottom-level BVHs built on the GPU
 };
 
 SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings);
@@ -57,6 +58,15 @@ SceneBlobs* build_scene(const pfxt_scene& scene, const pfxt_settings& settings);
 // moved instances' surface records, their emitters and the top-level BVH in
 // place (no buffer changes size) and returns whether anything moved.
 bool move_instances(SceneBlobs& blobs, const float* transforms, size_t count);
+
+// The binned-SAH BVH build on the GPU (bvh_gpu.cu): the host build's nodes and
+// order byte for byte, for boxes with no NaN and no -0.0 coordinate.
+bool gpu_bvh_available();
+void gpu_bvh_build(const float* boxes, uint32_t n, uint32_t leaf, uint32_t most, std::vector<GpuNode>& nodes,
+                   std::vector<uint32_t>& order);
+// Whether large triangle BVHs are built on the GPU when one is present (1, the
+// default) or always on the host (0); returns the previous setting.
+int set_gpu_bvh(int on);
 
 // slice::select_nth_unstable_by as the light tree runs it, on bare keys (tests).
 void select_nth_for_test(const float* keys, uint32_t n, uint32_t index, int rounds, uint32_t* order);

@@ -57,3 +57,43 @@ def test_image_of_a_window_of_the_full_4k_room(gpu, room, sampler):
     got, exact = render_both(w, 2, [31, 32], window=((3840, 2160), (1700, 1300)))
     assert got[..., :3].mean() > 0.0
     assert exact > 0.99
+
+
+@pytest.mark.parametrize("name", ["room_4k", "instanced_1080", "clip_1m"])
+def test_gpu_bvh_build_equals_the_host_build(gpu, room, name):
+    """The binned-SAH build on the GPU (bvh_gpu.cu) gives the host build's and
+    the oracle's nodes and triangle order byte for byte (bvh.rs:95-266), and
+    the whole packed scene is unchanged."""
+    import time
+
+    from pfx_b200 import abi, clip
+    from pfx_b200.trace import SceneBuffers
+    if name == "room_4k":
+        w = room
+    elif name == "instanced_1080":
+        w = synth.instanced_1080()
+    else:
+        w = clip.room_shot(1_000_000, 9).workload
+    lib = abi.load()
+    t0 = time.perf_counter()
+    gpu = SceneBuffers(w.scene, w.settings)
+    gpu_s = time.perf_counter() - t0
+    lib.pfxt_debug_gpu_bvh(0)
+    try:
+        t0 = time.perf_counter()
+        host = SceneBuffers(w.scene, w.settings)
+        host_s = time.perf_counter() - t0
+    finally:
+        lib.pfxt_debug_gpu_bvh(1)
+    big = len(w.scene.triangles) >= (1 << 16)
+    assert lib.pfxt_debug_scene_gpu_builds(gpu._h) == (1 if big else 0)
+    assert lib.pfxt_debug_scene_gpu_builds(host._h) == 0
+    for blob in ("nodes", "triangles", "uv", "surfaces", "emitters", "lights"):
+        assert np.array_equal(gpu.array(blob), host.array(blob)), blob
+    assert np.array_equal(gpu.order(), host.order())
+    if big:
+        nodes, order = oracle.bvh_build(w.scene.triangles["v"])
+        if not len(w.scene.instances):
+            assert np.array_equal(gpu.array("nodes"), nodes)
+        assert np.array_equal(gpu.order(), order)
+        print(f"{name}: scene build {gpu_s:.2f} s with the GPU BVH, {host_s:.2f} s on the host")
