@@ -201,10 +201,17 @@ __device__ __forceinline__ void sync_tc() {
   umma::fence_after();
 }
 
-__device__ __forceinline__ void copy_weights(uint8_t* sw, const uint16_t* __restrict__ weights) {
-  const uint4* src = reinterpret_cast<const uint4*>(weights);
-  uint4* dst = reinterpret_cast<uint4*>(sw);
-  for (uint32_t k = threadIdx.x; k < 18432u / 16u; k += blockDim.x) dst[k] = __ldg(src + k);
+// The 18 KB of BF16 weights into shared memory with one bulk copy (TMA), the
+// barrier `wbar` initialised for one arrival: thread 0 expects the bytes and
+// issues the copy, every thread waits.  False when the wait ran out (the copy
+// then counts as not finished; the kernel reports it and stops).
+constexpr uint32_t WEIGHT_BYTES = 18432;
+__device__ __forceinline__ bool load_weights(uint8_t* sw, const uint16_t* __restrict__ weights, uint32_t wbar) {
+  if (threadIdx.x == 0) {
+    umma::mbar_expect_tx(wbar, WEIGHT_BYTES);
+    umma::bulk_load(umma::smem_addr(sw), weights, WEIGHT_BYTES, wbar);
+  }
+  return __syncthreads_and(umma::mbar_wait(wbar, 0u, DRAIN_LIMIT));
 }
 
 // End of a tensor-core kernel: after a wait that ran out, flag the error and
@@ -246,9 +253,16 @@ __global__ void __launch_bounds__(128, 4)
   uint32_t* slot = reinterpret_cast<uint32_t*>(smem + I_CTRL + 8);
   const uint32_t a_x = umma::smem_addr(smem + I_X), a_h1 = umma::smem_addr(smem + I_H1),
                  a_h2 = umma::smem_addr(smem + I_H2), a_w = umma::smem_addr(smem + I_W);
-  const uint32_t mb = umma::smem_addr(mbar);
-  copy_weights(smem + I_W, weights);
-  if (tid == 0) umma::mbar_init(mb, 1);
+  const uint32_t mb = umma::smem_addr(mbar), wb = umma::smem_addr(smem + I_CTRL + 16);
+  if (tid == 0) {
+    umma::mbar_init(mb, 1);
+    umma::mbar_init(wb, 1);
+  }
+  __syncthreads();
+  if (!load_weights(smem + I_W, weights, wb)) {
+    if (tid == 0) atomicOr(error, ERR_WAIT | ERR_DRAIN);
+    return;  // no TMEM allocated yet
+  }
   if (warp == 0) umma::tmem_alloc(slot, I_TMEM);
   umma::fence_async_smem();
   sync_tc();
@@ -337,9 +351,16 @@ __global__ void __launch_bounds__(128, 1)
                  a_dh1 = umma::smem_addr(smem + T_DH1), a_x = umma::smem_addr(smem + T_X),
                  a_h1 = umma::smem_addr(smem + T_H1), a_h2 = umma::smem_addr(smem + T_H2),
                  a_w = umma::smem_addr(smem + T_W);
-  const uint32_t mb = umma::smem_addr(mbar);
-  copy_weights(smem + T_W, weights);
-  if (tid == 0) umma::mbar_init(mb, 1);
+  const uint32_t mb = umma::smem_addr(mbar), wb = umma::smem_addr(smem + T_CTRL + 16);
+  if (tid == 0) {
+    umma::mbar_init(mb, 1);
+    umma::mbar_init(wb, 1);
+  }
+  __syncthreads();
+  if (!load_weights(smem + T_W, weights, wb)) {
+    if (tid == 0) atomicOr(error, ERR_WAIT | ERR_DRAIN);
+    return;  // no TMEM allocated yet
+  }
   if (warp == 0) umma::tmem_alloc(slot, 512);
   umma::fence_async_smem();
   sync_tc();

@@ -1,7 +1,8 @@
 // Blackwell (sm_100a) tensor-core building blocks for the radiance cache's
 // MLP: tcgen05.mma with operands in shared memory and the accumulator in
 // tensor memory (TMEM), TMEM allocation, completion through an mbarrier and
-// TMEM -> register loads.  Inline PTX only; one CTA, no clusters, no TMA.
+// TMEM -> register loads, and the untiled bulk copy (TMA) that stages the
+// weights.  Inline PTX only; one CTA, no clusters, no multicast.
 //
 // Operand tiles use the no-swizzle canonical layout: an R x C bf16 tile is
 // stored as 8-row x 16-byte core matrices (128 contiguous bytes each), core
@@ -63,6 +64,20 @@ __device__ __forceinline__ void commit(uint32_t mbar) {
 __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// One arrival that also expects `bytes` of asynchronous copies on the barrier.
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// Untiled bulk copy (TMA) of `bytes` from global memory into this CTA's shared
+// memory, completing on `mbar`: both addresses 16-byte aligned, `bytes` a
+// multiple of 16.  No multicast: the copy lands in the issuing CTA only.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
 }
 
 // Bounded wait for the completion of phase `parity`; false when the limit ran out.
