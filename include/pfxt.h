@@ -407,6 +407,8 @@ typedef struct pfxt_tuning {
                            * 0 or 8 (0) */
   uint32_t from_cache;    /* set by pfxt_autotune: 1 when the choice came from an earlier tuning of the same
                            * scene, film and settings in this process */
+  uint32_t slot_kernels;  /* with the shadow queue and three shade kernels: the light slots one launch per slot
+                           * kind, slot after slot (1), or every slot of a path in one kernel (0) (1) */
 } pfxt_tuning;
 
 int pfxt_get_tuning(pfxt_trace* trace, pfxt_tuning* out);

@@ -258,6 +258,7 @@ pub struct PfxtTuning {
     pub shadow_queue: u32,
     pub short_stack: u32,
     pub from_cache: u32,
+    pub slot_kernels: u32,
 }
 
 #[repr(C)]

@@ -131,7 +131,8 @@ class Keeper(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("trace_threads", C.c_uint32), ("sort_shading", C.c_uint32), ("graphs", C.c_uint32),
                 ("split_shade", C.c_uint32), ("sort_rays", C.c_uint32), ("pass_ms", C.c_float),
-                ("shadow_queue", C.c_uint32), ("short_stack", C.c_uint32), ("from_cache", C.c_uint32)]
+                ("shadow_queue", C.c_uint32), ("short_stack", C.c_uint32), ("from_cache", C.c_uint32),
+                ("slot_kernels", C.c_uint32)]
 
 
 class CacheSettings(C.Structure):

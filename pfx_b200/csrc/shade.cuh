@@ -22,7 +22,9 @@ namespace pfxt {
 constexpr float SH_PI = 0x1.921fb6p+1f;
 
 // Heavy helpers are kept out of line (one copy each in the shading kernel).
+#ifndef SH_CALL
 #define SH_CALL static __device__ __noinline__
+#endif
 // Small helpers: out of line as well unless a build inlines them.
 #ifndef SH_SMALL
 #define SH_SMALL SH_CALL

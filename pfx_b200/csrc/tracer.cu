@@ -92,6 +92,8 @@ struct Wave {
   // queue items the traversal handed over to the IEEE walk (rays that are not
   // bounded), counted at counters[13] (extend) and counters[14] (connect)
   uint32_t* retry;
+  // the light tree's pick of each path that scatters (row, pmf), by lit index
+  float2* pick;
 };
 
 // The radiance cache as the wave sees it (all null/zero when none is attached).
@@ -1002,18 +1004,21 @@ __global__ void __launch_bounds__(kThreads, SHADE_LIGHTS_MIN_BLOCKS) k_shade_lig
     uint32_t pixel = __float_as_uint(rs.w);
     uint32_t px = pixel % P.width + P.f.window[2], py = pixel / P.width + P.f.window[3];
     Rng r{hash_iqnt2d(px, py) ^ pass_seed(P), pass_accum(P) + P.sample, 16u * (bounce + 1u)};
-    const Surface S = load_surface_record(P.w.surf + (size_t)i * 9u);
-    const Shaded& s = S.s;
-    const v3 p = S.p, geometric = S.geometric;
-    m3 transform = basis(S.nn);
-    v3 wo = mulmtv(transform, neg3(d));
-    v3 origin = spawn_point(p, S.nn, o, S.t);
+    // The surface's geometry is held across the slots; its material record is
+    // read again where a slot evaluates the BSDF, so that it is not live across
+    // the light-tree descent (fewer values to keep in local memory there).
+    const float4* record = P.w.surf + (size_t)i * 9u;
+    const float4 g0 = record[0], g1 = record[1], g2 = record[2];
+    const v3 p = mk3(g0.x, g0.y, g0.z), nn = mk3(g1.x, g1.y, g1.z), geometric = mk3(g2.x, g2.y, g2.z);
+    const float roughness = g2.w;
+    m3 transform = basis(nn);
+    v3 origin = spawn_point(p, nn, o, g0.w);
     uint32_t pending = 0u;
     for (uint32_t k = 0u; k < P.slots; ++k) {
       float4 u;  // the slot's Sobol sample, looked up once the slot is known to be live
       v3 local = mk3(0.0f, 0.0f, 1.0f), direction = mk3(0.0f, 0.0f, 1.0f), strength = splat3(0.0f);
       float limit = 1e19f, pdf = 0.0f;
-      float lit_roughness = s.roughness;
+      float lit_roughness = roughness;
       if (k == 0u) {
         if (P.f.sun_color[3] <= 0.0f) continue;
         u = sobol4(V, sp, r, light_dim(k));
@@ -1068,8 +1073,11 @@ __global__ void __launch_bounds__(kThreads, SHADE_LIGHTS_MIN_BLOCKS) k_shade_lig
         strength = picked.scale;
         pdf = picked.pdf;
         limit = picked.limit;
-        lit_roughness = fmax_(s.roughness, picked.roughness);
+        lit_roughness = fmax_(roughness, picked.roughness);
       }
+      const Surface S = load_surface_record(record);
+      const Shaded& s = S.s;
+      const v3 wo = mulmtv(transform, neg3(d));
       if (pdf > 0.0f) {
         float bsdf = bsdf_pdf(s, wo, local);
         if (k == 1u) {
@@ -1101,6 +1109,172 @@ __global__ void __launch_bounds__(kThreads, SHADE_LIGHTS_MIN_BLOCKS) k_shade_lig
     P.w.ray_d[i] = make_float4(d.x, d.y, d.z, __uint_as_float(flags | (pending << F_PEND)));
     P.w.thr[i] = make_float4(throughput.x, throughput.y, throughput.z, __uint_as_float(state));
     if (!DEFERRED) P.w.res[i] = make_float4(result.x, result.y, result.z, __uint_as_float(pixel));
+  }
+}
+
+// ------------------------------------------------------------------ light slots, one kind per launch
+// The light slots of the paths that scatter, one launch per live slot in slot
+// order (sun, sky, emissive triangles, each looped light, the light tree)
+// instead of every slot of a path in one thread.  A launch holds the state of
+// one slot kind only, which fits its registers, where the kernel of all slots
+// keeps the union of every kind's state in local memory.  The values are the
+// same: a path's draws come in the same order (slot k's after slot k-1's; the
+// pcg state travels in thr.w between launches), and the k-th live slot of a
+// path writes shadow entry i * cap + pending, the pending count travelling in
+// the flag word.  The tree's slot is two launches: the descent (k_tree_pick,
+// one (row, pmf) per path), then its light's candidate and the BSDF.
+constexpr int SLOT_SUN = 0, SLOT_SKY = 1, SLOT_EMITTER = 2, SLOT_LOOPED = 3, SLOT_TREE = 4;
+
+#ifndef SLOT_MIN_BLOCKS
+#define SLOT_MIN_BLOCKS 8
+#endif
+#ifndef PICK_MIN_BLOCKS
+#define PICK_MIN_BLOCKS 12
+#endif
+
+__device__ __forceinline__ Rng slot_rng(const Pass& P, uint32_t pixel) {
+  uint32_t px = pixel % P.width + P.f.window[2], py = pixel / P.width + P.f.window[3];
+  return Rng{hash_iqnt2d(px, py) ^ pass_seed(P), pass_accum(P) + P.sample, 16u * (P.bounce + 1u)};
+}
+
+// The light tree's descent for every scattering path (slot k of tree_pick's
+// caller in k_shade_lights): the pick (light row, pmf) at P.w.pick[qi].
+__global__ void __launch_bounds__(kThreads, PICK_MIN_BLOCKS) k_tree_pick(const __grid_constant__ Pass P, uint32_t k) {
+  const uint32_t n = P.w.counters[12];
+  const Specialise& sp = P.sp;
+  const ShadeView& V = P.v;
+  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n; qi += gridDim.x * blockDim.x) {
+    const uint32_t i = P.w.lit[qi];
+    const float4* record = P.w.surf + (size_t)i * 9u;
+    const float4 g0 = record[0], g1 = record[1];
+    uint32_t state = __float_as_uint(reinterpret_cast<const float*>(P.w.thr + i)[3]);
+    float start;
+    if (sp.sobol) {
+      start = sobol4(V, sp, slot_rng(P, __float_as_uint(reinterpret_cast<const float*>(P.w.res + i)[3])),
+                     light_dim(k)).z;
+    } else {
+      start = random01(state);
+      reinterpret_cast<float*>(P.w.thr + i)[3] = __uint_as_float(state);
+    }
+    P.w.pick[qi] = tree_pick(V, P.light_rows, mk3(g0.x, g0.y, g0.z), mk3(g1.x, g1.y, g1.z), start, nullptr);
+  }
+}
+
+// Slot k of kind KIND for every scattering path: the body of k_shade_lights'
+// slot loop for that kind, with the deferred shadow entry.
+template <int KIND>
+__global__ void __launch_bounds__(kThreads, SLOT_MIN_BLOCKS) k_light_slot(const __grid_constant__ Pass P, uint32_t k) {
+  const uint32_t n = P.w.counters[12];
+  const uint32_t bounce = P.bounce;
+  const Specialise& sp = P.sp;
+  const ShadeView& V = P.v;
+  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n; qi += gridDim.x * blockDim.x) {
+    const uint32_t i = P.w.lit[qi];
+    float2 pk = make_float2(0.0f, 0.0f);
+    if (KIND == SLOT_TREE) {
+      pk = P.w.pick[qi];
+      if (!(pk.y > 0.0f)) continue;  // no light picked: the slot adds nothing and draws nothing more
+    }
+    const float4 rd = P.w.ray_d[i], th = P.w.thr[i];
+    const v3 d = mk3(rd.x, rd.y, rd.z);
+    const uint32_t flags = __float_as_uint(rd.w);
+    uint32_t state = __float_as_uint(th.w);
+    const uint32_t state_in = state;
+    const float4* record = P.w.surf + (size_t)i * 9u;
+    const float4 g0 = record[0], g1 = record[1], g2 = record[2];
+    const v3 p = mk3(g0.x, g0.y, g0.z), nn = mk3(g1.x, g1.y, g1.z);
+    const m3 transform = basis(nn);
+    float4 u = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (sp.sobol) u = sobol4(V, sp, slot_rng(P, __float_as_uint(reinterpret_cast<const float*>(P.w.res + i)[3])),
+                             light_dim(k));
+    v3 local = mk3(0.0f, 0.0f, 1.0f), direction = mk3(0.0f, 0.0f, 1.0f), strength = splat3(0.0f);
+    v3 origin = p;
+    float limit = 1e19f, pdf = 0.0f;
+    float lit_roughness = g2.w;
+    bool live = true;
+    if (KIND == SLOT_SUN) {
+      direction = normalize3(mk3(P.f.sun_dir[0], P.f.sun_dir[1], P.f.sun_dir[2]));
+      if (P.f.sun_dir[3] < 1.0f) {
+        float height = 1.0f - rnd(sp, state, u.x) * (1.0f - P.f.sun_dir[3]);
+        float radius = sqrtf(fmax_(0.0f, 1.0f - height * height));
+        float phi = 2.0f * SH_PI * rnd(sp, state, u.y);
+        m3 orient = basis(direction);
+        direction = normalize3(mulmv(orient, mk3(radius * cos_(phi), radius * sin_(phi), height)));
+      }
+      local = mulmtv(transform, direction);
+      live = local.z > 0.0f;
+      strength = scl3(mk3(P.f.sun_color[0], P.f.sun_color[1], P.f.sun_color[2]), P.f.sun_color[3] * 1.0f);
+      const float4 ro = P.w.ray_o[i];
+      origin = spawn_point(p, nn, mk3(ro.x, ro.y, ro.z), g0.w);
+    } else if (KIND == SLOT_SKY) {
+      float ux = rnd(sp, state, u.x);
+      float uy = rnd(sp, state, u.y);
+      if (V.sky_radiance[0] == 0.0f && V.sky_radiance[1] == 0.0f && V.sky_radiance[2] == 0.0f) {
+        live = false;
+      } else {
+        SkySample light = sky_sample(V, ux, uy);
+        direction = light.direction;
+        local = mulmtv(transform, direction);
+        strength = scl3(sky_radiance(V), 1.0f);
+        pdf = light.pdf;
+        live = local.z > 0.0f && pdf > 0.0f;
+        const float4 ro = P.w.ray_o[i];
+        origin = spawn_point(p, nn, mk3(ro.x, ro.y, ro.z), g0.w);
+      }
+    } else {
+      const float4 ro = P.w.ray_o[i];
+      origin = spawn_point(p, nn, mk3(ro.x, ro.y, ro.z), g0.w);
+      Candidate picked;
+      if (KIND == SLOT_TREE) {
+        picked = light_candidate(sp, V, f2u(pk.x), transform, p, origin, mk3(g2.x, g2.y, g2.z), state, u);
+        picked.scale = divs3(picked.scale, pk.y);
+      } else if (KIND == SLOT_LOOPED) {
+        picked = light_candidate(sp, V, k - 3u, transform, p, origin, mk3(g2.x, g2.y, g2.z), state, u);
+      } else {
+        picked = emitter_candidate(V, sp, transform, p, origin, state, u);
+      }
+      live = !(picked.limit < 0.0f);
+      local = picked.wi;
+      direction = picked.direction;
+      strength = picked.scale;
+      pdf = picked.pdf;
+      limit = picked.limit;
+      lit_roughness = fmax_(lit_roughness, picked.roughness);
+    }
+    if (live) {
+      const Surface S = load_surface_record(record);
+      const Shaded& s = S.s;
+      const v3 wo = mulmtv(transform, neg3(d));
+      if (pdf > 0.0f) {
+        float bsdf = bsdf_pdf(s, wo, local);
+        if (KIND == SLOT_SKY) {
+          strength = divs3(strength, pdf + bsdf);
+        } else {
+          float ratio = bsdf / pdf;
+          strength = divs3(strength, pdf * (1.0f + ratio * ratio));
+        }
+      }
+      const float4 t4 = th;
+      v3 term = mul3(scl3(scl3(mul3(mk3(t4.x, t4.y, t4.z), bsdf_eval(s, wo, local, lit_roughness)),
+                               pdf > 0.0f ? glossy_share(s) : 1.0f),
+                          local.z),
+                     strength);
+      term = capped(P, term, bounce > 0u);
+      live = !(term.x == 0.0f && term.y == 0.0f && term.z == 0.0f);  // adds nothing, traces nothing
+      if (live) {
+        const uint32_t pending = (flags >> F_PEND) & 15u;
+        uint32_t slot_index = i * P.cap + pending;
+        P.w.sh_c[slot_index] = make_float4(term.x, term.y, term.z, 0.0f);
+        P.w.sh_o[slot_index] = make_float4(origin.x, origin.y, origin.z, limit);
+        P.w.sh_d[slot_index] =
+            make_float4(direction.x, direction.y, direction.z, __uint_as_float(limit > 0.0f ? 0u : 1u));
+        reinterpret_cast<float*>(P.w.ray_d + i)[3] =
+            __uint_as_float((flags & ~(15u << F_PEND)) | ((pending + 1u) << F_PEND));
+      }
+    }
+    uint32_t at = claim(P.w.counters + 2, live && limit > 0.0f);  // one atomic per warp
+    if (live && limit > 0.0f) P.w.squeue[at] = i * P.cap + ((flags >> F_PEND) & 15u);
+    if (state != state_in) reinterpret_cast<float*>(P.w.thr + i)[3] = __uint_as_float(state);
   }
 }
 
@@ -1258,6 +1432,7 @@ struct Grids {
   int trace_closest[3][2] = {}, trace_any[3][2] = {}, shade = 0, shade_inline = 0, flat = 0;
   int shade_hit = 0, shade_lights = 0, shade_lights_inline = 0, shade_bsdf = 0;
   int retry = 0;  // blocks of the retry walks: one per SM (their work is rare)
+  int tree_pick = 0, slot[5] = {};  // the light slots, one kind per launch
 };
 Grids& grids() {
   static Grids g;
@@ -1280,6 +1455,12 @@ Grids& grids() {
     g.shade_lights = grid_for((const void*)k_shade_lights<true>, kThreads);
     g.shade_lights_inline = grid_for((const void*)k_shade_lights<false>, kThreads);
     g.shade_bsdf = grid_for((const void*)k_shade_bsdf, kThreads);
+    g.tree_pick = grid_for((const void*)k_tree_pick, kThreads);
+    g.slot[SLOT_SUN] = grid_for((const void*)k_light_slot<SLOT_SUN>, kThreads);
+    g.slot[SLOT_SKY] = grid_for((const void*)k_light_slot<SLOT_SKY>, kThreads);
+    g.slot[SLOT_EMITTER] = grid_for((const void*)k_light_slot<SLOT_EMITTER>, kThreads);
+    g.slot[SLOT_LOOPED] = grid_for((const void*)k_light_slot<SLOT_LOOPED>, kThreads);
+    g.slot[SLOT_TREE] = grid_for((const void*)k_light_slot<SLOT_TREE>, kThreads);
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1314,6 +1495,23 @@ void launch_trace_queue(int sel, uint32_t short_stack, const Pass& P, uint32_t w
 
 int thread_select(uint32_t threads) { return threads == 64u ? 0 : (threads == 256u ? 2 : 1); }
 
+// The deferred light slots one kind per launch, in slot order, each launched
+// only where the scene has that kind (the slots k_shade_lights skips without
+// a draw: no sun, no sky, no emissive triangles, no looped lights, no tree).
+void launch_light_slots(const Pass& P, cudaStream_t st) {
+  Grids& g = grids();
+  if (P.f.sun_color[3] > 0.0f) k_light_slot<SLOT_SUN><<<g.slot[SLOT_SUN], kThreads, 0, st>>>(P, 0u);
+  if (P.v.sky_width != 0u) k_light_slot<SLOT_SKY><<<g.slot[SLOT_SKY], kThreads, 0, st>>>(P, 1u);
+  if (P.v.emitter_count != 0u) k_light_slot<SLOT_EMITTER><<<g.slot[SLOT_EMITTER], kThreads, 0, st>>>(P, 2u);
+  for (uint32_t s = 1u; s <= P.v.looped; ++s)
+    k_light_slot<SLOT_LOOPED><<<g.slot[SLOT_LOOPED], kThreads, 0, st>>>(P, 2u + s);
+  if (P.slots > 3u + P.v.looped) {
+    const uint32_t k = 3u + P.v.looped;
+    k_tree_pick<<<g.tree_pick, kThreads, 0, st>>>(P, k);
+    k_light_slot<SLOT_TREE><<<g.slot[SLOT_TREE], kThreads, 0, st>>>(P, k);
+  }
+}
+
 // Path-state buffers for `capacity` paths and `cap` slots per path.
 void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
   size_t need = 0;
@@ -1330,7 +1528,7 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
          o_cnt = add(64), o_keys = add(4ull * capacity), o_sorted = add(4ull * capacity),
          o_hist = add(4ull * SORT_BINS), o_cursor = add(4ull * SORT_BINS), o_lit = add(4ull * capacity),
          o_surf = add(144ull * capacity), o_rhist = add(4ull * RAY_BINS), o_rcursor = add(4ull * RAY_BINS),
-         o_retry = add(4ull * capacity * (cap > 0 ? cap : 1));
+         o_retry = add(4ull * capacity * (cap > 0 ? cap : 1)), o_pick = add(8ull * capacity);
   if (need > t.wave_bytes) {
     if (t.d_wave) cudaFree(t.d_wave);
     t.d_wave = nullptr;
@@ -1369,6 +1567,7 @@ void ensure_wave(pfxt_trace& t, uint32_t capacity, uint32_t cap) {
   w.rhist = reinterpret_cast<uint32_t*>(b + o_rhist);
   w.rcursor = reinterpret_cast<uint32_t*>(b + o_rcursor);
   w.retry = reinterpret_cast<uint32_t*>(b + o_retry);
+  w.pick = reinterpret_cast<float2*>(b + o_pick);
 }
 
 // Cache scratch for `pixels` paths: queries, their path indices and
@@ -1532,7 +1731,7 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
                          t.cache ? (uint64_t)t.cache->s.steps : 0u, t.cache ? (uint64_t)t.cache->s.batch : 0u,
                          (uint64_t)(uintptr_t)t.d_accum,
                          (uint64_t)pixels | ((uint64_t)t.trace_threads << 32) | ((uint64_t)t.split_shade << 48) |
-                             ((uint64_t)t.short_stack << 52)};
+                             ((uint64_t)t.short_stack << 52) | ((uint64_t)t.slot_kernels << 60)};
     memcpy(key.data() + sizeof(P), extra, sizeof(extra));
     cudaGraphExec_t exec = nullptr;
     for (auto& e : t.graphs)
@@ -1607,7 +1806,9 @@ void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_
       }
       if (t.split_shade) {
         k_shade_hit<<<g.shade_hit, kThreads, 0, st>>>(P, cur);
-        if (deferred)
+        if (deferred && t.slot_kernels)
+          launch_light_slots(P, st);
+        else if (deferred)
           k_shade_lights<true><<<g.shade_lights, kThreads, 0, st>>>(P);
         else
           k_shade_lights<false><<<g.shade_lights_inline, kThreads, 0, st>>>(P);

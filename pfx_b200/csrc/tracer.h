@@ -125,6 +125,7 @@ struct pfxt_trace {
   bool sort_rays = false;                      // group the extend queue of later bounces by ray
   bool shadow_queue = true;                    // light slots' shadow rays through the connect queue
   uint32_t short_stack = 0;                    // traversal stack entries per lane in shared memory (0 or 8)
+  bool slot_kernels = true;                    // deferred light slots one kind per launch (or all in one kernel)
   uint64_t tune_key = 0;                       // hash of the scene's buffers, film and settings (autotune cache)
   float tuned_pass_ms = 0.0f;                  // the autotuner's measured pass time, 0 = not tuned
   uint32_t* d_error = nullptr;  // device error word

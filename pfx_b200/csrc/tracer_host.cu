@@ -443,6 +443,7 @@ void trace_set_tuning(pfxt_trace& t, const pfxt_tuning& k) {
   t.sort_rays = k.sort_rays != 0u;
   t.shadow_queue = k.shadow_queue != 0u;
   t.short_stack = k.short_stack;
+  t.slot_kernels = k.slot_kernels != 0u;
 }
 
 pfxt_tuning trace_get_tuning(const pfxt_trace& t) {
@@ -456,6 +457,7 @@ pfxt_tuning trace_get_tuning(const pfxt_trace& t) {
   k.shadow_queue = t.shadow_queue ? 1u : 0u;
   k.short_stack = t.short_stack;
   k.from_cache = 0u;
+  k.slot_kernels = t.slot_kernels ? 1u : 0u;
   return k;
 }
 
@@ -545,13 +547,14 @@ pfxt_tuning trace_autotune(pfxt_trace& t, uint32_t passes) {
       k.trace_threads = threads;
       consider(k);
     }
-  for (int knob = 0; knob < 5; ++knob) {
+  for (int knob = 0; knob < 6; ++knob) {
     pfxt_tuning k = best;
     switch (knob) {
       case 0: k.sort_shading ^= 1u; break;
       case 1: k.split_shade ^= 1u; break;
       case 2: k.sort_rays ^= 1u; break;
       case 3: k.shadow_queue ^= 1u; break;
+      case 4: k.slot_kernels ^= 1u; break;
       default: k.short_stack = k.short_stack ? 0u : 8u; break;
     }
     consider(k);

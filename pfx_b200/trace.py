@@ -463,13 +463,13 @@ class Trace:
         return {"trace_threads": k.trace_threads, "sort_shading": bool(k.sort_shading), "graphs": bool(k.graphs),
                 "split_shade": bool(k.split_shade), "sort_rays": bool(k.sort_rays), "pass_ms": float(k.pass_ms),
                 "shadow_queue": bool(k.shadow_queue), "short_stack": int(k.short_stack),
-                "from_cache": bool(k.from_cache)}
+                "from_cache": bool(k.from_cache), "slot_kernels": bool(k.slot_kernels)}
 
     def set_tuning(self, trace_threads: int = 128, sort_shading: bool = True, graphs: bool = True,
                    split_shade: bool = True, sort_rays: bool = False, shadow_queue: bool = True,
-                   short_stack: int = 0) -> None:
+                   short_stack: int = 0, slot_kernels: bool = True) -> None:
         k = abi.Tuning(trace_threads, int(sort_shading), int(graphs), int(split_shade), int(sort_rays), 0.0,
-                       int(shadow_queue), int(short_stack), 0)
+                       int(shadow_queue), int(short_stack), 0, int(slot_kernels))
         check(self._lib.pfxt_set_tuning(self._h, C.byref(k)))
 
     def autotune(self, passes: int = 3) -> dict:

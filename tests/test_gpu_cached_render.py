@@ -55,15 +55,19 @@ def test_open_cache_ends_paths(gpu):
 
 def test_the_cache_lowers_the_error_at_equal_device_time(gpu):
     """What the trained network gains over the tracer without it: on the
-    reduced room, with both tracers given the same device time (CUDA events on
-    each tracer's stream; the cache starts untrained and trains online inside
-    its passes), the cached image's relMSE against a 256-spp plain reference
-    is lower than the plain image's."""
+    reduced room (60 k triangles) at 1920x1080 with the default cache, both
+    tracers given the same device time (CUDA events on each tracer's stream;
+    the cache starts untrained and trains online inside its passes), the
+    cached image's relMSE against a 128-spp plain reference is lower than the
+    plain image's.  At a few hundred pixels a pass is launch-bound and the
+    cache's fixed cost per pass (inference and training launches) buys
+    nothing; the film here is large enough for the pass to be bandwidth-bound,
+    as at the full 4K frame."""
     import torch
 
     from pfx_b200.trace import Settings
 
-    w = synth.small("room_4k", (480, 270), sampler="sobol")
+    w = synth.small("room_4k", (1920, 1080), sampler="sobol")
     w.settings = Settings.deep(8, sampler="sobol", sobol_samples=256, filter_glossy=0.25, clamp_indirect=4.0)
 
     def stream_of(t):
@@ -79,7 +83,7 @@ def test_the_cache_lowers_the_error_at_equal_device_time(gpu):
         return a.elapsed_time(b)
 
     reference = Trace(w.scene, w.settings, w.width, w.height)
-    reference.sample(256, 9000)
+    reference.sample(128, 9000)
     ref = reference.readback().color[..., :3].astype(np.float64)
     reference.close()
 
@@ -88,9 +92,9 @@ def test_the_cache_lowers_the_error_at_equal_device_time(gpu):
         return float(np.mean((img - ref) ** 2 / (ref * ref + 0.01)))
 
     cached = Trace(w.scene, w.settings, w.width, w.height)
-    cache = RadianceCache(CacheSettings(log2_entries=17, batch=16384, steps=2, train_fraction=0.05))
+    cache = RadianceCache(CacheSettings())
     cached.set_cache(cache)
-    budget = sum(timed_pass(cached, seed) for seed in range(48))
+    budget = sum(timed_pass(cached, seed) for seed in range(32))
     cached_err = relmse(cached)
 
     plain = Trace(w.scene, w.settings, w.width, w.height)
@@ -99,5 +103,7 @@ def test_the_cache_lowers_the_error_at_equal_device_time(gpu):
         spent += timed_pass(plain, passes)
         passes += 1
     plain_err = relmse(plain)
+    print(f"equal device time {budget:.1f} ms: cached relMSE {cached_err:.5f} (32 passes), "
+          f"plain {plain_err:.5f} ({passes} passes)")
     assert cache.stats()["queries"] > 0
     assert cached_err < plain_err, (cached_err, plain_err, passes, budget)

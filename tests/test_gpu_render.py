@@ -255,3 +255,41 @@ def test_emissive_world_triangles_and_a_uniform_sky(gpu, sampler):
     got, exact = render_both(w, 4, [4, 5])
     assert got[..., :3].mean() > 0.0
     assert exact > 0.99
+
+
+@pytest.mark.parametrize("sampler", ["pcg", "sobol"])
+def test_slot_kernels_equal_the_one_kernel_slots(gpu, sampler):
+    """The light slots one kind per launch (k_tree_pick, k_light_slot) against
+    every slot of a path in one kernel (k_shade_lights): a scene with every
+    slot kind live (a soft sun, a uniform sky, emissive world triangles, three
+    looped rect lights and a light tree over point and spot lights) gives the
+    same accumulation bit for bit, and the same image as the oracle."""
+    from pfx_b200.trace import Sun
+
+    w = synth.small("plain_512", (48, 40), sampler=sampler)
+    mats = w.scene.materials.copy()
+    mats["emission"][5] = (4.0, 3.0, 2.0)
+    w.scene.materials = mats
+    w.scene.sky = (0.2, 0.25, 0.3)
+    w.scene.sun = Sun((0.3, 1.0, 0.2), (1.0, 0.9, 0.8), 1.5, radius_deg=2.0)  # soft: two draws
+    street = []
+    for k in range(24):
+        p = (-8.0 + (k % 6) * 3.2, 14.0 + (k % 3), -8.0 + (k // 6) * 5.0)
+        if k % 3 == 0:
+            street.append(synth.spot_light(p, (0.0, -1.0, 0.1), 30.0, 50.0, 30.0, (1.0, 0.8, 0.6), rng_range=30.0))
+        else:
+            street.append(synth.point_light(p, 20.0, (0.6, 0.8, 1.0), radius=0.2, rng_range=30.0))
+    w.scene.lights = np.concatenate([w.scene.lights, *street])
+    w.settings = Settings.deep(4, sampler=sampler, sobol_samples=16)
+    images = []
+    for slot_kernels in (True, False):
+        t = Trace(w.scene, w.settings, w.width, w.height)
+        t.set_tuning(trace_threads=128, sort_shading=False, slot_kernels=slot_kernels)
+        for s in range(3):
+            t.sample(1, 40 + s)
+        images.append(t.read_accum())
+        t.close()
+    assert images[0][..., :3].mean() > 0.0
+    assert np.array_equal(images[0].view(np.uint32), images[1].view(np.uint32))
+    got, exact = render_both(w, 1, [40, 41, 42])
+    assert exact > 0.99
