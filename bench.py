@@ -484,11 +484,8 @@ def main():
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(w.width * w.height * 16),
                     "note": "scene uploaded once by Trace::new (create_s); per step one pass and the colour film"},
-            # per pass: collect, gen, seed counts, finish, films, and per bounce reset,
-            # extend and its retry walk, (material sort: 2), shade (split: 3), rewind,
-            # connect and its retry walk
-            "gpu_launches": args.steps * (5 + (w.settings.bounces[0] + 2) * (
-                7 + (2 if tuning["sort_shading"] else 0) + (2 if tuning["split_shade"] else 0))),
+            # the kernel nodes of the pass's captured graph, one pass per step
+            "gpu_launches": args.steps * trace.pass_kernels(),
             "clocks": clk.summary(),
         }
         line["roofline"] = traversal_roofline(trace, w, dev, stream, flush)

@@ -227,6 +227,7 @@ EXTRA = [
     ("pfxt_debug_sort", C.c_int, [C.c_void_p, C.c_uint32]),
     ("pfxt_debug_graphs", C.c_int, [C.c_void_p, C.c_uint32]),
     ("pfxt_debug_graph_captures", C.c_uint32, [C.c_void_p]),
+    ("pfxt_debug_pass_kernels", C.c_uint32, [C.c_void_p]),
     ("pfxt_debug_select_nth", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_int32, C.c_void_p]),
     ("pfxt_debug_gpu_bvh", C.c_int, [C.c_int32]),
     ("pfxt_debug_scene_gpu_builds", C.c_uint32, [C.c_void_p]),

@@ -463,6 +463,7 @@ uint32_t pfxt_debug_scene_gpu_builds(const pfxt_scene_blobs* b) {
 
 /* How many sampling passes have been captured as graphs so far. */
 uint32_t pfxt_debug_graph_captures(pfxt_trace* t) { return t ? t->graph_captures : 0u; }
+uint32_t pfxt_debug_pass_kernels(pfxt_trace* t) { return t ? t->pass_kernels : 0u; }
 
 /* Restrict sampling to the pixels whose mask byte is non-zero (width*height
  * host bytes), or lift the restriction with NULL.  A measurement aid: it lets a

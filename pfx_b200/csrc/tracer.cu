@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(THREADS, TRACE_WARPS_PER_SM * 32 / THREADS) k_
     st.sh_near = short_near + threadIdx.x;
     st.lanes = THREADS;
   }
-  Walker<ANY, false, BOX_BOUNDED> w;
+  Walker<ANY, false, TRACE_BOX> w;
   const int lane = threadIdx.x & 31;
   uint32_t idx = 0, item = 0;
   bool have = false, retired = false;
@@ -478,7 +478,12 @@ __global__ void __launch_bounds__(THREADS, TRACE_WARPS_PER_SM * 32 / THREADS) k_
     }
     if (__all_sync(FULL, retired)) break;
     if (have) {
-      w.inner_phase(P.s, st);
+      w.inner_phase(P.s, st, [&](v3& o, v3& d) {
+        float4 a = ANY ? P.w.sh_o[item] : P.w.ray_o[item];
+        float4 b = ANY ? P.w.sh_d[item] : P.w.ray_d[item];
+        o = mk3(a.x, a.y, a.z);
+        d = mk3(b.x, b.y, b.z);
+      });
       if (!w.done) w.leaf_phase(P.s, st);
       if (w.done) {
         if (w.retry) {
@@ -509,7 +514,10 @@ __global__ void __launch_bounds__(128) k_trace_queue_retry(const __grid_constant
     LaneStack<0> st;
     Walker<ANY, false, BOX_IEEE> w;
     w.start(P.s, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), ANY ? a.w : 1e20f);
-    w.run(P.s, st);
+    w.run(P.s, st, [&](v3& o, v3& d) {
+      o = mk3(a.x, a.y, a.z);
+      d = mk3(b.x, b.y, b.z);
+    });
     if (ANY) {
       reinterpret_cast<float*>(P.w.sh_d + item)[3] = __uint_as_float(w.hit.hit ? 0u : 1u);
     } else {
@@ -1747,6 +1755,17 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
         throw;
       }
       check(cudaStreamEndCapture(st, &graph), "pass capture");
+      // the pass's kernel launches: the graph's kernel nodes
+      uint32_t kernels = 0;
+      size_t nodes = 0;
+      if (cudaGraphGetNodes(graph, nullptr, &nodes) == cudaSuccess && nodes > 0) {
+        std::vector<cudaGraphNode_t> list(nodes);
+        if (cudaGraphGetNodes(graph, list.data(), &nodes) == cudaSuccess)
+          for (size_t k = 0; k < nodes; ++k) {
+            cudaGraphNodeType type;
+            if (cudaGraphNodeGetType(list[k], &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) ++kernels;
+          }
+      }
       cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
       cudaGraphDestroy(graph);
       check(e, "pass graph");
@@ -1754,9 +1773,11 @@ void trace_sample(pfxt_trace& t, uint32_t count, uint32_t seed) {
         cudaGraphExecDestroy(t.graphs.front().exec);
         t.graphs.erase(t.graphs.begin());
       }
-      t.graphs.push_back(GraphEntry{std::move(key), exec});
+      t.graphs.push_back(GraphEntry{std::move(key), exec, kernels});
       t.graph_captures += 1u;
     }
+    for (auto& e : t.graphs)
+      if (e.exec == exec) t.pass_kernels = e.kernels;
     check(cudaGraphLaunch(exec, st), "pass graph launch");
   }
   check(cudaGetLastError(), "tracer launch");

@@ -72,6 +72,7 @@ struct Accum {
 struct GraphEntry {
   std::vector<unsigned char> key;
   cudaGraphExec_t exec;
+  uint32_t kernels;  // kernel launches of the captured pass
 };
 
 }  // namespace pfxt
@@ -149,6 +150,7 @@ struct pfxt_trace {
   std::vector<pfxt::GraphEntry> graphs;
   bool use_graphs = true;
   uint32_t graph_captures = 0;  // passes captured so far
+  uint32_t pass_kernels = 0;    // kernel launches of the last pass replayed from a graph
 };
 
 namespace pfxt {

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(kThreads, TRACE_WARPS_PER_SM * 32 / kThreads) 
   constexpr bool COUNT = (MODE >= 2);
   constexpr unsigned FULL = 0xffffffffu;
   LaneStack<0> st;  // local memory: a shared-memory top measured slower (more registers, fewer warps)
-  Walker<ANY, COUNT, COUNT ? BOX_EITHER : BOX_BOUNDED> w;
+  Walker<ANY, COUNT, COUNT ? BOX_EITHER : TRACE_BOX> w;
   const int lane = threadIdx.x & 31;
   uint32_t idx = 0;
   bool have = false, retired = false;
@@ -73,7 +73,10 @@ __global__ void __launch_bounds__(kThreads, TRACE_WARPS_PER_SM * 32 / kThreads) 
     }
     if (__all_sync(FULL, retired)) break;
     if (have) {
-      w.inner_phase(s, st);
+      w.inner_phase(s, st, [&](v3& o, v3& d) {
+        float tmax;
+        load_ray(rays, idx, o, d, tmax);
+      });
       if (!w.done) w.leaf_phase(s, st);
       if (w.done) {
         if (MODE == 0) {
@@ -106,7 +109,10 @@ __global__ void __launch_bounds__(kThreads) k_trace_retry(SceneView s, const pfx
     float tmax;
     load_ray(rays, i, o, d, tmax);
     w.start(s, o, d, tmax);
-    w.run(s, st);
+    w.run(s, st, [&](v3& wo, v3& wd) {
+      wo = o;
+      wd = d;
+    });
     if (MODE == 0)
       reinterpret_cast<uint4*>(out)[i] = make_uint4(__float_as_uint(w.hit.t), w.hit.slot, w.hit.record, w.hit.hit);
     else

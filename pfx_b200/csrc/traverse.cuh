@@ -174,6 +174,78 @@ __device__ __forceinline__ bool box_geometry_bounded(float lx, float ly, float l
   return !(n > f);
 }
 
+// Two fp32 lanes in one 64-bit register and the sm_100 paired instructions on
+// them: each lane is one IEEE round-to-nearest add, multiply or fused
+// multiply-add, the same operation as the scalar instruction, two per issue.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pair(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void unpair(f32x2 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+// A bounded ray whose direction has no degenerate axis, paired the way a
+// child box's six coordinates lie in a node, (lx, ly), (lz, hx), (hy, hz):
+// origins (ox, oy), (oz, ox), (oy, oz), reciprocals and negated directions
+// likewise.
+struct PRay {
+  f32x2 o[3], r[3], nd[3];
+};
+__device__ __forceinline__ PRay make_pray(const TRay& t) {
+  PRay p;
+  p.o[0] = pair(t.o.x, t.o.y);
+  p.o[1] = pair(t.o.z, t.o.x);
+  p.o[2] = pair(t.o.y, t.o.z);
+  p.r[0] = pair(t.r.x, t.r.y);
+  p.r[1] = pair(t.r.z, t.r.x);
+  p.r[2] = pair(t.r.y, t.r.z);
+  p.nd[0] = pair(-t.d.x, -t.d.y);
+  p.nd[1] = pair(-t.d.z, -t.d.x);
+  p.nd[2] = pair(-t.d.y, -t.d.z);
+  return p;
+}
+__device__ __forceinline__ bool packable(const TRay& t) {
+  return t.bounded && fabsf(t.d.x) >= 1e-12f && fabsf(t.d.y) >= 1e-12f && fabsf(t.d.z) >= 1e-12f;
+}
+
+// Markstein quotients of a pair: (x0/d0, x1/d1) correctly rounded, as quotient().
+__device__ __forceinline__ f32x2 quotient2(f32x2 x, f32x2 nd, f32x2 r) {
+  f32x2 q = mul2(x, r);
+  f32x2 e = fma2(q, nd, x);  // q * (-d) + x = fma(-q, d, x) exactly
+  return fma2(e, r, q);
+}
+
+// box_geometry_bounded for a ray with no degenerate axis, the box given as
+// the three coordinate pairs of its node: (lx, ly), (lz, hx), (hy, hz).
+__device__ __forceinline__ bool box_geometry_paired(f32x2 b0, f32x2 b1, f32x2 b2, const PRay& p, float& near) {
+  float lx, ly, lz, hx, hy, hz;
+  unpair(quotient2(sub2(b0, p.o[0]), p.nd[0], p.r[0]), lx, ly);
+  unpair(quotient2(sub2(b1, p.o[1]), p.nd[1], p.r[1]), lz, hx);
+  unpair(quotient2(sub2(b2, p.o[2]), p.nd[2], p.r[2]), hy, hz);
+  float n = fmaxf(fmaxf(fmaxf(0.0f, fminf(lx, hx)), fminf(ly, hy)), fminf(lz, hz));
+  float f = fminf(fminf(fmaxf(lx, hx), fmaxf(ly, hy)), fmaxf(lz, hz));
+  near = n;
+  return !(n > f);
+}
+
 // How a walk tests boxes.
 //  BOX_EITHER:  bounded rays with the Markstein quotients, other rays with the
 //               out-of-line IEEE test (one walk for every ray; the call costs
@@ -182,9 +254,15 @@ __device__ __forceinline__ bool box_geometry_bounded(float lx, float ly, float l
 //               space or in an instance's space) stops at once with `retry`
 //               set, and a second kernel walks it again from the start with
 //               BOX_IEEE, so the walk loop has no call;
-//  BOX_IEEE:    IEEE division throughout, inline.
-// All three give the same bits for every box they test.
-constexpr int BOX_EITHER = 0, BOX_BOUNDED = 1, BOX_IEEE = 2;
+//  BOX_IEEE:    IEEE division throughout, inline;
+//  BOX_PAIRED:  BOX_BOUNDED with the quotients in paired instructions; a ray
+//               with a degenerate axis is handed over like an unbounded one.
+// All four give the same bits for every box they test.
+constexpr int BOX_EITHER = 0, BOX_BOUNDED = 1, BOX_IEEE = 2, BOX_PAIRED = 3;
+// The flavour of the batch and queue traversal kernels (their retry kernels walk with BOX_IEEE).
+#ifndef TRACE_BOX
+#define TRACE_BOX BOX_BOUNDED
+#endif
 
 template <int BOX>
 __device__ __forceinline__ bool box_test(float lx, float ly, float lz, float hx, float hy, float hz, const TRay& ray,
@@ -259,8 +337,8 @@ struct LaneStack<0> {
 // One query's traversal state; the stack is the caller's.
 template <bool ANY, bool COUNT, int BOX = BOX_EITHER>
 struct Walker {
-  v3 o, d;      // world ray
-  TRay ray;     // ray in the current space
+  TRay ray;     // ray in the current space (the world ray itself is the caller's: see inner_phase)
+  PRay pr;      // BOX_PAIRED: `ray` paired for the box test
   float limit;
   uint32_t base, record, word;
   float inv_det;
@@ -268,13 +346,12 @@ struct Walker {
   float near_cur;
   int top;
   bool done;
-  bool retry;  // BOX_BOUNDED: the ray is not bounded; walk it again with BOX_IEEE
+  bool retry;  // BOX_BOUNDED, BOX_PAIRED: the ray is not bounded (or, paired, has a degenerate axis); walk
+               // it again with BOX_IEEE
   TraceHit hit;
   TraceCounts counts;
 
   __device__ __forceinline__ void start(const SceneView& s, v3 wo, v3 wd, float lim) {
-    o = wo;
-    d = wd;
     ray = make_tray(wo, wd, s.small);
     limit = lim;
     base = record = word = 0u;
@@ -287,6 +364,14 @@ struct Walker {
     if (BOX == BOX_BOUNDED && !done && !ray.bounded) {
       retry = true;
       done = true;
+    }
+    if (BOX == BOX_PAIRED && !done) {
+      if (!packable(ray)) {
+        retry = true;
+        done = true;
+      } else {
+        pr = make_pray(ray);
+      }
     }
     hit.t = lim;
     hit.slot = hit.record = hit.hit = 0u;
@@ -310,12 +395,17 @@ struct Walker {
   }
 
   // Walk inner nodes until the current entry is a leaf that passes its
-  // near check, or the traversal is finished.
-  template <class Stack>
-  __device__ __forceinline__ void inner_phase(const SceneView& s, Stack& st) {
+  // near check, or the traversal is finished.  world(o, d) gives the world
+  // ray again where an instance is entered or left (the walk keeps only the
+  // ray of the current space; callers read it back from where it came from).
+  template <class Stack, class World>
+  __device__ __forceinline__ void inner_phase(const SceneView& s, Stack& st, const World& world) {
     while (!done) {
       if (ref == STACK_SENTINEL) {
+        v3 o, d;
+        world(o, d);
         ray = make_tray(o, d, s.small);
+        if (BOX == BOX_PAIRED) pr = make_pray(ray);
         base = record = word = 0u;
         inv_det = 1.0f;
         pop(st);
@@ -327,12 +417,21 @@ struct Walker {
       }
       if ((ref & REF_LEAF) == 0u) {
         const float4* p = reinterpret_cast<const float4*>(s.wide + ref);
-        float4 q0 = __ldg(p + 0), q1 = __ldg(p + 1), q2 = __ldg(p + 2);
         uint4 q3 = __ldg(reinterpret_cast<const uint4*>(p + 3));
         float n0 = 0.0f, n1 = 0.0f;
-        bool ok0 = box_test<BOX>(q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, ray, n0) && n0 <= hit.t;
+        bool ok0, ok1;
         bool has1 = q3.y != REF_NONE;
-        bool ok1 = has1 && box_test<BOX>(q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, ray, n1) && n1 <= hit.t;
+        if constexpr (BOX == BOX_PAIRED) {
+          // the node's twelve coordinates as six pairs: (lx, ly), (lz, hx), (hy, hz) of each child
+          const ulonglong2* pp = reinterpret_cast<const ulonglong2*>(p);
+          ulonglong2 a = __ldg(pp + 0), b = __ldg(pp + 1), c = __ldg(pp + 2);
+          ok0 = box_geometry_paired(a.x, a.y, b.x, pr, n0) && n0 <= hit.t;
+          ok1 = has1 && box_geometry_paired(b.y, c.x, c.y, pr, n1) && n1 <= hit.t;
+        } else {
+          float4 q0 = __ldg(p + 0), q1 = __ldg(p + 1), q2 = __ldg(p + 2);
+          ok0 = box_test<BOX>(q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, ray, n0) && n0 <= hit.t;
+          ok1 = has1 && box_test<BOX>(q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, ray, n1) && n1 <= hit.t;
+        }
         if (COUNT) counts.boxes += 1u;  // the left child, popped next by the reference
         if ((ok1 || (COUNT && has1)) && top < (int)REF_STACK) {
           st.put(top, q3.y, ok1 ? n1 : INFINITY);
@@ -362,11 +461,21 @@ struct Walker {
         word = m.w;
         inv_det = m2.x;
         if (__float_as_uint(m2.y) != 0u) {
+          v3 o, d;
+          world(o, d);
           ray = make_tray(to_object(r0, r1, r2, o, 1.0f), to_object(r0, r1, r2, d, 0.0f), s.small);
           if (BOX == BOX_BOUNDED && !ray.bounded) {
             retry = true;
             done = true;
             return;
+          }
+          if (BOX == BOX_PAIRED) {
+            if (!packable(ray)) {
+              retry = true;
+              done = true;
+              return;
+            }
+            pr = make_pray(ray);
           }
         }
         ref = m.x;
@@ -391,19 +500,45 @@ struct Walker {
         const float4* tp = reinterpret_cast<const float4*>(s.tris + i);
         float4 ta = __ldg(tp + 0), te1 = __ldg(tp + 1), te2 = __ldg(tp + 2);
         v3 a = mk3(ta.x, ta.y, ta.z), e1 = mk3(te1.x, te1.y, te1.z), e2 = mk3(te2.x, te2.y, te2.z);
-        v3 pv = cross3(ray.d, e2);
-        float det = dot3(e1, pv);
-        float seen = det * inv_det;
-        if (fabsf(seen) < 1e-9f) continue;
-        if (!ANY && (word & ONE_SIDED) != 0u && seen < 0.0f) continue;
-        float inv = 1.0f / det;
-        v3 sv = sub3(ray.o, a);
-        float u = dot3(sv, pv) * inv;
-        if (u < 0.0f || u > 1.0f) continue;
-        v3 qv = cross3(sv, e1);
-        float v = dot3(ray.d, qv) * inv;
-        if (v < 0.0f || u + v > 1.0f) continue;
-        float t = dot3(e2, qv) * inv;
+        float u, v, t;
+        if constexpr (BOX == BOX_PAIRED) {
+          // The same test on the negated direction n = -d the paired ray
+          // holds: pv, det and inv change sign exactly (round-to-nearest is
+          // symmetric), so u and v are the same bits and t = -(e2.qv * inv).
+          v3 rn, ro;
+          float spare;
+          unpair(pr.nd[0], rn.x, rn.y);
+          unpair(pr.nd[1], rn.z, spare);
+          unpair(pr.o[0], ro.x, ro.y);
+          unpair(pr.o[1], ro.z, spare);
+          v3 pv = cross3(rn, e2);
+          float det = dot3(e1, pv);
+          float seen = det * inv_det;
+          if (fabsf(seen) < 1e-9f) continue;
+          if (!ANY && (word & ONE_SIDED) != 0u && seen > 0.0f) continue;
+          float inv = 1.0f / det;
+          v3 sv = sub3(ro, a);
+          u = dot3(sv, pv) * inv;
+          if (u < 0.0f || u > 1.0f) continue;
+          v3 qv = cross3(sv, e1);
+          v = dot3(rn, qv) * inv;
+          if (v < 0.0f || u + v > 1.0f) continue;
+          t = -(dot3(e2, qv) * inv);
+        } else {
+          v3 pv = cross3(ray.d, e2);
+          float det = dot3(e1, pv);
+          float seen = det * inv_det;
+          if (fabsf(seen) < 1e-9f) continue;
+          if (!ANY && (word & ONE_SIDED) != 0u && seen < 0.0f) continue;
+          float inv = 1.0f / det;
+          v3 sv = sub3(ray.o, a);
+          u = dot3(sv, pv) * inv;
+          if (u < 0.0f || u > 1.0f) continue;
+          v3 qv = cross3(sv, e1);
+          v = dot3(ray.d, qv) * inv;
+          if (v < 0.0f || u + v > 1.0f) continue;
+          t = dot3(e2, qv) * inv;
+        }
         if (ANY) {
           if (t <= 0.0001f || t >= limit) continue;
           hit.hit = 1u;
@@ -426,10 +561,10 @@ struct Walker {
   }
 
   // Run to completion (one query, no work sharing).
-  template <class Stack>
-  __device__ __forceinline__ void run(const SceneView& s, Stack& st) {
+  template <class Stack, class World>
+  __device__ __forceinline__ void run(const SceneView& s, Stack& st, const World& world) {
     while (!done) {
-      inner_phase(s, st);
+      inner_phase(s, st, world);
       if (done) break;
       leaf_phase(s, st);
     }
@@ -442,7 +577,10 @@ __device__ __forceinline__ TraceHit traverse(const SceneView& s, v3 o, v3 d, flo
   LaneStack<0> st;
   Walker<ANY, false, BOX_EITHER> w;
   w.start(s, o, d, limit);
-  w.run(s, st);
+  w.run(s, st, [&](v3& wo, v3& wd) {
+    wo = o;
+    wd = d;
+  });
   return w.hit;
 }
 

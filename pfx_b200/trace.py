@@ -472,6 +472,11 @@ class Trace:
                        int(shadow_queue), int(short_stack), 0, int(slot_kernels))
         check(self._lib.pfxt_set_tuning(self._h, C.byref(k)))
 
+    def pass_kernels(self) -> int:
+        """Kernel launches of the last pass, counted in its captured graph (0
+        when passes are not captured)."""
+        return int(self._lib.pfxt_debug_pass_kernels(self._h))
+
     def autotune(self, passes: int = 3) -> dict:
         """Time passes of this scene under each launch choice and keep the
         fastest, or take an earlier tuning of the same scene (restarts the

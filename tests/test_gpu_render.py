@@ -281,15 +281,20 @@ def test_slot_kernels_equal_the_one_kernel_slots(gpu, sampler):
             street.append(synth.point_light(p, 20.0, (0.6, 0.8, 1.0), radius=0.2, rng_range=30.0))
     w.scene.lights = np.concatenate([w.scene.lights, *street])
     w.settings = Settings.deep(4, sampler=sampler, sobol_samples=16)
-    images = []
+    images, kernels = [], []
     for slot_kernels in (True, False):
         t = Trace(w.scene, w.settings, w.width, w.height)
         t.set_tuning(trace_threads=128, sort_shading=False, slot_kernels=slot_kernels)
         for s in range(3):
             t.sample(1, 40 + s)
         images.append(t.read_accum())
+        kernels.append(t.pass_kernels())
         t.close()
     assert images[0][..., :3].mean() > 0.0
     assert np.array_equal(images[0].view(np.uint32), images[1].view(np.uint32))
+    # per bounce: sun, sky, emitters, three looped lights, the tree's descent and its
+    # slot, against one kernel
+    extra = kernels[0] - kernels[1]
+    assert kernels[1] > 0 and extra > 0 and extra % 7 == 0
     got, exact = render_both(w, 1, [40, 41, 42])
     assert exact > 0.99
