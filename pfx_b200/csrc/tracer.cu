@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(THREADS, TRACE_WARPS_PER_SM * 32 / THREADS) k_
     st.sh_near = short_near + threadIdx.x;
     st.lanes = THREADS;
   }
-  Walker<ANY, false, TRACE_BOX> w;
+  Walker<ANY, false, TRACE_BOX, TRACE_SPEC> w;
   const int lane = threadIdx.x & 31;
   uint32_t idx = 0, item = 0;
   bool have = false, retired = false;
@@ -484,8 +484,8 @@ __global__ void __launch_bounds__(THREADS, TRACE_WARPS_PER_SM * 32 / THREADS) k_
         o = mk3(a.x, a.y, a.z);
         d = mk3(b.x, b.y, b.z);
       });
-      if (!w.done) w.leaf_phase(P.s, st);
-      if (w.done) {
+      if (w.leaf_ready()) w.leaf_phase(P.s, st);
+      if (!w.leaf_ready()) {
         if (w.retry) {
           P.w.retry[atomicAdd(P.w.counters + (ANY ? 14 : 13), 1u)] = item;
         } else if (ANY) {

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(kThreads, TRACE_WARPS_PER_SM * 32 / kThreads) 
   constexpr bool COUNT = (MODE >= 2);
   constexpr unsigned FULL = 0xffffffffu;
   LaneStack<0> st;  // local memory: a shared-memory top measured slower (more registers, fewer warps)
-  Walker<ANY, COUNT, COUNT ? BOX_EITHER : TRACE_BOX> w;
+  Walker<ANY, COUNT, COUNT ? BOX_EITHER : TRACE_BOX, !COUNT && TRACE_SPEC> w;
   const int lane = threadIdx.x & 31;
   uint32_t idx = 0;
   bool have = false, retired = false;
@@ -77,8 +77,8 @@ __global__ void __launch_bounds__(kThreads, TRACE_WARPS_PER_SM * 32 / kThreads) 
         float tmax;
         load_ray(rays, idx, o, d, tmax);
       });
-      if (!w.done) w.leaf_phase(s, st);
-      if (w.done) {
+      if (w.leaf_ready()) w.leaf_phase(s, st);
+      if (!w.leaf_ready()) {
         if (MODE == 0) {
           reinterpret_cast<uint4*>(out)[idx] =
               make_uint4(__float_as_uint(w.hit.t), w.hit.slot, w.hit.record, w.retry ? RETRY : w.hit.hit);

@@ -263,6 +263,10 @@ constexpr int BOX_EITHER = 0, BOX_BOUNDED = 1, BOX_IEEE = 2, BOX_PAIRED = 3;
 #ifndef TRACE_BOX
 #define TRACE_BOX BOX_BOUNDED
 #endif
+// Whether those kernels set leaves aside (Walker's SPEC).
+#ifndef TRACE_SPEC
+#define TRACE_SPEC false
+#endif
 
 template <int BOX>
 __device__ __forceinline__ bool box_test(float lx, float ly, float lz, float hx, float hy, float hz, const TRay& ray,
@@ -335,7 +339,21 @@ struct LaneStack<0> {
 };
 
 // One query's traversal state; the stack is the caller's.
-template <bool ANY, bool COUNT, int BOX = BOX_EITHER>
+// SPEC: a lane that reaches a leaf while other lanes of its warp still walk
+// inner nodes sets the leaf aside (`held`) and walks on, so that the warp's
+// leaf tests run with more lanes at once (Aila and Laine, "Understanding the
+// efficiency of ray traversal on GPUs", 2009).  It tests the leaves the
+// reference tests, in the reference's order, with the same hit distance at
+// each: the held leaf is the next one in the reference's order and is tested
+// before any other; everything walked past it was decided against the hit
+// distance from before its test, which is not smaller than the reference's, so
+// the walk only keeps more entries; and each of those is checked again
+// against the current distance before it is opened or tested (a node's entry
+// distance is at least its ancestors' in the same space, as a box holds its
+// children's).  A held leaf is tested before the walk enters or leaves an
+// instance, so it is tested in its own space.  Entries are right siblings of
+// the current path, as in the reference, so the stack is no deeper.
+template <bool ANY, bool COUNT, int BOX = BOX_EITHER, bool SPEC = false>
 struct Walker {
   TRay ray;     // ray in the current space (the world ray itself is the caller's: see inner_phase)
   PRay pr;      // BOX_PAIRED: `ray` paired for the box test
@@ -345,6 +363,7 @@ struct Walker {
   uint32_t ref;
   float near_cur;
   int top;
+  uint32_t held;  // SPEC: the leaf set aside, REF_NONE when none
   bool done;
   bool retry;  // BOX_BOUNDED, BOX_PAIRED: the ray is not bounded (or, paired, has a degenerate axis); walk
                // it again with BOX_IEEE
@@ -359,6 +378,7 @@ struct Walker {
     ref = s.root;
     near_cur = -INFINITY;
     top = 0;
+    held = REF_NONE;
     done = (s.root == REF_NONE);
     retry = false;
     if (BOX == BOX_BOUNDED && !done && !ray.bounded) {
@@ -390,10 +410,6 @@ struct Walker {
     if (COUNT && ref != STACK_SENTINEL) counts.boxes += 1u;
   }
 
-  __device__ __forceinline__ bool holds_leaf() const {
-    return (ref & REF_INST) == REF_LEAF && ref != STACK_SENTINEL && ref != REF_NONE;
-  }
-
   // Walk inner nodes until the current entry is a leaf that passes its
   // near check, or the traversal is finished.  world(o, d) gives the world
   // ray again where an instance is entered or left (the walk keeps only the
@@ -401,7 +417,12 @@ struct Walker {
   template <class Stack, class World>
   __device__ __forceinline__ void inner_phase(const SceneView& s, Stack& st, const World& world) {
     while (!done) {
+      if constexpr (SPEC) {
+        // a lane holding a leaf walks on only while another lane of the warp still looks for one
+        if (held != REF_NONE && !__any_sync(__activemask(), held == REF_NONE)) return;
+      }
       if (ref == STACK_SENTINEL) {
+        if (SPEC && held != REF_NONE) return;  // the held leaf is tested in its own space
         v3 o, d;
         world(o, d);
         ray = make_tray(o, d, s.small);
@@ -446,6 +467,7 @@ struct Walker {
         continue;
       }
       if ((ref & REF_INST) == REF_INST) {
+        if (SPEC && held != REF_NONE) return;  // the held leaf is tested in its own space
         if (top >= (int)REF_STACK) {  // refused at creation; never taken
           pop(st);
           continue;
@@ -482,15 +504,30 @@ struct Walker {
         near_cur = -INFINITY;
         continue;
       }
-      return;  // a leaf that passed its near check
+      // a leaf that passed its near check
+      if constexpr (SPEC) {
+        if (held == REF_NONE) {
+          held = ref;
+          pop(st);
+          continue;
+        }
+      }
+      return;
     }
   }
+
+  // SPEC: is there a leaf to test (the held one, or the current entry)?
+  __device__ __forceinline__ bool leaf_ready() const { return SPEC ? (held != REF_NONE || !done) : !done; }
 
   // Test the triangles of the held leaf, then move to the next entry.
   template <class Stack>
   __device__ __forceinline__ void leaf_phase(const SceneView& s, Stack& st) {
-    uint32_t first = ref & LEAF_FIRST_MASK;
-    uint32_t n = ((ref >> LEAF_FIRST_BITS) & 15u) + 1u;
+    // SPEC: the held leaf first; the current entry stays, to be checked again
+    const bool from_held = SPEC && held != REF_NONE;
+    const uint32_t leaf = from_held ? held : ref;
+    if (SPEC) held = REF_NONE;
+    uint32_t first = leaf & LEAF_FIRST_MASK;
+    uint32_t n = ((leaf >> LEAF_FIRST_BITS) & 15u) + 1u;
     bool skip = ANY ? ((word & CASTS_NO_SHADOW) != 0u) : ((word & SHADOW_ONLY) != 0u);
     if (COUNT && skip) counts.tris += n;
     if (!skip) {
@@ -557,15 +594,15 @@ struct Walker {
         }
       }
     }
-    pop(st);
+    if (!from_held) pop(st);
   }
 
   // Run to completion (one query, no work sharing).
   template <class Stack, class World>
   __device__ __forceinline__ void run(const SceneView& s, Stack& st, const World& world) {
-    while (!done) {
+    while (leaf_ready()) {
       inner_phase(s, st, world);
-      if (done) break;
+      if (!leaf_ready()) break;
       leaf_phase(s, st);
     }
   }

@@ -37,7 +37,13 @@ def test_traversal_on_the_full_scene(gpu, room, name):
     closest, shadow = raymix.pass_mix(trace, w.scene, w.width, w.height, 1 << 18, seed=17)
     got, counts = compare_closest(trace, closest, ref)
     assert got["hit"].mean() > 0.5
-    assert int(got["slot"][got["hit"] == 1].max()) > w.scene.world_triangle_count // 2
+    hit = got["hit"] == 1
+    if len(w.scene.instances):
+        # slots of instanced meshes are indices into the shared mesh's triangles:
+        # hits spread over many placed records instead
+        assert len(np.unique(got["record"][hit])) > 100
+    else:
+        assert int(got["slot"][hit].max()) > w.scene.world_triangle_count // 2
     blocked = compare_any(trace, shadow, ref)
     assert 0.02 < blocked.mean() < 0.98
     assert np.array_equal(device_counts(trace, closest, False), counts)
