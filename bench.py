@@ -273,6 +273,12 @@ def cache_settings(args):
         s.error_bound = args.cache_error_bound
     if args.cache_min_roughness is not None:
         s.min_roughness = args.cache_min_roughness
+    if args.cache_query_bounce is not None:
+        s.query_bounce = args.cache_query_bounce
+    if args.cache_delay_bounces is not None:
+        s.delay_bounces = args.cache_delay_bounces
+    if args.cache_train_fraction is not None:
+        s.train_fraction = args.cache_train_fraction
     return s
 
 
@@ -402,6 +408,9 @@ def main():
     ap.add_argument("--max-cached-spp", type=int, default=1024)
     ap.add_argument("--cache-error-bound", type=float, default=None)
     ap.add_argument("--cache-min-roughness", type=float, default=None)
+    ap.add_argument("--cache-query-bounce", type=int, default=None)
+    ap.add_argument("--cache-delay-bounces", type=int, default=None)
+    ap.add_argument("--cache-train-fraction", type=float, default=None)
     ap.add_argument("--no-relmse", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -622,8 +622,11 @@ __device__ __forceinline__ float sin_from_cos(float c) { return sqrtf(fmax_(1.0f
 
 // tree_importance (lights.wgsl:204-237) -> (max, min)
 // trig = (cos theta_o, sin theta_o, cos(theta_o + theta_e), cos(theta_e - theta_o)).
-SH_SMALL float2 tree_importance(v3 n, v3 to, float cos_u, v3 axis, float theta_o, float theta_e,
-                                                  float far, float near, float energy, float4 trig) {
+// The light-tree functions are written once as inline bodies (`*_b`); IN
+// selects whether a body calls the next ones inline (the descent kernel) or
+// through their out-of-line copies (the kernels that keep them out of line).
+__device__ __forceinline__ float2 tree_importance_b(v3 n, v3 to, float cos_u, v3 axis, float theta_o, float theta_e,
+                                                    float far, float near, float energy, float4 trig) {
   float sin_u = sin_from_cos(cos_u);
   float cos_i = dot3(to, n);
   float sin_i = sin_from_cos(cos_i);
@@ -654,7 +657,18 @@ SH_SMALL float2 tree_importance(v3 n, v3 to, float cos_u, v3 axis, float theta_o
   float cos_max_out = cos_t_plus_u * cos_o - sin_from_cos(cos_t_plus_u) * sin_o;
   return make_float2(most, abs_(cos_max_i * energy * cos_max_out / (far * far)));
 }
-SH_SMALL float2 node_importance(const LightRow& node, float4 trig, v3 p, v3 n) {
+SH_SMALL float2 tree_importance(v3 n, v3 to, float cos_u, v3 axis, float theta_o, float theta_e, float far,
+                                float near, float energy, float4 trig) {
+  return tree_importance_b(n, to, cos_u, axis, theta_o, theta_e, far, near, energy, trig);
+}
+template <bool IN>
+__device__ __forceinline__ float2 tree_importance_to(v3 n, v3 to, float cos_u, v3 axis, float theta_o, float theta_e,
+                                                     float far, float near, float energy, float4 trig) {
+  if constexpr (IN) return tree_importance_b(n, to, cos_u, axis, theta_o, theta_e, far, near, energy, trig);
+  return tree_importance(n, to, cos_u, axis, theta_o, theta_e, far, near, energy, trig);
+}
+template <bool IN>
+__device__ __forceinline__ float2 node_importance_b(const LightRow& node, float4 trig, v3 p, v3 n) {
   v3 lo = f3of(node.a), hi = f3of(node.b);
   v3 centroid = scl3(add3(lo, hi), 0.5f);
   v3 extent = sub3(hi, centroid);
@@ -666,11 +680,15 @@ SH_SMALL float2 node_importance(const LightRow& node, float4 trig, v3 p, v3 n) {
   float cos_u = -1.0f;
   if (reach * reach > radius2) cos_u = sqrtf(fmax_(1.0f - radius2 / (reach * reach), 0.0f));
   float distance = fmax_(fmax_(0.5f * sqrtf(radius2), reach), 1e-6f);
-  return tree_importance(n, divs3(to, fmax_(reach, 1e-30f)), cos_u, f3of(node.c), node.c.w, node.d.x, distance,
-                         distance, node.a.w, trig);
+  return tree_importance_to<IN>(n, divs3(to, fmax_(reach, 1e-30f)), cos_u, f3of(node.c), node.c.w, node.d.x,
+                                distance, distance, node.a.w, trig);
+}
+SH_SMALL float2 node_importance(const LightRow& node, float4 trig, v3 p, v3 n) {
+  return node_importance_b<false>(node, trig, p, n);
 }
 // trig: the light's RowTrig::light.
-SH_SMALL float2 emitter_importance(const LightRow& light, float4 trig, v3 p, v3 n) {
+template <bool IN>
+__device__ __forceinline__ float2 emitter_importance_b(const LightRow& light, float4 trig, v3 p, v3 n) {
   v3 to = sub3(f3of(light.a), p);
   float near = length3(to);
   if (near >= light.b.w || near <= 1e-6f) return make_float2(0.0f, 0.0f);
@@ -685,22 +703,33 @@ SH_SMALL float2 emitter_importance(const LightRow& light, float4 trig, v3 p, v3 
     float cos_min_out = cos_(fmax_(0.0f, acos_(clamp_(dot3(f3of(light.c), neg3(toward)), -1.0f, 1.0f)) - acos_(cos_u)));
     float along = clamp_(cos_min_out * light.d.x + light.d.y, 0.0f, 1.0f);
     energy = energy * (along * along);
-    return tree_importance(n, toward, cos_u, f3of(light.c), 0.0f, theta_e, far, near, energy, cones);
+    return tree_importance_to<IN>(n, toward, cos_u, f3of(light.c), 0.0f, theta_e, far, near, energy, cones);
   }
-  return tree_importance(n, toward, cos_u, neg3(toward), 0.0f, trig.x, far, near, energy, cones);
+  return tree_importance_to<IN>(n, toward, cos_u, neg3(toward), 0.0f, trig.x, far, near, energy, cones);
 }
+SH_SMALL float2 emitter_importance(const LightRow& light, float4 trig, v3 p, v3 n) {
+  return emitter_importance_b<false>(light, trig, p, n);
+}
+template <bool IN>
+__device__ __forceinline__ float2 emitter_importance_to(const LightRow& light, float4 trig, v3 p, v3 n) {
+  if constexpr (IN) return emitter_importance_b<true>(light, trig, p, n);
+  return emitter_importance(light, trig, p, n);
+}
+template <bool IN>
 __device__ __forceinline__ float2 child_importance(const ShadeView& v, uint32_t row, v3 p, v3 n) {
   LightRow node = load_light(v, row);
   if (f2u(node.d.y) == 1u) {
     uint32_t light = f2u(node.d.z);
-    return emitter_importance(load_light(v, light), load_trig(v, light).light, p, n);
+    return emitter_importance_to<IN>(load_light(v, light), load_trig(v, light).light, p, n);
   }
+  if constexpr (IN) return node_importance_b<true>(node, load_trig(v, row).node, p, n);
   return node_importance(node, load_trig(v, row).node, p, n);
 }
 
 // tree_leaf (lights.wgsl:276-349): (selected row, pmf)
-SH_TREE float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n,
-                                            float start) {
+template <bool IN>
+__device__ __forceinline__ float2 tree_leaf_b(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n,
+                                              float start) {
   float rand = start;
   bool sample_max = rand > 0.5f;
   if (count > 1u) rand = rand * 2.0f - (sample_max ? 1.0f : 0.0f);
@@ -709,7 +738,7 @@ SH_TREE float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 
   uint32_t has = 0u;
   for (uint32_t i = 0u; i < count; ++i) {
     int32_t index = (int32_t)(first + i);
-    float2 importance = emitter_importance(load_light(v, first + i), load_trig(v, first + i).light, p, n);
+    float2 importance = emitter_importance_to<IN>(load_light(v, first + i), load_trig(v, first + i).light, p, n);
     float weight = sample_max ? importance.x : importance.y;
     float other = sample_max ? importance.y : importance.x;
     if (weight > 0.0f) {
@@ -766,8 +795,8 @@ SH_TREE float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 
       }
       chosen_min = 1.0f;
       total_min = valid;
-      chosen_max =
-          emitter_importance(load_light(v, (uint32_t)selected), load_trig(v, (uint32_t)selected).light, p, n).x;
+      chosen_max = emitter_importance_to<IN>(load_light(v, (uint32_t)selected), load_trig(v, (uint32_t)selected).light,
+                                             p, n).x;
     }
   }
   return make_float2((float)selected, 0.5f * (chosen_max / total_max + chosen_min / total_min));
@@ -775,8 +804,12 @@ SH_TREE float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 
 
 // tree_pick (lights.wgsl:350-386): (light row, pmf).  The descent is bounded
 // by the number of tree rows; a malformed tree ends the descent with pmf 0.
-SH_TREE float2 tree_pick(const ShadeView& v, uint32_t rows, v3 p, v3 n, float start,
-                                            uint32_t* leaf_row) {
+SH_TREE float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n, float start) {
+  return tree_leaf_b<false>(v, first, count, p, n, start);
+}
+template <bool IN>
+__device__ __forceinline__ float2 tree_pick_b(const ShadeView& v, uint32_t rows, v3 p, v3 n, float start,
+                                              uint32_t* leaf_row) {
   uint32_t at = f2u((float)v.looped + (float)v.tree);
   float rand = start;
   float pdf = 1.0f;
@@ -786,14 +819,15 @@ SH_TREE float2 tree_pick(const ShadeView& v, uint32_t rows, v3 p, v3 n, float st
     uint32_t count = f2u(node.d.y);
     if (count > 0u) {
       if (leaf_row) *leaf_row = at;
-      float2 leaf = tree_leaf(v, f2u(node.d.z), count, p, n, rand);
+      float2 leaf = IN ? tree_leaf_b<true>(v, f2u(node.d.z), count, p, n, rand)
+                       : tree_leaf(v, f2u(node.d.z), count, p, n, rand);
       return make_float2(leaf.x, leaf.y * pdf);
     }
     uint32_t left = at + 1u;
     uint32_t right = f2u(node.d.z);
     if (right >= rows) break;
-    float2 l = child_importance(v, left, p, n);
-    float2 r = child_importance(v, right, p, n);
+    float2 l = child_importance<IN>(v, left, p, n);
+    float2 r = child_importance<IN>(v, right, p, n);
     float total_max = l.x + r.x;
     if (total_max == 0.0f) return make_float2(0.0f, 0.0f);
     float total_min = l.y + r.y;
@@ -815,6 +849,9 @@ SH_TREE float2 tree_pick(const ShadeView& v, uint32_t rows, v3 p, v3 n, float st
     pdf = pdf * (at == left ? left_probability : 1.0f - left_probability);
   }
   return make_float2(0.0f, 0.0f);
+}
+SH_TREE float2 tree_pick(const ShadeView& v, uint32_t rows, v3 p, v3 n, float start, uint32_t* leaf_row) {
+  return tree_pick_b<false>(v, rows, p, n, start, leaf_row);
 }
 
 // ------------------------------------------------------------ emitters

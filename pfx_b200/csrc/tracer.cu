@@ -1137,7 +1137,13 @@ constexpr int SLOT_SUN = 0, SLOT_SKY = 1, SLOT_EMITTER = 2, SLOT_LOOPED = 3, SLO
 #define SLOT_MIN_BLOCKS 8
 #endif
 #ifndef PICK_MIN_BLOCKS
-#define PICK_MIN_BLOCKS 12
+#define PICK_MIN_BLOCKS 8
+#endif
+// Whether the descent kernel runs the light-tree functions inline or through their out-of-line copies.
+// Plain 4K pass: out of line at 12 blocks per SM 93.1 ms, at 8 blocks 92.5; inline at 12, 10 and 8
+// blocks 102.8, 104.8 and 108.1 ms (more code, fewer lanes per instruction).
+#ifndef PICK_INLINE
+#define PICK_INLINE false
 #endif
 
 __device__ __forceinline__ Rng slot_rng(const Pass& P, uint32_t pixel) {
@@ -1164,7 +1170,8 @@ __global__ void __launch_bounds__(kThreads, PICK_MIN_BLOCKS) k_tree_pick(const _
       start = random01(state);
       reinterpret_cast<float*>(P.w.thr + i)[3] = __uint_as_float(state);
     }
-    P.w.pick[qi] = tree_pick(V, P.light_rows, mk3(g0.x, g0.y, g0.z), mk3(g1.x, g1.y, g1.z), start, nullptr);
+    P.w.pick[qi] = tree_pick_b<PICK_INLINE>(V, P.light_rows, mk3(g0.x, g0.y, g0.z), mk3(g1.x, g1.y, g1.z), start,
+                                           nullptr);
   }
 }
 
@@ -1506,10 +1513,14 @@ int thread_select(uint32_t threads) { return threads == 64u ? 0 : (threads == 25
 // The deferred light slots one kind per launch, in slot order, each launched
 // only where the scene has that kind (the slots k_shade_lights skips without
 // a draw: no sun, no sky, no emissive triangles, no looped lights, no tree).
+// A black sky's slot adds nothing; it still draws two numbers from a path's
+// pcg state, so it is launched for the pcg sampler only.
 void launch_light_slots(const Pass& P, cudaStream_t st) {
   Grids& g = grids();
+  const bool black_sky = P.v.sky_radiance[0] == 0.0f && P.v.sky_radiance[1] == 0.0f && P.v.sky_radiance[2] == 0.0f;
   if (P.f.sun_color[3] > 0.0f) k_light_slot<SLOT_SUN><<<g.slot[SLOT_SUN], kThreads, 0, st>>>(P, 0u);
-  if (P.v.sky_width != 0u) k_light_slot<SLOT_SKY><<<g.slot[SLOT_SKY], kThreads, 0, st>>>(P, 1u);
+  if (P.v.sky_width != 0u && !(black_sky && P.sp.sobol))
+    k_light_slot<SLOT_SKY><<<g.slot[SLOT_SKY], kThreads, 0, st>>>(P, 1u);
   if (P.v.emitter_count != 0u) k_light_slot<SLOT_EMITTER><<<g.slot[SLOT_EMITTER], kThreads, 0, st>>>(P, 2u);
   for (uint32_t s = 1u; s <= P.v.looped; ++s)
     k_light_slot<SLOT_LOOPED><<<g.slot[SLOT_LOOPED], kThreads, 0, st>>>(P, 2u + s);

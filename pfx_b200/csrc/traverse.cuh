@@ -269,6 +269,10 @@ constexpr int BOX_EITHER = 0, BOX_BOUNDED = 1, BOX_IEEE = 2, BOX_PAIRED = 3;
 #ifndef TRACE_SPEC
 #define TRACE_SPEC true
 #endif
+// Whether any-hit walks open the nearer child first (their result does not depend on the order).
+#ifndef TRACE_ANY_NEAR
+#define TRACE_ANY_NEAR false
+#endif
 
 template <int BOX>
 __device__ __forceinline__ bool box_test(float lx, float ly, float lz, float hx, float hy, float hz, const TRay& ray,
@@ -456,12 +460,24 @@ struct Walker {
           ok1 = has1 && box_test<BOX>(q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, ray, n1) && n1 <= hit.t;
         }
         if (COUNT) counts.boxes += 1u;  // the left child, popped next by the reference
+        uint32_t r0 = q3.x, r1 = q3.y;
+        if constexpr (ANY && !COUNT && TRACE_ANY_NEAR) {
+          // any hit: whether the ray is blocked does not depend on the order,
+          // so the nearer child goes first
+          if (ok0 && ok1 && n1 < n0) {
+            r0 = q3.y;
+            r1 = q3.x;
+            float t = n0;
+            n0 = n1;
+            n1 = t;
+          }
+        }
         if ((ok1 || (COUNT && has1)) && top < (int)REF_STACK) {
-          st.put(top, q3.y, ok1 ? n1 : INFINITY);
+          st.put(top, r1, ok1 ? n1 : INFINITY);
           ++top;
         }
         if (ok0) {
-          ref = q3.x;
+          ref = r0;
           near_cur = n0;
         } else {
           pop(st);

@@ -79,12 +79,12 @@ def passes(cached: bool) -> None:
     w = synth.room_4k()
     t = Trace(w.scene, w.settings, w.width, w.height)
     # the launch choices the autotuner makes for this scene (bench.py reports them)
-    t.set_tuning(trace_threads=128, sort_shading=False)
+    t.set_tuning(trace_threads=64, sort_shading=False)
     n = 3
     if cached:
         c = RadianceCache()
         t.set_cache(c)
-        t.set_tuning(trace_threads=256, sort_shading=False)
+        t.set_tuning(trace_threads=64, sort_shading=False)
         n = 8
     for s in range(n):
         t.sample(1, s)
