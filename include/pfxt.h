@@ -524,6 +524,56 @@ int pfxt_cache_encoding(pfxt_cache* cache, float scales[16], uint32_t resolution
  * Sets that limit (0 makes every wait run out: a way to test the error path). */
 int pfxt_cache_set_wait_limit(pfxt_cache* cache, uint32_t polls);
 
+/* ------------------------------------------------------------ denoiser
+ *
+ * OIDN's RT filter (U-Net over colour, albedo and normal), as the reference's
+ * crates/denoise runs it (Denoiser, crates/denoise/src/lib.rs:58-361): the
+ * same weights, autoexposure, transfer function and tile split.  Images are
+ * row-major RGBA32F, width x height pixels; alpha passes through from the
+ * colour; normals in any space in [-1, 1], albedo in [0, 1], colour linear
+ * HDR.  The convolutions run on the tensor cores with FP32 accumulation; the
+ * result is within 1e-3 x (1 + |v|) of OIDN's FP32 output, the reference's
+ * own bar (crates/denoise/tests/oidn.rs). */
+typedef struct pfxt_denoiser pfxt_denoiser;
+
+/* Denoiser::new (lib.rs:81-110): parses an OIDN tensor archive (version 2;
+ * the reference embeds rt_hdr_alb_nrm.tza, OIDN 2.5.1's default RT weights)
+ * and uploads the network to the current device.  The blob is not kept.
+ * PFXT_ERR_INVALID: "invalid or corrupted weights blob", "unsupported weights
+ * blob version", "invalid tensor dimension|layout|data type", "<layer>: the
+ * weights do not match the network", "<layer>: weights not exact in half
+ * precision". */
+int pfxt_denoiser_create(const void* tza, size_t bytes, pfxt_denoiser** out);
+void pfxt_denoiser_destroy(pfxt_denoiser* denoiser);
+/* Denoiser::denoise (lib.rs:112-140): host images in, the denoised colour
+ * out (host), waits.  PFXT_ERR_INVALID for a zero size ("image dimensions
+ * must be nonzero"). */
+int pfxt_denoise(pfxt_denoiser* denoiser, uint32_t width, uint32_t height, const float* color, const float* albedo,
+                 const float* normal, float* out);
+/* Denoiser::denoise_textures_into (lib.rs:157-183): device images in and out
+ * (16-byte aligned), enqueued on `stream` (a cudaStream_t; NULL: the legacy
+ * stream); returns without waiting. */
+int pfxt_denoise_device(pfxt_denoiser* denoiser, uint32_t width, uint32_t height, const float* color,
+                        const float* albedo, const float* normal, float* out, void* stream);
+/* The same with a tracer's colour, albedo and normal films
+ * (pfxt_films_device) as the inputs, on the tracer's stream: what pfx does
+ * with Trace::color/albedo/normal after a frame's last sample. */
+int pfxt_denoise_trace(pfxt_denoiser* denoiser, pfxt_trace* trace, float* out_device);
+/* Denoiser::tiles (lib.rs:112-116): the tile size and count of the split for
+ * the last image size (0s before the first denoise). */
+int pfxt_denoiser_tiles(pfxt_denoiser* denoiser, uint32_t* tile_w, uint32_t* tile_h, uint32_t* count);
+/* Waits for the last denoise: its device time (ms) and multiply-adds.
+ * PFXT_ERR_DEVICE when a convolution's bounded wait ran out (see below). */
+int pfxt_denoiser_last(pfxt_denoiser* denoiser, float* ms, uint64_t* macs);
+/* The largest tile in pixels (default 2160 x 2160, OIDN's); smaller values
+ * split a frame into more tiles, as OIDN does on a device with less memory. */
+int pfxt_denoiser_set_max_tile_pixels(pfxt_denoiser* denoiser, uint64_t pixels);
+/* The convolutions wait for their tensor-core work and weight copies on
+ * mbarriers with a bounded number of polls (default 2^26).  A wait that runs
+ * out makes the denoise fail with PFXT_ERR_DEVICE once the kernel has drained
+ * its own work; the denoiser stays usable.  0 makes every wait run out. */
+int pfxt_denoiser_set_wait_limit(pfxt_denoiser* denoiser, uint32_t polls);
+
 #ifdef __cplusplus
 }
 #endif

@@ -332,6 +332,10 @@ pub struct PfxtSceneBlobs {
 pub struct PfxtCache {
     _private: [u8; 0],
 }
+#[repr(C)]
+pub struct PfxtDenoiser {
+    _private: [u8; 0],
+}
 
 /// `between(user, milliseconds)` of pfxt_sample_paced.
 pub type PfxtBetween = Option<unsafe extern "C" fn(*mut c_void, f64)>;
@@ -391,6 +395,15 @@ extern "C" {
     pub fn pfxt_cache_set_params(cache: *mut PfxtCache, mlp: *const f32, table: *const f32) -> c_int;
     pub fn pfxt_cache_encoding(cache: *mut PfxtCache, scales: *mut f32, resolutions: *mut u32, dense: *mut u32) -> c_int;
     pub fn pfxt_cache_set_wait_limit(cache: *mut PfxtCache, polls: u32) -> c_int;
+    pub fn pfxt_denoiser_create(tza: *const c_void, bytes: usize, out: *mut *mut PfxtDenoiser) -> c_int;
+    pub fn pfxt_denoiser_destroy(denoiser: *mut PfxtDenoiser);
+    pub fn pfxt_denoise(denoiser: *mut PfxtDenoiser, width: u32, height: u32, color: *const f32, albedo: *const f32, normal: *const f32, out: *mut f32) -> c_int;
+    pub fn pfxt_denoise_device(denoiser: *mut PfxtDenoiser, width: u32, height: u32, color: *const f32, albedo: *const f32, normal: *const f32, out: *mut f32, stream: *mut c_void) -> c_int;
+    pub fn pfxt_denoise_trace(denoiser: *mut PfxtDenoiser, trace: *mut PfxtTrace, out_device: *mut f32) -> c_int;
+    pub fn pfxt_denoiser_tiles(denoiser: *mut PfxtDenoiser, tile_w: *mut u32, tile_h: *mut u32, count: *mut u32) -> c_int;
+    pub fn pfxt_denoiser_last(denoiser: *mut PfxtDenoiser, ms: *mut f32, macs: *mut u64) -> c_int;
+    pub fn pfxt_denoiser_set_max_tile_pixels(denoiser: *mut PfxtDenoiser, pixels: u64) -> c_int;
+    pub fn pfxt_denoiser_set_wait_limit(denoiser: *mut PfxtDenoiser, polls: u32) -> c_int;
 }
 
 // Layout checks against the header's sizes.

@@ -339,3 +339,72 @@ impl Drop for Trace {
         unsafe { ffi::pfxt_destroy(self.raw) }
     }
 }
+
+/// `pfx_denoise::Denoiser` (crates/denoise/src/lib.rs:58-361) on the GPU:
+/// OIDN's RT filter with the weights the caller hands it (the reference
+/// embeds `rt_hdr_alb_nrm.tza`).
+pub struct Denoiser {
+    raw: *mut ffi::PfxtDenoiser,
+}
+
+impl Denoiser {
+    /// Denoiser::new (lib.rs:81-110).
+    pub fn new(weights: &[u8]) -> Result<Self, TraceError> {
+        let mut raw = ptr::null_mut();
+        // SAFETY: the blob is read during the call only.
+        check(unsafe { ffi::pfxt_denoiser_create(weights.as_ptr() as *const c_void, weights.len(), &mut raw) })?;
+        Ok(Self { raw })
+    }
+
+    /// Denoiser::denoise (lib.rs:112-140): row-major RGBA pixels in and out.
+    pub fn denoise(
+        &mut self,
+        width: u32,
+        height: u32,
+        color: &[[f32; 4]],
+        albedo: &[[f32; 4]],
+        normal: &[[f32; 4]],
+    ) -> Result<Vec<[f32; 4]>, TraceError> {
+        let pixels = width as usize * height as usize;
+        if color.len() != pixels || albedo.len() != pixels || normal.len() != pixels {
+            return Err(TraceError::Setup("image size mismatch".into()));
+        }
+        let mut out = vec![[0f32; 4]; pixels];
+        // SAFETY: every image holds width * height RGBA pixels.
+        check(unsafe {
+            ffi::pfxt_denoise(
+                self.raw,
+                width,
+                height,
+                color.as_ptr() as *const f32,
+                albedo.as_ptr() as *const f32,
+                normal.as_ptr() as *const f32,
+                out.as_mut_ptr() as *mut f32,
+            )
+        })?;
+        Ok(out)
+    }
+
+    /// Denoiser::denoise_textures_into (lib.rs:157-183) with a trace's films:
+    /// `out` is device memory of width * height RGBA32F, written on the
+    /// trace's stream.
+    pub fn denoise_trace_into(&mut self, trace: &mut Trace, out: *mut f32) -> Result<(), TraceError> {
+        // SAFETY: `out` is the caller's device buffer of the trace's size.
+        check(unsafe { ffi::pfxt_denoise_trace(self.raw, trace.raw(), out) })
+    }
+
+    /// Denoiser::tiles (lib.rs:112-116).
+    pub fn tiles(&self) -> Option<(u32, u32, usize)> {
+        let (mut w, mut h, mut n) = (0u32, 0u32, 0u32);
+        // SAFETY: plain out-parameters.
+        let ok = unsafe { ffi::pfxt_denoiser_tiles(self.raw, &mut w, &mut h, &mut n) } == 0;
+        (ok && n > 0).then_some((w, h, n as usize))
+    }
+}
+
+impl Drop for Denoiser {
+    fn drop(&mut self) {
+        // SAFETY: the handle is owned and destroyed once.
+        unsafe { ffi::pfxt_denoiser_destroy(self.raw) }
+    }
+}

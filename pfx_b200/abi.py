@@ -215,6 +215,18 @@ PROTOTYPES = [
     ("pfxt_adaptive_mark", C.c_int, [C.c_void_p, C.c_uint32, C.c_float, C.POINTER(C.c_uint32)]),
     ("pfxt_adaptive_snaps_device", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("pfxt_set_pixel_mask", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pfxt_denoiser_create", C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)]),
+    ("pfxt_denoiser_destroy", None, [C.c_void_p]),
+    ("pfxt_denoise", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_void_p]),
+    ("pfxt_denoise_device", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]),
+    ("pfxt_denoise_trace", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pfxt_denoiser_tiles", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                      C.POINTER(C.c_uint32)]),
+    ("pfxt_denoiser_last", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint64)]),
+    ("pfxt_denoiser_set_max_tile_pixels", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("pfxt_denoiser_set_wait_limit", C.c_int, [C.c_void_p, C.c_uint32]),
 ]
 NOALLOC_MAX_RAYS = 1 << 20
 
@@ -231,6 +243,7 @@ EXTRA = [
     ("pfxt_debug_select_nth", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_int32, C.c_void_p]),
     ("pfxt_debug_gpu_bvh", C.c_int, [C.c_int32]),
     ("pfxt_debug_scene_gpu_builds", C.c_uint32, [C.c_void_p]),
+    ("pfxt_debug_denoise_plan", C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("pfxt_trace_counts_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                            C.c_void_p]),
 ]

@@ -38,6 +38,7 @@ SOURCES = [
     ("noalloc.cu", EXACT),
     ("bvh_gpu.cu", EXACT),
     ("cache.cu", EXACT),
+    ("denoise.cu", EXACT),
 ]
 
 HEADERS = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [REPO / "include" / "pfxt.h"]

@@ -14,6 +14,7 @@
 #include "pfxt_internal.h"
 #include "tracer.h"
 #include "cache.h"
+#include "denoise.h"
 
 using namespace pfxt;
 
@@ -994,4 +995,137 @@ int pfxt_cache_encoding(pfxt_cache* c, float scales[16], uint32_t resolutions[16
     if (dense) *dense = c->grid.dense;
   });
 }
+}  // extern "C"
+
+/* ------------------------------------------------------------ denoiser */
+
+struct pfxt_denoiser {
+  std::unique_ptr<pfxt::Denoiser> d;
+};
+
+extern "C" {
+
+int pfxt_denoiser_create(const void* tza, size_t bytes, pfxt_denoiser** out) {
+  return guarded([&]() {
+    if (!out) throw Invalid("null argument");
+    *out = nullptr;
+    auto h = std::make_unique<pfxt_denoiser>();
+    h->d.reset(denoiser_create(tza, bytes));
+    *out = h.release();
+  });
+}
+
+void pfxt_denoiser_destroy(pfxt_denoiser* denoiser) { delete denoiser; }
+
+int pfxt_denoise(pfxt_denoiser* h, uint32_t width, uint32_t height, const float* color, const float* albedo,
+                 const float* normal, float* out) {
+  return guarded([&]() {
+    if (!h || !color || !albedo || !normal || !out) throw Invalid("null argument");
+    if (width == 0 || height == 0) throw Invalid("image dimensions must be nonzero");
+    Denoiser& d = *h->d;
+    check(cudaSetDevice(d.device), "denoiser device");
+    if (!d.stream) check(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking), "denoiser stream");
+    const size_t pixels = (size_t)width * height;
+    if (pixels > d.images_pixels) {
+      if (d.d_images) cudaFree(d.d_images);
+      d.d_images = nullptr;
+      d.images_pixels = 0;
+      check(cudaMalloc(&d.d_images, pixels * 4u * sizeof(float4)), "denoiser images");
+      d.images_pixels = pixels;
+    }
+    float4* img = d.d_images;
+    const float* in[3] = {color, albedo, normal};
+    for (int k = 0; k < 3; ++k)
+      check(cudaMemcpyAsync(img + k * pixels, in[k], pixels * sizeof(float4), cudaMemcpyHostToDevice, d.stream),
+            "denoiser upload");
+    denoise_device(d, width, height, img, img + pixels, img + 2 * pixels, img + 3 * pixels, d.stream);
+    check(cudaMemcpyAsync(out, img + 3 * pixels, pixels * sizeof(float4), cudaMemcpyDeviceToHost, d.stream),
+          "denoiser readback");
+    check(cudaStreamSynchronize(d.stream), "denoise");
+    denoiser_finish(d);
+  });
+}
+
+int pfxt_denoise_device(pfxt_denoiser* h, uint32_t width, uint32_t height, const float* color, const float* albedo,
+                        const float* normal, float* out, void* stream) {
+  return guarded([&]() {
+    if (!h) throw Invalid("null argument");
+    for (const float* p : {color, albedo, normal, const_cast<const float*>(out)})
+      if (!p || (reinterpret_cast<uintptr_t>(p) & 15u)) throw Invalid("device images must be 16-byte aligned");
+    denoise_device(*h->d, width, height, reinterpret_cast<const float4*>(color),
+                   reinterpret_cast<const float4*>(albedo), reinterpret_cast<const float4*>(normal),
+                   reinterpret_cast<float4*>(out), static_cast<cudaStream_t>(stream));
+  });
+}
+
+int pfxt_denoise_trace(pfxt_denoiser* h, pfxt_trace* t, float* out) {
+  return guarded([&]() {
+    if (!h || !t || !out) throw Invalid("null argument");
+    if (reinterpret_cast<uintptr_t>(out) & 15u) throw Invalid("device images must be 16-byte aligned");
+    check(cudaSetDevice(t->device), "trace device");
+    denoise_device(*h->d, t->width, t->height, reinterpret_cast<const float4*>(t->d_color),
+                   reinterpret_cast<const float4*>(t->d_albedo), reinterpret_cast<const float4*>(t->d_normal),
+                   reinterpret_cast<float4*>(out), t->stream);
+  });
+}
+
+int pfxt_denoiser_tiles(pfxt_denoiser* h, uint32_t* tile_w, uint32_t* tile_h, uint32_t* count) {
+  return guarded([&]() {
+    if (!h) throw Invalid("null argument");
+    const Denoiser& d = *h->d;
+    if (tile_w) *tile_w = d.width ? d.plan.tile_w : 0u;
+    if (tile_h) *tile_h = d.width ? d.plan.tile_h : 0u;
+    if (count) *count = d.width ? (uint32_t)d.plan.tiles.size() : 0u;
+  });
+}
+
+int pfxt_denoiser_last(pfxt_denoiser* h, float* ms, uint64_t* macs) {
+  return guarded([&]() {
+    if (!h) throw Invalid("null argument");
+    float m = denoiser_finish(*h->d);
+    if (ms) *ms = m;
+    if (macs) *macs = h->d->last_macs;
+  });
+}
+
+int pfxt_denoiser_set_max_tile_pixels(pfxt_denoiser* h, uint64_t pixels) {
+  return guarded([&]() {
+    if (!h) throw Invalid("null argument");
+    if (pixels < 16u * 16u) throw Invalid("a tile holds at least 16 x 16 pixels");
+    h->d->max_tile_pixels = pixels;
+    h->d->width = h->d->height = 0;  // the next denoise plans again
+  });
+}
+
+// The tile split of a height x width image (test hook): up to `capacity`
+// tiles as 12 words each (src, dst, size, out_src, out_dst, out_size as (y, x)),
+// then tile_h, tile_w, overlap and the count in `head`.
+int pfxt_debug_denoise_plan(uint32_t height, uint32_t width, uint64_t max_tile_pixels, uint32_t* tiles,
+                            uint32_t capacity, uint32_t* head) {
+  return guarded([&]() {
+    if (!head || (capacity && !tiles)) throw Invalid("null argument");
+    if (width == 0 || height == 0) throw Invalid("image dimensions must be nonzero");
+    DenoisePlan p = denoise_plan(height, width, max_tile_pixels);
+    head[0] = p.tile_h;
+    head[1] = p.tile_w;
+    head[2] = p.overlap;
+    head[3] = (uint32_t)p.tiles.size();
+    for (size_t i = 0; i < p.tiles.size() && i < capacity; ++i) {
+      const DenoiseTile& t = p.tiles[i];
+      const uint32_t* parts[6] = {t.src, t.dst, t.size, t.out_src, t.out_dst, t.out_size};
+      for (int k = 0; k < 6; ++k) {
+        tiles[12 * i + 2 * k] = parts[k][0];
+        tiles[12 * i + 2 * k + 1] = parts[k][1];
+      }
+    }
+  });
+}
+
+int pfxt_denoiser_set_wait_limit(pfxt_denoiser* h, uint32_t polls) {
+  return guarded([&]() {
+    if (!h) throw Invalid("null argument");
+    h->d->wait_limit = polls;
+  });
+}
+
 }  // extern "C"

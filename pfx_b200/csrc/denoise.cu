@@ -1,0 +1,764 @@
+// The denoiser on sm_100a: OIDN's RT filter as the reference's crates/denoise
+// runs it (lib.rs, net.rs, tile.rs, process.wgsl, wgsl.rs), with the U-Net's
+// 3x3 convolutions as implicit GEMMs on the 5th-generation tensor cores.
+//
+// Layout.  A tensor of the U-Net is FP32, channels last, [y][x][C] with C
+// padded to a multiple of 16, at its level's size (the tile's size >> level).
+// A convolution is a GEMM per tile of R = 4 output rows x 128 pixels: M = the
+// 128 pixels of a row, N = the output channels, K = 9 taps x the input
+// channels, walked in chunks of 16 input channels.  For a chunk, the R + 2
+// input rows x 130 pixels (one pixel of border each side) are staged in shared
+// memory in the no-swizzle K-major canonical layout, pixel after pixel
+// (16 bytes = 8 channels per row of a core matrix), so the A operand of tap
+// (ky, kx) for output row r is the same bytes at a start address moved by
+// (r + ky) rows and kx pixels: no data moves per tap.  The chunk's weights
+// (9 taps x 16 channels x N) are one contiguous block, staged by one bulk
+// copy (TMA, no multicast).  One thread issues tcgen05.mma.kind::f16 (M =
+// 128, K = 16) into R accumulators in TMEM (columns 128 r), and the next
+// chunk is staged while those MMAs run (two stages).
+//
+// Precision.  The reference computes in FP32 (weights are FP16 in the blob,
+// exact in FP32).  Each staged activation is split into hi = fp16(a) and lo =
+// fp16(a - hi), and both are multiplied by the FP16 weights with FP32
+// accumulation, so an activation keeps ~22 significant bits; the products
+// are exact, and the sums round in FP32 as the reference's do (in another
+// order).  Weights that are not exact in FP16 are refused.
+//
+// Epilogue.  tcgen05.ld per 16 columns, bias, ReLU; a pooling layer takes the
+// max of its two rows in the thread and of the neighbouring pixel's lane by
+// a shuffle (max pooling after ReLU = ReLU after max pooling).  Upsampling and
+// concatenation are in the staging: channels of the first source are read at
+// (y / 2, x / 2) of the half-size tensor, the skip source's at (y, x).
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+
+#include "denoise.h"
+#include "pfxt_internal.h"
+#include "tracer.h"
+#include "umma.cuh"
+
+namespace pfxt {
+
+namespace {
+
+void dcheck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw DeviceError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ------------------------------------------------------------------ weights blob
+constexpr const char* CORRUPT = "invalid or corrupted weights blob";
+
+struct Tensor {
+  std::vector<uint32_t> dims;
+  std::vector<float> data;
+  std::vector<uint16_t> half;  // the FP16 bits of every value (exact)
+  bool exact_half = true;
+};
+
+struct Reader {
+  const uint8_t* bytes;
+  size_t size, at;
+  const uint8_t* take(size_t count) {
+    if (at > size || count > size - at) throw Invalid(CORRUPT);
+    const uint8_t* p = bytes + at;
+    at += count;
+    return p;
+  }
+  template <class T>
+  T get() {
+    T v;
+    memcpy(&v, take(sizeof(T)), sizeof(T));
+    return v;
+  }
+};
+
+float half_bits_to_float(uint16_t h) { return __half2float(__ushort_as_half(h)); }
+
+// OIDN's tensor archive, version 2 (tza.rs:51-118; OIDN core/tza.cpp): magic
+// 0x41D7, major version 2, the table's offset; per tensor its name, dims,
+// layout ("x" or "oihw"), type ('f' or 'h') and data offset.
+std::map<std::string, Tensor> parse_tza(const uint8_t* bytes, size_t size) {
+  Reader head{bytes, size, 0};
+  if (head.get<uint16_t>() != 0x41D7u) throw Invalid(CORRUPT);
+  uint8_t major = head.get<uint8_t>();
+  head.get<uint8_t>();
+  if (major != 2) throw Invalid("unsupported weights blob version");
+  uint64_t table = head.get<uint64_t>();
+  if (table > size) throw Invalid(CORRUPT);
+  Reader in{bytes, size, (size_t)table};
+  uint32_t count = in.get<uint32_t>();
+  std::map<std::string, Tensor> out;
+  for (uint32_t i = 0; i < count; ++i) {
+    uint16_t name_len = in.get<uint16_t>();
+    const uint8_t* name = in.take(name_len);
+    uint8_t rank = in.get<uint8_t>();
+    Tensor t;
+    uint64_t elements = 1;
+    for (uint8_t r = 0; r < rank; ++r) {
+      uint32_t dim = in.get<uint32_t>();
+      if (dim == 0 || dim > (1u << 30)) throw Invalid("invalid tensor dimension");
+      t.dims.push_back(dim);
+      elements *= dim;
+      if (elements > (1ull << 32)) throw Invalid(CORRUPT);
+    }
+    const uint8_t* layout = in.take(rank);
+    bool x = rank == 1 && layout[0] == 'x';
+    bool oihw = rank == 4 && memcmp(layout, "oihw", 4) == 0;
+    if (!x && !oihw) throw Invalid("invalid tensor layout");
+    uint8_t type = in.get<uint8_t>();
+    if (type != 'f' && type != 'h') throw Invalid("invalid tensor data type");
+    uint64_t offset = in.get<uint64_t>();
+    Reader data{bytes, size, (size_t)offset};
+    if (offset > size) throw Invalid(CORRUPT);
+    const uint8_t* raw = data.take((size_t)(elements * (type == 'f' ? 4 : 2)));
+    t.data.resize(elements);
+    t.half.resize(elements);
+    for (uint64_t e = 0; e < elements; ++e) {
+      if (type == 'h') {
+        uint16_t h;
+        memcpy(&h, raw + 2 * e, 2);
+        t.half[e] = h;
+        t.data[e] = half_bits_to_float(h);
+      } else {
+        float f;
+        memcpy(&f, raw + 4 * e, 4);
+        t.data[e] = f;
+        uint16_t h = __half_as_ushort(__float2half_rn(f));
+        t.half[e] = h;
+        if (!(half_bits_to_float(h) == f)) t.exact_half = false;
+      }
+    }
+    out.emplace(std::string(reinterpret_cast<const char*>(name), name_len), std::move(t));
+  }
+  return out;
+}
+
+uint32_t pad16(uint32_t c) { return (c + 15u) / 16u * 16u; }
+
+// The weights of one layer as conv kernels stage them: for each chunk of 16
+// padded input channels (the first source's padded channels, then the skip
+// source's), 9 taps x 2 groups of 8 channels x n output rows x 8 halves,
+//   index = (((chunk * 9 + tap) * 2 + group) * n + o) * 8 + j,
+// the K-major canonical layout of the B operand of one tap (rows = output
+// channels, 16-byte rows of 8 input channels).  Padding is zero.
+std::vector<uint16_t> conv_chunks(const DenoiseLayer& L, const Tensor& w) {
+  const uint32_t chunks = (L.c0 + L.c1) / 16u, inputs = L.in0 + L.in1;
+  std::vector<uint16_t> out((size_t)chunks * 9u * 2u * L.n * 8u, 0u);
+  for (uint32_t k = 0; k < chunks; ++k)
+    for (uint32_t t = 0; t < 9; ++t)
+      for (uint32_t g = 0; g < 2; ++g)
+        for (uint32_t o = 0; o < L.out; ++o)
+          for (uint32_t j = 0; j < 8; ++j) {
+            uint32_t pc = k * 16u + g * 8u + j;
+            int64_t ch = -1;
+            if (pc < L.c0) {
+              if (pc < L.in0) ch = pc;
+            } else if (pc - L.c0 < L.in1) {
+              ch = L.in0 + (pc - L.c0);
+            }
+            if (ch < 0) continue;
+            out[((((size_t)k * 9u + t) * 2u + g) * L.n + o) * 8u + j] = w.half[((size_t)o * inputs + ch) * 9u + t];
+          }
+  return out;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ kernels
+namespace {
+
+constexpr uint32_t CONV_THREADS = 256;               // 8 warps: staging; the epilogue by lane quarters
+constexpr uint32_t CONV_ROWS = 4;                    // output rows per CTA, one TMEM accumulator each
+constexpr uint32_t CONV_PIX = 128;                   // pixels per output row (M of the MMA)
+constexpr uint32_t PATCH_W = CONV_PIX + 2;           // staged pixels per input row
+constexpr uint32_t PATCH_ROWS = CONV_ROWS + 2;       // staged input rows
+constexpr uint32_t A_PLANE = PATCH_W * 16u;          // bytes of one (row, group of 8 channels) plane
+constexpr uint32_t A_BYTES = PATCH_ROWS * 2u * A_PLANE;  // one chunk of one half (hi or lo)
+constexpr uint32_t N_MAX = 128;                      // output channels a CTA holds (TMEM columns per row)
+constexpr uint32_t W_MAX = 9u * 2u * N_MAX * 16u;    // one chunk of weights at N_MAX
+constexpr uint32_t STAGE = 2u * A_BYTES + W_MAX;
+constexpr uint32_t CTRL = 2u * STAGE;                // mbarriers and the TMEM slot after the two stages
+constexpr uint32_t CONV_SMEM = CTRL + 64u;
+constexpr uint32_t TMEM_COLS = 512;                  // CONV_ROWS x N_MAX
+static_assert(CONV_ROWS * N_MAX <= TMEM_COLS, "accumulators fit TMEM");
+static_assert(CONV_SMEM <= 227u * 1024u, "shared memory per CTA");
+constexpr uint32_t ERR_CONV_WAIT = 1u, ERR_CONV_DRAIN = 2u;
+// Polls of the waits that drain a CTA's own work in flight (its MMAs and
+// weight copies) before it frees its TMEM and leaves, whatever the main
+// loop's limit: work this kernel issued itself always completes.
+constexpr uint32_t DRAIN_LIMIT = 1u << 26;
+
+// Instruction descriptor of kind::f16 with FP16 A and B and an FP32 accumulator, K-major operands.
+__host__ __device__ constexpr uint32_t idesc_f16(uint32_t M, uint32_t N) {
+  return (1u << 4) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+struct ConvArgs {
+  const float* src0;          // [H >> up][W >> up][c0]
+  const float* src1;          // [H][W][c1] (c1 = 0: none)
+  const uint16_t* weights;    // conv_chunks() layout
+  const float* bias;          // n
+  float* dst;                 // [H][W][n], or [H/2][W/2][n] when pooling
+  uint32_t H, W, c0, c1, n, up, pool;
+  uint32_t* error;
+  uint32_t wait_limit;        // polls of a bounded mbarrier wait
+};
+
+__device__ __forceinline__ uint32_t pack_half2(__half a, __half b) {
+  return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
+}
+
+// Stage chunk k's input rows into one stage: hi and lo halves of every value.
+__device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint32_t y0, uint32_t x0, uint8_t* hi,
+                                            uint8_t* lo) {
+  const uint32_t chunks0 = a.c0 >> 4;
+  const bool first = k < chunks0;
+  const float* src = first ? a.src0 : a.src1;
+  const uint32_t C = first ? a.c0 : a.c1;
+  const uint32_t ch = (first ? k : k - chunks0) * 16u;
+  const uint32_t sh = first ? a.up : 0u;
+  const uint32_t SW = a.W >> sh;
+  for (uint32_t item = threadIdx.x; item < PATCH_ROWS * PATCH_W * 4u; item += CONV_THREADS) {
+    const uint32_t q = item & 3u, pix = item >> 2;
+    const uint32_t row = pix / PATCH_W, px = pix - row * PATCH_W;
+    const int y = (int)(y0 + row) - 1, x = (int)(x0 + px) - 1;
+    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (y >= 0 && y < (int)a.H && x >= 0 && x < (int)a.W)
+      v = __ldg(reinterpret_cast<const float4*>(src + ((size_t)((uint32_t)y >> sh) * SW + ((uint32_t)x >> sh)) * C +
+                                                ch) + q);
+    __half h0 = __float2half_rn(v.x), h1 = __float2half_rn(v.y), h2 = __float2half_rn(v.z), h3 = __float2half_rn(v.w);
+    __half l0 = __float2half_rn(v.x - __half2float(h0)), l1 = __float2half_rn(v.y - __half2float(h1)),
+           l2 = __float2half_rn(v.z - __half2float(h2)), l3 = __float2half_rn(v.w - __half2float(h3));
+    const uint32_t off = (row * 2u + (q >> 1)) * A_PLANE + px * 16u + (q & 1u) * 8u;
+    *reinterpret_cast<uint2*>(hi + off) = make_uint2(pack_half2(h0, h1), pack_half2(h2, h3));
+    *reinterpret_cast<uint2*>(lo + off) = make_uint2(pack_half2(l0, l1), pack_half2(l2, l3));
+  }
+}
+
+// One 3x3 convolution (+ bias, ReLU, and 2x2 max pooling when a.pool) of a
+// tile of CONV_ROWS rows x 128 pixels.  Grid: (ceil(W / 128), ceil(H / CONV_ROWS)).
+__global__ void __launch_bounds__(CONV_THREADS, 1) k_conv(const __grid_constant__ ConvArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+  const uint32_t x0 = blockIdx.x * CONV_PIX, y0 = blockIdx.y * CONV_ROWS;
+  const uint32_t base = umma::smem_addr(smem);
+  const uint32_t wbar[2] = {base + CTRL, base + CTRL + 8u}, mbar[2] = {base + CTRL + 16u, base + CTRL + 24u};
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + CTRL + 32u);
+  if (tid == 0) {
+    for (int s = 0; s < 2; ++s) {
+      umma::mbar_init(wbar[s], 1);
+      umma::mbar_init(mbar[s], 1);
+    }
+  }
+  if (warp == 0) umma::tmem_alloc(slot, TMEM_COLS);
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = *slot;
+  const uint32_t chunks = (a.c0 + a.c1) >> 4;
+  const uint32_t wbytes = 9u * 2u * a.n * 16u;
+  const uint32_t id = idesc_f16(128, a.n);
+  uint32_t issued = 0, loads = 0;  // chunks whose MMAs were committed; weight copies issued
+  bool late = false;
+  for (uint32_t k = 0; k < chunks; ++k) {
+    const uint32_t s = k & 1u;
+    uint8_t* hi = smem + s * STAGE;
+    uint8_t* lo = hi + A_BYTES;
+    const uint32_t w_addr = base + s * STAGE + 2u * A_BYTES;
+    if (k >= 2) {  // the MMAs of chunk k - 2 read this stage
+      bool ok = umma::mbar_wait(mbar[s], ((k - 2u) >> 1) & 1u, a.wait_limit);
+      if (__syncthreads_or(!ok)) {
+        late = true;
+        break;
+      }
+    }
+    if (tid == 0) {
+      umma::mbar_expect_tx(wbar[s], wbytes);
+      umma::bulk_load(w_addr, a.weights + (size_t)k * (wbytes / 2u), wbytes, wbar[s]);
+    }
+    loads = k + 1u;
+    stage_chunk(a, k, y0, x0, hi, lo);
+    umma::fence_async_smem();
+    __syncthreads();
+    bool failed = false;
+    if (tid == 0) {
+      if (umma::mbar_wait(wbar[s], (k >> 1) & 1u, a.wait_limit)) {
+        umma::fence_after();
+        const uint32_t a_hi = base + s * STAGE, a_lo = a_hi + A_BYTES;
+#pragma unroll 1
+        for (uint32_t r = 0; r < CONV_ROWS; ++r) {
+#pragma unroll
+          for (uint32_t t = 0; t < 9; ++t) {
+            const uint32_t off = (r + t / 3u) * 2u * A_PLANE + (t % 3u) * 16u;
+            const uint64_t bd = umma::desc(w_addr + t * 2u * a.n * 16u, a.n * 16u, 128u);
+            umma::mma(tmem + r * N_MAX, umma::desc(a_hi + off, A_PLANE, 128u), bd, id, (k > 0 || t > 0) ? 1u : 0u);
+            umma::mma(tmem + r * N_MAX, umma::desc(a_lo + off, A_PLANE, 128u), bd, id, 1u);
+          }
+        }
+        umma::commit(mbar[s]);
+      } else {
+        failed = true;
+      }
+    }
+    if (__syncthreads_or(failed)) {
+      late = true;
+      break;
+    }
+    issued = k + 1u;
+  }
+  // every MMA issued is done when the last commit's phase completes
+  bool drained = true;
+  if (issued > 0) drained = umma::mbar_wait(mbar[(issued - 1u) & 1u], ((issued - 1u) >> 1) & 1u, DRAIN_LIMIT);
+  if (loads > issued) {  // a weight copy whose wait ran out: let it land before the CTA leaves
+    const uint32_t k = loads - 1u;
+    drained = umma::mbar_wait(wbar[k & 1u], (k >> 1) & 1u, DRAIN_LIMIT) && drained;
+  }
+  drained = __syncthreads_and(drained);
+  umma::fence_after();
+  if (late || !drained) {
+    if (tid == 0) atomicOr(a.error, (late ? ERR_CONV_WAIT : 0u) | (drained ? 0u : ERR_CONV_DRAIN));
+  } else {
+    // epilogue: warp w reads TMEM lanes 32 (w % 4).., rows 2 (w / 4) and 2 (w / 4) + 1
+    const uint32_t quarter = warp & 3u, r0 = (warp >> 2) * 2u;
+    const uint32_t x = x0 + quarter * 32u + lane;
+    for (uint32_t j = 0; j < a.n; j += 16u) {
+      float v0[16], v1[16];
+      umma::ld16(umma::taddr(tmem, quarter * 32u, r0 * N_MAX + j), v0);
+      umma::ld16(umma::taddr(tmem, quarter * 32u, (r0 + 1u) * N_MAX + j), v1);
+      float b[16];
+#pragma unroll
+      for (int c = 0; c < 16; ++c) b[c] = __ldg(a.bias + j + c);
+      if (a.pool) {
+        float m[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          m[c] = fmaxf(v0[c], v1[c]);
+          m[c] = fmaxf(m[c], __shfl_xor_sync(0xffffffffu, m[c], 1));
+          m[c] = fmaxf(m[c] + b[c], 0.0f);
+        }
+        const uint32_t oy = (y0 + r0) >> 1, ox = x >> 1, OH = a.H >> 1, OW = a.W >> 1;
+        if ((lane & 1u) == 0u && oy < OH && ox < OW) {
+          float4* o = reinterpret_cast<float4*>(a.dst + ((size_t)oy * OW + ox) * a.n + j);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) o[c] = make_float4(m[4 * c], m[4 * c + 1], m[4 * c + 2], m[4 * c + 3]);
+        }
+      } else {
+#pragma unroll
+        for (uint32_t rr = 0; rr < 2; ++rr) {
+          const uint32_t y = y0 + r0 + rr;
+          if (y < a.H && x < a.W) {
+            const float* v = rr ? v1 : v0;
+            float4* o = reinterpret_cast<float4*>(a.dst + ((size_t)y * a.W + x) * a.n + j);
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+              o[c] = make_float4(fmaxf(v[4 * c] + b[4 * c], 0.0f), fmaxf(v[4 * c + 1] + b[4 * c + 1], 0.0f),
+                                 fmaxf(v[4 * c + 2] + b[4 * c + 2], 0.0f), fmaxf(v[4 * c + 3] + b[4 * c + 3], 0.0f));
+          }
+        }
+      }
+    }
+  }
+  umma::fence_before();
+  __syncthreads();
+  if (drained && warp == 0) umma::tmem_free(tmem, TMEM_COLS);
+}
+
+// ------------------------------------------------------------------ image processing
+constexpr float DN_FLT_MAX = 3.4028234663852886e38f;
+
+__device__ __forceinline__ float nan_to_zero(float v) { return isnan(v) ? 0.0f : v; }
+
+// OIDN's PU transfer function (process.wgsl:45-63; OIDN devices/gpu/gpu_input_process.h).
+__device__ __forceinline__ float pu_forward(float y) {
+  if (y <= 1.57945760e-06f) return 1.41283765e+03f * y;
+  if (y <= 3.22087631e-02f) return 1.64593172e+00f * powf(y, 4.31384981e-01f) + -2.94139609e-03f;
+  return 1.92653254e-01f * logf(y + 6.26026094e-03f) + 9.98620152e-01f;
+}
+__device__ __forceinline__ float pu_inverse(float x) {
+  if (x <= 2.23151711e-03f) return x / 1.41283765e+03f;
+  if (x <= 3.70974749e-01f) return powf((x - -2.94139609e-03f) / 1.64593172e+00f, 1.0f / 4.31384981e-01f);
+  return expf((x - 9.98620152e-01f) / 1.92653254e-01f) - 6.26026094e-03f;
+}
+
+__device__ __forceinline__ float luminance(float4 c) {
+  float r = fminf(fmaxf(nan_to_zero(c.x), 0.0f), DN_FLT_MAX), g = fminf(fmaxf(nan_to_zero(c.y), 0.0f), DN_FLT_MAX),
+        b = fminf(fmaxf(nan_to_zero(c.z), 0.0f), DN_FLT_MAX);
+  return 0.212671f * r + 0.715160f * g + 0.072169f * b;
+}
+
+// Autoexposure, step 1 (process.wgsl:108-134): the mean luminance of bin
+// (blockIdx.x, blockIdx.y) of a ceil(W/16) x ceil(H/16) split of the image.
+__global__ void __launch_bounds__(256) k_exposure_bins(const float4* __restrict__ color, uint32_t W, uint32_t H,
+                                                       float* __restrict__ bins) {
+  __shared__ float sums[256];
+  const uint32_t gx = gridDim.x, gy = gridDim.y;
+  const uint32_t bh = blockIdx.y * H / gy, eh = (blockIdx.y + 1u) * H / gy;
+  const uint32_t bw = blockIdx.x * W / gx, ew = (blockIdx.x + 1u) * W / gx;
+  const uint32_t h = bh + (threadIdx.x >> 4), w = bw + (threadIdx.x & 15u);
+  sums[threadIdx.x] = (h < eh && w < ew) ? luminance(color[(size_t)h * W + w]) : 0.0f;
+  for (uint32_t i = 128; i > 0; i >>= 1) {
+    __syncthreads();
+    if (threadIdx.x < i) sums[threadIdx.x] += sums[threadIdx.x + i];
+  }
+  if (threadIdx.x == 0) bins[blockIdx.y * gx + blockIdx.x] = sums[0] / (float)((eh - bh) * (ew - bw));
+}
+
+// Autoexposure, step 2 (process.wgsl:136-157): 0.18 over the geometric mean
+// of the bins above 1e-8 (1 when there are none).  One block of 256.
+__global__ void __launch_bounds__(256) k_exposure_reduce(const float* __restrict__ bins, uint32_t count,
+                                                         float* __restrict__ scale) {
+  __shared__ float sums[256];
+  __shared__ uint32_t counts[256];
+  float sum = 0.0f;
+  uint32_t n = 0;
+  for (uint32_t i = threadIdx.x; i < count; i += 256u) {
+    float l = bins[i];
+    if (l > 1e-8f) {
+      sum += log2f(l);
+      n += 1u;
+    }
+  }
+  sums[threadIdx.x] = sum;
+  counts[threadIdx.x] = n;
+  for (uint32_t i = 128; i > 0; i >>= 1) {
+    __syncthreads();
+    if (threadIdx.x < i) {
+      sums[threadIdx.x] += sums[threadIdx.x + i];
+      counts[threadIdx.x] += counts[threadIdx.x + i];
+    }
+  }
+  if (threadIdx.x == 0) scale[0] = counts[0] > 0u ? 0.18f / exp2f(sums[0] / (float)counts[0]) : 1.0f;
+}
+
+struct TileArgs {
+  uint32_t src[2], dst[2], size[2], out_src[2], out_dst[2], out_size[2];
+  uint32_t tile_h, tile_w, width;
+  float norm, rcp_norm;
+};
+
+// The tile's input tensor (process.wgsl:65-86): colour times the exposure,
+// NaN to 0, clamped, through the PU curve and normalised; albedo clamped to
+// [0, 1]; normal clamped to [-1, 1] and mapped to [0, 1]; 9 channels of 16.
+__global__ void __launch_bounds__(256) k_input(const __grid_constant__ TileArgs t, const float4* __restrict__ color,
+                                               const float4* __restrict__ albedo, const float4* __restrict__ normal,
+                                               const float* __restrict__ scale, float* __restrict__ out) {
+  const uint32_t n = t.tile_h * t.tile_w;
+  const float s = scale[0];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t y = i / t.tile_w, x = i - y * t.tile_w;
+    float v[12] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    const int ix = (int)x - (int)t.dst[1], iy = (int)y - (int)t.dst[0];
+    if (ix >= 0 && ix < (int)t.size[1] && iy >= 0 && iy < (int)t.size[0]) {
+      const size_t at = (size_t)(iy + t.src[0]) * t.width + (ix + t.src[1]);
+      const float4 c = color[at], a = albedo[at], m = normal[at];
+      const float cs[3] = {c.x * s, c.y * s, c.z * s}, as[3] = {a.x, a.y, a.z}, ms[3] = {m.x, m.y, m.z};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        v[k] = pu_forward(fminf(fmaxf(nan_to_zero(cs[k]), 0.0f), DN_FLT_MAX)) * t.norm;
+        v[3 + k] = fminf(fmaxf(nan_to_zero(as[k]), 0.0f), 1.0f);
+        v[6 + k] = fminf(fmaxf(nan_to_zero(ms[k]), -1.0f), 1.0f) * 0.5f + 0.5f;
+      }
+    }
+    float4* o = reinterpret_cast<float4*>(out + (size_t)i * 16u);
+    o[0] = make_float4(v[0], v[1], v[2], v[3]);
+    o[1] = make_float4(v[4], v[5], v[6], v[7]);
+    o[2] = make_float4(v[8], 0.0f, 0.0f, 0.0f);
+    o[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
+}
+
+// The kept part of a tile back into the image (process.wgsl:88-101): the
+// network's three channels, NaN to 0, clamped, denormalised, through the
+// inverse PU curve and divided by the exposure; alpha from the colour.
+__global__ void __launch_bounds__(256) k_output(const __grid_constant__ TileArgs t, const float* __restrict__ net,
+                                                uint32_t net_channels, const float4* __restrict__ color,
+                                                const float* __restrict__ scale, float4* __restrict__ out) {
+  const uint32_t n = t.out_size[0] * t.out_size[1];
+  const float s = scale[0];
+  const float inv = s != 0.0f ? 1.0f / s : 0.0f;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t gy = i / t.out_size[1], gx = i - gy * t.out_size[1];
+    const float* v = net + ((size_t)(gy + t.out_src[0]) * t.tile_w + gx + t.out_src[1]) * net_channels;
+    float r[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r[k] = pu_inverse(fminf(fmaxf(nan_to_zero(v[k]), 0.0f), DN_FLT_MAX) * t.rcp_norm) * inv;
+    const size_t at = (size_t)(gy + t.out_dst[0]) * t.width + gx + t.out_dst[1];
+    out[at] = make_float4(r[0], r[1], r[2], color[at].w);
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ tiling
+// OIDN's tile split (tile.rs:30-95, from UNetFilter::init): the same
+// arithmetic, so a frame splits into the reference's tiles.
+namespace {
+uint32_t round_up(uint32_t a, uint32_t b) { return (a + b - 1u) / b * b; }
+uint32_t round_up_rem(uint32_t a, uint32_t b, uint32_t c) { return (a + b - c - 1u) / b * b + c; }
+uint32_t div_ceil(uint32_t a, uint32_t b) { return (a + b - 1u) / b; }
+constexpr uint32_t ALIGN = 16, RECEPTIVE_FIELD = 174;
+}  // namespace
+
+DenoisePlan denoise_plan(uint32_t h, uint32_t w, uint64_t max_tile_pixels) {
+  DenoisePlan p;
+  const uint32_t overlap = round_up(RECEPTIVE_FIELD / 2u, ALIGN);
+  uint32_t tile_h = round_up(h, ALIGN), tile_w = round_up(w, ALIGN);
+  const uint32_t pad_h = tile_h % ALIGN, pad_w = tile_w % ALIGN;
+  uint32_t count_h = 1, count_w = 1;
+  const uint32_t min_dim = std::max(4u * overlap, 768u);
+  const uint32_t min_tile_h = round_up_rem(min_dim, ALIGN, pad_h), min_tile_w = round_up_rem(min_dim, ALIGN, pad_w);
+  const uint32_t span_h = 2u * overlap + pad_h, span_w = 2u * overlap + pad_w;
+  while ((uint64_t)tile_h * tile_w > max_tile_pixels) {
+    if (tile_h > min_tile_h && tile_h > tile_w) {
+      uint32_t next = div_ceil(h + span_h * count_h, count_h + 1u);
+      tile_h = std::min(std::max(round_up_rem(next, ALIGN, pad_h), min_tile_h), tile_h - ALIGN);
+      count_h = std::max(div_ceil(h > span_h ? h - span_h : 0u, tile_h - span_h), 1u);
+    } else if (tile_w > min_tile_w) {
+      uint32_t next = div_ceil(w + span_w * count_w, count_w + 1u);
+      tile_w = std::min(std::max(round_up_rem(next, ALIGN, pad_w), min_tile_w), tile_w - ALIGN);
+      count_w = std::max(div_ceil(w > span_w ? w - span_w : 0u, tile_w - span_w), 1u);
+    } else {
+      break;
+    }
+  }
+  p.tile_h = tile_h;
+  p.tile_w = tile_w;
+  p.overlap = overlap;
+  for (uint32_t i = 0; i < count_h; ++i) {
+    uint32_t y = i * (tile_h > span_h ? tile_h - span_h : 0u);
+    uint32_t begin_h = i > 0 ? overlap : 0u, end_h = i < count_h - 1u ? overlap + pad_h : 0u;
+    uint32_t th1 = std::min(h - y, tile_h), th2 = th1 - begin_h - end_h;
+    uint32_t align_h = tile_h - round_up(th1, ALIGN);
+    for (uint32_t j = 0; j < count_w; ++j) {
+      uint32_t x = j * (tile_w > span_w ? tile_w - span_w : 0u);
+      uint32_t begin_w = j > 0 ? overlap : 0u, end_w = j < count_w - 1u ? overlap + pad_w : 0u;
+      uint32_t tw1 = std::min(w - x, tile_w), tw2 = tw1 - begin_w - end_w;
+      uint32_t align_w = tile_w - round_up(tw1, ALIGN);
+      p.tiles.push_back(DenoiseTile{{y, x},
+                                    {align_h, align_w},
+                                    {th1, tw1},
+                                    {align_h + begin_h, align_w + begin_w},
+                                    {y + begin_h, x + begin_w},
+                                    {th2, tw2}});
+    }
+  }
+  return p;
+}
+
+// ------------------------------------------------------------------ host
+Denoiser::~Denoiser() {
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  for (auto& L : layers) {
+    if (L.d_weights) cudaFree(L.d_weights);
+    if (L.d_bias) cudaFree(L.d_bias);
+  }
+  for (float* t : tensors)
+    if (t) cudaFree(t);
+  if (d_scale) cudaFree(d_scale);
+  if (d_bins) cudaFree(d_bins);
+  if (d_error) cudaFree(d_error);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (d_images) cudaFree(d_images);
+  if (stream) cudaStreamDestroy(stream);
+  if (prev >= 0) cudaSetDevice(prev);
+}
+
+// The U-Net of net.rs:193-232 over the parsed tensors, its weights uploaded.
+Denoiser* denoiser_create(const void* blob, size_t bytes) {
+  if (!blob || bytes == 0) throw Invalid(CORRUPT);
+  auto tensors = parse_tza(static_cast<const uint8_t*>(blob), bytes);
+  std::unique_ptr<Denoiser> d(new Denoiser());
+  const uint32_t input_channels = 9;
+  auto channels = [&](int src) { return src == -1 ? input_channels : d->layers[src].out; };
+  auto padded = [&](int src) { return src == -1 ? pad16(input_channels) : d->layers[src].n; };
+  auto level = [&](int src) { return src == -1 ? 0u : d->layers[src].out_level(); };
+  auto push = [&](const char* name, int src0, int src1, bool pool) {
+    auto w = tensors.find(std::string(name) + ".weight");
+    auto b = tensors.find(std::string(name) + ".bias");
+    if (w == tensors.end() || b == tensors.end()) throw Invalid(CORRUPT);
+    DenoiseLayer L;
+    L.name = name;
+    L.src0 = src0;
+    L.src1 = src1;
+    L.pool = pool;
+    L.upsample = src1 != -2;
+    L.in0 = channels(src0);
+    L.in1 = src1 != -2 ? channels(src1) : 0u;
+    L.level = src1 != -2 ? level(src1) : level(src0);
+    if (L.upsample && level(src0) != L.level + 1u)
+      throw Invalid(std::string(name) + ": the upsampled source is not one level down");
+    if (w->second.dims.size() != 4 || b->second.dims.size() != 1) throw Invalid("invalid convolution weight/bias");
+    L.out = w->second.dims[0];
+    if (w->second.dims[1] != L.in0 + L.in1 || w->second.dims[2] != 3 || w->second.dims[3] != 3 ||
+        b->second.dims[0] != L.out)
+      throw Invalid(std::string(name) + ": the weights do not match the network");
+    if (!w->second.exact_half) throw Invalid(std::string(name) + ": weights not exact in half precision");
+    L.c0 = padded(src0);
+    L.c1 = src1 != -2 ? padded(src1) : 0u;
+    L.n = pad16(L.out);
+    if (L.n > N_MAX) throw Invalid(std::string(name) + ": more than 128 output channels");
+    L.weights = conv_chunks(L, w->second);
+    L.bias.assign(L.n, 0.0f);
+    std::copy(b->second.data.begin(), b->second.data.end(), L.bias.begin());
+    d->layers.push_back(std::move(L));
+    return (int)d->layers.size() - 1;
+  };
+  int x = push("enc_conv0", -1, -2, false);
+  int pool1 = push("enc_conv1", x, -2, true);
+  int pool2 = push("enc_conv2", pool1, -2, true);
+  int pool3 = push("enc_conv3", pool2, -2, true);
+  int pool4 = push("enc_conv4", pool3, -2, true);
+  x = push("enc_conv5a", pool4, -2, false);
+  x = push("enc_conv5b", x, -2, false);
+  x = push("dec_conv4a", x, pool3, false);
+  x = push("dec_conv4b", x, -2, false);
+  x = push("dec_conv3a", x, pool2, false);
+  x = push("dec_conv3b", x, -2, false);
+  x = push("dec_conv2a", x, pool1, false);
+  x = push("dec_conv2b", x, -2, false);
+  x = push("dec_conv1a", x, -1, false);
+  x = push("dec_conv1b", x, -2, false);
+  push("dec_conv0", x, -2, false);
+  if (d->layers.back().out != 3) throw Invalid("the network does not end in three channels");
+  // the blob is valid: now the device
+  int devices = 0;
+  if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) {
+    cudaGetLastError();
+    throw Refused("no CUDA device");
+  }
+  dcheck(cudaGetDevice(&d->device), "denoiser device");
+  for (auto& L : d->layers) {
+    dcheck(cudaMalloc(&L.d_weights, L.weights.size() * 2u), "denoiser weights");
+    dcheck(cudaMemcpy(L.d_weights, L.weights.data(), L.weights.size() * 2u, cudaMemcpyHostToDevice),
+           "denoiser weights");
+    dcheck(cudaMalloc(&L.d_bias, L.bias.size() * 4u), "denoiser bias");
+    dcheck(cudaMemcpy(L.d_bias, L.bias.data(), L.bias.size() * 4u, cudaMemcpyHostToDevice), "denoiser bias");
+  }
+  dcheck(cudaMalloc(&d->d_scale, 16), "denoiser exposure");
+  dcheck(cudaMalloc(&d->d_error, 4), "denoiser error word");
+  dcheck(cudaMemset(d->d_error, 0, 4), "denoiser error word");
+  dcheck(cudaEventCreate(&d->ev0), "denoiser events");
+  dcheck(cudaEventCreate(&d->ev1), "denoiser events");
+  dcheck(cudaFuncSetAttribute(k_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM),
+         "convolution shared memory");
+  return d.release();
+}
+
+// The plan and the tile tensors for a width x height image (setup.rs:82-156;
+// every tensor of a tile has its own buffer).
+void denoiser_prepare(Denoiser& d, uint32_t width, uint32_t height) {
+  if (width == 0 || height == 0) throw Invalid("image dimensions must be nonzero");
+  if (d.width == width && d.height == height) return;
+  for (float* t : d.tensors)
+    if (t) cudaFree(t);
+  d.tensors.clear();
+  d.width = d.height = 0;
+  d.plan = denoise_plan(height, width, d.max_tile_pixels);
+  auto alloc = [&](uint32_t level, uint32_t channels) {
+    float* p = nullptr;
+    size_t bytes = (size_t)(d.plan.tile_h >> level) * (d.plan.tile_w >> level) * channels * 4u;
+    dcheck(cudaMalloc(&p, std::max<size_t>(bytes, 16)), "denoiser tensors");
+    d.tensors.push_back(p);
+  };
+  alloc(0, 16);
+  for (auto& L : d.layers) alloc(L.out_level(), L.n);
+  size_t bins = (size_t)div_ceil(width, 16) * div_ceil(height, 16);
+  if (bins > d.bins_capacity) {
+    if (d.d_bins) cudaFree(d.d_bins);
+    d.d_bins = nullptr;
+    dcheck(cudaMalloc(&d.d_bins, bins * 4u), "denoiser exposure bins");
+    d.bins_capacity = bins;
+  }
+  d.width = width;
+  d.height = height;
+}
+
+// norm_scales (lib.rs:75-78): the PU value of 65504 and its reciprocal.
+static void norm_scales(float& norm, float& rcp_norm) {
+  const float max = 1.926'532'5e-1f * std::log(65504.0f + 6.260'261e-3f) + 9.986'201'5e-1f;
+  norm = (float)(1.0 / (double)max);
+  rcp_norm = max;
+}
+
+void denoise_device(Denoiser& d, uint32_t width, uint32_t height, const float4* color, const float4* albedo,
+                    const float4* normal, float4* out, cudaStream_t st) {
+  if (!color || !albedo || !normal || !out) throw Invalid("null argument");
+  dcheck(cudaSetDevice(d.device), "denoiser device");
+  denoiser_prepare(d, width, height);
+  const DenoisePlan& p = d.plan;
+  float norm, rcp_norm;
+  norm_scales(norm, rcp_norm);
+  int sms = 0;
+  dcheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d.device), "device");
+  dcheck(cudaEventRecord(d.ev0, st), "denoiser timing");
+  const uint32_t gx = div_ceil(width, 16), gy = div_ceil(height, 16);
+  k_exposure_bins<<<dim3(gx, gy), 256, 0, st>>>(color, width, height, d.d_bins);
+  k_exposure_reduce<<<1, 256, 0, st>>>(d.d_bins, gx * gy, d.d_scale);
+  uint64_t macs = 0;
+  for (const DenoiseTile& tile : p.tiles) {
+    TileArgs t;
+    for (int k = 0; k < 2; ++k) {
+      t.src[k] = tile.src[k];
+      t.dst[k] = tile.dst[k];
+      t.size[k] = tile.size[k];
+      t.out_src[k] = tile.out_src[k];
+      t.out_dst[k] = tile.out_dst[k];
+      t.out_size[k] = tile.out_size[k];
+    }
+    t.tile_h = p.tile_h;
+    t.tile_w = p.tile_w;
+    t.width = width;
+    t.norm = norm;
+    t.rcp_norm = rcp_norm;
+    k_input<<<sms * 8, 256, 0, st>>>(t, color, albedo, normal, d.d_scale, d.tensors[0]);
+    for (size_t i = 0; i < d.layers.size(); ++i) {
+      const DenoiseLayer& L = d.layers[i];
+      ConvArgs a;
+      a.src0 = d.tensors[L.src0 + 1];
+      a.src1 = L.src1 != -2 ? d.tensors[L.src1 + 1] : nullptr;
+      a.weights = L.d_weights;
+      a.bias = L.d_bias;
+      a.dst = d.tensors[i + 1];
+      a.H = p.tile_h >> L.level;
+      a.W = p.tile_w >> L.level;
+      a.c0 = L.c0;
+      a.c1 = L.c1;
+      a.n = L.n;
+      a.up = L.upsample ? 1u : 0u;
+      a.pool = L.pool ? 1u : 0u;
+      a.error = d.d_error;
+      a.wait_limit = d.wait_limit;
+      dim3 grid(div_ceil(a.W, CONV_PIX), div_ceil(a.H, CONV_ROWS));
+      k_conv<<<grid, CONV_THREADS, CONV_SMEM, st>>>(a);
+      macs += (uint64_t)a.H * a.W * 9u * (a.c0 + a.c1) * a.n;
+    }
+    k_output<<<sms * 8, 256, 0, st>>>(t, d.tensors.back(), d.layers.back().n, color, d.d_scale, out);
+  }
+  dcheck(cudaGetLastError(), "denoiser launch");
+  dcheck(cudaEventRecord(d.ev1, st), "denoiser timing");
+  d.last_macs = macs;
+}
+
+// Device time of the last denoise (waits for it) and its error word.
+float denoiser_finish(Denoiser& d) {
+  dcheck(cudaEventSynchronize(d.ev1), "denoise");
+  uint32_t error = 0;
+  dcheck(cudaMemcpy(&error, d.d_error, 4, cudaMemcpyDeviceToHost), "denoiser error word");
+  if (error) {
+    cudaMemset(d.d_error, 0, 4);
+    throw DeviceError("a denoiser convolution's wait for the tensor cores ran out");
+  }
+  float ms = 0.0f;
+  dcheck(cudaEventElapsedTime(&ms, d.ev0, d.ev1), "denoiser timing");
+  d.last_ms = ms;
+  return ms;
+}
+
+}  // namespace pfxt

