@@ -55,11 +55,23 @@ METRIC = "time to relMSE 0.01 at 4K, cached vs plain tracer on one B200; Mrays/s
 TARGET_RELMSE = 0.01
 
 
+FALLBACK_BF16_TFLOPS = 1590.0  # dense bf16 burst, used only when MEASURED_PEAKS.json is absent
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
     return FALLBACK_HBM_GBS, "fallback"
+
+
+def tensor_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured"
+    return FALLBACK_BF16_TFLOPS, "fallback"
 
 
 def ncu_traffic(kernel: str, rays: int):
@@ -378,6 +390,65 @@ def cpu_baseline(w, budget_s=12.0):
             "sample": f"{ww}x{wh} centre window of the 4K frame, {spp} x 1 spp, oracle path tracer on all host threads"}
 
 
+def denoise_line(trace, w, stream):
+    """The denoiser on the 4K frame's films (after the timed passes): device
+    time of the whole filter (exposure, both tiles' 16 convolutions, input and
+    output processing) with CUDA events, 3 warm-up runs then the median of 5;
+    end to end through the host-buffer call (three images up, one down); the
+    convolutions' FLOPs (2 x multiply-adds at the padded channel counts, once:
+    the hi/lo split doubles the tensor-core work, not the algorithm's) against
+    the dense FP16/BF16 tensor peak.  OIDN's weights when fetched, else seeded
+    FP16 weights of the same shapes (the same work)."""
+    import statistics
+
+    import torch
+
+    from pfx_b200.denoise import DEFAULT_WEIGHTS, Denoiser, write_tza
+    if DEFAULT_WEIGHTS.exists():
+        den, weights = Denoiser(), "OIDN 2.5.1 rt_hdr_alb_nrm.tza"
+    else:
+        rng = np.random.default_rng(0)
+        shapes = [("enc_conv0", 32, 9), ("enc_conv1", 32, 32), ("enc_conv2", 48, 32), ("enc_conv3", 64, 48),
+                  ("enc_conv4", 80, 64), ("enc_conv5a", 96, 80), ("enc_conv5b", 96, 96), ("dec_conv4a", 112, 160),
+                  ("dec_conv4b", 112, 112), ("dec_conv3a", 96, 160), ("dec_conv3b", 96, 96),
+                  ("dec_conv2a", 64, 128), ("dec_conv2b", 64, 64), ("dec_conv1a", 64, 73),
+                  ("dec_conv1b", 32, 64), ("dec_conv0", 3, 32)]
+        t = {}
+        for name, o, i in shapes:
+            t[f"{name}.weight"] = rng.normal(0, np.sqrt(2.0 / (9 * i)), (o, i, 3, 3)).astype(np.float16)
+            t[f"{name}.bias"] = np.zeros(o, np.float16)
+        den, weights = Denoiser(write_tza(t)), "seeded FP16 weights of OIDN's shapes (OIDN's not fetched)"
+    color, albedo, normal = (f.data_ptr() for f in trace.films_device())
+    out = torch.empty((w.height, w.width, 4), dtype=torch.float32, device="cuda")
+    ms = []
+    for k in range(8):
+        den.denoise_device(w.width, w.height, color, albedo, normal, out.data_ptr(), stream.cuda_stream)
+        m, macs = den.last()
+        if k >= 3:
+            ms.append(m)
+    device_ms = statistics.median(ms)
+    films = trace.readback()
+    e2e = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        den.denoise(films.color, films.albedo, films.normal)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    peak, source = tensor_peak()
+    tflops = 2.0 * macs / (device_ms * 1e-3) / 1e12
+    tiles = den.tiles()
+    den.close()
+    return {"workload": f"OIDN RT filter on the {w.width}x{w.height} frame's colour/albedo/normal films, "
+                        f"{tiles[2]} tiles of {tiles[0]}x{tiles[1]}", "weights": weights,
+            "device_ms": round(device_ms, 3), "frames_per_s": round(1e3 / device_ms, 2),
+            "e2e_ms": round(statistics.median(e2e), 3),
+            "e2e": {"h2d_bytes": 3 * w.width * w.height * 16, "d2h_bytes": w.width * w.height * 16},
+            "roofline": {"bound": "tensor", "kernel": "k_conv (16 layers x tiles)",
+                         "achieved": round(tflops, 1), "peak": peak, "unit": "TFLOP/s",
+                         "frac": round(tflops / peak, 4), "peak_source": source,
+                         "flops_per_frame": 2 * macs},
+            "reference": "274 ms on an RX 9060 XT, textures in and out (docs/denoise.md:63-67)"}
+
+
 def clip_line(frames: int):
     """The batched clip workload (1280x720, 16 spp per frame, shots over rooms
     of 10k/100k/400k/1M triangles, the camera moving every frame): `frames`
@@ -414,6 +485,7 @@ def main():
     ap.add_argument("--no-relmse", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-denoise", action="store_true")
     ap.add_argument("--clip-frames", type=int, default=48, help="frames of the clip line (0: none)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -521,6 +593,8 @@ def main():
                 "plain_curve": [(n, round(e, 5)) for n, e in curve[:: max(1, len(curve) // 12)] + curve[-1:]],
                 "cached_curve": [(n, t, round(e, 5)) for n, t, e in
                                  curve_c[:: max(1, len(curve_c) // 12)] + curve_c[-1:]]}
+        if world == 1 and not args.no_denoise:
+            line["denoise"] = denoise_line(trace, w, stream)
         if world == 1 and args.clip_frames > 0:
             line["clip"] = clip_line(args.clip_frames)
         if world == 1 and not args.no_cpu_baseline:  # the host baseline is timed at N=1 only

@@ -212,9 +212,15 @@ __device__ __forceinline__ uint32_t pack_half2(__half a, __half b) {
   return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
 }
 
-// Stage chunk k's input rows into one stage: hi and lo halves of every value.
-__device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint32_t y0, uint32_t x0, uint8_t* hi,
-                                            uint8_t* lo) {
+// Stage chunk k's input rows into one stage: hi and lo halves of every
+// value.  The staging threads issue every load of their share first and
+// convert afterwards, so a chunk waits for one memory latency, not one per load.
+constexpr uint32_t STAGERS = CONV_THREADS - 32u;  // warps 1..7 stage; warp 0 issues copies and MMAs
+constexpr uint32_t STAGE_ITEMS = PATCH_ROWS * PATCH_W * 4u;
+constexpr uint32_t STAGE_PER = (STAGE_ITEMS + STAGERS - 1u) / STAGERS;
+
+__device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint32_t y0, uint32_t x0, uint32_t t,
+                                            uint8_t* hi, uint8_t* lo) {
   const uint32_t chunks0 = a.c0 >> 4;
   const bool first = k < chunks0;
   const float* src = first ? a.src0 : a.src1;
@@ -222,17 +228,28 @@ __device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint3
   const uint32_t ch = (first ? k : k - chunks0) * 16u;
   const uint32_t sh = first ? a.up : 0u;
   const uint32_t SW = a.W >> sh;
-  for (uint32_t item = threadIdx.x; item < PATCH_ROWS * PATCH_W * 4u; item += CONV_THREADS) {
+  float4 v[STAGE_PER];
+#pragma unroll
+  for (uint32_t j = 0; j < STAGE_PER; ++j) {
+    const uint32_t item = t + j * STAGERS;
     const uint32_t q = item & 3u, pix = item >> 2;
     const uint32_t row = pix / PATCH_W, px = pix - row * PATCH_W;
     const int y = (int)(y0 + row) - 1, x = (int)(x0 + px) - 1;
-    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (y >= 0 && y < (int)a.H && x >= 0 && x < (int)a.W)
-      v = __ldg(reinterpret_cast<const float4*>(src + ((size_t)((uint32_t)y >> sh) * SW + ((uint32_t)x >> sh)) * C +
-                                                ch) + q);
-    __half h0 = __float2half_rn(v.x), h1 = __float2half_rn(v.y), h2 = __float2half_rn(v.z), h3 = __float2half_rn(v.w);
-    __half l0 = __float2half_rn(v.x - __half2float(h0)), l1 = __float2half_rn(v.y - __half2float(h1)),
-           l2 = __float2half_rn(v.z - __half2float(h2)), l3 = __float2half_rn(v.w - __half2float(h3));
+    v[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (item < STAGE_ITEMS && y >= 0 && y < (int)a.H && x >= 0 && x < (int)a.W)
+      v[j] = __ldg(reinterpret_cast<const float4*>(src + ((size_t)((uint32_t)y >> sh) * SW + ((uint32_t)x >> sh)) * C +
+                                                   ch) + q);
+  }
+#pragma unroll
+  for (uint32_t j = 0; j < STAGE_PER; ++j) {
+    const uint32_t item = t + j * STAGERS;
+    if (item >= STAGE_ITEMS) break;
+    const uint32_t q = item & 3u, pix = item >> 2;
+    const uint32_t row = pix / PATCH_W, px = pix - row * PATCH_W;
+    __half h0 = __float2half_rn(v[j].x), h1 = __float2half_rn(v[j].y), h2 = __float2half_rn(v[j].z),
+           h3 = __float2half_rn(v[j].w);
+    __half l0 = __float2half_rn(v[j].x - __half2float(h0)), l1 = __float2half_rn(v[j].y - __half2float(h1)),
+           l2 = __float2half_rn(v[j].z - __half2float(h2)), l3 = __float2half_rn(v[j].w - __half2float(h3));
     const uint32_t off = (row * 2u + (q >> 1)) * A_PLANE + px * 16u + (q & 1u) * 8u;
     *reinterpret_cast<uint2*>(hi + off) = make_uint2(pack_half2(h0, h1), pack_half2(h2, h3));
     *reinterpret_cast<uint2*>(lo + off) = make_uint2(pack_half2(l0, l1), pack_half2(l2, l3));
@@ -241,18 +258,31 @@ __device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint3
 
 // One 3x3 convolution (+ bias, ReLU, and 2x2 max pooling when a.pool) of a
 // tile of CONV_ROWS rows x 128 pixels.  Grid: (ceil(W / 128), ceil(H / CONV_ROWS)).
+// Warp specialised: warps 1-7 stage chunk after chunk into the two stages;
+// lane 0 of warp 0 copies each chunk's weights (bulk copy) and issues its MMAs
+// once the stage is full; the commit of a chunk's MMAs frees its stage.
+// Barriers per stage: `full` (the 224 staging threads arrive), `wbar` (the
+// weight copy's bytes), `done` (the MMAs' commit).  Every wait is bounded: a
+// wait that runs out stops the CTA's pipeline (the others' waits then run
+// out too), the CTA drains what it issued and reports it in a.error.
 __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv(const __grid_constant__ ConvArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
   const uint32_t x0 = blockIdx.x * CONV_PIX, y0 = blockIdx.y * CONV_ROWS;
   const uint32_t base = umma::smem_addr(smem);
-  const uint32_t wbar[2] = {base + CTRL, base + CTRL + 8u}, mbar[2] = {base + CTRL + 16u, base + CTRL + 24u};
-  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + CTRL + 32u);
+  const uint32_t wbar[2] = {base + CTRL, base + CTRL + 8u}, done[2] = {base + CTRL + 16u, base + CTRL + 24u},
+                 full[2] = {base + CTRL + 32u, base + CTRL + 40u};
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + CTRL + 48u);
+  volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + CTRL + 52u);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(smem + CTRL + 56u);  // [0] chunks committed, [1] copies issued
   if (tid == 0) {
     for (int s = 0; s < 2; ++s) {
       umma::mbar_init(wbar[s], 1);
-      umma::mbar_init(mbar[s], 1);
+      umma::mbar_init(done[s], 1);
+      umma::mbar_init(full[s], STAGERS);
     }
+    *abort_flag = 0u;
+    counts[0] = counts[1] = 0u;
   }
   if (warp == 0) umma::tmem_alloc(slot, TMEM_COLS);
   umma::fence_before();
@@ -261,59 +291,64 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv(const __grid_constant_
   const uint32_t tmem = *slot;
   const uint32_t chunks = (a.c0 + a.c1) >> 4;
   const uint32_t wbytes = 9u * 2u * a.n * 16u;
-  const uint32_t id = idesc_f16(128, a.n);
-  uint32_t issued = 0, loads = 0;  // chunks whose MMAs were committed; weight copies issued
-  bool late = false;
-  for (uint32_t k = 0; k < chunks; ++k) {
-    const uint32_t s = k & 1u;
-    uint8_t* hi = smem + s * STAGE;
-    uint8_t* lo = hi + A_BYTES;
-    const uint32_t w_addr = base + s * STAGE + 2u * A_BYTES;
-    if (k >= 2) {  // the MMAs of chunk k - 2 read this stage
-      bool ok = umma::mbar_wait(mbar[s], ((k - 2u) >> 1) & 1u, a.wait_limit);
-      if (__syncthreads_or(!ok)) {
-        late = true;
+  if (warp > 0) {
+    const uint32_t t = tid - 32u;
+    for (uint32_t k = 0; k < chunks; ++k) {
+      const uint32_t s = k & 1u;
+      if (k >= 2 && !umma::mbar_wait(done[s], ((k - 2u) >> 1) & 1u, a.wait_limit)) {
+        *abort_flag = 1u;
         break;
       }
+      if (*abort_flag) break;
+      uint8_t* hi = smem + s * STAGE;
+      stage_chunk(a, k, y0, x0, t, hi, hi + A_BYTES);
+      umma::fence_async_smem();
+      umma::mbar_arrive(full[s]);
     }
-    if (tid == 0) {
+  } else if (lane == 0) {
+    const uint32_t id = idesc_f16(128, a.n);
+    uint32_t issued = 0, loads = 0;
+    for (uint32_t k = 0; k < chunks; ++k) {
+      const uint32_t s = k & 1u;
+      const uint32_t w_addr = base + s * STAGE + 2u * A_BYTES;
+      if (k >= 2 && !umma::mbar_wait(done[s], ((k - 2u) >> 1) & 1u, a.wait_limit)) {
+        *abort_flag = 1u;
+        break;
+      }
       umma::mbar_expect_tx(wbar[s], wbytes);
       umma::bulk_load(w_addr, a.weights + (size_t)k * (wbytes / 2u), wbytes, wbar[s]);
-    }
-    loads = k + 1u;
-    stage_chunk(a, k, y0, x0, hi, lo);
-    umma::fence_async_smem();
-    __syncthreads();
-    bool failed = false;
-    if (tid == 0) {
-      if (umma::mbar_wait(wbar[s], (k >> 1) & 1u, a.wait_limit)) {
-        umma::fence_after();
-        const uint32_t a_hi = base + s * STAGE, a_lo = a_hi + A_BYTES;
-#pragma unroll 1
-        for (uint32_t r = 0; r < CONV_ROWS; ++r) {
-#pragma unroll
-          for (uint32_t t = 0; t < 9; ++t) {
-            const uint32_t off = (r + t / 3u) * 2u * A_PLANE + (t % 3u) * 16u;
-            const uint64_t bd = umma::desc(w_addr + t * 2u * a.n * 16u, a.n * 16u, 128u);
-            umma::mma(tmem + r * N_MAX, umma::desc(a_hi + off, A_PLANE, 128u), bd, id, (k > 0 || t > 0) ? 1u : 0u);
-            umma::mma(tmem + r * N_MAX, umma::desc(a_lo + off, A_PLANE, 128u), bd, id, 1u);
-          }
-        }
-        umma::commit(mbar[s]);
-      } else {
-        failed = true;
+      loads = k + 1u;
+      if (!umma::mbar_wait(full[s], (k >> 1) & 1u, a.wait_limit) ||
+          !umma::mbar_wait(wbar[s], (k >> 1) & 1u, a.wait_limit) || *abort_flag) {
+        *abort_flag = 1u;
+        break;
       }
+      umma::fence_after();
+      const uint32_t a_hi = base + s * STAGE, a_lo = a_hi + A_BYTES;
+#pragma unroll 1
+      for (uint32_t r = 0; r < CONV_ROWS; ++r) {
+#pragma unroll
+        for (uint32_t tap = 0; tap < 9; ++tap) {
+          const uint32_t off = (r + tap / 3u) * 2u * A_PLANE + (tap % 3u) * 16u;
+          const uint64_t bd = umma::desc(w_addr + tap * 2u * a.n * 16u, a.n * 16u, 128u);
+          umma::mma(tmem + r * N_MAX, umma::desc(a_hi + off, A_PLANE, 128u), bd, id, (k > 0 || tap > 0) ? 1u : 0u);
+          umma::mma(tmem + r * N_MAX, umma::desc(a_lo + off, A_PLANE, 128u), bd, id, 1u);
+        }
+      }
+      umma::commit(done[s]);
+      issued = k + 1u;
     }
-    if (__syncthreads_or(failed)) {
-      late = true;
-      break;
-    }
-    issued = k + 1u;
+    counts[0] = issued;
+    counts[1] = loads;
   }
-  // every MMA issued is done when the last commit's phase completes
+  __syncthreads();
+  const uint32_t issued = counts[0], loads = counts[1];
+  const bool late = *abort_flag != 0u;
+  // every MMA issued is done when the last commit's phase completes; a weight
+  // copy whose wait ran out lands before the CTA leaves
   bool drained = true;
-  if (issued > 0) drained = umma::mbar_wait(mbar[(issued - 1u) & 1u], ((issued - 1u) >> 1) & 1u, DRAIN_LIMIT);
-  if (loads > issued) {  // a weight copy whose wait ran out: let it land before the CTA leaves
+  if (issued > 0) drained = umma::mbar_wait(done[(issued - 1u) & 1u], ((issued - 1u) >> 1) & 1u, DRAIN_LIMIT);
+  if (loads > issued) {
     const uint32_t k = loads - 1u;
     drained = umma::mbar_wait(wbar[k & 1u], (k >> 1) & 1u, DRAIN_LIMIT) && drained;
   }
