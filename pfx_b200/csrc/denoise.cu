@@ -172,20 +172,25 @@ std::vector<uint16_t> conv_chunks(const DenoiseLayer& L, const Tensor& w) {
 namespace {
 
 constexpr uint32_t CONV_THREADS = 256;               // 8 warps: staging; the epilogue by lane quarters
-constexpr uint32_t CONV_ROWS = 4;                    // output rows per CTA, one TMEM accumulator each
 constexpr uint32_t CONV_PIX = 128;                   // pixels per output row (M of the MMA)
 constexpr uint32_t PATCH_W = CONV_PIX + 2;           // staged pixels per input row
-constexpr uint32_t PATCH_ROWS = CONV_ROWS + 2;       // staged input rows
 constexpr uint32_t A_PLANE = PATCH_W * 16u;          // bytes of one (row, group of 8 channels) plane
-constexpr uint32_t A_BYTES = PATCH_ROWS * 2u * A_PLANE;  // one chunk of one half (hi or lo)
-constexpr uint32_t N_MAX = 128;                      // output channels a CTA holds (TMEM columns per row)
-constexpr uint32_t W_MAX = 9u * 2u * N_MAX * 16u;    // one chunk of weights at N_MAX
-constexpr uint32_t STAGE = 2u * A_BYTES + W_MAX;
-constexpr uint32_t CTRL = 2u * STAGE;                // mbarriers and the TMEM slot after the two stages
-constexpr uint32_t CONV_SMEM = CTRL + 64u;
-constexpr uint32_t TMEM_COLS = 512;                  // CONV_ROWS x N_MAX
-static_assert(CONV_ROWS * N_MAX <= TMEM_COLS, "accumulators fit TMEM");
-static_assert(CONV_SMEM <= 227u * 1024u, "shared memory per CTA");
+constexpr uint32_t TMEM_COLS = 512;                  // ROWS accumulators of N_MAX columns
+
+// The shape of a CTA for ROWS output rows (one TMEM accumulator each): 4 rows
+// for layers of up to 128 output channels, 8 rows for up to 64 (half the
+// halo rows per output row, half the fixed cost per row).
+template <uint32_t ROWS>
+struct ConvShape {
+  static constexpr uint32_t PATCH_ROWS = ROWS + 2u;              // staged input rows
+  static constexpr uint32_t A_BYTES = PATCH_ROWS * 2u * A_PLANE;   // one chunk of one half (hi or lo)
+  static constexpr uint32_t N_MAX = TMEM_COLS / ROWS;             // output channels a CTA holds
+  static constexpr uint32_t W_MAX = 9u * 2u * N_MAX * 16u;         // one chunk of weights at N_MAX
+  static constexpr uint32_t STAGE = 2u * A_BYTES + W_MAX;
+  static constexpr uint32_t CTRL = 2u * STAGE;                     // mbarriers, TMEM slot, flags
+  static constexpr uint32_t SMEM = CTRL + 64u;
+  static_assert(SMEM <= 227u * 1024u, "shared memory per CTA");
+};
 constexpr uint32_t ERR_CONV_WAIT = 1u, ERR_CONV_DRAIN = 2u;
 // Polls of the waits that drain a CTA's own work in flight (its MMAs and
 // weight copies) before it frees its TMEM and leaves, whatever the main
@@ -216,11 +221,15 @@ __device__ __forceinline__ uint32_t pack_half2(__half a, __half b) {
 // value.  The staging threads issue every load of their share first and
 // convert afterwards, so a chunk waits for one memory latency, not one per load.
 constexpr uint32_t STAGERS = CONV_THREADS - 32u;  // warps 1..7 stage; warp 0 issues copies and MMAs
-constexpr uint32_t STAGE_ITEMS = PATCH_ROWS * PATCH_W * 4u;
-constexpr uint32_t STAGE_PER = (STAGE_ITEMS + STAGERS - 1u) / STAGERS;
+constexpr uint32_t STAGE_BATCH = 14;              // loads a staging thread has in flight at once
 
+template <uint32_t ROWS>
 __device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint32_t y0, uint32_t x0, uint32_t t,
                                             uint8_t* hi, uint8_t* lo) {
+  constexpr uint32_t ITEMS = ConvShape<ROWS>::PATCH_ROWS * PATCH_W * 4u;
+  constexpr uint32_t PER = (ITEMS + STAGERS - 1u) / STAGERS;
+  constexpr uint32_t BATCHES = (PER + STAGE_BATCH - 1u) / STAGE_BATCH;
+  constexpr uint32_t BATCH = (PER + BATCHES - 1u) / BATCHES;
   const uint32_t chunks0 = a.c0 >> 4;
   const bool first = k < chunks0;
   const float* src = first ? a.src0 : a.src1;
@@ -228,36 +237,39 @@ __device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint3
   const uint32_t ch = (first ? k : k - chunks0) * 16u;
   const uint32_t sh = first ? a.up : 0u;
   const uint32_t SW = a.W >> sh;
-  float4 v[STAGE_PER];
+#pragma unroll 1
+  for (uint32_t bt = 0; bt < BATCHES; ++bt) {
+    float4 v[BATCH];
 #pragma unroll
-  for (uint32_t j = 0; j < STAGE_PER; ++j) {
-    const uint32_t item = t + j * STAGERS;
-    const uint32_t q = item & 3u, pix = item >> 2;
-    const uint32_t row = pix / PATCH_W, px = pix - row * PATCH_W;
-    const int y = (int)(y0 + row) - 1, x = (int)(x0 + px) - 1;
-    v[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (item < STAGE_ITEMS && y >= 0 && y < (int)a.H && x >= 0 && x < (int)a.W)
-      v[j] = __ldg(reinterpret_cast<const float4*>(src + ((size_t)((uint32_t)y >> sh) * SW + ((uint32_t)x >> sh)) * C +
-                                                   ch) + q);
-  }
+    for (uint32_t j = 0; j < BATCH; ++j) {
+      const uint32_t item = t + (bt * BATCH + j) * STAGERS;
+      const uint32_t q = item & 3u, pix = item >> 2;
+      const uint32_t row = pix / PATCH_W, px = pix - row * PATCH_W;
+      const int y = (int)(y0 + row) - 1, x = (int)(x0 + px) - 1;
+      v[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (item < ITEMS && y >= 0 && y < (int)a.H && x >= 0 && x < (int)a.W)
+        v[j] = __ldg(reinterpret_cast<const float4*>(src + ((size_t)((uint32_t)y >> sh) * SW + ((uint32_t)x >> sh)) *
+                                                               C + ch) + q);
+    }
 #pragma unroll
-  for (uint32_t j = 0; j < STAGE_PER; ++j) {
-    const uint32_t item = t + j * STAGERS;
-    if (item >= STAGE_ITEMS) break;
-    const uint32_t q = item & 3u, pix = item >> 2;
-    const uint32_t row = pix / PATCH_W, px = pix - row * PATCH_W;
-    __half h0 = __float2half_rn(v[j].x), h1 = __float2half_rn(v[j].y), h2 = __float2half_rn(v[j].z),
-           h3 = __float2half_rn(v[j].w);
-    __half l0 = __float2half_rn(v[j].x - __half2float(h0)), l1 = __float2half_rn(v[j].y - __half2float(h1)),
-           l2 = __float2half_rn(v[j].z - __half2float(h2)), l3 = __float2half_rn(v[j].w - __half2float(h3));
-    const uint32_t off = (row * 2u + (q >> 1)) * A_PLANE + px * 16u + (q & 1u) * 8u;
-    *reinterpret_cast<uint2*>(hi + off) = make_uint2(pack_half2(h0, h1), pack_half2(h2, h3));
-    *reinterpret_cast<uint2*>(lo + off) = make_uint2(pack_half2(l0, l1), pack_half2(l2, l3));
+    for (uint32_t j = 0; j < BATCH; ++j) {
+      const uint32_t item = t + (bt * BATCH + j) * STAGERS;
+      if (item >= ITEMS) break;
+      const uint32_t q = item & 3u, pix = item >> 2;
+      const uint32_t row = pix / PATCH_W, px = pix - row * PATCH_W;
+      __half h0 = __float2half_rn(v[j].x), h1 = __float2half_rn(v[j].y), h2 = __float2half_rn(v[j].z),
+             h3 = __float2half_rn(v[j].w);
+      __half l0 = __float2half_rn(v[j].x - __half2float(h0)), l1 = __float2half_rn(v[j].y - __half2float(h1)),
+             l2 = __float2half_rn(v[j].z - __half2float(h2)), l3 = __float2half_rn(v[j].w - __half2float(h3));
+      const uint32_t off = (row * 2u + (q >> 1)) * A_PLANE + px * 16u + (q & 1u) * 8u;
+      *reinterpret_cast<uint2*>(hi + off) = make_uint2(pack_half2(h0, h1), pack_half2(h2, h3));
+      *reinterpret_cast<uint2*>(lo + off) = make_uint2(pack_half2(l0, l1), pack_half2(l2, l3));
+    }
   }
 }
 
 // One 3x3 convolution (+ bias, ReLU, and 2x2 max pooling when a.pool) of a
-// tile of CONV_ROWS rows x 128 pixels.  Grid: (ceil(W / 128), ceil(H / CONV_ROWS)).
+// tile of ROWS rows x 128 pixels.  Grid: (ceil(W / 128), ceil(H / ROWS)).
 // Warp specialised: warps 1-7 stage chunk after chunk into the two stages;
 // lane 0 of warp 0 copies each chunk's weights (bulk copy) and issues its MMAs
 // once the stage is full; the commit of a chunk's MMAs frees its stage.
@@ -265,10 +277,13 @@ __device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint3
 // weight copy's bytes), `done` (the MMAs' commit).  Every wait is bounded: a
 // wait that runs out stops the CTA's pipeline (the others' waits then run
 // out too), the CTA drains what it issued and reports it in a.error.
+template <uint32_t ROWS>
 __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv(const __grid_constant__ ConvArgs a) {
+  using S = ConvShape<ROWS>;
+  constexpr uint32_t STAGE = S::STAGE, A_BYTES = S::A_BYTES, CTRL = S::CTRL, N_MAX = S::N_MAX;
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
-  const uint32_t x0 = blockIdx.x * CONV_PIX, y0 = blockIdx.y * CONV_ROWS;
+  const uint32_t x0 = blockIdx.x * CONV_PIX, y0 = blockIdx.y * ROWS;
   const uint32_t base = umma::smem_addr(smem);
   const uint32_t wbar[2] = {base + CTRL, base + CTRL + 8u}, done[2] = {base + CTRL + 16u, base + CTRL + 24u},
                  full[2] = {base + CTRL + 32u, base + CTRL + 40u};
@@ -301,7 +316,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv(const __grid_constant_
       }
       if (*abort_flag) break;
       uint8_t* hi = smem + s * STAGE;
-      stage_chunk(a, k, y0, x0, t, hi, hi + A_BYTES);
+      stage_chunk<ROWS>(a, k, y0, x0, t, hi, hi + A_BYTES);
       umma::fence_async_smem();
       umma::mbar_arrive(full[s]);
     }
@@ -324,15 +339,24 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv(const __grid_constant_
         break;
       }
       umma::fence_after();
-      const uint32_t a_hi = base + s * STAGE, a_lo = a_hi + A_BYTES;
-#pragma unroll 1
-      for (uint32_t r = 0; r < CONV_ROWS; ++r) {
+      // Descriptors move with their start address (bits 0-13, address / 16; a
+      // shared-memory address stays below 2^18, so adding to it never carries
+      // into the other fields): one base descriptor per operand, offsets known
+      // at compile time, so the lane issues ROWS x 18 MMAs back to back.
+      const uint64_t hi_desc = umma::desc(base + s * STAGE, A_PLANE, 128u);
+      const uint64_t lo_desc = umma::desc(base + s * STAGE + A_BYTES, A_PLANE, 128u);
+      const uint64_t w_desc = umma::desc(w_addr, a.n * 16u, 128u);
+      const uint32_t w_step = (2u * a.n * 16u) >> 4;
+      const uint32_t first = k == 0 ? 0u : 1u;
+#pragma unroll
+      for (uint32_t r = 0; r < ROWS; ++r) {
 #pragma unroll
         for (uint32_t tap = 0; tap < 9; ++tap) {
-          const uint32_t off = (r + tap / 3u) * 2u * A_PLANE + (tap % 3u) * 16u;
-          const uint64_t bd = umma::desc(w_addr + tap * 2u * a.n * 16u, a.n * 16u, 128u);
-          umma::mma(tmem + r * N_MAX, umma::desc(a_hi + off, A_PLANE, 128u), bd, id, (k > 0 || tap > 0) ? 1u : 0u);
-          umma::mma(tmem + r * N_MAX, umma::desc(a_lo + off, A_PLANE, 128u), bd, id, 1u);
+          constexpr uint32_t unit = 16u;
+          const uint32_t off = ((r + tap / 3u) * 2u * A_PLANE + (tap % 3u) * 16u) / unit;
+          const uint64_t bd = w_desc + tap * w_step;
+          umma::mma(tmem + r * N_MAX, hi_desc + off, bd, id, tap > 0 ? 1u : first);
+          umma::mma(tmem + r * N_MAX, lo_desc + off, bd, id, 1u);
         }
       }
       umma::commit(done[s]);
@@ -357,9 +381,11 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv(const __grid_constant_
   if (late || !drained) {
     if (tid == 0) atomicOr(a.error, (late ? ERR_CONV_WAIT : 0u) | (drained ? 0u : ERR_CONV_DRAIN));
   } else {
-    // epilogue: warp w reads TMEM lanes 32 (w % 4).., rows 2 (w / 4) and 2 (w / 4) + 1
-    const uint32_t quarter = warp & 3u, r0 = (warp >> 2) * 2u;
+    // epilogue: warp w reads TMEM lanes 32 (w % 4).. and the row pairs of its half of the rows
+    const uint32_t quarter = warp & 3u;
     const uint32_t x = x0 + quarter * 32u + lane;
+#pragma unroll 1
+    for (uint32_t r0 = (warp >> 2) * (ROWS / 2u); r0 < (warp >> 2) * (ROWS / 2u) + ROWS / 2u; r0 += 2u)
     for (uint32_t j = 0; j < a.n; j += 16u) {
       float v0[16], v1[16];
       umma::ld16(umma::taddr(tmem, quarter * 32u, r0 * N_MAX + j), v0);
@@ -638,7 +664,7 @@ Denoiser* denoiser_create(const void* blob, size_t bytes) {
     L.c0 = padded(src0);
     L.c1 = src1 != -2 ? padded(src1) : 0u;
     L.n = pad16(L.out);
-    if (L.n > N_MAX) throw Invalid(std::string(name) + ": more than 128 output channels");
+    if (L.n > ConvShape<4>::N_MAX) throw Invalid(std::string(name) + ": more than 128 output channels");
     L.weights = conv_chunks(L, w->second);
     L.bias.assign(L.n, 0.0f);
     std::copy(b->second.data.begin(), b->second.data.end(), L.bias.begin());
@@ -681,7 +707,9 @@ Denoiser* denoiser_create(const void* blob, size_t bytes) {
   dcheck(cudaMemset(d->d_error, 0, 4), "denoiser error word");
   dcheck(cudaEventCreate(&d->ev0), "denoiser events");
   dcheck(cudaEventCreate(&d->ev1), "denoiser events");
-  dcheck(cudaFuncSetAttribute(k_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM),
+  dcheck(cudaFuncSetAttribute(k_conv<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ConvShape<4>::SMEM),
+         "convolution shared memory");
+  dcheck(cudaFuncSetAttribute(k_conv<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ConvShape<8>::SMEM),
          "convolution shared memory");
   return d.release();
 }
@@ -770,8 +798,13 @@ void denoise_device(Denoiser& d, uint32_t width, uint32_t height, const float4* 
       a.pool = L.pool ? 1u : 0u;
       a.error = d.d_error;
       a.wait_limit = d.wait_limit;
-      dim3 grid(div_ceil(a.W, CONV_PIX), div_ceil(a.H, CONV_ROWS));
-      k_conv<<<grid, CONV_THREADS, CONV_SMEM, st>>>(a);
+      if (a.n <= ConvShape<8>::N_MAX) {
+        dim3 grid(div_ceil(a.W, CONV_PIX), div_ceil(a.H, 8u));
+        k_conv<8><<<grid, CONV_THREADS, ConvShape<8>::SMEM, st>>>(a);
+      } else {
+        dim3 grid(div_ceil(a.W, CONV_PIX), div_ceil(a.H, 4u));
+        k_conv<4><<<grid, CONV_THREADS, ConvShape<4>::SMEM, st>>>(a);
+      }
       macs += (uint64_t)a.H * a.W * 9u * (a.c0 + a.c1) * a.n;
     }
     k_output<<<sms * 8, 256, 0, st>>>(t, d.tensors.back(), d.layers.back().n, color, d.d_scale, out);
