@@ -221,7 +221,7 @@ __device__ __forceinline__ uint32_t pack_half2(__half a, __half b) {
 // value.  The staging threads issue every load of their share first and
 // convert afterwards, so a chunk waits for one memory latency, not one per load.
 constexpr uint32_t STAGERS = CONV_THREADS - 32u;  // warps 1..7 stage; warp 0 issues copies and MMAs
-constexpr uint32_t STAGE_BATCH = 14;              // loads a staging thread has in flight at once
+constexpr uint32_t STAGE_BATCH = 24;              // loads a staging thread has in flight at once
 
 template <uint32_t ROWS>
 __device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint32_t y0, uint32_t x0, uint32_t t,
