@@ -243,6 +243,7 @@ EXTRA = [
     ("pfxt_debug_select_nth", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_int32, C.c_void_p]),
     ("pfxt_debug_gpu_bvh", C.c_int, [C.c_int32]),
     ("pfxt_debug_scene_gpu_builds", C.c_uint32, [C.c_void_p]),
+    ("pfxt_debug_denoiser_shape", C.c_int, [C.c_void_p, C.c_uint32]),
     ("pfxt_debug_denoise_plan", C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("pfxt_trace_counts_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                            C.c_void_p]),

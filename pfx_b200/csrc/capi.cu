@@ -1121,6 +1121,16 @@ int pfxt_debug_denoise_plan(uint32_t height, uint32_t width, uint64_t max_tile_p
   });
 }
 
+// The conv CTA shape of the layers of up to 64 output channels (test and
+// measurement hook): 0 the default, 1 tall, 2 paired, 3 wide (denoise.cu).
+int pfxt_debug_denoiser_shape(pfxt_denoiser* h, uint32_t shape) {
+  return guarded([&]() {
+    if (!h) throw Invalid("null argument");
+    if (shape > 3u) throw Invalid("conv shape must be 0-3");
+    h->d->conv_shape = shape;
+  });
+}
+
 int pfxt_denoiser_set_wait_limit(pfxt_denoiser* h, uint32_t polls) {
   return guarded([&]() {
     if (!h) throw Invalid("null argument");

@@ -175,22 +175,33 @@ constexpr uint32_t CONV_THREADS = 256;               // 8 warps: staging; the ep
 constexpr uint32_t CONV_PIX = 128;                   // pixels per output row (M of the MMA)
 constexpr uint32_t PATCH_W = CONV_PIX + 2;           // staged pixels per input row
 constexpr uint32_t A_PLANE = PATCH_W * 16u;          // bytes of one (row, group of 8 channels) plane
-constexpr uint32_t TMEM_COLS = 512;                  // ROWS accumulators of N_MAX columns
 
-// The shape of a CTA for ROWS output rows (one TMEM accumulator each): 4 rows
-// for layers of up to 128 output channels, 8 rows for up to 64 (half the
-// halo rows per output row, half the fixed cost per row).
-template <uint32_t ROWS>
+// The shape of a conv CTA: ROWS output rows (one TMEM accumulator each, NMAX
+// columns), STAGES shared-memory stages, CTAS resident CTAs per SM, BATCH
+// loads in flight per staging thread.
+//  * Wide:   4 rows, up to 128 output channels, 2 stages, 1 CTA per SM;
+//  * Tall:   8 rows, up to 64 channels, 2 stages, 1 CTA per SM (half the halo
+//            rows and fixed cost per output row);
+//  * Paired: 4 rows, up to 64 channels, 1 stage, 2 CTAs per SM (one CTA's
+//            epilogue and staging run while the other's MMAs do): the
+//            fastest measured for those layers, the default for them.
+template <uint32_t ROWS_, uint32_t NMAX_, uint32_t STAGES_, uint32_t CTAS_, uint32_t BATCH_>
 struct ConvShape {
+  static constexpr uint32_t ROWS = ROWS_, N_MAX = NMAX_, STAGES = STAGES_, CTAS = CTAS_, BATCH_MAX = BATCH_;
+  static constexpr uint32_t TMEM_COLS = ROWS * N_MAX;            // a power of two of at least 32
   static constexpr uint32_t PATCH_ROWS = ROWS + 2u;              // staged input rows
   static constexpr uint32_t A_BYTES = PATCH_ROWS * 2u * A_PLANE;   // one chunk of one half (hi or lo)
-  static constexpr uint32_t N_MAX = TMEM_COLS / ROWS;             // output channels a CTA holds
   static constexpr uint32_t W_MAX = 9u * 2u * N_MAX * 16u;         // one chunk of weights at N_MAX
   static constexpr uint32_t STAGE = 2u * A_BYTES + W_MAX;
-  static constexpr uint32_t CTRL = 2u * STAGE;                     // mbarriers, TMEM slot, flags
+  static constexpr uint32_t CTRL = STAGES * STAGE;                 // mbarriers, TMEM slot, flags
   static constexpr uint32_t SMEM = CTRL + 64u;
-  static_assert(SMEM <= 227u * 1024u, "shared memory per CTA");
+  static_assert(SMEM * CTAS <= 228u * 1024u - CTAS * 1024u, "shared memory per SM");
+  static_assert(TMEM_COLS * CTAS <= 512u && (TMEM_COLS & (TMEM_COLS - 1u)) == 0u, "TMEM per SM");
+  static_assert(STAGES == 1u || STAGES == 2u, "one or two stages");
 };
+using Wide = ConvShape<4, 128, 2, 1, 14>;
+using Tall = ConvShape<8, 64, 2, 1, 24>;
+using Paired = ConvShape<4, 64, 1, 2, 7>;
 constexpr uint32_t ERR_CONV_WAIT = 1u, ERR_CONV_DRAIN = 2u;
 // Polls of the waits that drain a CTA's own work in flight (its MMAs and
 // weight copies) before it frees its TMEM and leaves, whatever the main
@@ -221,14 +232,13 @@ __device__ __forceinline__ uint32_t pack_half2(__half a, __half b) {
 // value.  The staging threads issue every load of their share first and
 // convert afterwards, so a chunk waits for one memory latency, not one per load.
 constexpr uint32_t STAGERS = CONV_THREADS - 32u;  // warps 1..7 stage; warp 0 issues copies and MMAs
-constexpr uint32_t STAGE_BATCH = 24;              // loads a staging thread has in flight at once
 
-template <uint32_t ROWS>
+template <class S>
 __device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint32_t y0, uint32_t x0, uint32_t t,
                                             uint8_t* hi, uint8_t* lo) {
-  constexpr uint32_t ITEMS = ConvShape<ROWS>::PATCH_ROWS * PATCH_W * 4u;
+  constexpr uint32_t ITEMS = S::PATCH_ROWS * PATCH_W * 4u;
   constexpr uint32_t PER = (ITEMS + STAGERS - 1u) / STAGERS;
-  constexpr uint32_t BATCHES = (PER + STAGE_BATCH - 1u) / STAGE_BATCH;
+  constexpr uint32_t BATCHES = (PER + S::BATCH_MAX - 1u) / S::BATCH_MAX;
   constexpr uint32_t BATCH = (PER + BATCHES - 1u) / BATCHES;
   const uint32_t chunks0 = a.c0 >> 4;
   const bool first = k < chunks0;
@@ -277,10 +287,10 @@ __device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint3
 // weight copy's bytes), `done` (the MMAs' commit).  Every wait is bounded: a
 // wait that runs out stops the CTA's pipeline (the others' waits then run
 // out too), the CTA drains what it issued and reports it in a.error.
-template <uint32_t ROWS>
-__global__ void __launch_bounds__(CONV_THREADS, 1) k_conv(const __grid_constant__ ConvArgs a) {
-  using S = ConvShape<ROWS>;
-  constexpr uint32_t STAGE = S::STAGE, A_BYTES = S::A_BYTES, CTRL = S::CTRL, N_MAX = S::N_MAX;
+template <class S>
+__global__ void __launch_bounds__(CONV_THREADS, S::CTAS) k_conv(const __grid_constant__ ConvArgs a) {
+  constexpr uint32_t STAGE = S::STAGE, A_BYTES = S::A_BYTES, CTRL = S::CTRL, N_MAX = S::N_MAX, ROWS = S::ROWS;
+  constexpr uint32_t NS = S::STAGES, TMEM_COLS = S::TMEM_COLS;
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
   const uint32_t x0 = blockIdx.x * CONV_PIX, y0 = blockIdx.y * ROWS;
@@ -309,14 +319,14 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv(const __grid_constant_
   if (warp > 0) {
     const uint32_t t = tid - 32u;
     for (uint32_t k = 0; k < chunks; ++k) {
-      const uint32_t s = k & 1u;
-      if (k >= 2 && !umma::mbar_wait(done[s], ((k - 2u) >> 1) & 1u, a.wait_limit)) {
+      const uint32_t s = k % NS;
+      if (k >= NS && !umma::mbar_wait(done[s], ((k - NS) / NS) & 1u, a.wait_limit)) {
         *abort_flag = 1u;
         break;
       }
       if (*abort_flag) break;
       uint8_t* hi = smem + s * STAGE;
-      stage_chunk<ROWS>(a, k, y0, x0, t, hi, hi + A_BYTES);
+      stage_chunk<S>(a, k, y0, x0, t, hi, hi + A_BYTES);
       umma::fence_async_smem();
       umma::mbar_arrive(full[s]);
     }
@@ -324,17 +334,17 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv(const __grid_constant_
     const uint32_t id = idesc_f16(128, a.n);
     uint32_t issued = 0, loads = 0;
     for (uint32_t k = 0; k < chunks; ++k) {
-      const uint32_t s = k & 1u;
+      const uint32_t s = k % NS;
       const uint32_t w_addr = base + s * STAGE + 2u * A_BYTES;
-      if (k >= 2 && !umma::mbar_wait(done[s], ((k - 2u) >> 1) & 1u, a.wait_limit)) {
+      if (k >= NS && !umma::mbar_wait(done[s], ((k - NS) / NS) & 1u, a.wait_limit)) {
         *abort_flag = 1u;
         break;
       }
       umma::mbar_expect_tx(wbar[s], wbytes);
       umma::bulk_load(w_addr, a.weights + (size_t)k * (wbytes / 2u), wbytes, wbar[s]);
       loads = k + 1u;
-      if (!umma::mbar_wait(full[s], (k >> 1) & 1u, a.wait_limit) ||
-          !umma::mbar_wait(wbar[s], (k >> 1) & 1u, a.wait_limit) || *abort_flag) {
+      if (!umma::mbar_wait(full[s], (k / NS) & 1u, a.wait_limit) ||
+          !umma::mbar_wait(wbar[s], (k / NS) & 1u, a.wait_limit) || *abort_flag) {
         *abort_flag = 1u;
         break;
       }
@@ -371,10 +381,10 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv(const __grid_constant_
   // every MMA issued is done when the last commit's phase completes; a weight
   // copy whose wait ran out lands before the CTA leaves
   bool drained = true;
-  if (issued > 0) drained = umma::mbar_wait(done[(issued - 1u) & 1u], ((issued - 1u) >> 1) & 1u, DRAIN_LIMIT);
+  if (issued > 0) drained = umma::mbar_wait(done[(issued - 1u) % NS], ((issued - 1u) / NS) & 1u, DRAIN_LIMIT);
   if (loads > issued) {
     const uint32_t k = loads - 1u;
-    drained = umma::mbar_wait(wbar[k & 1u], (k >> 1) & 1u, DRAIN_LIMIT) && drained;
+    drained = umma::mbar_wait(wbar[k % NS], (k / NS) & 1u, DRAIN_LIMIT) && drained;
   }
   drained = __syncthreads_and(drained);
   umma::fence_after();
@@ -664,7 +674,7 @@ Denoiser* denoiser_create(const void* blob, size_t bytes) {
     L.c0 = padded(src0);
     L.c1 = src1 != -2 ? padded(src1) : 0u;
     L.n = pad16(L.out);
-    if (L.n > ConvShape<4>::N_MAX) throw Invalid(std::string(name) + ": more than 128 output channels");
+    if (L.n > Wide::N_MAX) throw Invalid(std::string(name) + ": more than 128 output channels");
     L.weights = conv_chunks(L, w->second);
     L.bias.assign(L.n, 0.0f);
     std::copy(b->second.data.begin(), b->second.data.end(), L.bias.begin());
@@ -707,9 +717,11 @@ Denoiser* denoiser_create(const void* blob, size_t bytes) {
   dcheck(cudaMemset(d->d_error, 0, 4), "denoiser error word");
   dcheck(cudaEventCreate(&d->ev0), "denoiser events");
   dcheck(cudaEventCreate(&d->ev1), "denoiser events");
-  dcheck(cudaFuncSetAttribute(k_conv<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ConvShape<4>::SMEM),
+  dcheck(cudaFuncSetAttribute(k_conv<Wide>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Wide::SMEM),
          "convolution shared memory");
-  dcheck(cudaFuncSetAttribute(k_conv<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ConvShape<8>::SMEM),
+  dcheck(cudaFuncSetAttribute(k_conv<Tall>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Tall::SMEM),
+         "convolution shared memory");
+  dcheck(cudaFuncSetAttribute(k_conv<Paired>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Paired::SMEM),
          "convolution shared memory");
   return d.release();
 }
@@ -798,12 +810,15 @@ void denoise_device(Denoiser& d, uint32_t width, uint32_t height, const float4* 
       a.pool = L.pool ? 1u : 0u;
       a.error = d.d_error;
       a.wait_limit = d.wait_limit;
-      if (a.n <= ConvShape<8>::N_MAX) {
-        dim3 grid(div_ceil(a.W, CONV_PIX), div_ceil(a.H, 8u));
-        k_conv<8><<<grid, CONV_THREADS, ConvShape<8>::SMEM, st>>>(a);
+      // layers of up to 64 channels: paired CTAs (4K frame: paired 10.4 ms, tall 12.6, wide 13.6)
+      const uint32_t shape = a.n > Paired::N_MAX ? 0u : (d.conv_shape ? d.conv_shape : 2u);
+      if (shape == 1u) {
+        k_conv<Tall><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Tall::ROWS)), CONV_THREADS, Tall::SMEM, st>>>(a);
+      } else if (shape == 2u) {
+        k_conv<Paired>
+            <<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Paired::ROWS)), CONV_THREADS, Paired::SMEM, st>>>(a);
       } else {
-        dim3 grid(div_ceil(a.W, CONV_PIX), div_ceil(a.H, 4u));
-        k_conv<4><<<grid, CONV_THREADS, ConvShape<4>::SMEM, st>>>(a);
+        k_conv<Wide><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Wide::ROWS)), CONV_THREADS, Wide::SMEM, st>>>(a);
       }
       macs += (uint64_t)a.H * a.W * 9u * (a.c0 + a.c1) * a.n;
     }

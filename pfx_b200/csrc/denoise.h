@@ -54,6 +54,7 @@ struct Denoiser {
   size_t bins_capacity = 0;
   uint32_t* d_error = nullptr;  // set by a conv kernel whose bounded wait ran out
   uint32_t wait_limit = 1u << 26;  // polls of the conv kernels' bounded mbarrier waits
+  uint32_t conv_shape = 0;         // layers of up to 64 channels: 0 default, 1 tall, 2 paired, 3 wide
   cudaStream_t stream = nullptr;   // host-buffer calls
   float4* d_images = nullptr;      // host-buffer calls: colour, albedo, normal, output
   size_t images_pixels = 0;

@@ -726,10 +726,13 @@ __device__ __forceinline__ float2 child_importance(const ShadeView& v, uint32_t 
   return node_importance(node, load_trig(v, row).node, p, n);
 }
 
-// tree_leaf (lights.wgsl:276-349): (selected row, pmf)
+// tree_leaf (lights.wgsl:276-349): (selected row, pmf).  `use_known`: the
+// leaf holds one light whose importance the descent has already evaluated
+// (child_importance of that leaf: emitter_importance of the same light row
+// at the same point), passed as `known` instead of being evaluated again.
 template <bool IN>
 __device__ __forceinline__ float2 tree_leaf_b(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n,
-                                              float start) {
+                                              float start, float2 known, bool use_known) {
   float rand = start;
   bool sample_max = rand > 0.5f;
   if (count > 1u) rand = rand * 2.0f - (sample_max ? 1.0f : 0.0f);
@@ -738,7 +741,9 @@ __device__ __forceinline__ float2 tree_leaf_b(const ShadeView& v, uint32_t first
   uint32_t has = 0u;
   for (uint32_t i = 0u; i < count; ++i) {
     int32_t index = (int32_t)(first + i);
-    float2 importance = emitter_importance_to<IN>(load_light(v, first + i), load_trig(v, first + i).light, p, n);
+    float2 importance = (use_known && i == 0u)
+                            ? known
+                            : emitter_importance_to<IN>(load_light(v, first + i), load_trig(v, first + i).light, p, n);
     float weight = sample_max ? importance.x : importance.y;
     float other = sample_max ? importance.y : importance.x;
     if (weight > 0.0f) {
@@ -795,8 +800,10 @@ __device__ __forceinline__ float2 tree_leaf_b(const ShadeView& v, uint32_t first
       }
       chosen_min = 1.0f;
       total_min = valid;
-      chosen_max = emitter_importance_to<IN>(load_light(v, (uint32_t)selected), load_trig(v, (uint32_t)selected).light,
-                                             p, n).x;
+      chosen_max = (use_known && (uint32_t)selected == first)
+                       ? known.x
+                       : emitter_importance_to<IN>(load_light(v, (uint32_t)selected),
+                                                   load_trig(v, (uint32_t)selected).light, p, n).x;
     }
   }
   return make_float2((float)selected, 0.5f * (chosen_max / total_max + chosen_min / total_min));
@@ -804,8 +811,9 @@ __device__ __forceinline__ float2 tree_leaf_b(const ShadeView& v, uint32_t first
 
 // tree_pick (lights.wgsl:350-386): (light row, pmf).  The descent is bounded
 // by the number of tree rows; a malformed tree ends the descent with pmf 0.
-SH_TREE float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n, float start) {
-  return tree_leaf_b<false>(v, first, count, p, n, start);
+SH_TREE float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n, float start, float2 known,
+                         bool use_known) {
+  return tree_leaf_b<false>(v, first, count, p, n, start, known, use_known);
 }
 template <bool IN>
 __device__ __forceinline__ float2 tree_pick_b(const ShadeView& v, uint32_t rows, v3 p, v3 n, float start,
@@ -813,14 +821,17 @@ __device__ __forceinline__ float2 tree_pick_b(const ShadeView& v, uint32_t rows,
   uint32_t at = f2u((float)v.looped + (float)v.tree);
   float rand = start;
   float pdf = 1.0f;
+  float2 known = make_float2(0.0f, 0.0f);  // the importance of `at`, once the descent has evaluated it
+  bool evaluated = false;
   for (uint32_t guard = 0u; guard < rows; ++guard) {
     if (at >= rows) break;
     LightRow node = load_light(v, at);
     uint32_t count = f2u(node.d.y);
     if (count > 0u) {
       if (leaf_row) *leaf_row = at;
-      float2 leaf = IN ? tree_leaf_b<true>(v, f2u(node.d.z), count, p, n, rand)
-                       : tree_leaf(v, f2u(node.d.z), count, p, n, rand);
+      const bool use_known = evaluated && count == 1u;
+      float2 leaf = IN ? tree_leaf_b<true>(v, f2u(node.d.z), count, p, n, rand, known, use_known)
+                       : tree_leaf(v, f2u(node.d.z), count, p, n, rand, known, use_known);
       return make_float2(leaf.x, leaf.y * pdf);
     }
     uint32_t left = at + 1u;
@@ -847,6 +858,8 @@ __device__ __forceinline__ float2 tree_pick_b(const ShadeView& v, uint32_t rows,
       rand = clamp_(rand, 0.0f, 1.0f);
     }
     pdf = pdf * (at == left ? left_probability : 1.0f - left_probability);
+    known = at == left ? l : r;
+    evaluated = true;
   }
   return make_float2(0.0f, 0.0f);
 }

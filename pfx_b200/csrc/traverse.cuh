@@ -233,6 +233,19 @@ __device__ __forceinline__ f32x2 quotient2(f32x2 x, f32x2 nd, f32x2 r) {
   return fma2(e, r, q);
 }
 
+// The sm_100 three-input minimum and maximum: the same value as two two-input
+// ones (no NaN reaches them here; a signed zero only ever meets comparisons).
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
 // box_geometry_bounded for a ray with no degenerate axis, the box given as
 // the three coordinate pairs of its node: (lx, ly), (lz, hx), (hy, hz).
 __device__ __forceinline__ bool box_geometry_paired(f32x2 b0, f32x2 b1, f32x2 b2, const PRay& p, float& near) {
@@ -240,8 +253,9 @@ __device__ __forceinline__ bool box_geometry_paired(f32x2 b0, f32x2 b1, f32x2 b2
   unpair(quotient2(sub2(b0, p.o[0]), p.nd[0], p.r[0]), lx, ly);
   unpair(quotient2(sub2(b1, p.o[1]), p.nd[1], p.r[1]), lz, hx);
   unpair(quotient2(sub2(b2, p.o[2]), p.nd[2], p.r[2]), hy, hz);
-  float n = fmaxf(fmaxf(fmaxf(0.0f, fminf(lx, hx)), fminf(ly, hy)), fminf(lz, hz));
-  float f = fminf(fminf(fmaxf(lx, hx), fmaxf(ly, hy)), fmaxf(lz, hz));
+  // max(0, entries) and min(exits), as box_geometry_bounded's chains
+  float n = fmaxf(max3f(fminf(lx, hx), fminf(ly, hy), fminf(lz, hz)), 0.0f);
+  float f = min3f(fmaxf(lx, hx), fmaxf(ly, hy), fmaxf(lz, hz));
   near = n;
   return !(n > f);
 }

@@ -137,3 +137,18 @@ def test_a_wait_that_runs_out_fails_the_call_and_the_denoiser_recovers(gpu):
     den.set_wait_limit(1 << 26)
     again = den.denoise(color, albedo, normal)
     assert np.array_equal(again.view(np.uint32), good.view(np.uint32))
+
+
+@pytest.mark.parametrize("shape", [1, 2, 3])
+def test_every_conv_shape_matches_the_oracle(gpu, shape):
+    """The conv CTA shapes (tall: 8 rows, two stages; paired: 4 rows, one
+    stage, two CTAs per SM; wide: 4 rows, two stages) on the layers of up to
+    64 channels give the oracle's image."""
+    h, w = 130, 270
+    blob = write_tza(random_weights(seed=21))
+    den = Denoiser(blob)
+    assert den._lib.pfxt_debug_denoiser_shape(den.handle, shape) == abi.OK
+    color, albedo, normal = images(h, w, seed=22)
+    out = den.denoise(color, albedo, normal)
+    want = D.denoise(color, albedo, normal, D.build_net(D.parse_tza(blob)))
+    assert gap(out, want) <= TOL, gap(out, want)
