@@ -16,7 +16,7 @@ events recorded on the tracer's own stream.
                    the error is followed on those pixels alone (their values do
                    not depend on the other pixels) and the time is spp x the
                    full-frame pass time measured above.  The cached tracer
-                   (radiance cache at vertex 2, trained online from an untrained
+                   (radiance cache at vertex 1, trained online from an untrained
                    start) runs full-frame passes; its time is the sum of their
                    event-timed durations, training included, L2 flushed before
                    each; relMSE evaluation is outside the timed regions
@@ -278,7 +278,8 @@ def plain_convergence(w, mask, mask_idx, ref, max_spp):
 
 def cache_settings(args):
     """The radiance cache of the 4K workload: 16 levels x 2^19 entries, 64-wide
-    MLP, 2^16 records per step, 4 steps per pass, paths end at vertex 2."""
+    MLP, 2^16 records per step, 4 steps per pass, paths end at vertex 1 (the first scattering vertex after the
+    camera hit), glossy vertices delaying that by up to two."""
     from pfx_b200.cache import CacheSettings
     s = CacheSettings()
     if args.cache_error_bound is not None:

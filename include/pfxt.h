@@ -448,8 +448,8 @@ typedef struct pfxt_cache_settings {
   uint32_t batch;           /* training records per step, a multiple of 128 (65536) */
   uint32_t steps;           /* training steps per sampling pass, at most (4) */
   uint32_t seed;            /* parameter initialisation */
-  uint32_t query_bounce;    /* the path vertex that ends into the cache (2) */
-  uint32_t record_bounces;  /* training records from vertices 0..record_bounces (3) */
+  uint32_t query_bounce;    /* the path vertex that ends into the cache (1) */
+  uint32_t record_bounces;  /* training records from vertices 0..record_bounces (4) */
   float learning_rate;      /* Adam (1e-2) */
   float beta1, beta2, epsilon; /* Adam (0.9, 0.99, 1e-15) */
   float train_fraction;     /* fraction of paths that make training targets (0.01) */

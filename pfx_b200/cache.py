@@ -36,7 +36,7 @@ class CacheSettings:
     batch: int = 65536
     steps: int = 4
     seed: int = 1
-    query_bounce: int = 2
+    query_bounce: int = 1
     record_bounces: int = 4
     learning_rate: float = 1e-2
     beta1: float = 0.9

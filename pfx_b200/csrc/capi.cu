@@ -789,7 +789,7 @@ int pfxt_cache_defaults(pfxt_cache_settings* s) {
     s->batch = 65536;
     s->steps = 4;
     s->seed = 1;
-    s->query_bounce = 2;
+    s->query_bounce = 1;  // 4K room, relMSE 0.01: 3.65x sooner than plain at vertex 1, 2.47x at vertex 2
     s->record_bounces = 4;
     s->min_roughness = 0.25f;
     s->delay_bounces = 2;
