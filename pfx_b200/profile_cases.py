@@ -6,6 +6,7 @@
     python -m pfx_b200.profile_cases shade      # two 960x540 passes of the 4K room (all pass kernels)
     python -m pfx_b200.profile_cases pass-plain # three 4K passes, plain
     python -m pfx_b200.profile_cases pass-cached# eight 4K passes with the radiance cache
+    python -m pfx_b200.profile_cases denoise    # two denoises of a 1024x544 frame (one tile, 16 convolutions each)
 
 Each case runs its kernel a few times on inputs larger than L2 where the
 kernel's input allows, and holds a few GB on the device at most, so that a
@@ -90,10 +91,37 @@ def passes(cached: bool) -> None:
         t.sample(1, s)
 
 
+def denoise() -> None:
+    import torch
+
+    from .denoise import DEFAULT_WEIGHTS, Denoiser, write_tza
+
+    if DEFAULT_WEIGHTS.exists():
+        den = Denoiser()
+    else:  # seeded FP16 weights of the same shapes: the same work
+        rng = np.random.default_rng(0)
+        t = {}
+        for name, o, i in [("enc_conv0", 32, 9), ("enc_conv1", 32, 32), ("enc_conv2", 48, 32), ("enc_conv3", 64, 48),
+                           ("enc_conv4", 80, 64), ("enc_conv5a", 96, 80), ("enc_conv5b", 96, 96),
+                           ("dec_conv4a", 112, 160), ("dec_conv4b", 112, 112), ("dec_conv3a", 96, 160),
+                           ("dec_conv3b", 96, 96), ("dec_conv2a", 64, 128), ("dec_conv2b", 64, 64),
+                           ("dec_conv1a", 64, 73), ("dec_conv1b", 32, 64), ("dec_conv0", 3, 32)]:
+            t[f"{name}.weight"] = rng.normal(0, np.sqrt(2.0 / (9 * i)), (o, i, 3, 3)).astype(np.float16)
+            t[f"{name}.bias"] = np.zeros(o, np.float16)
+        den = Denoiser(write_tza(t))
+    h, w = 544, 1024
+    rng = np.random.default_rng(1)
+    imgs = [torch.from_numpy(rng.uniform(0, 1, (h, w, 4)).astype(np.float32)).cuda() for _ in range(3)]
+    out = torch.empty((h, w, 4), dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        den.denoise_device(w, h, *(x.data_ptr() for x in imgs), out.data_ptr(), 0)
+        den.last()
+
+
 def main() -> None:
     case = sys.argv[1] if len(sys.argv) > 1 else "traverse"
     {"traverse": traverse, "infer": infer, "train": train, "shade": shade,
-     "pass-plain": lambda: passes(False), "pass-cached": lambda: passes(True)}[case]()
+     "pass-plain": lambda: passes(False), "pass-cached": lambda: passes(True), "denoise": denoise}[case]()
     print("ok", case)
 
 
