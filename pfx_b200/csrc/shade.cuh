@@ -460,24 +460,6 @@ __device__ __forceinline__ RowTrig load_trig(const ShadeView& v, uint32_t i) {
   return RowTrig{__ldg(v.light_trig + 2u * i), __ldg(v.light_trig + 2u * i + 1u)};
 }
 
-// Where the light-tree functions read light rows and their trigonometry:
-// the tracer's device buffers, or a copy a kernel staged in shared memory
-// (the same bytes: rows of 4 float4, trigonometry of 2 float4 per row).
-struct GlobalRows {
-  const ShadeView& v;
-  __device__ __forceinline__ LightRow light(uint32_t i) const { return load_light(v, i); }
-  __device__ __forceinline__ RowTrig trig(uint32_t i) const { return load_trig(v, i); }
-};
-struct SharedRows {
-  const float4* rows;  // shared memory
-  const float4* trigs;
-  __device__ __forceinline__ LightRow light(uint32_t i) const {
-    const float4* p = rows + 4u * i;
-    return LightRow{p[0], p[1], p[2], p[3]};
-  }
-  __device__ __forceinline__ RowTrig trig(uint32_t i) const { return RowTrig{trigs[2u * i], trigs[2u * i + 1u]}; }
-};
-
 __device__ __forceinline__ v3 f3of(float4 q) { return mk3(q.x, q.y, q.z); }
 __device__ __forceinline__ float mis_power(float chosen, float other) {
   if (chosen <= 0.0f) return 0.0f;
@@ -733,23 +715,23 @@ __device__ __forceinline__ float2 emitter_importance_to(const LightRow& light, f
   if constexpr (IN) return emitter_importance_b<true>(light, trig, p, n);
   return emitter_importance(light, trig, p, n);
 }
-template <bool IN, class R>
-__device__ __forceinline__ float2 child_importance(const R& rows, uint32_t row, v3 p, v3 n) {
-  LightRow node = rows.light(row);
+template <bool IN>
+__device__ __forceinline__ float2 child_importance(const ShadeView& v, uint32_t row, v3 p, v3 n) {
+  LightRow node = load_light(v, row);
   if (f2u(node.d.y) == 1u) {
     uint32_t light = f2u(node.d.z);
-    return emitter_importance_to<IN>(rows.light(light), rows.trig(light).light, p, n);
+    return emitter_importance_to<IN>(load_light(v, light), load_trig(v, light).light, p, n);
   }
-  if constexpr (IN) return node_importance_b<true>(node, rows.trig(row).node, p, n);
-  return node_importance(node, rows.trig(row).node, p, n);
+  if constexpr (IN) return node_importance_b<true>(node, load_trig(v, row).node, p, n);
+  return node_importance(node, load_trig(v, row).node, p, n);
 }
 
 // tree_leaf (lights.wgsl:276-349): (selected row, pmf).  `use_known`: the
 // leaf holds one light whose importance the descent has already evaluated
 // (child_importance of that leaf: emitter_importance of the same light row
 // at the same point), passed as `known` instead of being evaluated again.
-template <bool IN, class R>
-__device__ __forceinline__ float2 tree_leaf_b(const R& rows, uint32_t first, uint32_t count, v3 p, v3 n,
+template <bool IN>
+__device__ __forceinline__ float2 tree_leaf_b(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n,
                                               float start, float2 known, bool use_known) {
   float rand = start;
   bool sample_max = rand > 0.5f;
@@ -761,7 +743,7 @@ __device__ __forceinline__ float2 tree_leaf_b(const R& rows, uint32_t first, uin
     int32_t index = (int32_t)(first + i);
     float2 importance = (use_known && i == 0u)
                             ? known
-                            : emitter_importance_to<IN>(rows.light(first + i), rows.trig(first + i).light, p, n);
+                            : emitter_importance_to<IN>(load_light(v, first + i), load_trig(v, first + i).light, p, n);
     float weight = sample_max ? importance.x : importance.y;
     float other = sample_max ? importance.y : importance.x;
     if (weight > 0.0f) {
@@ -820,8 +802,8 @@ __device__ __forceinline__ float2 tree_leaf_b(const R& rows, uint32_t first, uin
       total_min = valid;
       chosen_max = (use_known && (uint32_t)selected == first)
                        ? known.x
-                       : emitter_importance_to<IN>(rows.light((uint32_t)selected),
-                                                   rows.trig((uint32_t)selected).light, p, n).x;
+                       : emitter_importance_to<IN>(load_light(v, (uint32_t)selected),
+                                                   load_trig(v, (uint32_t)selected).light, p, n).x;
     }
   }
   return make_float2((float)selected, 0.5f * (chosen_max / total_max + chosen_min / total_min));
@@ -831,63 +813,32 @@ __device__ __forceinline__ float2 tree_leaf_b(const R& rows, uint32_t first, uin
 // by the number of tree rows; a malformed tree ends the descent with pmf 0.
 SH_TREE float2 tree_leaf(const ShadeView& v, uint32_t first, uint32_t count, v3 p, v3 n, float start, float2 known,
                          bool use_known) {
-  return tree_leaf_b<false>(GlobalRows{v}, first, count, p, n, start, known, use_known);
+  return tree_leaf_b<false>(v, first, count, p, n, start, known, use_known);
 }
-SH_TREE float2 tree_leaf_shared(const float4* rows, const float4* trigs, uint32_t first, uint32_t count, v3 p, v3 n,
-                                float start, float2 known, bool use_known) {
-  return tree_leaf_b<false>(SharedRows{rows, trigs}, first, count, p, n, start, known, use_known);
-}
-template <bool IN, class R>
-__device__ __forceinline__ float2 tree_leaf_via(const R& r, uint32_t first, uint32_t count, v3 p, v3 n,
-                                                float start, float2 known, bool use_known);
-template <>
-__device__ __forceinline__ float2 tree_leaf_via<false, GlobalRows>(const GlobalRows& r, uint32_t first, uint32_t count,
-                                                                   v3 p, v3 n, float start, float2 known,
-                                                                   bool use_known) {
-  return tree_leaf(r.v, first, count, p, n, start, known, use_known);
-}
-template <>
-__device__ __forceinline__ float2 tree_leaf_via<false, SharedRows>(const SharedRows& r, uint32_t first, uint32_t count,
-                                                                   v3 p, v3 n, float start, float2 known,
-                                                                   bool use_known) {
-  return tree_leaf_shared(r.rows, r.trigs, first, count, p, n, start, known, use_known);
-}
-template <>
-__device__ __forceinline__ float2 tree_leaf_via<true, GlobalRows>(const GlobalRows& r, uint32_t first, uint32_t count,
-                                                                  v3 p, v3 n, float start, float2 known,
-                                                                  bool use_known) {
-  return tree_leaf_b<true>(r, first, count, p, n, start, known, use_known);
-}
-template <>
-__device__ __forceinline__ float2 tree_leaf_via<true, SharedRows>(const SharedRows& r, uint32_t first, uint32_t count,
-                                                                  v3 p, v3 n, float start, float2 known,
-                                                                  bool use_known) {
-  return tree_leaf_b<true>(r, first, count, p, n, start, known, use_known);
-}
-// `looped`, `tree`: ShadeView::looped and ::tree (the tree's root row is looped + tree).
-template <bool IN, class R>
-__device__ __forceinline__ float2 tree_pick_b(const R& lrows, uint32_t looped, uint32_t tree, uint32_t rows, v3 p,
-                                              v3 n, float start, uint32_t* leaf_row) {
-  uint32_t at = f2u((float)looped + (float)tree);
+template <bool IN>
+__device__ __forceinline__ float2 tree_pick_b(const ShadeView& v, uint32_t rows, v3 p, v3 n, float start,
+                                              uint32_t* leaf_row) {
+  uint32_t at = f2u((float)v.looped + (float)v.tree);
   float rand = start;
   float pdf = 1.0f;
   float2 known = make_float2(0.0f, 0.0f);  // the importance of `at`, once the descent has evaluated it
   bool evaluated = false;
   for (uint32_t guard = 0u; guard < rows; ++guard) {
     if (at >= rows) break;
-    LightRow node = lrows.light(at);
+    LightRow node = load_light(v, at);
     uint32_t count = f2u(node.d.y);
     if (count > 0u) {
       if (leaf_row) *leaf_row = at;
       const bool use_known = evaluated && count == 1u;
-      float2 leaf = tree_leaf_via<IN>(lrows, f2u(node.d.z), count, p, n, rand, known, use_known);
+      float2 leaf = IN ? tree_leaf_b<true>(v, f2u(node.d.z), count, p, n, rand, known, use_known)
+                       : tree_leaf(v, f2u(node.d.z), count, p, n, rand, known, use_known);
       return make_float2(leaf.x, leaf.y * pdf);
     }
     uint32_t left = at + 1u;
     uint32_t right = f2u(node.d.z);
     if (right >= rows) break;
-    float2 l = child_importance<IN>(lrows, left, p, n);
-    float2 r = child_importance<IN>(lrows, right, p, n);
+    float2 l = child_importance<IN>(v, left, p, n);
+    float2 r = child_importance<IN>(v, right, p, n);
     float total_max = l.x + r.x;
     if (total_max == 0.0f) return make_float2(0.0f, 0.0f);
     float total_min = l.y + r.y;
@@ -913,7 +864,7 @@ __device__ __forceinline__ float2 tree_pick_b(const R& lrows, uint32_t looped, u
   return make_float2(0.0f, 0.0f);
 }
 SH_TREE float2 tree_pick(const ShadeView& v, uint32_t rows, v3 p, v3 n, float start, uint32_t* leaf_row) {
-  return tree_pick_b<false>(GlobalRows{v}, v.looped, v.tree, rows, p, n, start, leaf_row);
+  return tree_pick_b<false>(v, rows, p, n, start, leaf_row);
 }
 
 // ------------------------------------------------------------ emitters

@@ -1131,9 +1131,7 @@ __global__ void __launch_bounds__(kThreads, SHADE_LIGHTS_MIN_BLOCKS) k_shade_lig
 // path writes shadow entry i * cap + pending, the pending count travelling in
 // the flag word.  The tree's slot is two launches: the descent (k_tree_pick,
 // one (row, pmf) per path), then its light's candidate and the BSDF.
-// SLOT_TREE_FUSED: the tree's descent and its slot in one launch (a tuning
-// choice measured against the two launches).
-constexpr int SLOT_SUN = 0, SLOT_SKY = 1, SLOT_EMITTER = 2, SLOT_LOOPED = 3, SLOT_TREE = 4, SLOT_TREE_FUSED = 5;
+constexpr int SLOT_SUN = 0, SLOT_SKY = 1, SLOT_EMITTER = 2, SLOT_LOOPED = 3, SLOT_TREE = 4;
 
 #ifndef SLOT_MIN_BLOCKS
 #define SLOT_MIN_BLOCKS 8
@@ -1155,22 +1153,10 @@ __device__ __forceinline__ Rng slot_rng(const Pass& P, uint32_t pixel) {
 
 // The light tree's descent for every scattering path (slot k of tree_pick's
 // caller in k_shade_lights): the pick (light row, pmf) at P.w.pick[qi].
-// SHARED: the block first copies the light rows and their trigonometry
-// (P.light_rows x 96 bytes, launched with that much dynamic shared memory)
-// and descends through the copy: the same bytes, read at shared-memory
-// latency instead of L1's and L2's.
-template <bool SHARED>
 __global__ void __launch_bounds__(kThreads, PICK_MIN_BLOCKS) k_tree_pick(const __grid_constant__ Pass P, uint32_t k) {
-  extern __shared__ float4 tree_rows[];
   const uint32_t n = P.w.counters[12];
   const Specialise& sp = P.sp;
   const ShadeView& V = P.v;
-  if constexpr (SHARED) {
-    const float4* rows = reinterpret_cast<const float4*>(V.lights);
-    for (uint32_t j = threadIdx.x; j < 6u * P.light_rows; j += blockDim.x)
-      tree_rows[j] = j < 4u * P.light_rows ? __ldg(rows + j) : __ldg(V.light_trig + (j - 4u * P.light_rows));
-    __syncthreads();
-  }
   for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n; qi += gridDim.x * blockDim.x) {
     const uint32_t i = P.w.lit[qi];
     const float4* record = P.w.surf + (size_t)i * 9u;
@@ -1184,25 +1170,10 @@ __global__ void __launch_bounds__(kThreads, PICK_MIN_BLOCKS) k_tree_pick(const _
       start = random01(state);
       reinterpret_cast<float*>(P.w.thr + i)[3] = __uint_as_float(state);
     }
-    const v3 p = mk3(g0.x, g0.y, g0.z), nn = mk3(g1.x, g1.y, g1.z);
-    if constexpr (SHARED) {
-      P.w.pick[qi] = tree_pick_b<PICK_INLINE>(SharedRows{tree_rows, tree_rows + 4u * P.light_rows}, V.looped, V.tree,
-                                              P.light_rows, p, nn, start, nullptr);
-    } else {
-      P.w.pick[qi] = tree_pick_b<PICK_INLINE>(GlobalRows{V}, V.looped, V.tree, P.light_rows, p, nn, start, nullptr);
-    }
+    P.w.pick[qi] = tree_pick_b<PICK_INLINE>(V, P.light_rows, mk3(g0.x, g0.y, g0.z), mk3(g1.x, g1.y, g1.z), start,
+                                           nullptr);
   }
 }
-// Light rows a descent block copies into shared memory at most (96 bytes each).
-constexpr uint32_t PICK_SHARED_ROWS = 512;
-// Measured on the plain 4K pass: 95.1 ms through the shared-memory copy against
-// 91.3 ms through L1, so the copy is off by default.
-#ifndef PICK_SHARED
-#define PICK_SHARED false
-#endif
-#ifndef LIGHT_TREE_FUSED
-#define LIGHT_TREE_FUSED false
-#endif
 
 // Slot k of kind KIND for every scattering path: the body of k_shade_lights'
 // slot loop for that kind, with the deferred shadow entry.
@@ -1231,13 +1202,6 @@ __global__ void __launch_bounds__(kThreads, SLOT_MIN_BLOCKS) k_light_slot(const 
     float4 u = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (sp.sobol) u = sobol4(V, sp, slot_rng(P, __float_as_uint(reinterpret_cast<const float*>(P.w.res + i)[3])),
                              light_dim(k));
-    if (KIND == SLOT_TREE_FUSED) {  // k_tree_pick's descent, the same draw first
-      pk = tree_pick_b<false>(GlobalRows{V}, V.looped, V.tree, P.light_rows, p, nn, rnd(sp, state, u.z), nullptr);
-      if (!(pk.y > 0.0f)) {
-        if (state != state_in) reinterpret_cast<float*>(P.w.thr + i)[3] = __uint_as_float(state);
-        continue;
-      }
-    }
     v3 local = mk3(0.0f, 0.0f, 1.0f), direction = mk3(0.0f, 0.0f, 1.0f), strength = splat3(0.0f);
     v3 origin = p;
     float limit = 1e19f, pdf = 0.0f;
@@ -1276,7 +1240,7 @@ __global__ void __launch_bounds__(kThreads, SLOT_MIN_BLOCKS) k_light_slot(const 
       const float4 ro = P.w.ray_o[i];
       origin = spawn_point(p, nn, mk3(ro.x, ro.y, ro.z), g0.w);
       Candidate picked;
-      if (KIND == SLOT_TREE || KIND == SLOT_TREE_FUSED) {
+      if (KIND == SLOT_TREE) {
         picked = light_candidate(sp, V, f2u(pk.x), transform, p, origin, mk3(g2.x, g2.y, g2.z), state, u);
         picked.scale = divs3(picked.scale, pk.y);
       } else if (KIND == SLOT_LOOPED) {
@@ -1483,7 +1447,7 @@ struct Grids {
   int trace_closest[3][2] = {}, trace_any[3][2] = {}, shade = 0, shade_inline = 0, flat = 0;
   int shade_hit = 0, shade_lights = 0, shade_lights_inline = 0, shade_bsdf = 0;
   int retry = 0;  // blocks of the retry walks: one per SM (their work is rare)
-  int tree_pick = 0, slot[6] = {};  // the light slots, one kind per launch
+  int tree_pick = 0, slot[5] = {};  // the light slots, one kind per launch
 };
 Grids& grids() {
   static Grids g;
@@ -1506,13 +1470,12 @@ Grids& grids() {
     g.shade_lights = grid_for((const void*)k_shade_lights<true>, kThreads);
     g.shade_lights_inline = grid_for((const void*)k_shade_lights<false>, kThreads);
     g.shade_bsdf = grid_for((const void*)k_shade_bsdf, kThreads);
-    g.tree_pick = grid_for((const void*)k_tree_pick<false>, kThreads);
+    g.tree_pick = grid_for((const void*)k_tree_pick, kThreads);
     g.slot[SLOT_SUN] = grid_for((const void*)k_light_slot<SLOT_SUN>, kThreads);
     g.slot[SLOT_SKY] = grid_for((const void*)k_light_slot<SLOT_SKY>, kThreads);
     g.slot[SLOT_EMITTER] = grid_for((const void*)k_light_slot<SLOT_EMITTER>, kThreads);
     g.slot[SLOT_LOOPED] = grid_for((const void*)k_light_slot<SLOT_LOOPED>, kThreads);
     g.slot[SLOT_TREE] = grid_for((const void*)k_light_slot<SLOT_TREE>, kThreads);
-    g.slot[SLOT_TREE_FUSED] = grid_for((const void*)k_light_slot<SLOT_TREE_FUSED>, kThreads);
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1547,20 +1510,6 @@ void launch_trace_queue(int sel, uint32_t short_stack, const Pass& P, uint32_t w
 
 int thread_select(uint32_t threads) { return threads == 64u ? 0 : (threads == 256u ? 2 : 1); }
 
-// Blocks of the shared-memory descent for `bytes` of rows per block: as many as fit on every SM.
-int pick_grid_shared(size_t bytes) {
-  static size_t last_bytes = 0;
-  static int last_grid = 0;
-  if (bytes == last_bytes && last_grid) return last_grid;
-  int dev = 0, sms = 0, per = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k_tree_pick<true>, kThreads, bytes);
-  last_bytes = bytes;
-  last_grid = sms * (per > 0 ? per : 1);
-  return last_grid;
-}
-
 // The deferred light slots one kind per launch, in slot order, each launched
 // only where the scene has that kind (the slots k_shade_lights skips without
 // a draw: no sun, no sky, no emissive triangles, no looped lights, no tree).
@@ -1577,16 +1526,7 @@ void launch_light_slots(const Pass& P, cudaStream_t st) {
     k_light_slot<SLOT_LOOPED><<<g.slot[SLOT_LOOPED], kThreads, 0, st>>>(P, 2u + s);
   if (P.slots > 3u + P.v.looped) {
     const uint32_t k = 3u + P.v.looped;
-    if (LIGHT_TREE_FUSED) {
-      k_light_slot<SLOT_TREE_FUSED><<<g.slot[SLOT_TREE_FUSED], kThreads, 0, st>>>(P, k);
-      return;
-    }
-    if (PICK_SHARED && P.light_rows <= PICK_SHARED_ROWS) {
-      const size_t bytes = (size_t)P.light_rows * 96u;
-      k_tree_pick<true><<<pick_grid_shared(bytes), kThreads, bytes, st>>>(P, k);
-    } else {
-      k_tree_pick<false><<<g.tree_pick, kThreads, 0, st>>>(P, k);
-    }
+    k_tree_pick<<<g.tree_pick, kThreads, 0, st>>>(P, k);
     k_light_slot<SLOT_TREE><<<g.slot[SLOT_TREE], kThreads, 0, st>>>(P, k);
   }
 }
