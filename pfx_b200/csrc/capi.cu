@@ -1122,12 +1122,14 @@ int pfxt_debug_denoise_plan(uint32_t height, uint32_t width, uint64_t max_tile_p
 }
 
 // The conv CTA shape of the layers of up to 64 output channels (test and
-// measurement hook): 0 the default, 1 tall, 2 paired, 3 wide (denoise.cu).
+// measurement hook): 0 the default, 1-6 a shape of denoise.cu's list, run by
+// every layer whose outputs fit it.
 int pfxt_debug_denoiser_shape(pfxt_denoiser* h, uint32_t shape) {
   return guarded([&]() {
     if (!h) throw Invalid("null argument");
-    if (shape > 3u) throw Invalid("conv shape must be 0-3");
+    if (shape > 6u) throw Invalid("conv shape must be 0-6");
     h->d->conv_shape = shape;
+    h->d->width = h->d->height = 0;  // the next denoise prepares its launches again
   });
 }
 

@@ -29,6 +29,8 @@
 // a shuffle (max pooling after ReLU = ReLU after max pooling).  Upsampling and
 // concatenation are in the staging: channels of the first source are read at
 // (y / 2, x / 2) of the half-size tensor, the skip source's at (y, x).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -171,41 +173,47 @@ std::vector<uint16_t> conv_chunks(const DenoiseLayer& L, const Tensor& w) {
 // ------------------------------------------------------------------ kernels
 namespace {
 
-constexpr uint32_t CONV_THREADS = 256;               // 8 warps: staging; the epilogue by lane quarters
+constexpr uint32_t CONV_THREADS = 128;               // 4 warps: the epilogue by TMEM lane quarter
 constexpr uint32_t CONV_PIX = 128;                   // pixels per output row (M of the MMA)
 constexpr uint32_t PATCH_W = CONV_PIX + 2;           // staged pixels per input row
 constexpr uint32_t A_PLANE = PATCH_W * 16u;          // bytes of one (row, group of 8 channels) plane
 
 // The shape of a conv CTA: ROWS output rows (one TMEM accumulator each, NMAX
-// columns), STAGES shared-memory stages, CTAS resident CTAs per SM, BATCH
-// loads in flight per staging thread.
-//  * Wide:   4 rows, up to 128 output channels, 2 stages, 1 CTA per SM;
-//  * Tall:   8 rows, up to 64 channels, 2 stages, 1 CTA per SM (half the halo
-//            rows and fixed cost per output row);
-//  * Paired: 4 rows, up to 64 channels, 1 stage, 2 CTAs per SM (one CTA's
-//            epilogue and staging run while the other's MMAs do): the
-//            fastest measured for those layers, the default for them.
-template <uint32_t ROWS_, uint32_t NMAX_, uint32_t STAGES_, uint32_t CTAS_, uint32_t BATCH_>
+// columns), STAGES shared-memory stages, CTAS resident CTAs per SM. Two CTAs
+// per SM overlap one CTA's epilogue (TMEM to registers to HBM) with the
+// other's copies and MMAs; more stages in one CTA overlap only the copies.
+// The 4K frame (two tiles of 2016x2160), forcing one shape where it fits:
+//  * Tall:   8 rows, up to 64 channels, two stages, one CTA: 10.13 ms;
+//  * Quad:   4 rows, up to 64 channels, three stages, one CTA: 11.08 ms;
+//  * Wide:   4 rows, up to 128 channels, two stages, one CTA;
+//  * Paired: 4 rows, up to 64 channels, one stage, two CTAs: 8.82 ms;
+//  * Tall2:  8 rows, up to 32 channels, one stage, two CTAs (Paired for
+//    the 48 and 64 channel layers): 8.45 ms;
+//  * Wide2:  2 rows, up to 128 channels, one stage, two CTAs.
+template <uint32_t ROWS_, uint32_t NMAX_, uint32_t STAGES_, uint32_t CTAS_>
 struct ConvShape {
-  static constexpr uint32_t ROWS = ROWS_, N_MAX = NMAX_, STAGES = STAGES_, CTAS = CTAS_, BATCH_MAX = BATCH_;
+  static constexpr uint32_t ROWS = ROWS_, N_MAX = NMAX_, STAGES = STAGES_, CTAS = CTAS_;
   static constexpr uint32_t TMEM_COLS = ROWS * N_MAX;            // a power of two of at least 32
   static constexpr uint32_t PATCH_ROWS = ROWS + 2u;              // staged input rows
   static constexpr uint32_t A_BYTES = PATCH_ROWS * 2u * A_PLANE;   // one chunk of one half (hi or lo)
   static constexpr uint32_t W_MAX = 9u * 2u * N_MAX * 16u;         // one chunk of weights at N_MAX
   static constexpr uint32_t STAGE = 2u * A_BYTES + W_MAX;
   static constexpr uint32_t CTRL = STAGES * STAGE;                 // mbarriers, TMEM slot, flags
-  static constexpr uint32_t SMEM = CTRL + 64u;
+  static constexpr uint32_t SMEM = CTRL + 128u;
   static_assert(SMEM * CTAS <= 228u * 1024u - CTAS * 1024u, "shared memory per SM");
   static_assert(TMEM_COLS * CTAS <= 512u && (TMEM_COLS & (TMEM_COLS - 1u)) == 0u, "TMEM per SM");
-  static_assert(STAGES == 1u || STAGES == 2u, "one or two stages");
+  static_assert(STAGES >= 1u && STAGES <= 4u, "one to four stages");
 };
-using Wide = ConvShape<4, 128, 2, 1, 14>;
-using Tall = ConvShape<8, 64, 2, 1, 24>;
-using Paired = ConvShape<4, 64, 1, 2, 7>;
+using Wide = ConvShape<4, 128, 2, 1>;
+using Tall = ConvShape<8, 64, 2, 1>;
+using Quad = ConvShape<4, 64, 3, 1>;
+using Paired = ConvShape<4, 64, 1, 2>;
+using Tall2 = ConvShape<8, 32, 1, 2>;
+using Wide2 = ConvShape<2, 128, 1, 2>;
 constexpr uint32_t ERR_CONV_WAIT = 1u, ERR_CONV_DRAIN = 2u;
 // Polls of the waits that drain a CTA's own work in flight (its MMAs and
-// weight copies) before it frees its TMEM and leaves, whatever the main
-// loop's limit: work this kernel issued itself always completes.
+// copies) before it frees its TMEM and leaves, whatever the main loop's
+// limit: work this kernel issued itself always completes.
 constexpr uint32_t DRAIN_LIMIT = 1u << 26;
 
 // Instruction descriptor of kind::f16 with FP16 A and B and an FP32 accumulator, K-major operands.
@@ -213,13 +221,19 @@ __host__ __device__ constexpr uint32_t idesc_f16(uint32_t M, uint32_t N) {
   return (1u << 4) | ((N >> 3) << 17) | ((M >> 4) << 24);
 }
 
+// A tensor of the U-Net: two FP16 planes, hi = fp16(v) and lo = fp16(v - hi),
+// each [y][channel group of 8][x][8 halves] at its stored size; the planes
+// are the operand layout of the convolutions (16 bytes = 8 channels of one
+// pixel, pixels contiguous), so a chunk's rows reach shared memory as they are.
 struct ConvArgs {
-  const float* src0;          // [H >> up][W >> up][c0]
-  const float* src1;          // [H][W][c1] (c1 = 0: none)
+  CUtensorMap a0_hi, a0_lo;   // the first source (at this layer's level; an upsampled source is stored so)
+  CUtensorMap a1_hi, a1_lo;   // the skip source (c1 = 0: none)
   const uint16_t* weights;    // conv_chunks() layout
   const float* bias;          // n
-  float* dst;                 // [H][W][n], or [H/2][W/2][n] when pooling
-  uint32_t H, W, c0, c1, n, up, pool;
+  uint16_t* dst_hi;           // the output planes
+  uint16_t* dst_lo;
+  uint32_t H, W, c0, c1, n, pool;
+  uint32_t up;                // the output is stored at twice its size (its consumer upsamples it)
   uint32_t* error;
   uint32_t wait_limit;        // polls of a bounded mbarrier wait
 };
@@ -228,178 +242,37 @@ __device__ __forceinline__ uint32_t pack_half2(__half a, __half b) {
   return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
 }
 
-// Stage chunk k's input rows into one stage: hi and lo halves of every
-// value.  The staging threads issue every load of their share first and
-// convert afterwards, so a chunk waits for one memory latency, not one per load.
-constexpr uint32_t STAGERS = CONV_THREADS - 32u;  // warps 1..7 stage; warp 0 issues copies and MMAs
-
-template <class S>
-__device__ __forceinline__ void stage_chunk(const ConvArgs& a, uint32_t k, uint32_t y0, uint32_t x0, uint32_t t,
-                                            uint8_t* hi, uint8_t* lo) {
-  constexpr uint32_t ITEMS = S::PATCH_ROWS * PATCH_W * 4u;
-  constexpr uint32_t PER = (ITEMS + STAGERS - 1u) / STAGERS;
-  constexpr uint32_t BATCHES = (PER + S::BATCH_MAX - 1u) / S::BATCH_MAX;
-  constexpr uint32_t BATCH = (PER + BATCHES - 1u) / BATCHES;
-  const uint32_t chunks0 = a.c0 >> 4;
-  const bool first = k < chunks0;
-  const float* src = first ? a.src0 : a.src1;
-  const uint32_t C = first ? a.c0 : a.c1;
-  const uint32_t ch = (first ? k : k - chunks0) * 16u;
-  const uint32_t sh = first ? a.up : 0u;
-  const uint32_t SW = a.W >> sh;
-#pragma unroll 1
-  for (uint32_t bt = 0; bt < BATCHES; ++bt) {
-    float4 v[BATCH];
+// Eight channel values of one pixel into the two planes at `at` (halves).
+__device__ __forceinline__ void store_split8(uint16_t* hi, uint16_t* lo, size_t at, const float* v) {
+  uint32_t h[4], l[4];
 #pragma unroll
-    for (uint32_t j = 0; j < BATCH; ++j) {
-      const uint32_t item = t + (bt * BATCH + j) * STAGERS;
-      const uint32_t q = item & 3u, pix = item >> 2;
-      const uint32_t row = pix / PATCH_W, px = pix - row * PATCH_W;
-      const int y = (int)(y0 + row) - 1, x = (int)(x0 + px) - 1;
-      v[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      if (item < ITEMS && y >= 0 && y < (int)a.H && x >= 0 && x < (int)a.W)
-        v[j] = __ldg(reinterpret_cast<const float4*>(src + ((size_t)((uint32_t)y >> sh) * SW + ((uint32_t)x >> sh)) *
-                                                               C + ch) + q);
-    }
-#pragma unroll
-    for (uint32_t j = 0; j < BATCH; ++j) {
-      const uint32_t item = t + (bt * BATCH + j) * STAGERS;
-      if (item >= ITEMS) break;
-      const uint32_t q = item & 3u, pix = item >> 2;
-      const uint32_t row = pix / PATCH_W, px = pix - row * PATCH_W;
-      __half h0 = __float2half_rn(v[j].x), h1 = __float2half_rn(v[j].y), h2 = __float2half_rn(v[j].z),
-             h3 = __float2half_rn(v[j].w);
-      __half l0 = __float2half_rn(v[j].x - __half2float(h0)), l1 = __float2half_rn(v[j].y - __half2float(h1)),
-             l2 = __float2half_rn(v[j].z - __half2float(h2)), l3 = __float2half_rn(v[j].w - __half2float(h3));
-      const uint32_t off = (row * 2u + (q >> 1)) * A_PLANE + px * 16u + (q & 1u) * 8u;
-      *reinterpret_cast<uint2*>(hi + off) = make_uint2(pack_half2(h0, h1), pack_half2(h2, h3));
-      *reinterpret_cast<uint2*>(lo + off) = make_uint2(pack_half2(l0, l1), pack_half2(l2, l3));
-    }
+  for (int c = 0; c < 4; ++c) {
+    __half h0 = __float2half_rn(v[2 * c]), h1 = __float2half_rn(v[2 * c + 1]);
+    __half l0 = __float2half_rn(v[2 * c] - __half2float(h0)), l1 = __float2half_rn(v[2 * c + 1] - __half2float(h1));
+    h[c] = pack_half2(h0, h1);
+    l[c] = pack_half2(l0, l1);
   }
+  *reinterpret_cast<uint4*>(hi + at) = make_uint4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<uint4*>(lo + at) = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-// One 3x3 convolution (+ bias, ReLU, and 2x2 max pooling when a.pool) of a
-// tile of ROWS rows x 128 pixels.  Grid: (ceil(W / 128), ceil(H / ROWS)).
-// Warp specialised: warps 1-7 stage chunk after chunk into the two stages;
-// lane 0 of warp 0 copies each chunk's weights (bulk copy) and issues its MMAs
-// once the stage is full; the commit of a chunk's MMAs frees its stage.
-// Barriers per stage: `full` (the 224 staging threads arrive), `wbar` (the
-// weight copy's bytes), `done` (the MMAs' commit).  Every wait is bounded: a
-// wait that runs out stops the CTA's pipeline (the others' waits then run
-// out too), the CTA drains what it issued and reports it in a.error.
+// The epilogue: warp w reads TMEM lanes 32 w.. (pixels x0 + 32 w + lane) of
+// every accumulator, 16 columns at a time; bias and ReLU; a pooling layer
+// takes the max of its row pair in the thread and of the neighbouring lane
+// (max pooling after ReLU = ReLU after max pooling); the result is written as
+// its hi/lo planes, four times over (2x2) when the output is stored upsampled.
 template <class S>
-__global__ void __launch_bounds__(CONV_THREADS, S::CTAS) k_conv(const __grid_constant__ ConvArgs a) {
-  constexpr uint32_t STAGE = S::STAGE, A_BYTES = S::A_BYTES, CTRL = S::CTRL, N_MAX = S::N_MAX, ROWS = S::ROWS;
-  constexpr uint32_t NS = S::STAGES, TMEM_COLS = S::TMEM_COLS;
-  extern __shared__ __align__(1024) uint8_t smem[];
-  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
-  const uint32_t x0 = blockIdx.x * CONV_PIX, y0 = blockIdx.y * ROWS;
-  const uint32_t base = umma::smem_addr(smem);
-  const uint32_t wbar[2] = {base + CTRL, base + CTRL + 8u}, done[2] = {base + CTRL + 16u, base + CTRL + 24u},
-                 full[2] = {base + CTRL + 32u, base + CTRL + 40u};
-  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + CTRL + 48u);
-  volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + CTRL + 52u);
-  uint32_t* counts = reinterpret_cast<uint32_t*>(smem + CTRL + 56u);  // [0] chunks committed, [1] copies issued
-  if (tid == 0) {
-    for (int s = 0; s < 2; ++s) {
-      umma::mbar_init(wbar[s], 1);
-      umma::mbar_init(done[s], 1);
-      umma::mbar_init(full[s], STAGERS);
-    }
-    *abort_flag = 0u;
-    counts[0] = counts[1] = 0u;
-  }
-  if (warp == 0) umma::tmem_alloc(slot, TMEM_COLS);
-  umma::fence_before();
-  __syncthreads();
-  umma::fence_after();
-  const uint32_t tmem = *slot;
-  const uint32_t chunks = (a.c0 + a.c1) >> 4;
-  const uint32_t wbytes = 9u * 2u * a.n * 16u;
-  if (warp > 0) {
-    const uint32_t t = tid - 32u;
-    for (uint32_t k = 0; k < chunks; ++k) {
-      const uint32_t s = k % NS;
-      if (k >= NS && !umma::mbar_wait(done[s], ((k - NS) / NS) & 1u, a.wait_limit)) {
-        *abort_flag = 1u;
-        break;
-      }
-      if (*abort_flag) break;
-      uint8_t* hi = smem + s * STAGE;
-      stage_chunk<S>(a, k, y0, x0, t, hi, hi + A_BYTES);
-      umma::fence_async_smem();
-      umma::mbar_arrive(full[s]);
-    }
-  } else if (lane == 0) {
-    const uint32_t id = idesc_f16(128, a.n);
-    uint32_t issued = 0, loads = 0;
-    for (uint32_t k = 0; k < chunks; ++k) {
-      const uint32_t s = k % NS;
-      const uint32_t w_addr = base + s * STAGE + 2u * A_BYTES;
-      if (k >= NS && !umma::mbar_wait(done[s], ((k - NS) / NS) & 1u, a.wait_limit)) {
-        *abort_flag = 1u;
-        break;
-      }
-      umma::mbar_expect_tx(wbar[s], wbytes);
-      umma::bulk_load(w_addr, a.weights + (size_t)k * (wbytes / 2u), wbytes, wbar[s]);
-      loads = k + 1u;
-      if (!umma::mbar_wait(full[s], (k / NS) & 1u, a.wait_limit) ||
-          !umma::mbar_wait(wbar[s], (k / NS) & 1u, a.wait_limit) || *abort_flag) {
-        *abort_flag = 1u;
-        break;
-      }
-      umma::fence_after();
-      // Descriptors move with their start address (bits 0-13, address / 16; a
-      // shared-memory address stays below 2^18, so adding to it never carries
-      // into the other fields): one base descriptor per operand, offsets known
-      // at compile time, so the lane issues ROWS x 18 MMAs back to back.
-      const uint64_t hi_desc = umma::desc(base + s * STAGE, A_PLANE, 128u);
-      const uint64_t lo_desc = umma::desc(base + s * STAGE + A_BYTES, A_PLANE, 128u);
-      const uint64_t w_desc = umma::desc(w_addr, a.n * 16u, 128u);
-      const uint32_t w_step = (2u * a.n * 16u) >> 4;
-      const uint32_t first = k == 0 ? 0u : 1u;
-#pragma unroll
-      for (uint32_t r = 0; r < ROWS; ++r) {
-#pragma unroll
-        for (uint32_t tap = 0; tap < 9; ++tap) {
-          constexpr uint32_t unit = 16u;
-          const uint32_t off = ((r + tap / 3u) * 2u * A_PLANE + (tap % 3u) * 16u) / unit;
-          const uint64_t bd = w_desc + tap * w_step;
-          umma::mma(tmem + r * N_MAX, hi_desc + off, bd, id, tap > 0 ? 1u : first);
-          umma::mma(tmem + r * N_MAX, lo_desc + off, bd, id, 1u);
-        }
-      }
-      umma::commit(done[s]);
-      issued = k + 1u;
-    }
-    counts[0] = issued;
-    counts[1] = loads;
-  }
-  __syncthreads();
-  const uint32_t issued = counts[0], loads = counts[1];
-  const bool late = *abort_flag != 0u;
-  // every MMA issued is done when the last commit's phase completes; a weight
-  // copy whose wait ran out lands before the CTA leaves
-  bool drained = true;
-  if (issued > 0) drained = umma::mbar_wait(done[(issued - 1u) % NS], ((issued - 1u) / NS) & 1u, DRAIN_LIMIT);
-  if (loads > issued) {
-    const uint32_t k = loads - 1u;
-    drained = umma::mbar_wait(wbar[k % NS], (k / NS) & 1u, DRAIN_LIMIT) && drained;
-  }
-  drained = __syncthreads_and(drained);
-  umma::fence_after();
-  if (late || !drained) {
-    if (tid == 0) atomicOr(a.error, (late ? ERR_CONV_WAIT : 0u) | (drained ? 0u : ERR_CONV_DRAIN));
-  } else {
-    // epilogue: warp w reads TMEM lanes 32 (w % 4).. and the row pairs of its half of the rows
-    const uint32_t quarter = warp & 3u;
-    const uint32_t x = x0 + quarter * 32u + lane;
+__device__ __forceinline__ void conv_epilogue(const ConvArgs& a, uint32_t tmem, uint32_t warp, uint32_t lane,
+                                              uint32_t x0, uint32_t y0) {
+  const uint32_t x = x0 + warp * 32u + lane;
+  const uint32_t G = a.n >> 3;
 #pragma unroll 1
-    for (uint32_t r0 = (warp >> 2) * (ROWS / 2u); r0 < (warp >> 2) * (ROWS / 2u) + ROWS / 2u; r0 += 2u)
+  for (uint32_t r0 = 0; r0 < S::ROWS; r0 += 2u) {
+#pragma unroll 1
     for (uint32_t j = 0; j < a.n; j += 16u) {
       float v0[16], v1[16];
-      umma::ld16(umma::taddr(tmem, quarter * 32u, r0 * N_MAX + j), v0);
-      umma::ld16(umma::taddr(tmem, quarter * 32u, (r0 + 1u) * N_MAX + j), v1);
+      umma::ld16(umma::taddr(tmem, warp * 32u, r0 * S::N_MAX + j), v0);
+      umma::ld16(umma::taddr(tmem, warp * 32u, (r0 + 1u) * S::N_MAX + j), v1);
       float b[16];
 #pragma unroll
       for (int c = 0; c < 16; ++c) b[c] = __ldg(a.bias + j + c);
@@ -413,25 +286,141 @@ __global__ void __launch_bounds__(CONV_THREADS, S::CTAS) k_conv(const __grid_con
         }
         const uint32_t oy = (y0 + r0) >> 1, ox = x >> 1, OH = a.H >> 1, OW = a.W >> 1;
         if ((lane & 1u) == 0u && oy < OH && ox < OW) {
-          float4* o = reinterpret_cast<float4*>(a.dst + ((size_t)oy * OW + ox) * a.n + j);
-#pragma unroll
-          for (int c = 0; c < 4; ++c) o[c] = make_float4(m[4 * c], m[4 * c + 1], m[4 * c + 2], m[4 * c + 3]);
+          store_split8(a.dst_hi, a.dst_lo, (((size_t)oy * G + (j >> 3)) * OW + ox) * 8u, m);
+          store_split8(a.dst_hi, a.dst_lo, (((size_t)oy * G + (j >> 3) + 1u) * OW + ox) * 8u, m + 8);
         }
       } else {
 #pragma unroll
         for (uint32_t rr = 0; rr < 2; ++rr) {
           const uint32_t y = y0 + r0 + rr;
-          if (y < a.H && x < a.W) {
-            const float* v = rr ? v1 : v0;
-            float4* o = reinterpret_cast<float4*>(a.dst + ((size_t)y * a.W + x) * a.n + j);
+          float v[16];
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
-              o[c] = make_float4(fmaxf(v[4 * c] + b[4 * c], 0.0f), fmaxf(v[4 * c + 1] + b[4 * c + 1], 0.0f),
-                                 fmaxf(v[4 * c + 2] + b[4 * c + 2], 0.0f), fmaxf(v[4 * c + 3] + b[4 * c + 3], 0.0f));
+          for (int c = 0; c < 16; ++c) v[c] = fmaxf((rr ? v1[c] : v0[c]) + b[c], 0.0f);
+          if (y < a.H && x < a.W) {
+            if (!a.up) {
+              store_split8(a.dst_hi, a.dst_lo, (((size_t)y * G + (j >> 3)) * a.W + x) * 8u, v);
+              store_split8(a.dst_hi, a.dst_lo, (((size_t)y * G + (j >> 3) + 1u) * a.W + x) * 8u, v + 8);
+            } else {
+              const uint32_t W2 = 2u * a.W;
+#pragma unroll
+              for (uint32_t q = 0; q < 4; ++q) {
+                const size_t Y = 2u * y + (q >> 1), X = 2u * x + (q & 1u);
+                store_split8(a.dst_hi, a.dst_lo, ((Y * G + (j >> 3)) * W2 + X) * 8u, v);
+                store_split8(a.dst_hi, a.dst_lo, ((Y * G + (j >> 3) + 1u) * W2 + X) * 8u, v + 8);
+              }
+            }
           }
         }
       }
     }
+  }
+}
+
+// One 3x3 convolution (+ bias, ReLU, and 2x2 max pooling when a.pool) of a
+// tile of ROWS rows x 128 pixels.  Grid: (ceil(W / 128), ceil(H / ROWS)).
+// Lane 0 of warp 0 copies each chunk of 16 input channels into a stage: the
+// hi and lo planes' boxes of 8 halves x 130 pixels x 2 groups x (ROWS + 2)
+// rows from the source's tensor maps (zeros outside the tensor: the
+// convolution's padding), and the chunk's weights by a bulk copy, all on the
+// stage's `full` barrier; lane 0 of warp 1 issues the chunk's MMAs once it is
+// full, and their commit frees the stage.  Every wait is bounded: a wait that
+// runs out stops the CTA's pipeline (the other lane's waits then run out too),
+// the CTA drains what it issued and reports it in a.error.
+template <class S>
+__global__ void __launch_bounds__(CONV_THREADS, S::CTAS) k_conv(const __grid_constant__ ConvArgs a) {
+  constexpr uint32_t STAGE = S::STAGE, A_BYTES = S::A_BYTES, CTRL = S::CTRL, N_MAX = S::N_MAX, ROWS = S::ROWS;
+  constexpr uint32_t NS = S::STAGES, TMEM_COLS = S::TMEM_COLS;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+  const uint32_t x0 = blockIdx.x * CONV_PIX, y0 = blockIdx.y * ROWS;
+  const uint32_t base = umma::smem_addr(smem);
+  const uint32_t full0 = base + CTRL, done0 = base + CTRL + 32u;  // NS barriers of 8 bytes each
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + CTRL + 64u);
+  volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + CTRL + 68u);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(smem + CTRL + 72u);  // [0] chunks committed, [1] chunks loaded
+  if (tid == 0) {
+    for (uint32_t s = 0; s < NS; ++s) {
+      umma::mbar_init(full0 + 8u * s, 1);
+      umma::mbar_init(done0 + 8u * s, 1);
+    }
+    *abort_flag = 0u;
+    counts[0] = counts[1] = 0u;
+  }
+  if (warp == 0) umma::tmem_alloc(slot, TMEM_COLS);
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = *slot;
+  const uint32_t chunks = (a.c0 + a.c1) >> 4, chunks0 = a.c0 >> 4;
+  const uint32_t wbytes = 9u * 2u * a.n * 16u;
+  if (tid == 0) {  // the copies
+    uint32_t loads = 0;
+    for (uint32_t k = 0; k < chunks; ++k) {
+      const uint32_t s = k % NS;
+      if (k >= NS && !umma::mbar_wait(done0 + 8u * s, ((k - NS) / NS) & 1u, a.wait_limit)) {
+        *abort_flag = 1u;
+        break;
+      }
+      if (*abort_flag) break;
+      const uint32_t st = base + s * STAGE, full = full0 + 8u * s;
+      umma::mbar_expect_tx(full, 2u * A_BYTES + wbytes);
+      const bool first = k < chunks0;
+      const int g = (int)(2u * (first ? k : k - chunks0));
+      umma::tensor_load_4d(st, first ? &a.a0_hi : &a.a1_hi, 0, (int)x0 - 1, g, (int)y0 - 1, full);
+      umma::tensor_load_4d(st + A_BYTES, first ? &a.a0_lo : &a.a1_lo, 0, (int)x0 - 1, g, (int)y0 - 1, full);
+      umma::bulk_load(st + 2u * A_BYTES, a.weights + (size_t)k * (wbytes / 2u), wbytes, full);
+      loads = k + 1u;
+    }
+    counts[1] = loads;
+  } else if (tid == 32) {  // the MMAs
+    const uint32_t id = idesc_f16(128, a.n);
+    uint32_t issued = 0;
+    for (uint32_t k = 0; k < chunks; ++k) {
+      const uint32_t s = k % NS;
+      if (!umma::mbar_wait(full0 + 8u * s, (k / NS) & 1u, a.wait_limit) || *abort_flag) {
+        *abort_flag = 1u;
+        break;
+      }
+      umma::fence_after();
+      // Descriptors move with their start address (bits 0-13, address / 16; a
+      // shared-memory address stays below 2^18, so adding to it never carries
+      // into the other fields): one base descriptor per operand, offsets known
+      // at compile time, so the lane issues ROWS x 18 MMAs back to back.
+      const uint64_t hi_desc = umma::desc(base + s * STAGE, A_PLANE, 128u);
+      const uint64_t lo_desc = umma::desc(base + s * STAGE + A_BYTES, A_PLANE, 128u);
+      const uint64_t w_desc = umma::desc(base + s * STAGE + 2u * A_BYTES, a.n * 16u, 128u);
+      const uint32_t w_step = (2u * a.n * 16u) >> 4;
+      const uint32_t first = k == 0 ? 0u : 1u;
+#pragma unroll
+      for (uint32_t r = 0; r < ROWS; ++r) {
+#pragma unroll
+        for (uint32_t tap = 0; tap < 9; ++tap) {
+          const uint32_t off = ((r + tap / 3u) * 2u * A_PLANE + (tap % 3u) * 16u) / 16u;
+          const uint64_t bd = w_desc + tap * w_step;
+          umma::mma(tmem + r * N_MAX, hi_desc + off, bd, id, tap > 0 ? 1u : first);
+          umma::mma(tmem + r * N_MAX, lo_desc + off, bd, id, 1u);
+        }
+      }
+      umma::commit(done0 + 8u * s);
+      issued = k + 1u;
+    }
+    counts[0] = issued;
+  }
+  __syncthreads();
+  const uint32_t issued = counts[0], loads = counts[1];
+  const bool late = *abort_flag != 0u;
+  // every MMA issued is done when the last commit's phase completes; copies
+  // whose MMAs were never issued land before the CTA leaves
+  bool drained = true;
+  if (issued > 0) drained = umma::mbar_wait(done0 + 8u * ((issued - 1u) % NS), ((issued - 1u) / NS) & 1u, DRAIN_LIMIT);
+  for (uint32_t k = issued; k < loads; ++k)
+    drained = umma::mbar_wait(full0 + 8u * (k % NS), (k / NS) & 1u, DRAIN_LIMIT) && drained;
+  drained = __syncthreads_and(drained);
+  umma::fence_after();
+  if (late || !drained) {
+    if (tid == 0) atomicOr(a.error, (late ? ERR_CONV_WAIT : 0u) | (drained ? 0u : ERR_CONV_DRAIN));
+  } else {
+    conv_epilogue<S>(a, tmem, warp, lane, x0, y0);
   }
   umma::fence_before();
   __syncthreads();
@@ -513,15 +502,17 @@ struct TileArgs {
 
 // The tile's input tensor (process.wgsl:65-86): colour times the exposure,
 // NaN to 0, clamped, through the PU curve and normalised; albedo clamped to
-// [0, 1]; normal clamped to [-1, 1] and mapped to [0, 1]; 9 channels of 16.
+// [0, 1]; normal clamped to [-1, 1] and mapped to [0, 1]; 9 channels of 16,
+// written as the hi/lo planes of the U-Net's tensors (out: hi, out + plane: lo).
 __global__ void __launch_bounds__(256) k_input(const __grid_constant__ TileArgs t, const float4* __restrict__ color,
                                                const float4* __restrict__ albedo, const float4* __restrict__ normal,
-                                               const float* __restrict__ scale, float* __restrict__ out) {
+                                               const float* __restrict__ scale, uint16_t* __restrict__ out) {
   const uint32_t n = t.tile_h * t.tile_w;
+  const size_t plane = (size_t)n * 16u;
   const float s = scale[0];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t y = i / t.tile_w, x = i - y * t.tile_w;
-    float v[12] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    float v[16] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     const int ix = (int)x - (int)t.dst[1], iy = (int)y - (int)t.dst[0];
     if (ix >= 0 && ix < (int)t.size[1] && iy >= 0 && iy < (int)t.size[0]) {
       const size_t at = (size_t)(iy + t.src[0]) * t.width + (ix + t.src[1]);
@@ -534,31 +525,33 @@ __global__ void __launch_bounds__(256) k_input(const __grid_constant__ TileArgs 
         v[6 + k] = fminf(fmaxf(nan_to_zero(ms[k]), -1.0f), 1.0f) * 0.5f + 0.5f;
       }
     }
-    float4* o = reinterpret_cast<float4*>(out + (size_t)i * 16u);
-    o[0] = make_float4(v[0], v[1], v[2], v[3]);
-    o[1] = make_float4(v[4], v[5], v[6], v[7]);
-    o[2] = make_float4(v[8], 0.0f, 0.0f, 0.0f);
-    o[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    store_split8(out, out + plane, (((size_t)y * 2u) * t.tile_w + x) * 8u, v);
+    store_split8(out, out + plane, (((size_t)y * 2u + 1u) * t.tile_w + x) * 8u, v + 8);
   }
 }
 
 // The kept part of a tile back into the image (process.wgsl:88-101): the
-// network's three channels, NaN to 0, clamped, denormalised, through the
-// inverse PU curve and divided by the exposure; alpha from the colour.
-__global__ void __launch_bounds__(256) k_output(const __grid_constant__ TileArgs t, const float* __restrict__ net,
+// network's three channels (hi + lo of its output's first group), NaN to 0,
+// clamped, denormalised, through the inverse PU curve and divided by the
+// exposure; alpha from the colour.
+__global__ void __launch_bounds__(256) k_output(const __grid_constant__ TileArgs t, const uint16_t* __restrict__ net,
                                                 uint32_t net_channels, const float4* __restrict__ color,
                                                 const float* __restrict__ scale, float4* __restrict__ out) {
   const uint32_t n = t.out_size[0] * t.out_size[1];
+  const size_t plane = (size_t)t.tile_h * t.tile_w * net_channels;
   const float s = scale[0];
   const float inv = s != 0.0f ? 1.0f / s : 0.0f;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t gy = i / t.out_size[1], gx = i - gy * t.out_size[1];
-    const float* v = net + ((size_t)(gy + t.out_src[0]) * t.tile_w + gx + t.out_src[1]) * net_channels;
+    const size_t at = ((size_t)(gy + t.out_src[0]) * (net_channels >> 3) * t.tile_w + gx + t.out_src[1]) * 8u;
     float r[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) r[k] = pu_inverse(fminf(fmaxf(nan_to_zero(v[k]), 0.0f), DN_FLT_MAX) * t.rcp_norm) * inv;
-    const size_t at = (size_t)(gy + t.out_dst[0]) * t.width + gx + t.out_dst[1];
-    out[at] = make_float4(r[0], r[1], r[2], color[at].w);
+    for (int k = 0; k < 3; ++k) {
+      const float v = __half2float(__ushort_as_half(net[at + k])) + __half2float(__ushort_as_half(net[plane + at + k]));
+      r[k] = pu_inverse(fminf(fmaxf(nan_to_zero(v), 0.0f), DN_FLT_MAX) * t.rcp_norm) * inv;
+    }
+    const size_t o = (size_t)(gy + t.out_dst[0]) * t.width + gx + t.out_dst[1];
+    out[o] = make_float4(r[0], r[1], r[2], color[o].w);
   }
 }
 
@@ -629,7 +622,7 @@ Denoiser::~Denoiser() {
     if (L.d_weights) cudaFree(L.d_weights);
     if (L.d_bias) cudaFree(L.d_bias);
   }
-  for (float* t : tensors)
+  for (uint16_t* t : tensors)
     if (t) cudaFree(t);
   if (d_scale) cudaFree(d_scale);
   if (d_bins) cudaFree(d_bins);
@@ -721,29 +714,129 @@ Denoiser* denoiser_create(const void* blob, size_t bytes) {
          "convolution shared memory");
   dcheck(cudaFuncSetAttribute(k_conv<Tall>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Tall::SMEM),
          "convolution shared memory");
+  dcheck(cudaFuncSetAttribute(k_conv<Quad>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Quad::SMEM),
+         "convolution shared memory");
   dcheck(cudaFuncSetAttribute(k_conv<Paired>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Paired::SMEM),
+         "convolution shared memory");
+  dcheck(cudaFuncSetAttribute(k_conv<Tall2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Tall2::SMEM),
+         "convolution shared memory");
+  dcheck(cudaFuncSetAttribute(k_conv<Wide2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Wide2::SMEM),
          "convolution shared memory");
   return d.release();
 }
 
 // The plan and the tile tensors for a width x height image (setup.rs:82-156;
 // every tensor of a tile has its own buffer).
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    dcheck(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q), "tensor map entry point");
+    if (q != cudaDriverEntryPointSuccess || !p) throw DeviceError("cuTensorMapEncodeTiled is not available");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// The tensor map of one plane of a U-Net tensor ([H][C/8][W][8] halves) for
+// boxes of 8 halves x 130 pixels x 2 groups x `rows` rows.
+CUtensorMap plane_map(const uint16_t* plane, uint32_t H, uint32_t W, uint32_t C, uint32_t rows) {
+  CUtensorMap m;
+  const cuuint64_t dims[4] = {8u, W, C / 8u, H};
+  const cuuint64_t strides[3] = {16u, (cuuint64_t)W * 16u, (cuuint64_t)(C / 8u) * W * 16u};
+  const cuuint32_t box[4] = {8u, PATCH_W, 2u, rows + 2u}, elem[4] = {1u, 1u, 1u, 1u};
+  CUresult r = encode_tiled()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, const_cast<uint16_t*>(plane), dims, strides, box,
+                              elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw DeviceError("denoiser tensor map: error " + std::to_string((int)r));
+  return m;
+}
+
+// The shapes by number (the measurement hook's values): 1 Tall, 2 Quad,
+// 3 Wide, 4 Paired, 5 Tall2, 6 Wide2.
+constexpr uint32_t SHAPE_ROWS[7] = {0, Tall::ROWS, Quad::ROWS, Wide::ROWS, Paired::ROWS, Tall2::ROWS, Wide2::ROWS};
+constexpr uint32_t SHAPE_NMAX[7] = {0, Tall::N_MAX, Quad::N_MAX, Wide::N_MAX, Paired::N_MAX, Tall2::N_MAX, Wide2::N_MAX};
+
+// Which conv shape a layer runs: the one set for measurement where the
+// layer's outputs fit it, else the fastest measured for its output count.
+uint32_t shape_of(const Denoiser& d, const DenoiseLayer& L) {
+  if (d.conv_shape && d.conv_shape <= 6u && L.n <= SHAPE_NMAX[d.conv_shape]) return d.conv_shape;
+  if (L.n <= Tall2::N_MAX) return 5u;
+  if (L.n <= Paired::N_MAX) return 4u;
+  return 3u;
+}
+uint32_t rows_of(uint32_t shape) { return SHAPE_ROWS[shape]; }
+
+struct Launches {
+  std::vector<ConvArgs> args;
+  std::vector<uint32_t> shapes;
+};
+}  // namespace
+
+// The plan, the tile tensors and every convolution's arguments for a width x
+// height image (setup.rs:82-156; every tensor of a tile has its own buffer).
 void denoiser_prepare(Denoiser& d, uint32_t width, uint32_t height) {
   if (width == 0 || height == 0) throw Invalid("image dimensions must be nonzero");
   if (d.width == width && d.height == height) return;
-  for (float* t : d.tensors)
+  for (uint16_t* t : d.tensors)
     if (t) cudaFree(t);
   d.tensors.clear();
+  d.stored_level.clear();
+  d.launches.reset();
   d.width = d.height = 0;
   d.plan = denoise_plan(height, width, d.max_tile_pixels);
+  const uint32_t TH = d.plan.tile_h, TW = d.plan.tile_w;
   auto alloc = [&](uint32_t level, uint32_t channels) {
-    float* p = nullptr;
-    size_t bytes = (size_t)(d.plan.tile_h >> level) * (d.plan.tile_w >> level) * channels * 4u;
+    uint16_t* p = nullptr;
+    size_t bytes = 2u * (size_t)(TH >> level) * (TW >> level) * channels * 2u;
     dcheck(cudaMalloc(&p, std::max<size_t>(bytes, 16)), "denoiser tensors");
     d.tensors.push_back(p);
+    d.stored_level.push_back(level);
   };
   alloc(0, 16);
-  for (auto& L : d.layers) alloc(L.out_level(), L.n);
+  for (size_t i = 0; i < d.layers.size(); ++i) {
+    const DenoiseLayer& L = d.layers[i];
+    bool upsampled = false;  // the first source of an upsampling layer is stored at that layer's size
+    for (const auto& M : d.layers) upsampled = upsampled || (M.upsample && M.src0 == (int)i);
+    if (upsampled && L.pool) throw Invalid("a pooled output cannot feed an upsampling layer");
+    alloc(upsampled ? L.out_level() - 1u : L.out_level(), L.n);
+  }
+  auto plane = [&](int src, bool lo) {
+    const uint32_t t = (uint32_t)(src + 1);
+    const uint32_t lv = d.stored_level[t];
+    const uint32_t C = src == -1 ? 16u : d.layers[src].n;
+    return d.tensors[t] + (lo ? (size_t)(TH >> lv) * (TW >> lv) * C : 0u);
+  };
+  auto launches = std::make_shared<Launches>();
+  for (size_t i = 0; i < d.layers.size(); ++i) {
+    const DenoiseLayer& L = d.layers[i];
+    ConvArgs a;
+    memset(&a, 0, sizeof(a));
+    a.H = TH >> L.level;
+    a.W = TW >> L.level;
+    const uint32_t shape = shape_of(d, L), rows = rows_of(shape);
+    a.a0_hi = plane_map(plane(L.src0, false), a.H, a.W, L.c0, rows);
+    a.a0_lo = plane_map(plane(L.src0, true), a.H, a.W, L.c0, rows);
+    if (L.src1 != -2) {
+      a.a1_hi = plane_map(plane(L.src1, false), a.H, a.W, L.c1, rows);
+      a.a1_lo = plane_map(plane(L.src1, true), a.H, a.W, L.c1, rows);
+    }
+    a.weights = L.d_weights;
+    a.bias = L.d_bias;
+    a.dst_hi = plane((int)i, false);
+    a.dst_lo = plane((int)i, true);
+    a.c0 = L.c0;
+    a.c1 = L.c1;
+    a.n = L.n;
+    a.pool = L.pool ? 1u : 0u;
+    a.up = d.stored_level[i + 1] + 1u == L.out_level() ? 1u : 0u;
+    a.error = d.d_error;
+    launches->args.push_back(a);
+    launches->shapes.push_back(shape);
+  }
+  d.launches = launches;
   size_t bins = (size_t)div_ceil(width, 16) * div_ceil(height, 16);
   if (bins > d.bins_capacity) {
     if (d.d_bins) cudaFree(d.d_bins);
@@ -768,6 +861,7 @@ void denoise_device(Denoiser& d, uint32_t width, uint32_t height, const float4* 
   dcheck(cudaSetDevice(d.device), "denoiser device");
   denoiser_prepare(d, width, height);
   const DenoisePlan& p = d.plan;
+  const Launches& launches = *static_cast<const Launches*>(d.launches.get());
   float norm, rcp_norm;
   norm_scales(norm, rcp_norm);
   int sms = 0;
@@ -794,29 +888,20 @@ void denoise_device(Denoiser& d, uint32_t width, uint32_t height, const float4* 
     t.rcp_norm = rcp_norm;
     k_input<<<sms * 8, 256, 0, st>>>(t, color, albedo, normal, d.d_scale, d.tensors[0]);
     for (size_t i = 0; i < d.layers.size(); ++i) {
-      const DenoiseLayer& L = d.layers[i];
-      ConvArgs a;
-      a.src0 = d.tensors[L.src0 + 1];
-      a.src1 = L.src1 != -2 ? d.tensors[L.src1 + 1] : nullptr;
-      a.weights = L.d_weights;
-      a.bias = L.d_bias;
-      a.dst = d.tensors[i + 1];
-      a.H = p.tile_h >> L.level;
-      a.W = p.tile_w >> L.level;
-      a.c0 = L.c0;
-      a.c1 = L.c1;
-      a.n = L.n;
-      a.up = L.upsample ? 1u : 0u;
-      a.pool = L.pool ? 1u : 0u;
-      a.error = d.d_error;
+      ConvArgs a = launches.args[i];
       a.wait_limit = d.wait_limit;
-      // layers of up to 64 channels: paired CTAs (4K frame: paired 10.4 ms, tall 12.6, wide 13.6)
-      const uint32_t shape = a.n > Paired::N_MAX ? 0u : (d.conv_shape ? d.conv_shape : 2u);
+      const uint32_t shape = launches.shapes[i];
       if (shape == 1u) {
         k_conv<Tall><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Tall::ROWS)), CONV_THREADS, Tall::SMEM, st>>>(a);
       } else if (shape == 2u) {
+        k_conv<Quad><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Quad::ROWS)), CONV_THREADS, Quad::SMEM, st>>>(a);
+      } else if (shape == 4u) {
         k_conv<Paired>
             <<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Paired::ROWS)), CONV_THREADS, Paired::SMEM, st>>>(a);
+      } else if (shape == 5u) {
+        k_conv<Tall2><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Tall2::ROWS)), CONV_THREADS, Tall2::SMEM, st>>>(a);
+      } else if (shape == 6u) {
+        k_conv<Wide2><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Wide2::ROWS)), CONV_THREADS, Wide2::SMEM, st>>>(a);
       } else {
         k_conv<Wide><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Wide::ROWS)), CONV_THREADS, Wide::SMEM, st>>>(a);
       }

@@ -6,6 +6,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -48,13 +49,15 @@ struct Denoiser {
   // per image size: the plan and the tile tensors
   uint32_t width = 0, height = 0;
   DenoisePlan plan;
-  std::vector<float*> tensors;  // [0] the input tensor, [1 + i] layer i's output
+  std::vector<uint16_t*> tensors;  // [0] the input tensor, [1 + i] layer i's output: hi plane, then lo plane
+  std::vector<uint32_t> stored_level;  // the level each tensor is stored at (an upsampled source: one below)
+  std::shared_ptr<void> launches;      // per layer: the convolution's arguments and tensor maps (denoise.cu)
   float* d_scale = nullptr;     // autoexposure: one float
   float* d_bins = nullptr;
   size_t bins_capacity = 0;
   uint32_t* d_error = nullptr;  // set by a conv kernel whose bounded wait ran out
   uint32_t wait_limit = 1u << 26;  // polls of the conv kernels' bounded mbarrier waits
-  uint32_t conv_shape = 0;         // layers of up to 64 channels: 0 default, 1 tall, 2 paired, 3 wide
+  uint32_t conv_shape = 0;         // 0 the per-layer default, 1-6 one shape wherever it fits
   cudaStream_t stream = nullptr;   // host-buffer calls
   float4* d_images = nullptr;      // host-buffer calls: colour, albedo, normal, output
   size_t images_pixels = 0;

@@ -85,6 +85,20 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
                : "memory");
 }
 
+// Tiled 4-D bulk tensor copy (TMA) of the box at coordinates (c0, c1, c2, c3)
+// of the tensor map `map` (a __grid_constant__ kernel parameter) into this
+// CTA's shared memory, completing on `mbar`.  No multicast.  Coordinates may
+// lie outside the tensor (the box reads zeros there); c0, the innermost, must
+// be a multiple of 16 bytes of elements.
+__device__ __forceinline__ void tensor_load_4d(uint32_t dst, const void* map, int c0, int c1, int c2, int c3,
+                                               uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(dst),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(mbar)
+      : "memory");
+}
+
 // Bounded wait for the completion of phase `parity`; false when the limit ran out.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32_t limit) {
   for (uint32_t i = 0; i < limit; ++i) {

@@ -139,11 +139,10 @@ def test_a_wait_that_runs_out_fails_the_call_and_the_denoiser_recovers(gpu):
     assert np.array_equal(again.view(np.uint32), good.view(np.uint32))
 
 
-@pytest.mark.parametrize("shape", [1, 2, 3])
+@pytest.mark.parametrize("shape", [1, 2, 3, 4, 5, 6])
 def test_every_conv_shape_matches_the_oracle(gpu, shape):
-    """The conv CTA shapes (tall: 8 rows, two stages; paired: 4 rows, one
-    stage, two CTAs per SM; wide: 4 rows, two stages) on the layers of up to
-    64 channels give the oracle's image."""
+    """Every conv CTA shape (rows per CTA, stages, CTAs per SM), forced on
+    the layers whose outputs it fits, gives the oracle's image."""
     h, w = 130, 270
     blob = write_tza(random_weights(seed=21))
     den = Denoiser(blob)
