@@ -1,11 +1,13 @@
 // Kernels and host side of the neural radiance cache (cache.h).
 //
 // Inference and training run the MLP on the 5th-generation tensor cores:
-// a CTA of 128 threads owns 128 rows (one per thread and per TMEM lane),
-// writes its rows' BF16 operands into shared memory, and one thread issues
-// tcgen05.mma (M = 128, K = 16 per instruction) with the FP32 accumulator in
-// TMEM; the epilogue reads each row back with tcgen05.ld, applies ReLU and
-// writes the next layer's operand.  Training fuses forward, loss, backward
+// a CTA of 128 threads owns a tile of 128 rows (one per thread and per TMEM
+// lane), one thread issues tcgen05.mma (M = 128, K = 16 per instruction)
+// with the FP32 accumulator in TMEM, and the epilogue reads each row back
+// with tcgen05.ld, applies ReLU and writes the next layer's operand into
+// shared memory.  Inference gathers the hash grid in a kernel of its own
+// (k_encode, four threads per query), which writes the tiles' inputs in the
+// operand layout; k_mlp copies them into shared memory in bulk.  Training fuses forward, loss, backward
 // and the hash-grid gradient scatter in one kernel; the weight gradients of
 // all the CTA's tiles accumulate in TMEM (dW = dH^T x H, the batch rows as
 // the K dimension, with the activation tiles read MN-major) and are added
@@ -40,12 +42,6 @@ constexpr uint32_t DRAIN_LIMIT = 1u << 26;
 constexpr uint32_t ERR_WAIT = 1u;
 constexpr uint32_t ERR_DRAIN = 2u;
 
-// Shared memory of the inference kernel (bytes).
-// The second hidden layer's operand reuses the input tile (whose MMA has
-// completed by then); the output layer's accumulator reuses the first's.
-constexpr uint32_t I_X = 0, I_H1 = 16384, I_H2 = I_X, I_W = 32768, I_CTRL = I_W + 18432;
-constexpr uint32_t I_SMEM = 52 * 1024;  // four CTAs (4 x 128 TMEM columns) per SM
-constexpr uint32_t I_TMEM = 128;
 // Shared memory of the training kernel.  dY, dH2 and dH1 are read as M = 128
 // MN-major operands whose rows 64..127 (16..127 for dY) are not data: the
 // 32 KB the descriptor spans from each of them stays inside the allocation,
@@ -132,6 +128,47 @@ __device__ __forceinline__ void one_blob(float v, float* out) {
   }
 }
 
+__device__ __forceinline__ uint32_t pick4(const uint4& w, uint32_t j) {
+  return j == 0u ? w.x : j == 1u ? w.y : j == 2u ? w.z : w.w;
+}
+__device__ __forceinline__ float2 entry(uint32_t bits) {
+  return __half22float2(*reinterpret_cast<const __half2*>(&bits));
+}
+
+// The two features of level l at unit position u: the trilinear blend of
+// the cell's 8 corner entries.  Corners 2p and 2p + 1 differ in x only, and
+// their entries share an aligned group of four (16 bytes, one sector) unless
+// the x + 1 entry carries out of it (dense index i + 1, or hashed index
+// (x + 1) ^ h): one 16-byte load fetches the group of the x entry, and a
+// second, 4-byte load runs only for the lanes whose x + 1 entry lies outside.
+__device__ __forceinline__ void level_features(const CacheGrid& g, const __half2* __restrict__ table, uint32_t l,
+                                               const float u[3], float& f0, float& f1) {
+  Corners cn = corners(g, l, u);
+  const uint32_t* level = reinterpret_cast<const uint32_t*>(table) + (size_t)l * g.entries;
+  float2 f[8];
+#pragma unroll
+  for (uint32_t p = 0; p < 4; ++p) {
+    const uint32_t y = cn.iy + (p & 1u), z = cn.iz + (p >> 1);
+    const uint32_t i0 = grid_index(g, l, cn.ix, y, z), i1 = grid_index(g, l, cn.ix + 1u, y, z);
+    const uint4 w = __ldg(reinterpret_cast<const uint4*>(level + (i0 & ~3u)));
+    uint32_t e1;
+    if ((i1 & ~3u) == (i0 & ~3u))
+      e1 = pick4(w, i1 & 3u);
+    else
+      e1 = __ldg(level + i1);
+    f[2 * p] = entry(pick4(w, i0 & 3u));
+    f[2 * p + 1] = entry(e1);
+  }
+  f0 = 0.0f;
+  f1 = 0.0f;
+#pragma unroll
+  for (uint32_t k = 0; k < 8; ++k) {
+    float w = corner_weight(cn, k);
+    f0 = f0 + w * f[k].x;
+    f1 = f1 + w * f[k].y;
+  }
+}
+
 // The 64 network inputs of one query (5 float4: position + roughness,
 // direction + transmission, normal, diffuse, specular).
 __device__ __forceinline__ void encode(const CacheGrid& g, const __half2* __restrict__ table, const float4* q,
@@ -140,24 +177,7 @@ __device__ __forceinline__ void encode(const CacheGrid& g, const __half2* __rest
   float u[3] = {unit_coord(a.x, g.lo[0], g.inv_extent[0]), unit_coord(a.y, g.lo[1], g.inv_extent[1]),
                 unit_coord(a.z, g.lo[2], g.inv_extent[2])};
 #pragma unroll
-  for (uint32_t l = 0; l < NRC_LEVELS; ++l) {
-    Corners cn = corners(g, l, u);
-    const __half2* level = table + (size_t)l * g.entries;
-    float2 f[8];
-#pragma unroll
-    for (uint32_t k = 0; k < 8; ++k)
-      f[k] = __half22float2(__ldg(level + grid_index(g, l, cn.ix + (k & 1u), cn.iy + ((k >> 1) & 1u),
-                                                        cn.iz + (k >> 2))));
-    float f0 = 0.0f, f1 = 0.0f;
-#pragma unroll
-    for (uint32_t k = 0; k < 8; ++k) {
-      float w = corner_weight(cn, k);
-      f0 = f0 + w * f[k].x;
-      f1 = f1 + w * f[k].y;
-    }
-    x[2 * l] = f0;
-    x[2 * l + 1] = f1;
-  }
+  for (uint32_t l = 0; l < NRC_LEVELS; ++l) level_features(g, table, l, u, x[2 * l], x[2 * l + 1]);
   one_blob(b.x, x + 32);
   one_blob(b.y, x + 36);
   one_blob(b.z, x + 40);
@@ -243,94 +263,196 @@ __device__ __forceinline__ void ld64(uint32_t tbase, uint32_t warp, uint32_t col
 }
 
 // ------------------------------------------------------------------ inference
-__global__ void __launch_bounds__(128, 4)
-    k_infer(CacheGrid g, const __half2* __restrict__ table, const uint16_t* __restrict__ weights,
-            const float4* __restrict__ queries, const uint32_t* __restrict__ n_dev, uint32_t n_max,
-            const uint32_t* __restrict__ scatter, float4* __restrict__ out, uint32_t* error) {
+// The gather and the MLP as two kernels: k_encode gathers the hash grid with
+// four threads per query (all the warps an SM holds, no shared memory or
+// TMEM to limit them) and writes each 128-query tile's inputs in the MMA's
+// operand layout; k_mlp streams those tiles into shared memory with bulk
+// copies, two in flight per CTA, and runs the three layers on the tensor
+// cores.  The tiles cross HBM once each way (128 bytes per query).
+constexpr uint32_t X_TILE = NRC_ROWS * NRC_IN * 2u;  // 16 KB: one tile's inputs, BF16
+
+// Lane (q, r) of a warp encodes row 8w + r of the queries (w the warp):
+// levels 4q..4q+3 (32 corner entries) into column group q, and the extras of
+// column group 4 + q; each is one 16-byte store, and the 8 lanes of a q
+// write one 128-byte line of the tile.  Rows from the count up to the end
+// of the last tile are written as zeros.
+__global__ void __launch_bounds__(256)
+    k_encode(CacheGrid g, const __half2* __restrict__ table, const float4* __restrict__ queries,
+             const uint32_t* __restrict__ n_dev, uint32_t n_max, uint8_t* __restrict__ x) {
+  const uint32_t lane = threadIdx.x & 31u, q = lane >> 3;
+  const uint32_t row = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 8u + (lane & 7u);
+  const uint32_t count = n_dev ? min(*n_dev, n_max) : n_max;
+  if (row >= ((count + NRC_ROWS - 1u) & ~(NRC_ROWS - 1u))) return;
+  float v[16];
+  if (row < count) {
+    const float4* qp = queries + (size_t)row * 5u;
+    const float4 a = __ldg(qp);
+    const float u[3] = {unit_coord(a.x, g.lo[0], g.inv_extent[0]), unit_coord(a.y, g.lo[1], g.inv_extent[1]),
+                        unit_coord(a.z, g.lo[2], g.inv_extent[2])};
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) level_features(g, table, 4u * q + j, u, v[2 * j], v[2 * j + 1]);
+    // inputs 32 + 8q .. 39 + 8q, as encode() writes them
+    if (q == 0u) {
+      const float4 b = __ldg(qp + 1);
+      one_blob(b.x, v + 8);
+      one_blob(b.y, v + 12);
+    } else if (q == 1u) {
+      const float4 b = __ldg(qp + 1), c = __ldg(qp + 2);
+      one_blob(b.z, v + 8);
+      one_blob(c.x, v + 12);
+    } else if (q == 2u) {
+      const float4 c = __ldg(qp + 2);
+      one_blob(c.y, v + 8);
+      one_blob(c.z, v + 12);
+    } else {
+      const float4 b = __ldg(qp + 1), d = __ldg(qp + 3), e = __ldg(qp + 4);
+      v[8] = a.w > 0.0f ? (a.w < 1.0f ? a.w : 1.0f) : 0.0f;
+      v[9] = d.x;
+      v[10] = d.y;
+      v[11] = d.z;
+      v[12] = e.x;
+      v[13] = e.y;
+      v[14] = e.z;
+      v[15] = b.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = 0.0f;
+  }
+  uint8_t* tile = x + (size_t)(row / NRC_ROWS) * X_TILE;
+  const uint32_t r = row % NRC_ROWS;
+  const uint32_t at = (r >> 3) * 128u + (r & 7u) * 16u;
+  *reinterpret_cast<uint4*>(tile + q * 2048u + at) =
+      make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
+  *reinterpret_cast<uint4*>(tile + (4u + q) * 2048u + at) =
+      make_uint4(pack2(v[8], v[9]), pack2(v[10], v[11]), pack2(v[12], v[13]), pack2(v[14], v[15]));
+}
+
+// Shared memory of k_mlp: the weights, two input stages and one hidden
+// operand (the second hidden layer's overwrites the first's once the MMA
+// that read it has completed).
+constexpr uint32_t M_W = 0, M_X = WEIGHT_BYTES, M_H = M_X + 2u * X_TILE, M_CTRL = M_H + X_TILE;
+constexpr uint32_t M_SMEM = M_CTRL + 64u;  // three CTAs (3 x 128 TMEM columns) per SM
+constexpr uint32_t M_TMEM = 128;
+static_assert(3u * (M_SMEM + 1024u) <= 228u * 1024u, "three CTAs per SM");
+
+__global__ void __launch_bounds__(128, 3)
+    k_mlp(const uint16_t* __restrict__ weights, const uint8_t* __restrict__ x, const uint32_t* __restrict__ n_dev,
+          uint32_t n_max, const uint32_t* __restrict__ scatter, float4* __restrict__ out, uint32_t wait_limit,
+          uint32_t* error) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t tid = threadIdx.x, warp = tid >> 5;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + I_CTRL);
-  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + I_CTRL + 8);
-  const uint32_t a_x = umma::smem_addr(smem + I_X), a_h1 = umma::smem_addr(smem + I_H1),
-                 a_h2 = umma::smem_addr(smem + I_H2), a_w = umma::smem_addr(smem + I_W);
-  const uint32_t mb = umma::smem_addr(mbar), wb = umma::smem_addr(smem + I_CTRL + 16);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + M_CTRL + 32);
+  const uint32_t a_w = umma::smem_addr(smem + M_W), a_h = umma::smem_addr(smem + M_H);
+  const uint32_t mb = umma::smem_addr(smem + M_CTRL), wb = mb + 8u, xb0 = mb + 16u;  // xb0, xb0 + 8: the stages
   if (tid == 0) {
     umma::mbar_init(mb, 1);
     umma::mbar_init(wb, 1);
+    umma::mbar_init(xb0, 1);
+    umma::mbar_init(xb0 + 8u, 1);
   }
   __syncthreads();
-  if (!load_weights(smem + I_W, weights, wb)) {
+  if (!load_weights(smem + M_W, weights, wb)) {
     if (tid == 0) atomicOr(error, ERR_WAIT | ERR_DRAIN);
     return;  // no TMEM allocated yet
   }
-  if (warp == 0) umma::tmem_alloc(slot, I_TMEM);
-  umma::fence_async_smem();
+  const uint32_t count = n_dev ? min(*n_dev, n_max) : n_max;
+  const uint32_t tiles = (count + NRC_ROWS - 1u) / NRC_ROWS;
+  // thread 0's record of the stages with a copy in flight (drained before the CTA leaves)
+  uint32_t pending = 0;
+  auto fetch = [&](uint32_t stage, uint32_t tile) {
+    if (tile >= tiles) return;
+    const uint32_t bar = xb0 + 8u * stage;
+    umma::mbar_expect_tx(bar, X_TILE);
+    umma::bulk_load(umma::smem_addr(smem + M_X + stage * X_TILE), x + (size_t)tile * X_TILE, X_TILE, bar);
+    pending |= 1u << stage;
+  };
+  if (tid == 0) {
+    fetch(0u, blockIdx.x);
+    fetch(1u, blockIdx.x + gridDim.x);
+  }
+  if (warp == 0) umma::tmem_alloc(slot, M_TMEM);
   sync_tc();
   const uint32_t tbase = *slot;
-  const uint32_t T0 = tbase, T1 = tbase + 64, T2 = tbase;  // T2: the output layer over T0's columns 0..15
-  uint32_t count = n_dev ? min(*n_dev, n_max) : n_max;
-  uint32_t phase = 0;
-  bool late = false;
-  for (uint32_t tile = blockIdx.x; tile * NRC_ROWS < count; tile += gridDim.x) {
-    const uint32_t row = tile * NRC_ROWS + tid;
-    float x[64];
-    if (row < count) {
-      encode(g, table, queries + (size_t)row * 5u, x);
-    } else {
-#pragma unroll
-      for (int k = 0; k < 64; ++k) x[k] = 0.0f;
-    }
-    store_row<64>(smem + I_X, tid, 128, x);
-    umma::fence_async_smem();
-    sync_tc();
+  const uint32_t T0 = tbase, T1 = tbase + 64;
+  uint32_t phase = 0, xphase = 0;  // xphase bit s: the parity of stage s's next fill
+  bool late = false, mma_pending = false;
+  uint32_t i = 0;
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++i) {
+    const uint32_t s = i & 1u, a_x = umma::smem_addr(smem + M_X + s * X_TILE);
+    late = !umma::mbar_wait(xb0 + 8u * s, (xphase >> s) & 1u, wait_limit);
+    if (__syncthreads_or(late)) break;  // no MMA in flight; the stage's copy is drained below
+    xphase ^= 1u << s;
+    mma_pending = true;  // from the commit until its wait completes
     if (tid == 0) {
+      pending &= ~(1u << s);
 #pragma unroll
-      for (uint32_t s = 0; s < 4; ++s)
-        umma::mma(T0, umma::desc_k(a_x, 128, s), umma::desc_k(a_w + W_1, 64, s), ID_F64, s);
+      for (uint32_t k = 0; k < 4; ++k)
+        umma::mma(T0, umma::desc_k(a_x, 128, k), umma::desc_k(a_w + W_1, 64, k), ID_F64, k);
       umma::commit(mb);
     }
-    late = !umma::mbar_wait(mb, phase, g.wait_limit);
+    late = !umma::mbar_wait(mb, phase, wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(late)) break;
     umma::fence_after();
-    ld64(tbase, warp, 0, x);
+    if (tid == 0) fetch(s, tile + 2u * gridDim.x);  // the stage's MMA has read it
+    float v[64];
+    ld64(tbase, warp, 0, v);
 #pragma unroll
-    for (int k = 0; k < 64; ++k) x[k] = x[k] > 0.0f ? x[k] : 0.0f;
-    store_row<64>(smem + I_H1, tid, 128, x);
+    for (int k = 0; k < 64; ++k) v[k] = v[k] > 0.0f ? v[k] : 0.0f;
+    store_row<64>(smem + M_H, tid, 128, v);
     umma::fence_async_smem();
     sync_tc();
     if (tid == 0) {
 #pragma unroll
-      for (uint32_t s = 0; s < 4; ++s)
-        umma::mma(T1, umma::desc_k(a_h1, 128, s), umma::desc_k(a_w + W_2, 64, s), ID_F64, s);
+      for (uint32_t k = 0; k < 4; ++k)
+        umma::mma(T1, umma::desc_k(a_h, 128, k), umma::desc_k(a_w + W_2, 64, k), ID_F64, k);
       umma::commit(mb);
     }
-    late = !umma::mbar_wait(mb, phase, g.wait_limit);
+    late = !umma::mbar_wait(mb, phase, wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(late)) break;
     umma::fence_after();
-    ld64(tbase, warp, 64, x);
+    ld64(tbase, warp, 64, v);
 #pragma unroll
-    for (int k = 0; k < 64; ++k) x[k] = x[k] > 0.0f ? x[k] : 0.0f;
-    store_row<64>(smem + I_H2, tid, 128, x);
+    for (int k = 0; k < 64; ++k) v[k] = v[k] > 0.0f ? v[k] : 0.0f;
+    store_row<64>(smem + M_H, tid, 128, v);
     umma::fence_async_smem();
     sync_tc();
     if (tid == 0) {
 #pragma unroll
-      for (uint32_t s = 0; s < 4; ++s)
-        umma::mma(T2, umma::desc_k(a_h2, 128, s), umma::desc_k(a_w + W_3, 16, s), ID_F16, s);
+      for (uint32_t k = 0; k < 4; ++k)
+        umma::mma(T0, umma::desc_k(a_h, 128, k), umma::desc_k(a_w + W_3, 16, k), ID_F16, k);
       umma::commit(mb);
     }
-    late = !umma::mbar_wait(mb, phase, g.wait_limit);
+    late = !umma::mbar_wait(mb, phase, wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(late)) break;
+    mma_pending = false;
     umma::fence_after();
     float y[16];
     umma::ld16(umma::taddr(tbase, 32u * warp, 0), y);
+    const uint32_t row = tile * NRC_ROWS + tid;
     if (row < count) out[scatter ? scatter[row] : row] = make_float4(y[0], y[1], y[2], 0.0f);
     sync_tc();
   }
-  finish(late, mb, phase, error, tbase, I_TMEM);
+  // Copies still in flight land before the shared memory is released: each
+  // waits on the phase of its own fill, which completes.
+  bool landed = true;
+  if (tid == 0) {
+    for (uint32_t st = 0; st < 2u; ++st)
+      if (((pending >> st) & 1u) && !umma::mbar_wait(xb0 + 8u * st, (xphase >> st) & 1u, DRAIN_LIMIT)) landed = false;
+  }
+  if (!landed) atomicOr(error, ERR_DRAIN);
+  if (late && !mma_pending) {
+    // the wait that ran out was a copy's: no MMA in flight writes the TMEM
+    if (tid == 0) atomicOr(error, ERR_WAIT);
+    umma::fence_before();
+    __syncthreads();
+    if (warp == 0) umma::tmem_free(tbase, M_TMEM);
+    return;
+  }
+  finish(late, mb, phase, error, tbase, M_TMEM);
 }
 
 // ------------------------------------------------------------------ training
@@ -625,7 +747,7 @@ int sm_count() {
 void attributes() {
   static bool done = false;
   if (done) return;
-  check(cudaFuncSetAttribute(k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I_SMEM), "cache inference");
+  check(cudaFuncSetAttribute(k_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M_SMEM), "cache inference");
   check(cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T_SMEM), "cache training");
   done = true;
 }
@@ -768,15 +890,17 @@ CacheView cache_view(pfxt_cache& c) {
   return v;
 }
 
+size_t cache_x_bytes(uint32_t n) { return (size_t)((n + NRC_ROWS - 1) / NRC_ROWS) * X_TILE; }
+
 void cache_infer_launch(pfxt_cache& c, const float4* queries, const uint32_t* n_dev, uint32_t n,
-                        const uint32_t* scatter, float4* out, cudaStream_t stream, uint32_t ctas_per_sm) {
+                        const uint32_t* scatter, float4* out, uint8_t* x, cudaStream_t stream) {
   if (n == 0) return;
   if (c.broken) throw DeviceError("cache: unusable after an undrained tensor-core wait");
-  uint32_t tiles = (n + NRC_ROWS - 1) / NRC_ROWS;
-  ctas_per_sm = std::min<uint32_t>(std::max<uint32_t>(ctas_per_sm, 1u), 4u);
-  uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)sm_count() * ctas_per_sm);
-  k_infer<<<grid, 128, I_SMEM, stream>>>(c.grid, c.d_table16, c.d_weights, queries, n_dev, n, scatter, out,
-                                         c.d_error);
+  const uint32_t tiles = (n + NRC_ROWS - 1) / NRC_ROWS;
+  // 8 rows per warp, 64 per block of 256 threads, over whole tiles
+  k_encode<<<(tiles * NRC_ROWS + 63u) / 64u, 256, 0, stream>>>(c.grid, c.d_table16, queries, n_dev, n, x);
+  const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)sm_count() * 3u);
+  k_mlp<<<grid, 128, M_SMEM, stream>>>(c.d_weights, x, n_dev, n, scatter, out, c.grid.wait_limit, c.d_error);
   check(cudaGetLastError(), "cache inference");
 }
 

@@ -88,12 +88,14 @@ void cache_create(pfxt_cache& c, const pfxt_cache_settings& s);
 void cache_release(pfxt_cache& c);
 void cache_set_bounds(pfxt_cache& c, const float lo[3], const float hi[3]);
 CacheView cache_view(pfxt_cache& c);
-// Inference over `n` queries (5 float4 each) on `stream`; out[k] = rgb.
-// `n_dev`, if set, is read on the device instead of `n` (an upper bound).
-// `ctas_per_sm` (1..4) sizes the persistent grid: fewer leave room on every SM
-// for kernels that run beside the inference.
+// Device bytes of the encoded inputs of `n` queries (cache_infer_launch's `x`).
+size_t cache_x_bytes(uint32_t n);
+// Inference over `n` queries (5 float4 each) on `stream`; out[k] = rgb, or
+// out[scatter[k]].  `n_dev`, if set, is read on the device instead of `n`
+// (an upper bound).  `x` (cache_x_bytes(n), 16-byte aligned) holds the
+// encoded inputs between the gather and the MLP.
 void cache_infer_launch(pfxt_cache& c, const float4* queries, const uint32_t* n_dev, uint32_t n, const uint32_t* scatter,
-                        float4* out, cudaStream_t stream, uint32_t ctas_per_sm = 4);
+                        float4* out, uint8_t* x, cudaStream_t stream);
 // One training step over records [first, first + batch) of `records`
 // (6 float4 each) when at least first + batch exist (`count_dev` on the
 // device, or `count` when it is null); then Adam.

@@ -890,11 +890,12 @@ int pfxt_cache_infer(pfxt_cache* c, const pfxt_cache_query* q, uint32_t count, f
     if (!c || (count && (!q || !rgb))) throw Invalid("null argument");
     if (count == 0) return;
     std::lock_guard<std::mutex> g(c->lock);
-    size_t qb = (size_t)count * sizeof(pfxt_cache_query);
-    char* d = cache_stage(*c, qb + (size_t)count * 16u);
+    size_t qb = (size_t)count * sizeof(pfxt_cache_query), xo = (qb + (size_t)count * 16u + 255u) & ~size_t(255);
+    char* d = cache_stage(*c, xo + cache_x_bytes(count));
     float4* d_out = reinterpret_cast<float4*>(d + qb);
     check(cudaMemcpyAsync(d, q, qb, cudaMemcpyHostToDevice, c->stream), "cache queries");
-    cache_infer_launch(*c, reinterpret_cast<const float4*>(d), nullptr, count, nullptr, d_out, c->stream);
+    cache_infer_launch(*c, reinterpret_cast<const float4*>(d), nullptr, count, nullptr, d_out,
+                       reinterpret_cast<uint8_t*>(d + xo), c->stream);
     std::vector<float4> out(count);
     check(cudaMemcpyAsync(out.data(), d_out, (size_t)count * 16u, cudaMemcpyDeviceToHost, c->stream), "cache output");
     check(cudaStreamSynchronize(c->stream), "cache inference");
@@ -1122,12 +1123,12 @@ int pfxt_debug_denoise_plan(uint32_t height, uint32_t width, uint64_t max_tile_p
 }
 
 // The conv CTA shape of the layers of up to 64 output channels (test and
-// measurement hook): 0 the default, 1-6 a shape of denoise.cu's list, run by
+// measurement hook): 0 the default, 1-9 a shape of denoise.cu's list, run by
 // every layer whose outputs fit it.
 int pfxt_debug_denoiser_shape(pfxt_denoiser* h, uint32_t shape) {
   return guarded([&]() {
     if (!h) throw Invalid("null argument");
-    if (shape > 6u) throw Invalid("conv shape must be 0-6");
+    if (shape > 9u) throw Invalid("conv shape must be 0-9");
     h->d->conv_shape = shape;
     h->d->width = h->d->height = 0;  // the next denoise prepares its launches again
   });

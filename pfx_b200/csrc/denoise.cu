@@ -173,23 +173,33 @@ std::vector<uint16_t> conv_chunks(const DenoiseLayer& L, const Tensor& w) {
 // ------------------------------------------------------------------ kernels
 namespace {
 
+__host__ __device__ constexpr uint32_t div_ceil(uint32_t a, uint32_t b) { return (a + b - 1u) / b; }
+
 constexpr uint32_t CONV_THREADS = 128;               // 4 warps: the epilogue by TMEM lane quarter
 constexpr uint32_t CONV_PIX = 128;                   // pixels per output row (M of the MMA)
 constexpr uint32_t PATCH_W = CONV_PIX + 2;           // staged pixels per input row
 constexpr uint32_t A_PLANE = PATCH_W * 16u;          // bytes of one (row, group of 8 channels) plane
 
 // The shape of a conv CTA: ROWS output rows (one TMEM accumulator each, NMAX
-// columns), STAGES shared-memory stages, CTAS resident CTAs per SM. Two CTAs
-// per SM overlap one CTA's epilogue (TMEM to registers to HBM) with the
-// other's copies and MMAs; more stages in one CTA overlap only the copies.
-// The 4K frame (two tiles of 2016x2160), forcing one shape where it fits:
-//  * Tall:   8 rows, up to 64 channels, two stages, one CTA: 10.13 ms;
-//  * Quad:   4 rows, up to 64 channels, three stages, one CTA: 11.08 ms;
-//  * Wide:   4 rows, up to 128 channels, two stages, one CTA;
-//  * Paired: 4 rows, up to 64 channels, one stage, two CTAs: 8.82 ms;
-//  * Tall2:  8 rows, up to 32 channels, one stage, two CTAs (Paired for
-//    the 48 and 64 channel layers): 8.45 ms;
-//  * Wide2:  2 rows, up to 128 channels, one stage, two CTAs.
+// columns), STAGES shared-memory stages, CTAS resident CTAs per SM.  In
+// k_conv, two CTAs per SM overlap one CTA's epilogue (TMEM to registers to
+// HBM) with the other's copies and MMAs, and more stages in one CTA overlap
+// only the copies; the persistent k_conv_ws overlaps all three in one CTA.
+// The 4K frame (two tiles of 2016x2160), forcing one shape wherever it fits
+// (the wide layers, above 64 channels, otherwise on Wide):
+//  * k_conv, Tall:   8 rows, up to 64 channels, two stages, one CTA: 10.13 ms;
+//  * k_conv, Quad:   4 rows, up to 64 channels, three stages, one CTA: 11.08 ms;
+//  * k_conv, Wide:   4 rows, up to 128 channels, two stages, one CTA: 11.07 ms;
+//  * k_conv, Paired: 4 rows, up to 64 channels, one stage, two CTAs: 8.82 ms;
+//  * k_conv, Tall2:  8 rows, up to 32 channels, one stage, two CTAs (with
+//    Paired on the 48 and 64 channel layers): 8.45 ms;
+//  * k_conv, Wide2:  2 rows, up to 128 channels, one stage, two CTAs: 10.40 ms;
+//  * k_conv_ws, Persist64:  4 rows, up to 64 channels, three stages: 7.66 ms;
+//  * k_conv_ws, Persist32:  8 rows, up to 32 channels, two stages (with
+//    Paired on the 48 and 64 channel layers): 7.98 ms;
+//  * k_conv_ws, Persist128: 2 rows, up to 128 channels, three stages: 8.49 ms.
+// Layer by layer the persistent shapes are the fastest: Persist32 up to 32
+// channels, Persist64 up to 64, Persist128 above (the default).
 template <uint32_t ROWS_, uint32_t NMAX_, uint32_t STAGES_, uint32_t CTAS_>
 struct ConvShape {
   static constexpr uint32_t ROWS = ROWS_, N_MAX = NMAX_, STAGES = STAGES_, CTAS = CTAS_;
@@ -210,6 +220,10 @@ using Quad = ConvShape<4, 64, 3, 1>;
 using Paired = ConvShape<4, 64, 1, 2>;
 using Tall2 = ConvShape<8, 32, 1, 2>;
 using Wide2 = ConvShape<2, 128, 1, 2>;
+// the persistent kernel's shapes (two accumulators: 2 x ROWS x N_MAX TMEM columns)
+using Persist64 = ConvShape<4, 64, 3, 1>;
+using Persist32 = ConvShape<8, 32, 2, 1>;
+using Persist128 = ConvShape<2, 128, 3, 1>;
 constexpr uint32_t ERR_CONV_WAIT = 1u, ERR_CONV_DRAIN = 2u;
 // Polls of the waits that drain a CTA's own work in flight (its MMAs and
 // copies) before it frees its TMEM and leaves, whatever the main loop's
@@ -427,6 +441,134 @@ __global__ void __launch_bounds__(CONV_THREADS, S::CTAS) k_conv(const __grid_con
   if (drained && warp == 0) umma::tmem_free(tmem, TMEM_COLS);
 }
 
+// The persistent form of k_conv: one CTA per SM walks the layer's tiles
+// (tile t: pixels 128 (t % gx).., rows ROWS (t / gx)..) in steps of gridDim.x.
+// Lane 0 of warp 0 streams every tile's chunks through the NS-stage ring;
+// lane 0 of warp 1 issues each tile's MMAs into one of two TMEM accumulators
+// (tiles alternate) and commits it to the accumulator's `full` barrier; warps
+// 2-5 (TMEM lane quarters 2, 3, 0, 1) run the epilogue of one accumulator while
+// the MMAs of the next tile fill the other, and free it on its `empty`
+// barrier (one arrival per warp).  Waits are bounded as in k_conv.
+constexpr uint32_t WS_THREADS = 192;
+template <class S>
+__global__ void __launch_bounds__(WS_THREADS, 1) k_conv_ws(const __grid_constant__ ConvArgs a) {
+  constexpr uint32_t STAGE = S::STAGE, A_BYTES = S::A_BYTES, CTRL = S::CTRL, N_MAX = S::N_MAX, ROWS = S::ROWS;
+  constexpr uint32_t NS = S::STAGES, ACC = ROWS * N_MAX, TMEM_COLS = 2u * ACC;
+  static_assert(TMEM_COLS <= 512u, "two accumulators in the TMEM of one SM");
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+  const uint32_t base = umma::smem_addr(smem);
+  const uint32_t full0 = base + CTRL, empty0 = base + CTRL + 32u;  // NS barriers each
+  const uint32_t accf0 = base + CTRL + 64u, acce0 = base + CTRL + 80u;  // two each
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + CTRL + 96u);
+  volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + CTRL + 100u);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(smem + CTRL + 104u);  // [0] chunks loaded, [1] chunks committed
+  if (tid == 0) {
+    for (uint32_t s = 0; s < NS; ++s) {
+      umma::mbar_init(full0 + 8u * s, 1);
+      umma::mbar_init(empty0 + 8u * s, 1);
+    }
+    for (uint32_t b = 0; b < 2u; ++b) {
+      umma::mbar_init(accf0 + 8u * b, 1);
+      umma::mbar_init(acce0 + 8u * b, 4);
+    }
+    *abort_flag = 0u;
+    counts[0] = counts[1] = 0u;
+  }
+  if (warp == 0) umma::tmem_alloc(slot, TMEM_COLS);
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = *slot;
+  const uint32_t gx = div_ceil(a.W, CONV_PIX), tiles = gx * div_ceil(a.H, ROWS);
+  const uint32_t chunks = (a.c0 + a.c1) >> 4, chunks0 = a.c0 >> 4;
+  const uint32_t wbytes = 9u * 2u * a.n * 16u;
+  if (tid == 0) {  // the copies
+    uint32_t c = 0;
+    for (uint32_t t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x) {
+      const int x0 = (int)((t % gx) * CONV_PIX), y0 = (int)((t / gx) * ROWS);
+      for (uint32_t k = 0; k < chunks; ++k, ++c) {
+        const uint32_t s = c % NS;
+        if (c >= NS && !umma::mbar_wait(empty0 + 8u * s, ((c - NS) / NS) & 1u, a.wait_limit)) *abort_flag = 1u;
+        if (*abort_flag) break;
+        const uint32_t st = base + s * STAGE, full = full0 + 8u * s;
+        umma::mbar_expect_tx(full, 2u * A_BYTES + wbytes);
+        const bool first = k < chunks0;
+        const int g = (int)(2u * (first ? k : k - chunks0));
+        umma::tensor_load_4d(st, first ? &a.a0_hi : &a.a1_hi, 0, x0 - 1, g, y0 - 1, full);
+        umma::tensor_load_4d(st + A_BYTES, first ? &a.a0_lo : &a.a1_lo, 0, x0 - 1, g, y0 - 1, full);
+        umma::bulk_load(st + 2u * A_BYTES, a.weights + (size_t)k * (wbytes / 2u), wbytes, full);
+        counts[0] = c + 1u;
+      }
+    }
+  } else if (tid == 32) {  // the MMAs
+    const uint32_t id = idesc_f16(128, a.n);
+    const uint32_t w_step = (2u * a.n * 16u) >> 4;
+    uint32_t c = 0, i = 0;
+    for (uint32_t t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x, ++i) {
+      const uint32_t b = i & 1u, acc = tmem + b * ACC;
+      if (i >= 2u && !umma::mbar_wait(acce0 + 8u * b, ((i - 2u) >> 1) & 1u, a.wait_limit)) *abort_flag = 1u;
+      if (*abort_flag) break;
+      umma::fence_after();
+      for (uint32_t k = 0; k < chunks; ++k, ++c) {
+        const uint32_t s = c % NS;
+        if (!umma::mbar_wait(full0 + 8u * s, (c / NS) & 1u, a.wait_limit)) *abort_flag = 1u;
+        if (*abort_flag) break;
+        umma::fence_after();
+        const uint64_t hi_desc = umma::desc(base + s * STAGE, A_PLANE, 128u);
+        const uint64_t lo_desc = umma::desc(base + s * STAGE + A_BYTES, A_PLANE, 128u);
+        const uint64_t w_desc = umma::desc(base + s * STAGE + 2u * A_BYTES, a.n * 16u, 128u);
+        const uint32_t first = k == 0 ? 0u : 1u;
+#pragma unroll
+        for (uint32_t r = 0; r < ROWS; ++r) {
+#pragma unroll
+          for (uint32_t tap = 0; tap < 9; ++tap) {
+            const uint32_t off = ((r + tap / 3u) * 2u * A_PLANE + (tap % 3u) * 16u) / 16u;
+            const uint64_t bd = w_desc + tap * w_step;
+            umma::mma(acc + r * N_MAX, hi_desc + off, bd, id, tap > 0 ? 1u : first);
+            umma::mma(acc + r * N_MAX, lo_desc + off, bd, id, 1u);
+          }
+        }
+        umma::commit(empty0 + 8u * s);
+        counts[1] = c + 1u;
+      }
+      if (*abort_flag) break;
+      umma::commit(accf0 + 8u * b);
+    }
+  } else if (warp >= 2u) {  // the epilogue
+    const uint32_t quarter = warp & 3u;
+    uint32_t i = 0;
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++i) {
+      const uint32_t b = i & 1u;
+      const bool ok = umma::mbar_wait(accf0 + 8u * b, (i >> 1) & 1u, a.wait_limit);
+      if (__any_sync(0xffffffffu, !ok || *abort_flag)) {
+        *abort_flag = 1u;
+        break;
+      }
+      umma::fence_after();
+      conv_epilogue<S>(a, tmem + b * ACC, quarter, lane, (t % gx) * CONV_PIX, (t / gx) * ROWS);
+      umma::fence_before();
+      __syncwarp();
+      if (lane == 0) umma::mbar_arrive(acce0 + 8u * b);
+    }
+  }
+  __syncthreads();
+  const uint32_t loads = counts[0], issued = counts[1];
+  const bool late = *abort_flag != 0u;
+  // every MMA issued is done when the last chunk's commit completes; copies
+  // whose MMAs were never issued land before the CTA leaves
+  bool drained = true;
+  if (issued > 0)
+    drained = umma::mbar_wait(empty0 + 8u * ((issued - 1u) % NS), ((issued - 1u) / NS) & 1u, DRAIN_LIMIT);
+  for (uint32_t k = issued; k < loads; ++k)
+    drained = umma::mbar_wait(full0 + 8u * (k % NS), (k / NS) & 1u, DRAIN_LIMIT) && drained;
+  drained = __syncthreads_and(drained);
+  if ((late || !drained) && tid == 0)
+    atomicOr(a.error, (late ? ERR_CONV_WAIT : 0u) | (drained ? 0u : ERR_CONV_DRAIN));
+  umma::fence_after();
+  if (drained && warp == 0) umma::tmem_free(tmem, TMEM_COLS);
+}
+
 // ------------------------------------------------------------------ image processing
 constexpr float DN_FLT_MAX = 3.4028234663852886e38f;
 
@@ -563,7 +705,6 @@ __global__ void __launch_bounds__(256) k_output(const __grid_constant__ TileArgs
 namespace {
 uint32_t round_up(uint32_t a, uint32_t b) { return (a + b - 1u) / b * b; }
 uint32_t round_up_rem(uint32_t a, uint32_t b, uint32_t c) { return (a + b - c - 1u) / b * b + c; }
-uint32_t div_ceil(uint32_t a, uint32_t b) { return (a + b - 1u) / b; }
 constexpr uint32_t ALIGN = 16, RECEPTIVE_FIELD = 174;
 }  // namespace
 
@@ -722,6 +863,13 @@ Denoiser* denoiser_create(const void* blob, size_t bytes) {
          "convolution shared memory");
   dcheck(cudaFuncSetAttribute(k_conv<Wide2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Wide2::SMEM),
          "convolution shared memory");
+  dcheck(cudaFuncSetAttribute(k_conv_ws<Persist64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Persist64::SMEM),
+         "convolution shared memory");
+  dcheck(cudaFuncSetAttribute(k_conv_ws<Persist32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Persist32::SMEM),
+         "convolution shared memory");
+  dcheck(cudaFuncSetAttribute(k_conv_ws<Persist128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)Persist128::SMEM),
+         "convolution shared memory");
   return d.release();
 }
 
@@ -755,17 +903,22 @@ CUtensorMap plane_map(const uint16_t* plane, uint32_t H, uint32_t W, uint32_t C,
 }
 
 // The shapes by number (the measurement hook's values): 1 Tall, 2 Quad,
-// 3 Wide, 4 Paired, 5 Tall2, 6 Wide2.
-constexpr uint32_t SHAPE_ROWS[7] = {0, Tall::ROWS, Quad::ROWS, Wide::ROWS, Paired::ROWS, Tall2::ROWS, Wide2::ROWS};
-constexpr uint32_t SHAPE_NMAX[7] = {0, Tall::N_MAX, Quad::N_MAX, Wide::N_MAX, Paired::N_MAX, Tall2::N_MAX, Wide2::N_MAX};
+// 3 Wide, 4 Paired, 5 Tall2, 6 Wide2; 7-9 the persistent kernel with
+// Persist64, Persist32, Persist128.
+constexpr uint32_t SHAPES = 10;
+constexpr uint32_t SHAPE_ROWS[SHAPES] = {0,           Tall::ROWS,      Quad::ROWS,      Wide::ROWS,     Paired::ROWS,
+                                         Tall2::ROWS, Wide2::ROWS,     Persist64::ROWS, Persist32::ROWS, Persist128::ROWS};
+constexpr uint32_t SHAPE_NMAX[SHAPES] = {0,            Tall::N_MAX,      Quad::N_MAX,      Wide::N_MAX,
+                                         Paired::N_MAX, Tall2::N_MAX,     Wide2::N_MAX,     Persist64::N_MAX,
+                                         Persist32::N_MAX, Persist128::N_MAX};
 
 // Which conv shape a layer runs: the one set for measurement where the
 // layer's outputs fit it, else the fastest measured for its output count.
 uint32_t shape_of(const Denoiser& d, const DenoiseLayer& L) {
-  if (d.conv_shape && d.conv_shape <= 6u && L.n <= SHAPE_NMAX[d.conv_shape]) return d.conv_shape;
-  if (L.n <= Tall2::N_MAX) return 5u;
-  if (L.n <= Paired::N_MAX) return 4u;
-  return 3u;
+  if (d.conv_shape && d.conv_shape < SHAPES && L.n <= SHAPE_NMAX[d.conv_shape]) return d.conv_shape;
+  if (L.n <= Persist32::N_MAX) return 8u;
+  if (L.n <= Persist64::N_MAX) return 7u;
+  return 9u;
 }
 uint32_t rows_of(uint32_t shape) { return SHAPE_ROWS[shape]; }
 
@@ -866,6 +1019,10 @@ void denoise_device(Denoiser& d, uint32_t width, uint32_t height, const float4* 
   norm_scales(norm, rcp_norm);
   int sms = 0;
   dcheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d.device), "device");
+  // the persistent kernel's grid: one CTA per SM, or per tile when there are fewer
+  auto persistent = [&](const ConvArgs& a, uint32_t rows) {
+    return std::min<uint32_t>(div_ceil(a.W, CONV_PIX) * div_ceil(a.H, rows), (uint32_t)sms);
+  };
   dcheck(cudaEventRecord(d.ev0, st), "denoiser timing");
   const uint32_t gx = div_ceil(width, 16), gy = div_ceil(height, 16);
   k_exposure_bins<<<dim3(gx, gy), 256, 0, st>>>(color, width, height, d.d_bins);
@@ -902,6 +1059,12 @@ void denoise_device(Denoiser& d, uint32_t width, uint32_t height, const float4* 
         k_conv<Tall2><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Tall2::ROWS)), CONV_THREADS, Tall2::SMEM, st>>>(a);
       } else if (shape == 6u) {
         k_conv<Wide2><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Wide2::ROWS)), CONV_THREADS, Wide2::SMEM, st>>>(a);
+      } else if (shape == 7u) {
+        k_conv_ws<Persist64><<<persistent(a, Persist64::ROWS), WS_THREADS, Persist64::SMEM, st>>>(a);
+      } else if (shape == 8u) {
+        k_conv_ws<Persist32><<<persistent(a, Persist32::ROWS), WS_THREADS, Persist32::SMEM, st>>>(a);
+      } else if (shape == 9u) {
+        k_conv_ws<Persist128><<<persistent(a, Persist128::ROWS), WS_THREADS, Persist128::SMEM, st>>>(a);
       } else {
         k_conv<Wide><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Wide::ROWS)), CONV_THREADS, Wide::SMEM, st>>>(a);
       }

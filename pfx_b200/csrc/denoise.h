@@ -57,7 +57,7 @@ struct Denoiser {
   size_t bins_capacity = 0;
   uint32_t* d_error = nullptr;  // set by a conv kernel whose bounded wait ran out
   uint32_t wait_limit = 1u << 26;  // polls of the conv kernels' bounded mbarrier waits
-  uint32_t conv_shape = 0;         // 0 the per-layer default, 1-6 one shape wherever it fits
+  uint32_t conv_shape = 0;         // 0 the per-layer default, 1-9 one shape wherever it fits
   cudaStream_t stream = nullptr;   // host-buffer calls
   float4* d_images = nullptr;      // host-buffer calls: colour, albedo, normal, output
   size_t images_pixels = 0;

@@ -111,6 +111,7 @@ struct CachePass {
   uint32_t* tslot;          // per path: training slot (low 24 bits) | recorded-vertex mask << 24, ~0 = none
   float4* tvert;            // per slot and recorded vertex: 5 float4 query, throughput, result so far
   float4* records;          // 6 float4 per training record
+  uint8_t* encoded;         // the queries' encoded inputs (cache_x_bytes)
   const uint8_t* cell_ok;   // fallback cells (NRC_CELLS^3)
   float lo[3], inv[3];      // grid bounds
 };
@@ -1616,7 +1617,8 @@ CachePass ensure_cache(pfxt_trace& t, uint32_t pixels) {
     return at;
   };
   size_t o_q = add(80ull * pixels), o_cq = add(4ull * pixels), o_pred = add(16ull * pixels),
-         o_ts = add(4ull * pixels), o_tv = add(112ull * c.tcap * vertices), o_rec = add(96ull * std::max(c.rcap, 1u));
+         o_ts = add(4ull * pixels), o_tv = add(112ull * c.tcap * vertices), o_rec = add(96ull * std::max(c.rcap, 1u)),
+         o_x = add(cache_x_bytes(pixels));
   if (need > t.cache_scratch_bytes) {
     if (t.d_cache_scratch) cudaFree(t.d_cache_scratch);
     t.d_cache_scratch = nullptr;
@@ -1632,6 +1634,7 @@ CachePass ensure_cache(pfxt_trace& t, uint32_t pixels) {
   c.tslot = reinterpret_cast<uint32_t*>(b + o_ts);
   c.tvert = reinterpret_cast<float4*>(b + o_tv);
   c.records = reinterpret_cast<float4*>(b + o_rec);
+  c.encoded = reinterpret_cast<uint8_t*>(b + o_x);
   c.cell_ok = k.d_cell_ok;
   for (int j = 0; j < 3; ++j) {
     c.lo[j] = k.grid.lo[j];
@@ -1853,12 +1856,10 @@ void enqueue_pass(pfxt_trace& t, Pass& P, uint32_t count, bool deferred, uint32_
       if (P.c.enabled && bounce == P.c.query_last) {
         // Every query is written by now, and the later bounces (training and
         // fallback paths) neither read the queries nor write the predictions,
-        // so the inference runs beside them until the accumulation, on half of
-        // every SM's inference slots (measured: 83.7 ms cached pass against
-        // 84.4 on all four and 84.8 run in line).
+        // so the inference runs beside them until the accumulation.
         check(cudaEventRecord(t.fork_ev, st), "inference fork");
         check(cudaStreamWaitEvent(t.side, t.fork_ev, 0), "inference fork");
-        cache_infer_launch(*t.cache, P.c.query, P.w.counters + 5, pixels, P.c.cqueue, P.c.pred, t.side, 2u);
+        cache_infer_launch(*t.cache, P.c.query, P.w.counters + 5, pixels, P.c.cqueue, P.c.pred, P.c.encoded, t.side);
         check(cudaEventRecord(t.join_ev, t.side), "inference join");
         inferred = true;
       }

@@ -139,7 +139,7 @@ def test_a_wait_that_runs_out_fails_the_call_and_the_denoiser_recovers(gpu):
     assert np.array_equal(again.view(np.uint32), good.view(np.uint32))
 
 
-@pytest.mark.parametrize("shape", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("shape", [1, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_every_conv_shape_matches_the_oracle(gpu, shape):
     """Every conv CTA shape (rows per CTA, stages, CTAs per SM), forced on
     the layers whose outputs it fits, gives the oracle's image."""
