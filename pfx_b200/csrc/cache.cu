@@ -76,16 +76,18 @@ __device__ __forceinline__ void store_row(uint8_t* tile, uint32_t r, uint32_t R,
     *reinterpret_cast<uint4*>(tile + ((uint32_t)g * (R >> 3) + (r >> 3)) * 128u + (r & 7u) * 16u) = v;
   }
 }
-// Zeroes x[c] where row r of the 128-row tile `act` is not positive (ReLU').
-__device__ __forceinline__ void relu_mask(const uint8_t* act, uint32_t r, float* x) {
+// Zeroes x[c] where column 16 s + c of row r of the 128-row, 64-column tile
+// `act` is not positive (ReLU'), for c in 0..15.
+__device__ __forceinline__ void relu_mask16(const uint8_t* act, uint32_t r, uint32_t s, float* x) {
 #pragma unroll
-  for (int g = 0; g < 8; ++g) {
-    uint4 v = *reinterpret_cast<const uint4*>(act + ((uint32_t)g * 16u + (r >> 3)) * 128u + (r & 7u) * 16u);
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t g = 2u * s + (uint32_t)h;
+    uint4 v = *reinterpret_cast<const uint4*>(act + (g * 16u + (r >> 3)) * 128u + (r & 7u) * 16u);
     uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      if (!(lo_bf(w[j]) > 0.0f)) x[8 * g + 2 * j] = 0.0f;
-      if (!(hi_bf(w[j]) > 0.0f)) x[8 * g + 2 * j + 1] = 0.0f;
+      if (!(lo_bf(w[j]) > 0.0f)) x[8 * h + 2 * j] = 0.0f;
+      if (!(hi_bf(w[j]) > 0.0f)) x[8 * h + 2 * j + 1] = 0.0f;
     }
   }
 }
@@ -169,40 +171,61 @@ __device__ __forceinline__ void level_features(const CacheGrid& g, const __half2
   }
 }
 
-// The 64 network inputs of one query (5 float4: position + roughness,
-// direction + transmission, normal, diffuse, specular).
-__device__ __forceinline__ void encode(const CacheGrid& g, const __half2* __restrict__ table, const float4* q,
-                                       float x[NRC_IN]) {
-  float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4);
-  float u[3] = {unit_coord(a.x, g.lo[0], g.inv_extent[0]), unit_coord(a.y, g.lo[1], g.inv_extent[1]),
-                unit_coord(a.z, g.lo[2], g.inv_extent[2])};
+// A quarter of one query's 64 network inputs (5 float4: position +
+// roughness, direction + transmission, normal, diffuse, specular): quarter q
+// gathers levels 4q..4q+3 of the hash grid into v[0..7] (inputs 8q..8q+7) and
+// writes inputs 32 + 8q .. 39 + 8q into v[8..15]: one-blob codes of the
+// direction (q 0, 1) and normal (q 1, 2), then roughness, diffuse,
+// specular and transmission (q 3).
+__device__ __forceinline__ void encode_quad(const CacheGrid& g, const __half2* __restrict__ table, const float4* qp,
+                                            uint32_t q, float v[16]) {
+  const float4 a = __ldg(qp);
+  const float u[3] = {unit_coord(a.x, g.lo[0], g.inv_extent[0]), unit_coord(a.y, g.lo[1], g.inv_extent[1]),
+                      unit_coord(a.z, g.lo[2], g.inv_extent[2])};
 #pragma unroll
-  for (uint32_t l = 0; l < NRC_LEVELS; ++l) level_features(g, table, l, u, x[2 * l], x[2 * l + 1]);
-  one_blob(b.x, x + 32);
-  one_blob(b.y, x + 36);
-  one_blob(b.z, x + 40);
-  one_blob(c.x, x + 44);
-  one_blob(c.y, x + 48);
-  one_blob(c.z, x + 52);
-  x[56] = a.w > 0.0f ? (a.w < 1.0f ? a.w : 1.0f) : 0.0f;
-  x[57] = d.x;
-  x[58] = d.y;
-  x[59] = d.z;
-  x[60] = e.x;
-  x[61] = e.y;
-  x[62] = e.z;
-  x[63] = b.w;
+  for (uint32_t j = 0; j < 4; ++j) level_features(g, table, 4u * q + j, u, v[2 * j], v[2 * j + 1]);
+  if (q == 0u) {
+    const float4 b = __ldg(qp + 1);
+    one_blob(b.x, v + 8);
+    one_blob(b.y, v + 12);
+  } else if (q == 1u) {
+    const float4 b = __ldg(qp + 1), c = __ldg(qp + 2);
+    one_blob(b.z, v + 8);
+    one_blob(c.x, v + 12);
+  } else if (q == 2u) {
+    const float4 c = __ldg(qp + 2);
+    one_blob(c.y, v + 8);
+    one_blob(c.z, v + 12);
+  } else {
+    const float4 b = __ldg(qp + 1), d = __ldg(qp + 3), e = __ldg(qp + 4);
+    v[8] = a.w > 0.0f ? (a.w < 1.0f ? a.w : 1.0f) : 0.0f;
+    v[9] = d.x;
+    v[10] = d.y;
+    v[11] = d.z;
+    v[12] = e.x;
+    v[13] = e.y;
+    v[14] = e.z;
+    v[15] = b.w;
+  }
 }
 
-// Gradient of the grid features of one query into the FP32 table gradient.
-__device__ __forceinline__ void scatter_grid(const CacheGrid& g, float* __restrict__ table_g, const float4* q,
-                                             const float dx[32]) {
+// Eight values into row r of column group `group` of an R-row BF16 operand tile.
+__device__ __forceinline__ void store_group(uint8_t* tile, uint32_t r, uint32_t R, uint32_t group, const float* v) {
+  *reinterpret_cast<uint4*>(tile + (group * (R >> 3) + (r >> 3)) * 128u + (r & 7u) * 16u) =
+      make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
+}
+
+// Gradient of grid features 8q..8q+7 of one query (levels 4q..4q+3) into
+// the FP32 table gradient.
+__device__ __forceinline__ void scatter_quad(const CacheGrid& g, float* __restrict__ table_g, const float4* q,
+                                             uint32_t quad, const float dx[8]) {
   float4 a = __ldg(q);
   float u[3] = {unit_coord(a.x, g.lo[0], g.inv_extent[0]), unit_coord(a.y, g.lo[1], g.inv_extent[1]),
                 unit_coord(a.z, g.lo[2], g.inv_extent[2])};
-#pragma unroll 4
-  for (uint32_t l = 0; l < NRC_LEVELS; ++l) {
-    float g0 = dx[2 * l], g1 = dx[2 * l + 1];
+#pragma unroll
+  for (uint32_t j = 0; j < 4; ++j) {
+    const uint32_t l = 4u * quad + j;
+    float g0 = dx[2 * j], g1 = dx[2 * j + 1];
     if (g0 == 0.0f && g1 == 0.0f) continue;
     Corners cn = corners(g, l, u);
     float2* level = reinterpret_cast<float2*>(table_g) + (size_t)l * g.entries;
@@ -285,47 +308,14 @@ __global__ void __launch_bounds__(256)
   if (row >= ((count + NRC_ROWS - 1u) & ~(NRC_ROWS - 1u))) return;
   float v[16];
   if (row < count) {
-    const float4* qp = queries + (size_t)row * 5u;
-    const float4 a = __ldg(qp);
-    const float u[3] = {unit_coord(a.x, g.lo[0], g.inv_extent[0]), unit_coord(a.y, g.lo[1], g.inv_extent[1]),
-                        unit_coord(a.z, g.lo[2], g.inv_extent[2])};
-#pragma unroll
-    for (uint32_t j = 0; j < 4; ++j) level_features(g, table, 4u * q + j, u, v[2 * j], v[2 * j + 1]);
-    // inputs 32 + 8q .. 39 + 8q, as encode() writes them
-    if (q == 0u) {
-      const float4 b = __ldg(qp + 1);
-      one_blob(b.x, v + 8);
-      one_blob(b.y, v + 12);
-    } else if (q == 1u) {
-      const float4 b = __ldg(qp + 1), c = __ldg(qp + 2);
-      one_blob(b.z, v + 8);
-      one_blob(c.x, v + 12);
-    } else if (q == 2u) {
-      const float4 c = __ldg(qp + 2);
-      one_blob(c.y, v + 8);
-      one_blob(c.z, v + 12);
-    } else {
-      const float4 b = __ldg(qp + 1), d = __ldg(qp + 3), e = __ldg(qp + 4);
-      v[8] = a.w > 0.0f ? (a.w < 1.0f ? a.w : 1.0f) : 0.0f;
-      v[9] = d.x;
-      v[10] = d.y;
-      v[11] = d.z;
-      v[12] = e.x;
-      v[13] = e.y;
-      v[14] = e.z;
-      v[15] = b.w;
-    }
+    encode_quad(g, table, queries + (size_t)row * 5u, q, v);
   } else {
 #pragma unroll
     for (int k = 0; k < 16; ++k) v[k] = 0.0f;
   }
   uint8_t* tile = x + (size_t)(row / NRC_ROWS) * X_TILE;
-  const uint32_t r = row % NRC_ROWS;
-  const uint32_t at = (r >> 3) * 128u + (r & 7u) * 16u;
-  *reinterpret_cast<uint4*>(tile + q * 2048u + at) =
-      make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
-  *reinterpret_cast<uint4*>(tile + (4u + q) * 2048u + at) =
-      make_uint4(pack2(v[8], v[9]), pack2(v[10], v[11]), pack2(v[12], v[13]), pack2(v[14], v[15]));
+  store_group(tile, row % NRC_ROWS, NRC_ROWS, q, v);
+  store_group(tile, row % NRC_ROWS, NRC_ROWS, 4u + q, v + 8);
 }
 
 // Shared memory of k_mlp: the weights, two input stages and one hidden
@@ -459,14 +449,22 @@ __global__ void __launch_bounds__(128, 3)
 // Records: 6 float4 (the query's 5, then target rgb + weight).  dY rows are
 // the gradient of mean_rows,channels (y - t)^2 / (y^2 + 0.01) (the
 // denominator held constant), the relative L2 loss of neural radiance caching.
-__global__ void __launch_bounds__(128, 1)
+//
+// Four threads share each row: warp w serves TMEM lane quarter w % 4 (rows
+// 32 (w % 4)..) and slice s = w / 4 of every row.  Slice s gathers and
+// scatters hash-grid levels 4s..4s+3, and moves columns 16s..16s+15 of each
+// 64-wide layer between TMEM and shared memory; slice 0 takes the output
+// layer and the loss.
+constexpr uint32_t TRAIN_THREADS = 512;
+__global__ void __launch_bounds__(TRAIN_THREADS, 1)
     k_train(CacheGrid g, const __half2* __restrict__ table, const uint16_t* __restrict__ weights,
             const float4* __restrict__ records, uint32_t first, uint32_t batch, const uint32_t* __restrict__ ran,
             float* __restrict__ mlp_g, float* __restrict__ table_g, float* __restrict__ loss,
             float* __restrict__ cell_stats, uint32_t* error) {
   if (*ran == 0u) return;
   extern __shared__ __align__(1024) uint8_t smem[];
-  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+  const uint32_t quarter = warp & 3u, sl = warp >> 2, row = 32u * quarter + lane;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + T_CTRL);
   uint32_t* slot = reinterpret_cast<uint32_t*>(smem + T_CTRL + 8);
   const uint32_t a_dy = umma::smem_addr(smem + T_DY), a_dh2 = umma::smem_addr(smem + T_DH2),
@@ -486,92 +484,96 @@ __global__ void __launch_bounds__(128, 1)
   if (warp == 0) umma::tmem_alloc(slot, 512);
   umma::fence_async_smem();
   sync_tc();
-  const uint32_t tbase = *slot;
-  const uint32_t T0 = tbase, T1 = tbase + 64, T2 = tbase + 128, DW1 = tbase + 192, DW2 = tbase + 256,
-                 DW3 = tbase + 320;
+  const uint32_t tbase = *slot, tlane = tbase + ((32u * quarter) << 16);
+  const uint32_t T0 = 0, T1 = 64, T2 = 128, DW1 = tbase + 192, DW2 = tbase + 256, DW3 = tbase + 320;
   const float scale = 1.0f / (3.0f * (float)batch);
   const uint32_t tiles = batch / NRC_ROWS;
   uint32_t phase = 0, done = 0;
   bool failed = false;
   float loss_sum = 0.0f;
+  // the MMAs of one step, then the bounded wait for them (false: it ran out)
+  auto wait_mma = [&]() {
+    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
+    phase ^= 1u;
+    failed = __syncthreads_or(failed);
+    if (!failed) umma::fence_after();
+    return !failed;
+  };
+  float v[16];
   for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++done) {
-    const float4* rec = records + ((size_t)first + (size_t)tile * NRC_ROWS + tid) * 6u;
-    float x[64];
-    encode(g, table, rec, x);
-    store_row<64>(smem + T_X, tid, 128, x);
+    const float4* rec = records + ((size_t)first + (size_t)tile * NRC_ROWS + row) * 6u;
+    encode_quad(g, table, rec, sl, v);
+    store_group(smem + T_X, row, 128, sl, v);
+    store_group(smem + T_X, row, 128, 4u + sl, v + 8);
     umma::fence_async_smem();
     sync_tc();
     // forward
     if (tid == 0) {
 #pragma unroll
       for (uint32_t s = 0; s < 4; ++s)
-        umma::mma(T0, umma::desc_k(a_x, 128, s), umma::desc_k(a_w + W_1, 64, s), ID_F64, s);
+        umma::mma(tbase + T0, umma::desc_k(a_x, 128, s), umma::desc_k(a_w + W_1, 64, s), ID_F64, s);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
-    phase ^= 1u;
-    if (__syncthreads_or(failed)) { failed = true; break; }
-    umma::fence_after();
-    ld64(tbase, warp, 0, x);
+    if (!wait_mma()) break;
+    umma::ld16(tlane + T0 + 16u * sl, v);
 #pragma unroll
-    for (int k = 0; k < 64; ++k) x[k] = x[k] > 0.0f ? x[k] : 0.0f;
-    store_row<64>(smem + T_H1, tid, 128, x);
+    for (int k = 0; k < 16; ++k) v[k] = v[k] > 0.0f ? v[k] : 0.0f;
+    store_group(smem + T_H1, row, 128, 2u * sl, v);
+    store_group(smem + T_H1, row, 128, 2u * sl + 1u, v + 8);
     umma::fence_async_smem();
     sync_tc();
     if (tid == 0) {
 #pragma unroll
       for (uint32_t s = 0; s < 4; ++s)
-        umma::mma(T1, umma::desc_k(a_h1, 128, s), umma::desc_k(a_w + W_2, 64, s), ID_F64, s);
+        umma::mma(tbase + T1, umma::desc_k(a_h1, 128, s), umma::desc_k(a_w + W_2, 64, s), ID_F64, s);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
-    phase ^= 1u;
-    if (__syncthreads_or(failed)) { failed = true; break; }
-    umma::fence_after();
-    ld64(tbase, warp, 64, x);
+    if (!wait_mma()) break;
+    umma::ld16(tlane + T1 + 16u * sl, v);
 #pragma unroll
-    for (int k = 0; k < 64; ++k) x[k] = x[k] > 0.0f ? x[k] : 0.0f;
-    store_row<64>(smem + T_H2, tid, 128, x);
+    for (int k = 0; k < 16; ++k) v[k] = v[k] > 0.0f ? v[k] : 0.0f;
+    store_group(smem + T_H2, row, 128, 2u * sl, v);
+    store_group(smem + T_H2, row, 128, 2u * sl + 1u, v + 8);
     umma::fence_async_smem();
     sync_tc();
     if (tid == 0) {
 #pragma unroll
       for (uint32_t s = 0; s < 4; ++s)
-        umma::mma(T2, umma::desc_k(a_h2, 128, s), umma::desc_k(a_w + W_3, 16, s), ID_F16, s);
+        umma::mma(tbase + T2, umma::desc_k(a_h2, 128, s), umma::desc_k(a_w + W_3, 16, s), ID_F16, s);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
-    phase ^= 1u;
-    if (__syncthreads_or(failed)) { failed = true; break; }
-    umma::fence_after();
-    float y[16];
-    umma::ld16(umma::taddr(tbase, 32u * warp, 128), y);
-    // loss and dY
-    float4 t = __ldg(rec + 5);
-    float target[3] = {t.x, t.y, t.z};
-    float dy[16];
+    if (!wait_mma()) break;
+    if (sl == 0u) {
+      // loss and dY
+      float y[16];
+      umma::ld16(tlane + T2, y);
+      float4 t = __ldg(rec + 5);
+      float target[3] = {t.x, t.y, t.z};
+      float dy[16];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) dy[k] = 0.0f;
+      for (int k = 0; k < 16; ++k) dy[k] = 0.0f;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      float d = y[c] - target[c];
-      float den = y[c] * y[c] + 0.01f;
-      loss_sum = loss_sum + d * d / den;
-      dy[c] = 2.0f * d / den * scale;
+      for (int c = 0; c < 3; ++c) {
+        float d = y[c] - target[c];
+        float den = y[c] * y[c] + 0.01f;
+        loss_sum = loss_sum + d * d / den;
+        dy[c] = 2.0f * d / den * scale;
+      }
+      if (cell_stats) {
+        float4 p = __ldg(rec);
+        uint32_t cx = min((uint32_t)(unit_coord(p.x, g.lo[0], g.inv_extent[0]) * (float)NRC_CELLS), NRC_CELLS - 1u);
+        uint32_t cy = min((uint32_t)(unit_coord(p.y, g.lo[1], g.inv_extent[1]) * (float)NRC_CELLS), NRC_CELLS - 1u);
+        uint32_t cz = min((uint32_t)(unit_coord(p.z, g.lo[2], g.inv_extent[2]) * (float)NRC_CELLS), NRC_CELLS - 1u);
+        float* cs = cell_stats + 4u * ((cz * NRC_CELLS + cy) * NRC_CELLS + cx);
+        float py = 0.2126f * fmaxf(y[0], 0.0f) + 0.7152f * fmaxf(y[1], 0.0f) + 0.0722f * fmaxf(y[2], 0.0f);
+        float ty = 0.2126f * target[0] + 0.7152f * target[1] + 0.0722f * target[2];
+        atomicAdd(cs + 0, py - ty);
+        atomicAdd(cs + 1, ty);
+        atomicAdd(cs + 2, 1.0f);
+      }
+      store_group(smem + T_DY, row, 128, 0u, dy);
+      store_group(smem + T_DY, row, 128, 1u, dy + 8);
     }
-    if (cell_stats) {
-      float4 p = __ldg(rec);
-      uint32_t cx = min((uint32_t)(unit_coord(p.x, g.lo[0], g.inv_extent[0]) * (float)NRC_CELLS), NRC_CELLS - 1u);
-      uint32_t cy = min((uint32_t)(unit_coord(p.y, g.lo[1], g.inv_extent[1]) * (float)NRC_CELLS), NRC_CELLS - 1u);
-      uint32_t cz = min((uint32_t)(unit_coord(p.z, g.lo[2], g.inv_extent[2]) * (float)NRC_CELLS), NRC_CELLS - 1u);
-      float* cs = cell_stats + 4u * ((cz * NRC_CELLS + cy) * NRC_CELLS + cx);
-      float py = 0.2126f * fmaxf(y[0], 0.0f) + 0.7152f * fmaxf(y[1], 0.0f) + 0.0722f * fmaxf(y[2], 0.0f);
-      float ty = 0.2126f * target[0] + 0.7152f * target[1] + 0.0722f * target[2];
-      atomicAdd(cs + 0, py - ty);
-      atomicAdd(cs + 1, ty);
-      atomicAdd(cs + 2, 1.0f);
-    }
-    store_row<16>(smem + T_DY, tid, 128, dy);
     umma::fence_async_smem();
     sync_tc();
     // dW3 += dY^T H2 ; dH2 = dY W3
@@ -579,16 +581,14 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
       for (uint32_t s = 0; s < 8; ++s)
         umma::mma(DW3, umma::desc_mn(a_dy, 128, s), umma::desc_mn(a_h2, 128, s), ID_DW, (done | s) ? 1u : 0u);
-      umma::mma(T0, umma::desc_k(a_dy, 128, 0), umma::desc_mn(a_w + W_3, 16, 0), ID_B64, 0u);
+      umma::mma(tbase + T0, umma::desc_k(a_dy, 128, 0), umma::desc_mn(a_w + W_3, 16, 0), ID_B64, 0u);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
-    phase ^= 1u;
-    if (__syncthreads_or(failed)) { failed = true; break; }
-    umma::fence_after();
-    ld64(tbase, warp, 0, x);
-    relu_mask(smem + T_H2, tid, x);
-    store_row<64>(smem + T_DH2, tid, 128, x);
+    if (!wait_mma()) break;
+    umma::ld16(tlane + T0 + 16u * sl, v);
+    relu_mask16(smem + T_H2, row, sl, v);
+    store_group(smem + T_DH2, row, 128, 2u * sl, v);
+    store_group(smem + T_DH2, row, 128, 2u * sl + 1u, v + 8);
     umma::fence_async_smem();
     sync_tc();
     // dW2 += dH2^T H1 ; dH1 = dH2 W2
@@ -598,59 +598,46 @@ __global__ void __launch_bounds__(128, 1)
         umma::mma(DW2, umma::desc_mn(a_dh2, 128, s), umma::desc_mn(a_h1, 128, s), ID_DW, (done | s) ? 1u : 0u);
 #pragma unroll
       for (uint32_t s = 0; s < 4; ++s)
-        umma::mma(T1, umma::desc_k(a_dh2, 128, s), umma::desc_mn(a_w + W_2, 64, s), ID_B64, s);
+        umma::mma(tbase + T1, umma::desc_k(a_dh2, 128, s), umma::desc_mn(a_w + W_2, 64, s), ID_B64, s);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
-    phase ^= 1u;
-    if (__syncthreads_or(failed)) { failed = true; break; }
-    umma::fence_after();
-    ld64(tbase, warp, 64, x);
-    relu_mask(smem + T_H1, tid, x);
-    store_row<64>(smem + T_DH1, tid, 128, x);
+    if (!wait_mma()) break;
+    umma::ld16(tlane + T1 + 16u * sl, v);
+    relu_mask16(smem + T_H1, row, sl, v);
+    store_group(smem + T_DH1, row, 128, 2u * sl, v);
+    store_group(smem + T_DH1, row, 128, 2u * sl + 1u, v + 8);
     umma::fence_async_smem();
     sync_tc();
-    // dW1 += dH1^T X ; dX = dH1 W1 (grid features only)
+    // dW1 += dH1^T X ; dX = dH1 W1 (grid features only: 32 columns)
     if (tid == 0) {
 #pragma unroll
       for (uint32_t s = 0; s < 8; ++s)
         umma::mma(DW1, umma::desc_mn(a_dh1, 128, s), umma::desc_mn(a_x, 128, s), ID_DW, (done | s) ? 1u : 0u);
 #pragma unroll
       for (uint32_t s = 0; s < 4; ++s)
-        umma::mma(T2, umma::desc_k(a_dh1, 128, s), umma::desc_mn(a_w + W_1, 64, s), ID_B32, s);
+        umma::mma(tbase + T2, umma::desc_k(a_dh1, 128, s), umma::desc_mn(a_w + W_1, 64, s), ID_B32, s);
       umma::commit(mb);
     }
-    failed = !umma::mbar_wait(mb, phase, g.wait_limit);
-    phase ^= 1u;
-    if (__syncthreads_or(failed)) { failed = true; break; }
-    umma::fence_after();
-    float dx[32];
-    {
-      float v[16];
-      umma::ld16(umma::taddr(tbase, 32u * warp, 128), v);
-#pragma unroll
-      for (int k = 0; k < 16; ++k) dx[k] = v[k];
-      umma::ld16(umma::taddr(tbase, 32u * warp, 144), v);
-#pragma unroll
-      for (int k = 0; k < 16; ++k) dx[16 + k] = v[k];
-    }
-    scatter_grid(g, table_g, rec, dx);
+    if (!wait_mma()) break;
+    // this slice's levels: dX columns 8 sl .. 8 sl + 7 (the load's other 8 columns are not used)
+    umma::ld16(tlane + T2 + 8u * sl, v);
+    scatter_quad(g, table_g, rec, sl, v);
     sync_tc();
   }
   // loss: warp sums, one atomic per warp
   for (int o = 16; o > 0; o >>= 1) loss_sum += __shfl_xor_sync(0xffffffffu, loss_sum, o);
-  if ((tid & 31u) == 0u && loss_sum != 0.0f) atomicAdd(loss, loss_sum);
-  if (!failed && done > 0u && warp < 2u) {
-    // weight gradients: TMEM lanes 0..63 hold the rows of dW1 and dW2 (dW3: lanes 0..2)
-    const uint32_t m = tid;  // output feature
-    float v[64];
-    ld64(tbase, warp, 192, v);
-    for (int k = 0; k < 64; ++k) atomicAdd(mlp_g + NRC_W1 + m * 64u + k, v[k]);
-    ld64(tbase, warp, 256, v);
-    for (int k = 0; k < 64; ++k) atomicAdd(mlp_g + NRC_W2 + m * 64u + k, v[k]);
-    ld64(tbase, warp, 320, v);
+  if (lane == 0u && loss_sum != 0.0f) atomicAdd(loss, loss_sum);
+  if (!failed && done > 0u && quarter < 2u) {
+    // weight gradients: TMEM lanes 0..63 hold the rows of dW1 and dW2 (dW3: lanes 0..2); slice sl adds
+    // columns 16 sl .. 16 sl + 15 of each
+    const uint32_t m = row;  // output feature
+    umma::ld16(tlane + 192u + 16u * sl, v);
+    for (int k = 0; k < 16; ++k) atomicAdd(mlp_g + NRC_W1 + m * 64u + 16u * sl + k, v[k]);
+    umma::ld16(tlane + 256u + 16u * sl, v);
+    for (int k = 0; k < 16; ++k) atomicAdd(mlp_g + NRC_W2 + m * 64u + 16u * sl + k, v[k]);
+    umma::ld16(tlane + 320u + 16u * sl, v);
     if (m < 3u)
-      for (int k = 0; k < 64; ++k) atomicAdd(mlp_g + NRC_W3 + m * 64u + k, v[k]);
+      for (int k = 0; k < 16; ++k) atomicAdd(mlp_g + NRC_W3 + m * 64u + 16u * sl + k, v[k]);
   }
   finish(failed, mb, phase, error, tbase, 512);
 }
@@ -912,7 +899,7 @@ void cache_train_launch(pfxt_cache& c, const float4* records, const uint32_t* co
   k_step<<<1, 32, 0, stream>>>(count_dev, count, first + batch, c.d_step, beta_pow(c), c.s.beta1, c.s.beta2,
                                adam ? 1u : 0u, c.d_loss);
   uint32_t grid = std::min<uint32_t>(batch / NRC_ROWS, (uint32_t)sm_count());
-  k_train<<<grid, 128, T_SMEM, stream>>>(c.grid, c.d_table16, c.d_weights, records, first, batch, c.d_step + 1,
+  k_train<<<grid, TRAIN_THREADS, T_SMEM, stream>>>(c.grid, c.d_table16, c.d_weights, records, first, batch, c.d_step + 1,
                                          c.d_mlp_g, c.d_table_g, c.d_loss, adam ? c.d_cell_stats : nullptr,
                                          c.d_error);
   check(cudaGetLastError(), "cache training");
