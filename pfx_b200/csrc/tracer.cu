@@ -1142,7 +1142,9 @@ constexpr int SLOT_SUN = 0, SLOT_SKY = 1, SLOT_EMITTER = 2, SLOT_LOOPED = 3, SLO
 #endif
 // Whether the descent kernel runs the light-tree functions inline or through their out-of-line copies.
 // Plain 4K pass: out of line at 12 blocks per SM 93.1 ms, at 8 blocks 92.5; inline at 12, 10 and 8
-// blocks 102.8, 104.8 and 108.1 ms (more code, fewer lanes per instruction).
+// blocks 102.8, 104.8 and 108.1 ms (more code, fewer lanes per instruction).  Later, with the one-light
+// leaves reusing the descent's importance: 8 blocks (64 registers) 91.5 ms, 6 blocks (72 registers, no
+// spills) 91.7, 4 blocks 91.8.
 #ifndef PICK_INLINE
 #define PICK_INLINE false
 #endif
