@@ -147,6 +147,9 @@ struct pfxt_trace {
   // query bounce and joined before the accumulation, beside the later bounces.
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  // the next bounce's extend, beside the current bounce's connect
+  cudaStream_t ahead = nullptr;
+  cudaEvent_t ahead_fork = nullptr, ahead_join = nullptr;
   std::vector<pfxt::GraphEntry> graphs;
   bool use_graphs = true;
   uint32_t graph_captures = 0;  // passes captured so far

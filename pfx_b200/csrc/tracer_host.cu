@@ -253,6 +253,14 @@ void trace_release(pfxt_trace& t) {
   if (t.join_ev) cudaEventDestroy(t.join_ev);
   t.side = nullptr;
   t.fork_ev = t.join_ev = nullptr;
+  if (t.ahead) {
+    cudaStreamSynchronize(t.ahead);
+    cudaStreamDestroy(t.ahead);
+  }
+  if (t.ahead_fork) cudaEventDestroy(t.ahead_fork);
+  if (t.ahead_join) cudaEventDestroy(t.ahead_join);
+  t.ahead = nullptr;
+  t.ahead_fork = t.ahead_join = nullptr;
   if (t.stream) cudaStreamDestroy(t.stream);
   t.stream = nullptr;
 }
