@@ -200,19 +200,31 @@ constexpr uint32_t A_PLANE = PATCH_W * 16u;          // bytes of one (row, group
 //  * k_conv_ws, Persist128: 2 rows, up to 128 channels, three stages: 8.49 ms.
 // Layer by layer the persistent shapes are the fastest: Persist32 up to 32
 // channels, Persist64 up to 64, Persist128 above (the default).
-template <uint32_t ROWS_, uint32_t NMAX_, uint32_t STAGES_, uint32_t CTAS_>
+template <uint32_t ROWS_, uint32_t NMAX_, uint32_t STAGES_, uint32_t CTAS_, bool EXPAND_ = false>
 struct ConvShape {
   static constexpr uint32_t ROWS = ROWS_, N_MAX = NMAX_, STAGES = STAGES_, CTAS = CTAS_;
+  // EXPAND (persistent kernel only): a first source stored at half size is
+  // copied into a raw buffer of ROWS / 2 + 2 rows x 66 pixels and widened 2x2
+  // into the stage by four more warps.
+  static constexpr bool EXPAND = EXPAND_;
+  static constexpr uint32_t RAW_ROWS = ROWS / 2u + 2u, RAW_W = CONV_PIX / 2u + 2u;
+  static constexpr uint32_t RAW_BOX = RAW_ROWS * 2u * RAW_W * 16u;   // one half (hi or lo) as copied
+  static constexpr uint32_t RAW_PLANE = (RAW_BOX + 127u) / 128u * 128u;  // its place in shared memory
+  static constexpr uint32_t RAW = EXPAND ? 2u * RAW_PLANE : 0u;
   static constexpr uint32_t TMEM_COLS = ROWS * N_MAX;            // a power of two of at least 32
   static constexpr uint32_t PATCH_ROWS = ROWS + 2u;              // staged input rows
   static constexpr uint32_t A_BYTES = PATCH_ROWS * 2u * A_PLANE;   // one chunk of one half (hi or lo)
   static constexpr uint32_t W_MAX = 9u * 2u * N_MAX * 16u;         // one chunk of weights at N_MAX
   static constexpr uint32_t STAGE = 2u * A_BYTES + W_MAX;
-  static constexpr uint32_t CTRL = STAGES * STAGE;                 // mbarriers, TMEM slot, flags
-  static constexpr uint32_t SMEM = CTRL + 128u;
+  static constexpr uint32_t RAW_AT = STAGES * STAGE;               // the raw buffer
+  static constexpr uint32_t CTRL = RAW_AT + RAW;                   // mbarriers, TMEM slot, flags
+  static constexpr uint32_t SMEM = CTRL + 256u;
   static_assert(SMEM * CTAS <= 228u * 1024u - CTAS * 1024u, "shared memory per SM");
   static_assert(TMEM_COLS * CTAS <= 512u && (TMEM_COLS & (TMEM_COLS - 1u)) == 0u, "TMEM per SM");
   static_assert(STAGES >= 1u && STAGES <= 4u, "one to four stages");
+  // a tensor copy's shared-memory destination is 128-byte aligned
+  static_assert(STAGE % 128u == 0u && A_BYTES % 128u == 0u && RAW_AT % 128u == 0u && RAW_PLANE % 128u == 0u,
+                "copy destinations");
 };
 using Wide = ConvShape<4, 128, 2, 1>;
 using Tall = ConvShape<8, 64, 2, 1>;
@@ -221,9 +233,9 @@ using Paired = ConvShape<4, 64, 1, 2>;
 using Tall2 = ConvShape<8, 32, 1, 2>;
 using Wide2 = ConvShape<2, 128, 1, 2>;
 // the persistent kernel's shapes (two accumulators: 2 x ROWS x N_MAX TMEM columns)
-using Persist64 = ConvShape<4, 64, 3, 1>;
+using Persist64 = ConvShape<4, 64, 3, 1, true>;
 using Persist32 = ConvShape<8, 32, 2, 1>;
-using Persist128 = ConvShape<2, 128, 3, 1>;
+using Persist128 = ConvShape<2, 128, 3, 1, true>;
 constexpr uint32_t ERR_CONV_WAIT = 1u, ERR_CONV_DRAIN = 2u;
 // Polls of the waits that drain a CTA's own work in flight (its MMAs and
 // copies) before it frees its TMEM and leaves, whatever the main loop's
@@ -240,7 +252,7 @@ __host__ __device__ constexpr uint32_t idesc_f16(uint32_t M, uint32_t N) {
 // are the operand layout of the convolutions (16 bytes = 8 channels of one
 // pixel, pixels contiguous), so a chunk's rows reach shared memory as they are.
 struct ConvArgs {
-  CUtensorMap a0_hi, a0_lo;   // the first source (at this layer's level; an upsampled source is stored so)
+  CUtensorMap a0_hi, a0_lo;   // the first source (at this layer's level, or at half of it when half0)
   CUtensorMap a1_hi, a1_lo;   // the skip source (c1 = 0: none)
   const uint16_t* weights;    // conv_chunks() layout
   const float* bias;          // n
@@ -248,6 +260,8 @@ struct ConvArgs {
   uint16_t* dst_lo;
   uint32_t H, W, c0, c1, n, pool;
   uint32_t up;                // the output is stored at twice its size (its consumer upsamples it)
+  uint32_t half0;             // the first source is stored at half this layer's size: the CTA widens it
+                              // (k_conv_ws with an EXPAND shape; its maps' boxes are RAW_ROWS x RAW_W)
   uint32_t* error;
   uint32_t wait_limit;        // polls of a bounded mbarrier wait
 };
@@ -448,12 +462,23 @@ __global__ void __launch_bounds__(CONV_THREADS, S::CTAS) k_conv(const __grid_con
 // (tiles alternate) and commits it to the accumulator's `full` barrier; warps
 // 2-5 (TMEM lane quarters 2, 3, 0, 1) run the epilogue of one accumulator while
 // the MMAs of the next tile fill the other, and free it on its `empty`
-// barrier (one arrival per warp).  Waits are bounded as in k_conv.
-constexpr uint32_t WS_THREADS = 192;
+// barrier (one arrival per warp).  With an EXPAND shape and a first source
+// stored at half size (a.half0), that source's chunks are copied into a raw
+// buffer of RAW_ROWS x RAW_W pixels, and warps 6-9 widen it 2x2 into the
+// stage (patch pixel p of row r reads raw pixel floor((x0 - 1 + p) / 2) -
+// floor((x0 - 1) / 2) of raw row floor((y0 - 1 + r) / 2) - floor((y0 - 1) / 2)),
+// then release the raw buffer (`raw empty`) and tell the MMA lane (the
+// stage's `widened` barrier).  The stage's own `full` barrier then counts the
+// weights alone.  Waits are bounded as in k_conv.
 template <class S>
-__global__ void __launch_bounds__(WS_THREADS, 1) k_conv_ws(const __grid_constant__ ConvArgs a) {
+constexpr uint32_t ws_threads() {
+  return S::EXPAND ? 320u : 192u;
+}
+template <class S>
+__global__ void __launch_bounds__(ws_threads<S>(), 1) k_conv_ws(const __grid_constant__ ConvArgs a) {
   constexpr uint32_t STAGE = S::STAGE, A_BYTES = S::A_BYTES, CTRL = S::CTRL, N_MAX = S::N_MAX, ROWS = S::ROWS;
   constexpr uint32_t NS = S::STAGES, ACC = ROWS * N_MAX, TMEM_COLS = 2u * ACC;
+  constexpr uint32_t RAW_PLANE = S::RAW_PLANE, RAW_W = S::RAW_W;
   static_assert(TMEM_COLS <= 512u, "two accumulators in the TMEM of one SM");
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
@@ -462,18 +487,25 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_conv_ws(const __grid_constant
   const uint32_t accf0 = base + CTRL + 64u, acce0 = base + CTRL + 80u;  // two each
   uint32_t* slot = reinterpret_cast<uint32_t*>(smem + CTRL + 96u);
   volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + CTRL + 100u);
-  uint32_t* counts = reinterpret_cast<uint32_t*>(smem + CTRL + 104u);  // [0] chunks loaded, [1] chunks committed
+  // [0] chunks loaded, [1] chunks committed, [2] raw copies issued, [3] raw copies widened
+  uint32_t* counts = reinterpret_cast<uint32_t*>(smem + CTRL + 104u);
+  const uint32_t wide0 = base + CTRL + 128u;  // NS barriers: the stage's widened source
+  const uint32_t raw_full = base + CTRL + 160u, raw_empty = base + CTRL + 168u;
+  const bool half0 = S::EXPAND && a.half0 != 0u;
   if (tid == 0) {
     for (uint32_t s = 0; s < NS; ++s) {
       umma::mbar_init(full0 + 8u * s, 1);
       umma::mbar_init(empty0 + 8u * s, 1);
+      umma::mbar_init(wide0 + 8u * s, 4);
     }
     for (uint32_t b = 0; b < 2u; ++b) {
       umma::mbar_init(accf0 + 8u * b, 1);
       umma::mbar_init(acce0 + 8u * b, 4);
     }
+    umma::mbar_init(raw_full, 1);
+    umma::mbar_init(raw_empty, 4);
     *abort_flag = 0u;
-    counts[0] = counts[1] = 0u;
+    counts[0] = counts[1] = counts[2] = counts[3] = 0u;
   }
   if (warp == 0) umma::tmem_alloc(slot, TMEM_COLS);
   umma::fence_before();
@@ -484,7 +516,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_conv_ws(const __grid_constant
   const uint32_t chunks = (a.c0 + a.c1) >> 4, chunks0 = a.c0 >> 4;
   const uint32_t wbytes = 9u * 2u * a.n * 16u;
   if (tid == 0) {  // the copies
-    uint32_t c = 0;
+    uint32_t c = 0, u = 0;  // chunks, raw copies
     for (uint32_t t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x) {
       const int x0 = (int)((t % gx) * CONV_PIX), y0 = (int)((t / gx) * ROWS);
       for (uint32_t k = 0; k < chunks; ++k, ++c) {
@@ -492,11 +524,23 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_conv_ws(const __grid_constant
         if (c >= NS && !umma::mbar_wait(empty0 + 8u * s, ((c - NS) / NS) & 1u, a.wait_limit)) *abort_flag = 1u;
         if (*abort_flag) break;
         const uint32_t st = base + s * STAGE, full = full0 + 8u * s;
-        umma::mbar_expect_tx(full, 2u * A_BYTES + wbytes);
         const bool first = k < chunks0;
         const int g = (int)(2u * (first ? k : k - chunks0));
-        umma::tensor_load_4d(st, first ? &a.a0_hi : &a.a1_hi, 0, x0 - 1, g, y0 - 1, full);
-        umma::tensor_load_4d(st + A_BYTES, first ? &a.a0_lo : &a.a1_lo, 0, x0 - 1, g, y0 - 1, full);
+        if (half0 && first) {
+          // the raw buffer is free once the widening warps are done with the previous copy
+          if (u > 0u && !umma::mbar_wait(raw_empty, (u - 1u) & 1u, a.wait_limit)) *abort_flag = 1u;
+          if (*abort_flag) break;
+          umma::mbar_expect_tx(full, wbytes);
+          umma::mbar_expect_tx(raw_full, 2u * S::RAW_BOX);
+          const uint32_t raw = base + S::RAW_AT;
+          umma::tensor_load_4d(raw, &a.a0_hi, 0, (x0 >> 1) - 1, g, (y0 >> 1) - 1, raw_full);
+          umma::tensor_load_4d(raw + RAW_PLANE, &a.a0_lo, 0, (x0 >> 1) - 1, g, (y0 >> 1) - 1, raw_full);
+          counts[2] = ++u;
+        } else {
+          umma::mbar_expect_tx(full, 2u * A_BYTES + wbytes);
+          umma::tensor_load_4d(st, first ? &a.a0_hi : &a.a1_hi, 0, x0 - 1, g, y0 - 1, full);
+          umma::tensor_load_4d(st + A_BYTES, first ? &a.a0_lo : &a.a1_lo, 0, x0 - 1, g, y0 - 1, full);
+        }
         umma::bulk_load(st + 2u * A_BYTES, a.weights + (size_t)k * (wbytes / 2u), wbytes, full);
         counts[0] = c + 1u;
       }
@@ -504,7 +548,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_conv_ws(const __grid_constant
   } else if (tid == 32) {  // the MMAs
     const uint32_t id = idesc_f16(128, a.n);
     const uint32_t w_step = (2u * a.n * 16u) >> 4;
-    uint32_t c = 0, i = 0;
+    uint32_t c = 0, i = 0, wph = 0;  // wph bit s: the parity of stage s's next widening
     for (uint32_t t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x, ++i) {
       const uint32_t b = i & 1u, acc = tmem + b * ACC;
       if (i >= 2u && !umma::mbar_wait(acce0 + 8u * b, ((i - 2u) >> 1) & 1u, a.wait_limit)) *abort_flag = 1u;
@@ -513,6 +557,10 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_conv_ws(const __grid_constant
       for (uint32_t k = 0; k < chunks; ++k, ++c) {
         const uint32_t s = c % NS;
         if (!umma::mbar_wait(full0 + 8u * s, (c / NS) & 1u, a.wait_limit)) *abort_flag = 1u;
+        if (half0 && k < chunks0 && !*abort_flag) {
+          if (!umma::mbar_wait(wide0 + 8u * s, (wph >> s) & 1u, a.wait_limit)) *abort_flag = 1u;
+          wph ^= 1u << s;
+        }
         if (*abort_flag) break;
         umma::fence_after();
         const uint64_t hi_desc = umma::desc(base + s * STAGE, A_PLANE, 128u);
@@ -535,7 +583,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_conv_ws(const __grid_constant
       if (*abort_flag) break;
       umma::commit(accf0 + 8u * b);
     }
-  } else if (warp >= 2u) {  // the epilogue
+  } else if (warp >= 2u && warp < 6u) {  // the epilogue
     const uint32_t quarter = warp & 3u;
     uint32_t i = 0;
     for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++i) {
@@ -551,17 +599,56 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_conv_ws(const __grid_constant
       __syncwarp();
       if (lane == 0) umma::mbar_arrive(acce0 + 8u * b);
     }
+  } else if (S::EXPAND && warp >= 6u && half0) {  // the widening of a half-size first source
+    constexpr uint32_t ITEMS = 2u * S::PATCH_ROWS * 2u * PATCH_W;  // planes x rows x groups x pixels
+    const uint32_t e = tid - 192u;
+    const uint8_t* raw = smem + S::RAW_AT;
+    uint32_t c = 0, u = 0;
+    bool stop = false;
+    for (uint32_t t = blockIdx.x; t < tiles && !stop; t += gridDim.x) {
+      const int x0 = (int)((t % gx) * CONV_PIX), y0 = (int)((t / gx) * ROWS);
+      const int xl = (x0 - 1) >> 1, yl = (y0 - 1) >> 1;  // the raw buffer's first pixel and row
+      for (uint32_t k = 0; k < chunks; ++k, ++c) {
+        if (k >= chunks0) continue;
+        const uint32_t s = c % NS;
+        const bool ok = umma::mbar_wait(raw_full, u & 1u, a.wait_limit);
+        if (__any_sync(0xffffffffu, !ok || *abort_flag)) {
+          *abort_flag = 1u;
+          stop = true;
+          break;
+        }
+        uint8_t* st = smem + s * STAGE;
+        for (uint32_t item = e; item < ITEMS; item += 128u) {
+          const uint32_t p = item % PATCH_W, rest = item / PATCH_W;  // rest = (plane x rows + r) x 2 + group
+          const uint32_t grp = rest & 1u, r = (rest >> 1) % S::PATCH_ROWS, plane = (rest >> 1) / S::PATCH_ROWS;
+          const uint32_t rl = (uint32_t)(((y0 - 1 + (int)r) >> 1) - yl), pl = (uint32_t)(((x0 - 1 + (int)p) >> 1) - xl);
+          const uint4 v = *reinterpret_cast<const uint4*>(raw + plane * RAW_PLANE + ((rl * 2u + grp) * RAW_W + pl) * 16u);
+          *reinterpret_cast<uint4*>(st + plane * A_BYTES + (r * 2u + grp) * A_PLANE + p * 16u) = v;
+        }
+        umma::fence_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          umma::mbar_arrive(raw_empty);
+          umma::mbar_arrive(wide0 + 8u * s);
+        }
+        ++u;
+        if (e == 0u) counts[3] = u;
+      }
+    }
   }
   __syncthreads();
-  const uint32_t loads = counts[0], issued = counts[1];
+  const uint32_t loads = counts[0], issued = counts[1], raws = counts[2], widened = counts[3];
   const bool late = *abort_flag != 0u;
   // every MMA issued is done when the last chunk's commit completes; copies
-  // whose MMAs were never issued land before the CTA leaves
+  // whose MMAs were never issued land before the CTA leaves (a widened
+  // chunk's `full` barrier counts its weights alone), and so does a raw copy
+  // that was not widened
   bool drained = true;
   if (issued > 0)
     drained = umma::mbar_wait(empty0 + 8u * ((issued - 1u) % NS), ((issued - 1u) / NS) & 1u, DRAIN_LIMIT);
   for (uint32_t k = issued; k < loads; ++k)
     drained = umma::mbar_wait(full0 + 8u * (k % NS), (k / NS) & 1u, DRAIN_LIMIT) && drained;
+  if (raws > widened) drained = umma::mbar_wait(raw_full, (raws - 1u) & 1u, DRAIN_LIMIT) && drained;
   drained = __syncthreads_and(drained);
   if ((late || !drained) && tid == 0)
     atomicOr(a.error, (late ? ERR_CONV_WAIT : 0u) | (drained ? 0u : ERR_CONV_DRAIN));
@@ -890,11 +977,13 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
 
 // The tensor map of one plane of a U-Net tensor ([H][C/8][W][8] halves) for
 // boxes of 8 halves x 130 pixels x 2 groups x `rows` rows.
-CUtensorMap plane_map(const uint16_t* plane, uint32_t H, uint32_t W, uint32_t C, uint32_t rows) {
+CUtensorMap plane_map(const uint16_t* plane, uint32_t H, uint32_t W, uint32_t C, uint32_t rows, bool half = false) {
   CUtensorMap m;
   const cuuint64_t dims[4] = {8u, W, C / 8u, H};
   const cuuint64_t strides[3] = {16u, (cuuint64_t)W * 16u, (cuuint64_t)(C / 8u) * W * 16u};
-  const cuuint32_t box[4] = {8u, PATCH_W, 2u, rows + 2u}, elem[4] = {1u, 1u, 1u, 1u};
+  // a half-size source is read as the raw box that k_conv_ws widens: RAW_W pixels, rows / 2 + 2 rows
+  const cuuint32_t box[4] = {8u, half ? CONV_PIX / 2u + 2u : PATCH_W, 2u, half ? rows / 2u + 2u : rows + 2u};
+  const cuuint32_t elem[4] = {1u, 1u, 1u, 1u};
   CUresult r = encode_tiled()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, const_cast<uint16_t*>(plane), dims, strides, box,
                               elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -921,6 +1010,8 @@ uint32_t shape_of(const Denoiser& d, const DenoiseLayer& L) {
   return 9u;
 }
 uint32_t rows_of(uint32_t shape) { return SHAPE_ROWS[shape]; }
+// Whether a shape widens a half-size first source itself (k_conv_ws with an EXPAND shape).
+bool widens(uint32_t shape) { return (shape == 7u && Persist64::EXPAND) || (shape == 9u && Persist128::EXPAND); }
 
 struct Launches {
   std::vector<ConvArgs> args;
@@ -951,8 +1042,9 @@ void denoiser_prepare(Denoiser& d, uint32_t width, uint32_t height) {
   alloc(0, 16);
   for (size_t i = 0; i < d.layers.size(); ++i) {
     const DenoiseLayer& L = d.layers[i];
-    bool upsampled = false;  // the first source of an upsampling layer is stored at that layer's size
-    for (const auto& M : d.layers) upsampled = upsampled || (M.upsample && M.src0 == (int)i);
+    // the first source of an upsampling layer is stored at that layer's size, unless the layer widens it
+    bool upsampled = false;
+    for (const auto& M : d.layers) upsampled = upsampled || (M.upsample && M.src0 == (int)i && !widens(shape_of(d, M)));
     if (upsampled && L.pool) throw Invalid("a pooled output cannot feed an upsampling layer");
     alloc(upsampled ? L.out_level() - 1u : L.out_level(), L.n);
   }
@@ -970,8 +1062,10 @@ void denoiser_prepare(Denoiser& d, uint32_t width, uint32_t height) {
     a.H = TH >> L.level;
     a.W = TW >> L.level;
     const uint32_t shape = shape_of(d, L), rows = rows_of(shape);
-    a.a0_hi = plane_map(plane(L.src0, false), a.H, a.W, L.c0, rows);
-    a.a0_lo = plane_map(plane(L.src0, true), a.H, a.W, L.c0, rows);
+    a.half0 = L.upsample && widens(shape) ? 1u : 0u;
+    const uint32_t h0 = a.half0 ? a.H / 2u : a.H, w0 = a.half0 ? a.W / 2u : a.W;
+    a.a0_hi = plane_map(plane(L.src0, false), h0, w0, L.c0, rows, a.half0 != 0u);
+    a.a0_lo = plane_map(plane(L.src0, true), h0, w0, L.c0, rows, a.half0 != 0u);
     if (L.src1 != -2) {
       a.a1_hi = plane_map(plane(L.src1, false), a.H, a.W, L.c1, rows);
       a.a1_lo = plane_map(plane(L.src1, true), a.H, a.W, L.c1, rows);
@@ -1060,11 +1154,11 @@ void denoise_device(Denoiser& d, uint32_t width, uint32_t height, const float4* 
       } else if (shape == 6u) {
         k_conv<Wide2><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Wide2::ROWS)), CONV_THREADS, Wide2::SMEM, st>>>(a);
       } else if (shape == 7u) {
-        k_conv_ws<Persist64><<<persistent(a, Persist64::ROWS), WS_THREADS, Persist64::SMEM, st>>>(a);
+        k_conv_ws<Persist64><<<persistent(a, Persist64::ROWS), ws_threads<Persist64>(), Persist64::SMEM, st>>>(a);
       } else if (shape == 8u) {
-        k_conv_ws<Persist32><<<persistent(a, Persist32::ROWS), WS_THREADS, Persist32::SMEM, st>>>(a);
+        k_conv_ws<Persist32><<<persistent(a, Persist32::ROWS), ws_threads<Persist32>(), Persist32::SMEM, st>>>(a);
       } else if (shape == 9u) {
-        k_conv_ws<Persist128><<<persistent(a, Persist128::ROWS), WS_THREADS, Persist128::SMEM, st>>>(a);
+        k_conv_ws<Persist128><<<persistent(a, Persist128::ROWS), ws_threads<Persist128>(), Persist128::SMEM, st>>>(a);
       } else {
         k_conv<Wide><<<dim3(div_ceil(a.W, CONV_PIX), div_ceil(a.H, Wide::ROWS)), CONV_THREADS, Wide::SMEM, st>>>(a);
       }
