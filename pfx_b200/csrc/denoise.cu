@@ -200,17 +200,19 @@ constexpr uint32_t A_PLANE = PATCH_W * 16u;          // bytes of one (row, group
 //  * k_conv_ws, Persist128: 2 rows, up to 128 channels, three stages: 8.49 ms.
 // Layer by layer the persistent shapes are the fastest: Persist32 up to 32
 // channels, Persist64 up to 64, Persist128 above (the default).
-template <uint32_t ROWS_, uint32_t NMAX_, uint32_t STAGES_, uint32_t CTAS_, bool EXPAND_ = false>
+template <uint32_t ROWS_, uint32_t NMAX_, uint32_t STAGES_, uint32_t CTAS_, bool EXPAND_ = false,
+          uint32_t RAWS_ = 1>
 struct ConvShape {
   static constexpr uint32_t ROWS = ROWS_, N_MAX = NMAX_, STAGES = STAGES_, CTAS = CTAS_;
   // EXPAND (persistent kernel only): a first source stored at half size is
-  // copied into a raw buffer of ROWS / 2 + 2 rows x 66 pixels and widened 2x2
-  // into the stage by four more warps.
+  // copied into one of RAWS raw buffers of ROWS / 2 + 2 rows x 66 pixels and
+  // widened 2x2 into the stage by four more warps.
   static constexpr bool EXPAND = EXPAND_;
+  static constexpr uint32_t RAWS = RAWS_;
   static constexpr uint32_t RAW_ROWS = ROWS / 2u + 2u, RAW_W = CONV_PIX / 2u + 2u;
   static constexpr uint32_t RAW_BOX = RAW_ROWS * 2u * RAW_W * 16u;   // one half (hi or lo) as copied
   static constexpr uint32_t RAW_PLANE = (RAW_BOX + 127u) / 128u * 128u;  // its place in shared memory
-  static constexpr uint32_t RAW = EXPAND ? 2u * RAW_PLANE : 0u;
+  static constexpr uint32_t RAW = EXPAND ? RAWS * 2u * RAW_PLANE : 0u;
   static constexpr uint32_t TMEM_COLS = ROWS * N_MAX;            // a power of two of at least 32
   static constexpr uint32_t PATCH_ROWS = ROWS + 2u;              // staged input rows
   static constexpr uint32_t A_BYTES = PATCH_ROWS * 2u * A_PLANE;   // one chunk of one half (hi or lo)
@@ -221,7 +223,7 @@ struct ConvShape {
   static constexpr uint32_t SMEM = CTRL + 256u;
   static_assert(SMEM * CTAS <= 228u * 1024u - CTAS * 1024u, "shared memory per SM");
   static_assert(TMEM_COLS * CTAS <= 512u && (TMEM_COLS & (TMEM_COLS - 1u)) == 0u, "TMEM per SM");
-  static_assert(STAGES >= 1u && STAGES <= 4u, "one to four stages");
+  static_assert(STAGES >= 1u && STAGES <= 4u && RAWS >= 1u && RAWS <= 2u, "one to four stages, one or two raw buffers");
   // a tensor copy's shared-memory destination is 128-byte aligned
   static_assert(STAGE % 128u == 0u && A_BYTES % 128u == 0u && RAW_AT % 128u == 0u && RAW_PLANE % 128u == 0u,
                 "copy destinations");
@@ -490,7 +492,8 @@ __global__ void __launch_bounds__(ws_threads<S>(), 1) k_conv_ws(const __grid_con
   // [0] chunks loaded, [1] chunks committed, [2] raw copies issued, [3] raw copies widened
   uint32_t* counts = reinterpret_cast<uint32_t*>(smem + CTRL + 104u);
   const uint32_t wide0 = base + CTRL + 128u;  // NS barriers: the stage's widened source
-  const uint32_t raw_full = base + CTRL + 160u, raw_empty = base + CTRL + 168u;
+  const uint32_t raw_full0 = base + CTRL + 160u, raw_empty0 = base + CTRL + 176u;  // RAWS barriers each
+  constexpr uint32_t RAWS = S::RAWS;
   const bool half0 = S::EXPAND && a.half0 != 0u;
   if (tid == 0) {
     for (uint32_t s = 0; s < NS; ++s) {
@@ -502,8 +505,10 @@ __global__ void __launch_bounds__(ws_threads<S>(), 1) k_conv_ws(const __grid_con
       umma::mbar_init(accf0 + 8u * b, 1);
       umma::mbar_init(acce0 + 8u * b, 4);
     }
-    umma::mbar_init(raw_full, 1);
-    umma::mbar_init(raw_empty, 4);
+    for (uint32_t j = 0; j < RAWS; ++j) {
+      umma::mbar_init(raw_full0 + 8u * j, 1);
+      umma::mbar_init(raw_empty0 + 8u * j, 4);
+    }
     *abort_flag = 0u;
     counts[0] = counts[1] = counts[2] = counts[3] = 0u;
   }
@@ -527,12 +532,14 @@ __global__ void __launch_bounds__(ws_threads<S>(), 1) k_conv_ws(const __grid_con
         const bool first = k < chunks0;
         const int g = (int)(2u * (first ? k : k - chunks0));
         if (half0 && first) {
-          // the raw buffer is free once the widening warps are done with the previous copy
-          if (u > 0u && !umma::mbar_wait(raw_empty, (u - 1u) & 1u, a.wait_limit)) *abort_flag = 1u;
+          // raw buffer u % RAWS is free once the widening warps are done with copy u - RAWS
+          const uint32_t j = u % RAWS, raw_full = raw_full0 + 8u * j;
+          if (u >= RAWS && !umma::mbar_wait(raw_empty0 + 8u * j, ((u - RAWS) / RAWS) & 1u, a.wait_limit))
+            *abort_flag = 1u;
           if (*abort_flag) break;
           umma::mbar_expect_tx(full, wbytes);
           umma::mbar_expect_tx(raw_full, 2u * S::RAW_BOX);
-          const uint32_t raw = base + S::RAW_AT;
+          const uint32_t raw = base + S::RAW_AT + j * 2u * RAW_PLANE;
           umma::tensor_load_4d(raw, &a.a0_hi, 0, (x0 >> 1) - 1, g, (y0 >> 1) - 1, raw_full);
           umma::tensor_load_4d(raw + RAW_PLANE, &a.a0_lo, 0, (x0 >> 1) - 1, g, (y0 >> 1) - 1, raw_full);
           counts[2] = ++u;
@@ -602,7 +609,6 @@ __global__ void __launch_bounds__(ws_threads<S>(), 1) k_conv_ws(const __grid_con
   } else if (S::EXPAND && warp >= 6u && half0) {  // the widening of a half-size first source
     constexpr uint32_t ITEMS = 2u * S::PATCH_ROWS * 2u * PATCH_W;  // planes x rows x groups x pixels
     const uint32_t e = tid - 192u;
-    const uint8_t* raw = smem + S::RAW_AT;
     uint32_t c = 0, u = 0;
     bool stop = false;
     for (uint32_t t = blockIdx.x; t < tiles && !stop; t += gridDim.x) {
@@ -610,14 +616,15 @@ __global__ void __launch_bounds__(ws_threads<S>(), 1) k_conv_ws(const __grid_con
       const int xl = (x0 - 1) >> 1, yl = (y0 - 1) >> 1;  // the raw buffer's first pixel and row
       for (uint32_t k = 0; k < chunks; ++k, ++c) {
         if (k >= chunks0) continue;
-        const uint32_t s = c % NS;
-        const bool ok = umma::mbar_wait(raw_full, u & 1u, a.wait_limit);
+        const uint32_t s = c % NS, j = u % RAWS;
+        const bool ok = umma::mbar_wait(raw_full0 + 8u * j, (u / RAWS) & 1u, a.wait_limit);
         if (__any_sync(0xffffffffu, !ok || *abort_flag)) {
           *abort_flag = 1u;
           stop = true;
           break;
         }
         uint8_t* st = smem + s * STAGE;
+        const uint8_t* raw = smem + S::RAW_AT + j * 2u * RAW_PLANE;
         for (uint32_t item = e; item < ITEMS; item += 128u) {
           const uint32_t p = item % PATCH_W, rest = item / PATCH_W;  // rest = (plane x rows + r) x 2 + group
           const uint32_t grp = rest & 1u, r = (rest >> 1) % S::PATCH_ROWS, plane = (rest >> 1) / S::PATCH_ROWS;
@@ -628,7 +635,7 @@ __global__ void __launch_bounds__(ws_threads<S>(), 1) k_conv_ws(const __grid_con
         umma::fence_async_smem();
         __syncwarp();
         if (lane == 0) {
-          umma::mbar_arrive(raw_empty);
+          umma::mbar_arrive(raw_empty0 + 8u * j);
           umma::mbar_arrive(wide0 + 8u * s);
         }
         ++u;
@@ -648,7 +655,8 @@ __global__ void __launch_bounds__(ws_threads<S>(), 1) k_conv_ws(const __grid_con
     drained = umma::mbar_wait(empty0 + 8u * ((issued - 1u) % NS), ((issued - 1u) / NS) & 1u, DRAIN_LIMIT);
   for (uint32_t k = issued; k < loads; ++k)
     drained = umma::mbar_wait(full0 + 8u * (k % NS), (k / NS) & 1u, DRAIN_LIMIT) && drained;
-  if (raws > widened) drained = umma::mbar_wait(raw_full, (raws - 1u) & 1u, DRAIN_LIMIT) && drained;
+  for (uint32_t k = widened; k < raws; ++k)
+    drained = umma::mbar_wait(raw_full0 + 8u * (k % RAWS), (k / RAWS) & 1u, DRAIN_LIMIT) && drained;
   drained = __syncthreads_and(drained);
   if ((late || !drained) && tid == 0)
     atomicOr(a.error, (late ? ERR_CONV_WAIT : 0u) | (drained ? 0u : ERR_CONV_DRAIN));
