@@ -199,7 +199,11 @@ constexpr uint32_t A_PLANE = PATCH_W * 16u;          // bytes of one (row, group
 //    Paired on the 48 and 64 channel layers): 7.98 ms;
 //  * k_conv_ws, Persist128: 2 rows, up to 128 channels, three stages: 8.49 ms.
 // Layer by layer the persistent shapes are the fastest: Persist32 up to 32
-// channels, Persist64 up to 64, Persist128 above (the default).
+// channels, Persist64 up to 64, Persist128 above (the default), 7.30 ms.
+// With the upsampled sources stored at their own size and widened in the
+// CTA (EXPAND): 6.66 ms with one raw buffer beside three stages, 6.52 ms
+// with two raw buffers beside two stages (the copies of the next chunk's raw
+// rows no longer wait for the widening of the last).
 template <uint32_t ROWS_, uint32_t NMAX_, uint32_t STAGES_, uint32_t CTAS_, bool EXPAND_ = false,
           uint32_t RAWS_ = 1>
 struct ConvShape {
@@ -235,9 +239,9 @@ using Paired = ConvShape<4, 64, 1, 2>;
 using Tall2 = ConvShape<8, 32, 1, 2>;
 using Wide2 = ConvShape<2, 128, 1, 2>;
 // the persistent kernel's shapes (two accumulators: 2 x ROWS x N_MAX TMEM columns)
-using Persist64 = ConvShape<4, 64, 3, 1, true>;
+using Persist64 = ConvShape<4, 64, 2, 1, true, 2>;
 using Persist32 = ConvShape<8, 32, 2, 1>;
-using Persist128 = ConvShape<2, 128, 3, 1, true>;
+using Persist128 = ConvShape<2, 128, 2, 1, true, 2>;
 constexpr uint32_t ERR_CONV_WAIT = 1u, ERR_CONV_DRAIN = 2u;
 // Polls of the waits that drain a CTA's own work in flight (its MMAs and
 // copies) before it frees its TMEM and leaves, whatever the main loop's
