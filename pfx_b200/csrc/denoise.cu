@@ -194,10 +194,12 @@ constexpr uint32_t A_PLANE = PATCH_W * 16u;          // bytes of one (row, group
 //  * k_conv, Tall2:  8 rows, up to 32 channels, one stage, two CTAs (with
 //    Paired on the 48 and 64 channel layers): 8.45 ms;
 //  * k_conv, Wide2:  2 rows, up to 128 channels, one stage, two CTAs: 10.40 ms;
-//  * k_conv_ws, Persist64:  4 rows, up to 64 channels, three stages: 7.66 ms;
+//  * k_conv_ws, Persist64:  4 rows, up to 64 channels, three stages (then):
+//    7.66 ms;
 //  * k_conv_ws, Persist32:  8 rows, up to 32 channels, two stages (with
 //    Paired on the 48 and 64 channel layers): 7.98 ms;
-//  * k_conv_ws, Persist128: 2 rows, up to 128 channels, three stages: 8.49 ms.
+//  * k_conv_ws, Persist128: 2 rows, up to 128 channels, three stages (then):
+//    8.49 ms.
 // Layer by layer the persistent shapes are the fastest: Persist32 up to 32
 // channels, Persist64 up to 64, Persist128 above (the default), 7.30 ms.
 // With the upsampled sources stored at their own size and widened in the
