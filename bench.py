@@ -429,6 +429,7 @@ def denoise_line(trace, w, stream):
             ms.append(m)
     device_ms = statistics.median(ms)
     films = trace.readback()
+    den.denoise(films.color, films.albedo, films.normal)  # untimed: allocates the pinned staging
     e2e = []
     for _ in range(3):
         t0 = time.perf_counter()

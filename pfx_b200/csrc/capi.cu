@@ -1021,29 +1021,8 @@ void pfxt_denoiser_destroy(pfxt_denoiser* denoiser) { delete denoiser; }
 int pfxt_denoise(pfxt_denoiser* h, uint32_t width, uint32_t height, const float* color, const float* albedo,
                  const float* normal, float* out) {
   return guarded([&]() {
-    if (!h || !color || !albedo || !normal || !out) throw Invalid("null argument");
-    if (width == 0 || height == 0) throw Invalid("image dimensions must be nonzero");
-    Denoiser& d = *h->d;
-    check(cudaSetDevice(d.device), "denoiser device");
-    if (!d.stream) check(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking), "denoiser stream");
-    const size_t pixels = (size_t)width * height;
-    if (pixels > d.images_pixels) {
-      if (d.d_images) cudaFree(d.d_images);
-      d.d_images = nullptr;
-      d.images_pixels = 0;
-      check(cudaMalloc(&d.d_images, pixels * 4u * sizeof(float4)), "denoiser images");
-      d.images_pixels = pixels;
-    }
-    float4* img = d.d_images;
-    const float* in[3] = {color, albedo, normal};
-    for (int k = 0; k < 3; ++k)
-      check(cudaMemcpyAsync(img + k * pixels, in[k], pixels * sizeof(float4), cudaMemcpyHostToDevice, d.stream),
-            "denoiser upload");
-    denoise_device(d, width, height, img, img + pixels, img + 2 * pixels, img + 3 * pixels, d.stream);
-    check(cudaMemcpyAsync(out, img + 3 * pixels, pixels * sizeof(float4), cudaMemcpyDeviceToHost, d.stream),
-          "denoiser readback");
-    check(cudaStreamSynchronize(d.stream), "denoise");
-    denoiser_finish(d);
+    if (!h) throw Invalid("null argument");
+    denoise_host(*h->d, width, height, color, albedo, normal, out);
   });
 }
 

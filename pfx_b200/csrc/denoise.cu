@@ -37,6 +37,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <thread>
 
 #include "denoise.h"
 #include "pfxt_internal.h"
@@ -873,6 +874,10 @@ Denoiser::~Denoiser() {
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (d_images) cudaFree(d_images);
+  if (stream) cudaStreamSynchronize(stream);
+  if (h_stage) cudaFreeHost(h_stage);
+  for (cudaEvent_t e : stage_ev)
+    if (e) cudaEventDestroy(e);
   if (stream) cudaStreamDestroy(stream);
   if (prev >= 0) cudaSetDevice(prev);
 }
@@ -1199,6 +1204,80 @@ float denoiser_finish(Denoiser& d) {
   dcheck(cudaEventElapsedTime(&ms, d.ev0, d.ev1), "denoiser timing");
   d.last_ms = ms;
   return ms;
+}
+
+namespace {
+// memcpy split over up to four host threads (pageable memory is copied by the
+// CPU either way; one thread does not reach the device copies' rate).
+void copy_parallel(char* dst, const char* src, size_t bytes) {
+  constexpr size_t PART_MIN = 1u << 20;
+  const size_t parts = std::min<size_t>(4, std::max<size_t>(1, bytes / PART_MIN));
+  if (parts == 1) {
+    memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t part = (bytes / parts + 63u) & ~size_t(63);
+  std::vector<std::thread> helpers;
+  for (size_t i = 1; i < parts && i * part < bytes; ++i)
+    helpers.emplace_back([=]() { memcpy(dst + i * part, src + i * part, std::min(part, bytes - i * part)); });
+  memcpy(dst, src, std::min(part, bytes));
+  for (std::thread& t : helpers) t.join();
+}
+}  // namespace
+
+void denoise_host(Denoiser& d, uint32_t width, uint32_t height, const float* color, const float* albedo,
+                  const float* normal, float* out) {
+  if (!color || !albedo || !normal || !out) throw Invalid("null argument");
+  if (width == 0 || height == 0) throw Invalid("image dimensions must be nonzero");
+  dcheck(cudaSetDevice(d.device), "denoiser device");
+  if (!d.stream) dcheck(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking), "denoiser stream");
+  if (!d.h_stage) {
+    dcheck(cudaHostAlloc(reinterpret_cast<void**>(&d.h_stage), 2u * DENOISE_STAGE_BYTES, cudaHostAllocDefault),
+           "denoiser staging");
+    for (cudaEvent_t& e : d.stage_ev) dcheck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "denoiser staging");
+  }
+  const size_t pixels = (size_t)width * height, image = pixels * sizeof(float4);
+  if (pixels > d.images_pixels) {
+    if (d.d_images) cudaFree(d.d_images);
+    d.d_images = nullptr;
+    d.images_pixels = 0;
+    dcheck(cudaMalloc(&d.d_images, pixels * 4u * sizeof(float4)), "denoiser images");
+    d.images_pixels = pixels;
+  }
+  char* dev = reinterpret_cast<char*>(d.d_images);
+  const char* in[3] = {reinterpret_cast<const char*>(color), reinterpret_cast<const char*>(albedo),
+                       reinterpret_cast<const char*>(normal)};
+  // up: half j & 1 takes piece j once the device copy out of it (piece j - 2) is done
+  uint32_t j = 0;
+  for (int k = 0; k < 3; ++k)
+    for (size_t off = 0; off < image; off += DENOISE_STAGE_BYTES, ++j) {
+      const size_t len = std::min(DENOISE_STAGE_BYTES, image - off);
+      char* half = d.h_stage + (j & 1u) * DENOISE_STAGE_BYTES;
+      if (j >= 2u) dcheck(cudaEventSynchronize(d.stage_ev[j & 1u]), "denoiser upload");
+      copy_parallel(half, in[k] + off, len);
+      dcheck(cudaMemcpyAsync(dev + k * image + off, half, len, cudaMemcpyHostToDevice, d.stream), "denoiser upload");
+      dcheck(cudaEventRecord(d.stage_ev[j & 1u], d.stream), "denoiser upload");
+    }
+  float4* img = d.d_images;
+  denoise_device(d, width, height, img, img + pixels, img + 2 * pixels, img + 3 * pixels, d.stream);
+  // down: the device copy of piece i + 1 runs while the host copies piece i out
+  const size_t pieces = (image + DENOISE_STAGE_BYTES - 1u) / DENOISE_STAGE_BYTES;
+  auto fetch = [&](size_t i) {
+    const size_t off = i * DENOISE_STAGE_BYTES, len = std::min(DENOISE_STAGE_BYTES, image - off);
+    dcheck(cudaMemcpyAsync(d.h_stage + (i & 1u) * DENOISE_STAGE_BYTES, dev + 3 * image + off, len,
+                           cudaMemcpyDeviceToHost, d.stream),
+           "denoiser readback");
+    dcheck(cudaEventRecord(d.stage_ev[i & 1u], d.stream), "denoiser readback");
+  };
+  fetch(0);
+  for (size_t i = 0; i < pieces; ++i) {
+    if (i + 1u < pieces) fetch(i + 1u);
+    dcheck(cudaEventSynchronize(d.stage_ev[i & 1u]), "denoiser readback");
+    const size_t off = i * DENOISE_STAGE_BYTES;
+    copy_parallel(reinterpret_cast<char*>(out) + off, d.h_stage + (i & 1u) * DENOISE_STAGE_BYTES,
+                  std::min(DENOISE_STAGE_BYTES, image - off));
+  }
+  denoiser_finish(d);
 }
 
 }  // namespace pfxt

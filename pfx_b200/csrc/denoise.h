@@ -61,6 +61,8 @@ struct Denoiser {
   cudaStream_t stream = nullptr;   // host-buffer calls
   float4* d_images = nullptr;      // host-buffer calls: colour, albedo, normal, output
   size_t images_pixels = 0;
+  char* h_stage = nullptr;         // host-buffer calls: two pinned halves of DENOISE_STAGE_BYTES
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};  // the last copy through each half
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.0f;          // device time of the last denoise
   uint64_t last_macs = 0;        // multiply-adds of the last denoise (padded channels included)
@@ -76,5 +78,12 @@ void denoise_device(Denoiser& d, uint32_t width, uint32_t height, const float4* 
 // Waits for the last denoise; its device time in ms.  Throws DeviceError when
 // a convolution's bounded wait ran out.
 float denoiser_finish(Denoiser& d);
+// The host-buffer form (pfxt_denoise): the images go up and the result comes
+// back through two pinned halves of a staging buffer, host copies into one
+// half overlapping the device copy of the other; returns when the result is
+// in `out`.
+constexpr size_t DENOISE_STAGE_BYTES = 16u << 20;
+void denoise_host(Denoiser& d, uint32_t width, uint32_t height, const float* color, const float* albedo,
+                  const float* normal, float* out);
 
 }  // namespace pfxt
