@@ -207,7 +207,8 @@ constexpr uint32_t A_PLANE = PATCH_W * 16u;          // bytes of one (row, group
 // CTA (EXPAND): 6.66 ms with one raw buffer beside three stages, 6.52 ms
 // with two raw buffers beside two stages (the copies of the next chunk's raw
 // rows no longer wait for the widening of the last).  Persist32 as 4 rows and
-// three stages instead: 6.66 ms against 6.54.
+// three stages instead: 6.66 ms against 6.54; as 6 rows and three stages
+// (384 of 512 TMEM columns): 6.62 ms, the same image bit for bit.
 template <uint32_t ROWS_, uint32_t NMAX_, uint32_t STAGES_, uint32_t CTAS_, bool EXPAND_ = false,
           uint32_t RAWS_ = 1>
 struct ConvShape {
